@@ -1,0 +1,484 @@
+/*
+ * oxiblas_oracle.c -- CPU restatement of OxiBLAS.jl's dense LU hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the parity oracle: the test suite,
+ * the smoke check and the CPU-baseline leg of the benchmark load it to check
+ * (or time beside) the CUDA path.  The product library never links it and
+ * never falls back to it.
+ *
+ * Everything is column-major (Julia layout) with a leading dimension, 0-based
+ * loops, and LAPACK-style 1-based global pivot indices (`ipiv`).  Each routine
+ * cites the reference function it restates (paths relative to the OxiBLAS.jl
+ * project root).  Arithmetic follows the reference's order where it is
+ * observable: the pivot rule (largest |a|, strict '>' so the first row wins a
+ * tie), division by the pivot (not a reciprocal multiply), fused multiply-add
+ * in the rank-1 update, and the GEMM's "dot product first, then C - s" form.
+ *
+ * Built with gcc (-O3 -fopenmp -ffp-contract=off, explicit fma()) by
+ * oracle/Makefile.  OpenMP parallelises the trailing GEMM, the TRSM right-hand
+ * sides and the residual, the way the reference splits work across Julia
+ * threads (src/blas/gemm.jl:561 worker grid, src/blas/level3.jl:383 RHS split).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <float.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+typedef int64_t i64;
+
+/* ------------------------------------------------------------------------ */
+/* Type-generic body: instantiated for double (d) and float (s).            */
+/* ------------------------------------------------------------------------ */
+#define DEFINE_LU(T, P, FMA, ABS)                                                        \
+                                                                                         \
+/* C[0:m,0:n] <- C - A[0:m,0:k] * B[0:k,0:n].                                        \
+ * src/blas/gemm.jl:286-298 (_reference!): s = sum_p muladd(A[i,p], B[p,j], s), then   \
+ * C = alpha*s + beta*C with alpha = -1, beta = 1 (the trailing update of             \
+ * src/lapack/factorizations.jl:69).  The dot products run along p in order. */       \
+static void P##_gemm_minus(i64 m, i64 n, i64 k, const T *A, i64 lda, const T *B,        \
+                           i64 ldb, T *C, i64 ldc) {                                     \
+    if (m <= 0 || n <= 0 || k <= 0) return;                                              \
+    int par = (double)m * n * k > 2e6;                                                   \
+    _Pragma("omp parallel if(par)")                                                      \
+    {                                                                                    \
+        T *s = (T *)malloc(sizeof(T) * (size_t)m);                                       \
+        _Pragma("omp for schedule(static)")                                              \
+        for (i64 j = 0; j < n; ++j) {                                                    \
+            for (i64 i = 0; i < m; ++i) s[i] = 0;                                        \
+            for (i64 p = 0; p < k; ++p) {                                                \
+                const T b = B[p + j * ldb];                                              \
+                const T *a = A + p * lda;                                                \
+                for (i64 i = 0; i < m; ++i) s[i] = FMA(a[i], b, s[i]);                   \
+            }                                                                            \
+            T *c = C + j * ldc;                                                          \
+            for (i64 i = 0; i < m; ++i) c[i] = c[i] - s[i];                              \
+        }                                                                                \
+        free(s);                                                                         \
+    }                                                                                    \
+}                                                                                        \
+                                                                                         \
+/* Leaf of the left TRSM: src/blas/level3.jl:309-321 (_trsm_leaf_generic!, left).    \
+ * Lower: rows top-down, s = B[i,j]; s = muladd(-A[i,p], B[p,j], s) for p < i;       \
+ * upper: rows bottom-up over p > i; a non-unit diagonal divides. */                   \
+static void P##_trsm_leaf(i64 nt, i64 nrhs, const T *A, i64 lda, T *B, i64 ldb,        \
+                          int upper, int unit) {                                         \
+    for (i64 j = 0; j < nrhs; ++j) {                                                     \
+        T *b = B + j * ldb;                                                              \
+        if (!upper) {                                                                    \
+            for (i64 i = 0; i < nt; ++i) {                                               \
+                T s = b[i];                                                              \
+                for (i64 p = 0; p < i; ++p) s = FMA(-A[i + p * lda], b[p], s);           \
+                b[i] = unit ? s : s / A[i + i * lda];                                    \
+            }                                                                            \
+        } else {                                                                         \
+            for (i64 i = nt - 1; i >= 0; --i) {                                          \
+                T s = b[i];                                                              \
+                for (i64 p = i + 1; p < nt; ++p) s = FMA(-A[i + p * lda], b[p], s);      \
+                b[i] = unit ? s : s / A[i + i * lda];                                    \
+            }                                                                            \
+        }                                                                                \
+    }                                                                                    \
+}                                                                                        \
+                                                                                         \
+/* Recursive left TRSM B <- op(A)^-1 B, src/blas/level3.jl:338-355                    \
+ * (_trsm_blocks_left!): halve the triangle, solve one half, GEMM-update the other,    \
+ * solve it; leaves of <= 8 (trsm! default blocksize, level3.jl:524). Only the         \
+ * non-transposed form is needed here (transposed solves build op(A) explicitly). */   \
+static void P##_trsm_rec(i64 nt, i64 nrhs, const T *A, i64 lda, T *B, i64 ldb,         \
+                         int upper, int unit) {                                          \
+    if (nt <= 8) { P##_trsm_leaf(nt, nrhs, A, lda, B, ldb, upper, unit); return; }      \
+    i64 h = nt / 2;                                                                      \
+    if (!upper) {                                                                        \
+        P##_trsm_rec(h, nrhs, A, lda, B, ldb, upper, unit);                              \
+        P##_gemm_minus(nt - h, nrhs, h, A + h, lda, B, ldb, B + h, ldb);                 \
+        P##_trsm_rec(nt - h, nrhs, A + h + h * lda, lda, B + h, ldb, upper, unit);       \
+    } else {                                                                             \
+        P##_trsm_rec(nt - h, nrhs, A + h + h * lda, lda, B + h, ldb, upper, unit);       \
+        P##_gemm_minus(h, nrhs, nt - h, A + h * lda, lda, B + h, ldb, B, ldb);           \
+        P##_trsm_rec(h, nrhs, A, lda, B, ldb, upper, unit);                              \
+    }                                                                                    \
+}                                                                                        \
+                                                                                         \
+/* RHS columns split across threads, src/blas/level3.jl:383-406. */                    \
+static void P##_trsm(i64 nt, i64 nrhs, const T *A, i64 lda, T *B, i64 ldb, int upper,  \
+                     int unit) {                                                         \
+    if (nt <= 0 || nrhs <= 0) return;                                                    \
+    if (nrhs >= 64 && (double)nt * nt * nrhs > 4e6) {                                    \
+        i64 chunk = 32;                                                                  \
+        _Pragma("omp parallel for schedule(dynamic)")                                    \
+        for (i64 j0 = 0; j0 < nrhs; j0 += chunk) {                                       \
+            i64 w = nrhs - j0 < chunk ? nrhs - j0 : chunk;                               \
+            P##_trsm_rec(nt, w, A, lda, B + j0 * ldb, ldb, upper, unit);                 \
+        }                                                                                \
+    } else {                                                                             \
+        P##_trsm_rec(nt, nrhs, A, lda, B, ldb, upper, unit);                             \
+    }                                                                                    \
+}                                                                                        \
+                                                                                         \
+/* laswp: src/lapack/factorizations.jl:82-88 (_lu_swap!).  Interchanges j1..j2        \
+ * (0-based pivot positions, inclusive), column by column, on columns [c0,c1).         \
+ * piv holds 1-based row indices relative to row 0 of A plus `off` (global -> local). */\
+static void P##_swap(T *A, i64 lda, const i64 *piv, i64 off, i64 j1, i64 j2, i64 c0,    \
+                     i64 c1) {                                                           \
+    for (i64 col = c0; col < c1; ++col) {                                                \
+        T *a = A + col * lda;                                                            \
+        for (i64 j = j1; j <= j2; ++j) {                                                 \
+            i64 p = piv[off + j] - 1 - off;                                              \
+            if (p != j) { T t = a[j]; a[j] = a[p]; a[p] = t; }                           \
+        }                                                                                \
+    }                                                                                    \
+}                                                                                        \
+                                                                                         \
+/* Pivot search: src/lapack/factorizations.jl:92-107 (_lu_pivot), real branch:        \
+ * first row of the largest |P[i,j]|, i >= j (strict '>'). */                          \
+static i64 P##_pivot(const T *Pm, i64 ldp, i64 mp, i64 j) {                             \
+    const T *c = Pm + j * ldp;                                                           \
+    i64 p = j; T best = ABS(c[j]);                                                       \
+    for (i64 i = j + 1; i < mp; ++i) { T v = ABS(c[i]); if (v > best) { best = v; p = i; } }\
+    return p;                                                                            \
+}                                                                                        \
+                                                                                         \
+/* Recursive panel LU (getrf2): src/lapack/factorizations.jl:114-152 (_lu_panel!).     \
+ * P is mp x np with global row/column index `off` at its (0,0).  Leaves of <= 32      \
+ * columns (_lu_leaf, :113) eliminate column by column.  Returns 1 when `check` and a   \
+ * zero pivot was met (the reference throws SingularException there). */              \
+static int P##_panel(T *Pm, i64 ldp, i64 mp, i64 np, i64 *piv, i64 off, i64 *info,     \
+                     int check) {                                                        \
+    if (np <= 32) {                                                                      \
+        i64 q = mp < np ? mp : np;                                                       \
+        for (i64 j = 0; j < q; ++j) {                                                    \
+            i64 p = P##_pivot(Pm, ldp, mp, j);                                           \
+            piv[off + j] = off + p + 1;                                                  \
+            if (p != j)                                                                  \
+                for (i64 col = 0; col < np; ++col) {                                     \
+                    T t = Pm[j + col * ldp]; Pm[j + col * ldp] = Pm[p + col * ldp];      \
+                    Pm[p + col * ldp] = t;                                               \
+                }                                                                        \
+            T d = Pm[j + j * ldp];                                                       \
+            if (d == 0) {                                                                \
+                if (*info == 0) *info = off + j + 1;                                     \
+                if (check) return 1;                                                     \
+                continue;                                                                \
+            }                                                                            \
+            for (i64 i = j + 1; i < mp; ++i) Pm[i + j * ldp] /= d;                       \
+            for (i64 col = j + 1; col < np; ++col) {                                     \
+                T u = Pm[j + col * ldp];                                                 \
+                T *pc = Pm + col * ldp; const T *pj = Pm + j * ldp;                      \
+                for (i64 i = j + 1; i < mp; ++i) pc[i] = FMA(-pj[i], u, pc[i]);          \
+            }                                                                            \
+        }                                                                                \
+        return 0;                                                                        \
+    }                                                                                    \
+    i64 h = np / 2;                                                                      \
+    if (P##_panel(Pm, ldp, mp, h, piv, off, info, check)) return 1;                      \
+    P##_swap(Pm, ldp, piv, off, 0, h - 1, h, np);                                        \
+    P##_trsm(h, np - h, Pm, ldp, Pm + h * ldp, ldp, 0, 1);                               \
+    if (mp > h) {                                                                        \
+        P##_gemm_minus(mp - h, np - h, h, Pm + h, ldp, Pm + h * ldp, ldp,                \
+                       Pm + h + h * ldp, ldp);                                           \
+        if (P##_panel(Pm + h + h * ldp, ldp, mp - h, np - h, piv, off + h, info, check)) \
+            return 1;                                                                    \
+        i64 q = mp < np ? mp : np;                                                       \
+        P##_swap(Pm, ldp, piv, off, h, q - 1, 0, h);                                     \
+    }                                                                                    \
+    return 0;                                                                            \
+}                                                                                        \
+                                                                                         \
+/* Blocked right-looking getrf: src/lapack/factorizations.jl:30-77 (_lu_factor!),      \
+ * sequential order (the reference's lookahead gives bit-identical factors,            \
+ * test/lapack/lapack_dense.jl:32-37).  Returns 0, or 1 if `check` hit a zero pivot.   \
+ * `steps` >= 0 stops after that many panels (used only to time a bounded prefix). */  \
+int orc_##P##getrf_steps(i64 m, i64 n, T *A, i64 lda, i64 nb, int check, i64 *ipiv,   \
+                         i64 *info, i64 steps) {                                         \
+    i64 q = m < n ? m : n;                                                               \
+    *info = 0;                                                                           \
+    if (nb <= 0) return 2;                                                               \
+    i64 done = 0;                                                                        \
+    for (i64 f = 0; f < q; f += nb) {                                                    \
+        if (steps >= 0 && done++ >= steps) break;                                        \
+        i64 l = f + nb < q ? f + nb : q; /* exclusive */                                 \
+        if (P##_panel(A + f + f * lda, lda, m - f, l - f, ipiv, f, info, check))         \
+            return 1;                                                                    \
+        P##_swap(A, lda, ipiv, 0, f, l - 1, 0, f);                                       \
+        P##_swap(A, lda, ipiv, 0, f, l - 1, l, n);                                       \
+        if (l >= n) continue;                                                            \
+        P##_trsm(l - f, n - l, A + f + f * lda, lda, A + f + l * lda, lda, 0, 1);        \
+        if (l >= m) continue;                                                            \
+        P##_gemm_minus(m - l, n - l, l - f, A + l + f * lda, lda, A + f + l * lda, lda,  \
+                       A + l + l * lda, lda);                                            \
+    }                                                                                    \
+    return 0;                                                                            \
+}                                                                                        \
+int orc_##P##getrf(i64 m, i64 n, T *A, i64 lda, i64 nb, int check, i64 *ipiv,          \
+                   i64 *info) {                                                          \
+    return orc_##P##getrf_steps(m, n, A, lda, nb, check, ipiv, info, -1);                \
+}                                                                                        \
+                                                                                         \
+/* ldiv!: src/api/linalg_api.jl:168-184.  trans == 'N': laswp forward (_rowswap!,      \
+ * :100-110), unit-lower solve, upper solve.  trans == 'T' (real: same as 'C'):        \
+ * U^T solve, unit L^T solve, laswp in reverse.  B is n x nrhs, overwritten. */       \
+int orc_##P##getrs(char trans, i64 n, i64 nrhs, const T *LU, i64 lda, const i64 *ipiv,  \
+                   T *B, i64 ldb) {                                                      \
+    if (n == 0 || nrhs == 0) return 0;                                                   \
+    if (trans == 'N') {                                                                  \
+        for (i64 c = 0; c < nrhs; ++c) {                                                 \
+            T *b = B + c * ldb;                                                          \
+            for (i64 j = 0; j < n; ++j) {                                                \
+                i64 p = ipiv[j] - 1;                                                     \
+                if (p != j) { T t = b[j]; b[j] = b[p]; b[p] = t; }                       \
+            }                                                                            \
+        }                                                                                \
+        P##_trsm(n, nrhs, LU, lda, B, ldb, 0, 1);                                        \
+        P##_trsm(n, nrhs, LU, lda, B, ldb, 1, 0);                                        \
+        return 0;                                                                        \
+    }                                                                                    \
+    /* transposed: build U^T and L^T explicitly and reuse the lower/upper solves */     \
+    T *Tt = (T *)malloc(sizeof(T) * (size_t)n * n);                                      \
+    if (!Tt) return 3;                                                                   \
+    for (i64 j = 0; j < n; ++j)                                                          \
+        for (i64 i = 0; i < n; ++i) Tt[j + i * n] = LU[i + j * lda];                     \
+    P##_trsm(n, nrhs, Tt, n, B, ldb, 0, 0);   /* U^T is lower, non-unit */               \
+    P##_trsm(n, nrhs, Tt, n, B, ldb, 1, 1);   /* L^T is upper, unit */                   \
+    free(Tt);                                                                            \
+    for (i64 c = 0; c < nrhs; ++c) {                                                     \
+        T *b = B + c * ldb;                                                              \
+        for (i64 j = n - 1; j >= 0; --j) {                                               \
+            i64 p = ipiv[j] - 1;                                                         \
+            if (p != j) { T t = b[j]; b[j] = b[p]; b[p] = t; }                           \
+        }                                                                                \
+    }                                                                                    \
+    return 0;                                                                            \
+}
+
+DEFINE_LU(double, d, fma, fabs)
+DEFINE_LU(float, s, fmaf, fabsf)
+
+/* ------------------------------------------------------------------------ */
+/* Mixed precision pieces (FP64 only)                                        */
+/* ------------------------------------------------------------------------ */
+
+/* _refinement_residual!: src/lapack/expert_refinement.jl:67-81.  R = B - A*X in
+ * FP64 (the residual work type of Float64) and the componentwise backward error
+ * max_i |r_i| / (|A||x| + |b|)_i with the reference's Inf/zero conventions. */
+double orc_refinement_residual(i64 n, i64 nrhs, const double *A, i64 lda, const double *X,
+                               i64 ldx, const double *B, i64 ldb, double *R, i64 ldr) {
+    double err = 0.0;
+    for (i64 j = 0; j < nrhs; ++j) {
+        double local = 0.0;
+#pragma omp parallel for reduction(max : local) schedule(static) if (n >= 512)
+        for (i64 i = 0; i < n; ++i) {
+            double value = B[i + j * ldb], den = fabs(B[i + j * ldb]);
+            for (i64 k = 0; k < n; ++k) {
+                double a = A[i + k * lda], x = X[k + j * ldx];
+                value -= a * x;
+                den += fabs(a) * fabs(x);
+            }
+            R[i + j * ldr] = value;
+            double rel;
+            if (!isfinite(den)) rel = INFINITY;
+            else if (den == 0.0) rel = (value == 0.0) ? 0.0 : INFINITY;
+            else rel = fabs(value) / den;
+            if (rel > local || isnan(rel)) local = rel;
+        }
+        if (local > err || isnan(local)) err = local;
+    }
+    return err;
+}
+
+/* Normwise backward error ||B - A X||_inf / (||A||_inf ||X||_inf + ||B||_inf), per RHS
+ * maximum: the error measure the benchmark's 1e-14 target is stated in. */
+double orc_normwise_backward_error(i64 n, i64 nrhs, const double *A, i64 lda, const double *X,
+                                   i64 ldx, const double *B, i64 ldb) {
+    double anorm = 0.0;
+    for (i64 i = 0; i < n; ++i) {
+        double s = 0.0;
+        for (i64 k = 0; k < n; ++k) s += fabs(A[i + k * lda]);
+        if (s > anorm) anorm = s;
+    }
+    double worst = 0.0;
+    for (i64 j = 0; j < nrhs; ++j) {
+        double rmax = 0.0, xmax = 0.0, bmax = 0.0;
+#pragma omp parallel for reduction(max : rmax) schedule(static) if (n >= 512)
+        for (i64 i = 0; i < n; ++i) {
+            double v = B[i + j * ldb];
+            for (i64 k = 0; k < n; ++k) v -= A[i + k * lda] * X[k + j * ldx];
+            if (fabs(v) > rmax) rmax = fabs(v);
+        }
+        for (i64 i = 0; i < n; ++i) {
+            if (fabs(X[i + j * ldx]) > xmax) xmax = fabs(X[i + j * ldx]);
+            if (fabs(B[i + j * ldb]) > bmax) bmax = fabs(B[i + j * ldb]);
+        }
+        double den = anorm * xmax + bmax;
+        double e = den > 0 ? rmax / den : (rmax == 0 ? 0.0 : INFINITY);
+        if (e > worst) worst = e;
+    }
+    return worst;
+}
+
+/* 2^round(log2(v)) clamped to the exponent range of Float64: the radix scale of
+ * equilibrate(A; radix=true), src/lapack/dense_utilities.jl:191-213.  Julia's
+ * round is round-half-to-even (nearbyint under the default rounding mode). */
+static double radix_scale(double v) {
+    double e = nearbyint(log2(v));
+    if (e < -1022) e = -1022;       /* exponent(floatmin(Float64)) */
+    if (e > 1023) e = 1023;         /* exponent(floatmax(Float64)) */
+    return ldexp(1.0, (int)e);
+}
+
+/* equilibrate(A; radix=true): rows first, then columns of the row-scaled matrix.
+ * Writes the scaled matrix to E (ldE) and the scales to rows/cols. */
+void orc_equilibrate_radix(i64 m, i64 n, const double *A, i64 lda, double *E, i64 lde,
+                           double *rows, double *cols) {
+    for (i64 j = 0; j < n; ++j)
+        for (i64 i = 0; i < m; ++i) E[i + j * lde] = A[i + j * lda];
+    for (i64 i = 0; i < m; ++i) {
+        double v = 0.0;
+        for (i64 j = 0; j < n; ++j) { double a = fabs(E[i + j * lde]); if (a > v) v = a; }
+        rows[i] = 1.0;
+        if (v > 0) {
+            rows[i] = radix_scale(v);
+            for (i64 j = 0; j < n; ++j) E[i + j * lde] /= rows[i];
+        }
+    }
+    for (i64 j = 0; j < n; ++j) {
+        double v = 0.0;
+        for (i64 i = 0; i < m; ++i) { double a = fabs(E[i + j * lde]); if (a > v) v = a; }
+        cols[j] = 1.0;
+        if (v > 0) {
+            cols[j] = radix_scale(v);
+            for (i64 i = 0; i < m; ++i) E[i + j * lde] /= cols[j];
+        }
+    }
+}
+
+/* _mixed_extended_correction: src/lapack/extended_lapack.jl:114-131 (Low = Float32).
+ * Row-scale the residual, scale by the power of two 2^exponent(max|.|), round to
+ * Float32, solve with the Float32 factors, widen, multiply back, column-unscale.
+ * Returns 0, or 4 when the scaled RHS overflows / is not finite. */
+static int mixed_correction(i64 n, i64 nrhs, const float *LU, i64 ldlu, const i64 *ipiv,
+                            const double *Rres, i64 ldr, const double *rows,
+                            const double *cols, double *Cout, i64 ldc, float *work) {
+    double mag = 0.0;
+    for (i64 j = 0; j < nrhs; ++j)
+        for (i64 i = 0; i < n; ++i) {
+            double v = fabs(Rres[i + j * ldr] / rows[i]);
+            if (v > mag || isnan(v)) mag = v;
+        }
+    if (mag == 0.0) {
+        for (i64 j = 0; j < nrhs; ++j)
+            for (i64 i = 0; i < n; ++i) Cout[i + j * ldc] = 0.0;
+        return 0;
+    }
+    if (!isfinite(mag)) return 4;
+    int ex; frexp(mag, &ex);         /* mag = f * 2^ex, f in [0.5,1) */
+    double scale = ldexp(1.0, ex - 1); /* Julia exponent(): floor(log2(mag)) */
+    for (i64 j = 0; j < nrhs; ++j)
+        for (i64 i = 0; i < n; ++i) {
+            float v = (float)((Rres[i + j * ldr] / rows[i]) / scale);
+            if (!isfinite(v)) return 4;
+            work[i + j * n] = v;
+        }
+    orc_sgetrs('N', n, nrhs, LU, ldlu, ipiv, work, n);
+    for (i64 j = 0; j < nrhs; ++j)
+        for (i64 i = 0; i < n; ++i)
+            Cout[i + j * ldc] = ((double)work[i + j * n] * scale) / cols[i];
+    return 0;
+}
+
+/* mixed_solve: src/lapack/factorizations.jl:425-427 -> _mixed_precision_impl,
+ * src/lapack/extended_lapack.jl:175-226, LU family, Low = Float32, fallback on.
+ * Outputs X (n x nrhs), the iteration count, the final componentwise backward
+ * error, and whether the working-precision fallback factor was used.  The
+ * fallback path (Float64 factor of the equilibrated matrix) is restated too.
+ * Returns 0 on success, 1 singular (both factors), 4 overflow without fallback. */
+int orc_mixed_solve(i64 n, i64 nrhs, const double *A, i64 lda, const double *B, i64 ldb,
+                    double *X, i64 ldx, i64 maxiter, double rtol, i64 *iterations,
+                    double *berr, int *fallback) {
+    double *E = (double *)malloc(sizeof(double) * (size_t)n * n);
+    double *rows = (double *)malloc(sizeof(double) * (size_t)n);
+    double *cols = (double *)malloc(sizeof(double) * (size_t)n);
+    float *F = (float *)malloc(sizeof(float) * (size_t)n * n);
+    double *Fd = NULL;
+    i64 *ipiv = (i64 *)malloc(sizeof(i64) * (size_t)(n > 0 ? n : 1));
+    double *R = (double *)malloc(sizeof(double) * (size_t)n * nrhs);
+    double *Cc = (double *)malloc(sizeof(double) * (size_t)n * nrhs);
+    float *work = (float *)malloc(sizeof(float) * (size_t)n * nrhs);
+    int rc = 0; *fallback = 0;
+    orc_equilibrate_radix(n, n, A, lda, E, n, rows, cols);
+    i64 info = 0;
+    int lowok = 1;
+    for (i64 i = 0; i < n * n; ++i) { F[i] = (float)E[i]; if (!isfinite(F[i])) lowok = 0; }
+    if (lowok) {
+        if (orc_sgetrf(n, n, F, n, 128, 1, ipiv, &info) != 0) lowok = 0;
+    }
+    if (!lowok) {
+        *fallback = 1;
+        Fd = (double *)malloc(sizeof(double) * (size_t)n * n);
+        memcpy(Fd, E, sizeof(double) * (size_t)n * n);
+        if (orc_dgetrf(n, n, Fd, n, 128, 1, ipiv, &info) != 0) { rc = 1; goto done; }
+    }
+    /* first solve: correction of B itself (extended_lapack.jl:207-212) */
+#define CORRECT(RES, LDRES, OUT, LDOUT)                                                    \
+    do {                                                                                 \
+        if (!*fallback) {                                                                \
+            if (mixed_correction(n, nrhs, F, n, ipiv, RES, LDRES, rows, cols, OUT, LDOUT, \
+                                 work)) { rc = 4; goto done; }                           \
+        } else {                                                                         \
+            for (i64 j = 0; j < nrhs; ++j)                                               \
+                for (i64 i = 0; i < n; ++i) OUT[i + j * LDOUT] = RES[i + j * LDRES] / rows[i]; \
+            orc_dgetrs('N', n, nrhs, Fd, n, ipiv, OUT, LDOUT);                           \
+            for (i64 j = 0; j < nrhs; ++j)                                               \
+                for (i64 i = 0; i < n; ++i) OUT[i + j * LDOUT] /= cols[i];               \
+        }                                                                                \
+    } while (0)
+    CORRECT(B, ldb, X, ldx);
+    double err = INFINITY; i64 it = 0;
+    for (i64 iter = 0; iter <= maxiter; ++iter) {
+        err = orc_refinement_residual(n, nrhs, A, lda, X, ldx, B, ldb, R, n);
+        it = iter;
+        if (err <= rtol || iter == maxiter || !isfinite(err)) break;
+        CORRECT(R, n, Cc, n);
+        for (i64 j = 0; j < nrhs; ++j)
+            for (i64 i = 0; i < n; ++i) X[i + j * ldx] += Cc[i + j * n];
+    }
+#undef CORRECT
+    *iterations = it; *berr = err;
+done:
+    free(E); free(rows); free(cols); free(F); free(Fd); free(ipiv); free(R); free(Cc);
+    free(work);
+    return rc;
+}
+
+/* Adjoint of x = A \ b for the loss with upstream gradient xbar:
+ * lambda = A^-T xbar (transposed solve with the stored factors, the primitive
+ * behind ldiv!(transpose(F), B), src/api/linalg_api.jl:176-184 and
+ * solve_transposed, src/lapack/expert_refinement.jl:2-23), bbar = lambda,
+ * Abar = -lambda x^T (column-major, ldabar). */
+int orc_lu_adjoint(i64 n, const double *LU, i64 lda, const i64 *ipiv, const double *x,
+                   const double *xbar, double *bbar, double *Abar, i64 ldabar) {
+    for (i64 i = 0; i < n; ++i) bbar[i] = xbar[i];
+    int rc = orc_dgetrs('T', n, 1, LU, lda, ipiv, bbar, n);
+    if (rc) return rc;
+    for (i64 j = 0; j < n; ++j)
+        for (i64 i = 0; i < n; ++i) Abar[i + j * ldabar] = -bbar[i] * x[j];
+    return 0;
+}
+
+int orc_num_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+void orc_set_num_threads(int t) {
+#ifdef _OPENMP
+    if (t > 0) omp_set_num_threads(t);
+#else
+    (void)t;
+#endif
+}

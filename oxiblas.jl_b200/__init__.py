@@ -1,0 +1,18 @@
+"""oxiblas_b200 -- B200-native (sm_100a) engine for OxiBLAS.jl's dense LU hot path.
+
+The package directory is ``oxiblas.jl_b200/``; it is imported under the module
+name ``oxiblas_b200`` (see ``load_package`` in the repository's
+``__graft_entry__.py``).  The compute lives in ``liboxiblas_b200.so`` (C ABI in
+``include/oxiblas_b200.h``); this Python layer mirrors the reference's public
+API for the path.
+"""
+from ._lib import (ArgumentError, DimensionMismatch, ExtensionMissing, Handle, SingularException,
+                   exported_symbols, load)
+from .lu import (LU, colmajor_copy, det, gemm_update, ldiv, ldiv_, ldiv_into, logabsdet, lu, lu_,
+                 options)
+
+__all__ = [
+    "LU", "lu", "lu_", "ldiv", "ldiv_", "ldiv_into", "det", "logabsdet", "gemm_update", "options",
+    "colmajor_copy", "SingularException", "DimensionMismatch", "ArgumentError", "ExtensionMissing",
+    "Handle", "load", "exported_symbols",
+]

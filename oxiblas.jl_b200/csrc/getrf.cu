@@ -1,0 +1,161 @@
+// Host driver of the blocked, partial-pivoted LU on the row-major working
+// matrix, and the oxi_?getrf entry points.
+//
+// Structure (src/lapack/factorizations.jl:30-77, _lu_factor!): panels of
+// `blocksize` columns; each panel factored recursively as getrf2 (:114-152,
+// _lu_panel!) down to a leaf (the cluster kernel); then the U block row by TRSM
+// and the trailing update by GEMM.  Each leaf's net row permutation is applied
+// to every other column right after the leaf (row-major: contiguous row moves),
+// which leaves each column with exactly the interchange sequence the reference
+// applies to it through its left/right laswp calls.
+#include <algorithm>
+#include <cstring>
+#include "oxi_internal.h"
+
+namespace oxi {
+
+static inline i64 round_up(i64 x, i64 a) { return (x + a - 1) / a * a; }
+
+// Split point of a recursion node.  Reference order keeps the reference's exact
+// halving (n / 2, src/lapack/factorizations.jl:141 and src/blas/level3.jl:340);
+// the tensor-core engine keeps column offsets on 8-element multiples so every
+// TMA tile base stays 16-byte aligned.
+static inline i64 split_point(const oxi_handle_s *h, i64 n) {
+    i64 half = n / 2;
+    if (h->opt.gemm == 1) return half;
+    i64 a = half & ~i64(7);
+    return a >= 8 ? a : half;
+}
+
+template <typename T>
+void gemm_minus(oxi_handle_s *h, T *C, i64 ldc, const T *A, i64 lda, const T *B, i64 ldb, i64 M,
+                i64 N, i64 K) {
+    if (M <= 0 || N <= 0 || K <= 0) return;
+    if constexpr (sizeof(T) == 8) {
+        if (h->opt.gemm == 0) {
+            launch_gemm_dmma(C, ldc, A, lda, B, ldb, M, N, K, h->stream);
+            return;
+        }
+    }
+    launch_gemm_ref<T>(C, ldc, A, lda, B, ldb, M, N, K, h->stream);
+}
+template void gemm_minus<double>(oxi_handle_s *, double *, i64, const double *, i64, const double *, i64, i64, i64, i64);
+template void gemm_minus<float>(oxi_handle_s *, float *, i64, const float *, i64, const float *, i64, i64, i64, i64);
+
+// B (t x N) <- L^-1 B, L unit lower: recursive halving with GEMM updates
+// (src/blas/level3.jl:338-355, _trsm_blocks_left!), leaves by k_trsm_leaf.
+template <typename T>
+void trsm_lower_unit(oxi_handle_s *h, const T *L, i64 ldl, T *B, i64 ldb, i64 t, i64 N) {
+    if (t <= 1 || N <= 0) return;
+    const i64 leaf = std::min<i64>(std::max<i64>(h->opt.trsm_leaf, 1), 32);
+    if (t <= leaf) {
+        launch_trsm_leaf<T>(L, ldl, B, ldb, (int)t, N, h->stream);
+        return;
+    }
+    const i64 t1 = split_point(h, t);
+    trsm_lower_unit<T>(h, L, ldl, B, ldb, t1, N);
+    gemm_minus<T>(h, B + t1 * ldb, ldb, L + t1 * ldl, ldl, B, ldb, t - t1, N, t1);
+    trsm_lower_unit<T>(h, L + t1 * ldl + t1, ldl, B + t1 * ldb, ldb, t - t1, N);
+}
+template void trsm_lower_unit<double>(oxi_handle_s *, const double *, i64, double *, i64, i64, i64);
+template void trsm_lower_unit<float>(oxi_handle_s *, const float *, i64, float *, i64, i64, i64);
+
+template <typename T>
+struct LuRun {
+    oxi_handle_s *h;
+    T *W;
+    i64 ld, m, n, ncols_moved;  // ncols_moved: columns the row moves reach (n, +1 id column)
+    int64_t *ipiv, *info;
+    int *moves, *nmoves;
+};
+
+// Recursive panel on columns [c0, c0+nc), rows [c0, m).
+template <typename T>
+static void panel_rec(LuRun<T> &R, i64 c0, i64 nc) {
+    oxi_handle_s *h = R.h;
+    const i64 mrows = R.m - c0;
+    if (mrows <= 0 || nc <= 0) return;
+    const int leafw = leaf_width_for<T>(mrows);
+    if (leafw == 0) throw CudaError{cudaErrorInvalidValue, "panel taller than the leaf capacity"};
+    if (nc <= leafw) {
+        OXI_CUDA(cudaMemsetAsync(R.nmoves, 0, sizeof(int), h->stream));
+        launch_leaf<T>(R.W + c0 * R.ld + c0, R.ld, mrows, (int)nc, c0, R.ipiv, R.info, R.moves,
+                       R.nmoves, leafw, h->stream);
+        launch_rowmoves<T>(R.W, R.ld, c0, R.moves, R.nmoves, 0, R.ncols_moved, c0, c0 + nc,
+                           h->stream);
+        return;
+    }
+    const i64 hh = split_point(h, nc);
+    panel_rec(R, c0, hh);
+    T *L11 = R.W + c0 * R.ld + c0;
+    trsm_lower_unit<T>(h, L11, R.ld, L11 + hh, R.ld, hh, nc - hh);
+    if (mrows > hh) {
+        gemm_minus<T>(h, L11 + hh * R.ld + hh, R.ld, L11 + hh * R.ld, R.ld, L11 + hh, R.ld,
+                      mrows - hh, nc - hh, hh);
+        panel_rec(R, c0 + hh, nc - hh);
+    }
+}
+
+template <typename T>
+void getrf_rowmajor(oxi_handle_s *h, T *W, i64 ld, i64 m, i64 n, int64_t *d_ipiv, int64_t *d_info,
+                    int *d_moves, int *d_nmoves) {
+    LuRun<T> R{h, W, ld, m, n, n, d_ipiv, d_info, d_moves, d_nmoves};
+    const i64 q = std::min(m, n);
+    const i64 nb = std::max<i64>(h->opt.blocksize, 1);
+    for (i64 f = 0; f < q; f += nb) {
+        const i64 l = std::min(q, f + nb);
+        panel_rec(R, f, l - f);
+        if (l >= n) continue;
+        T *L11 = W + f * ld + f;
+        trsm_lower_unit<T>(h, L11, ld, L11 + (l - f), ld, l - f, n - l);
+        if (l >= m) continue;
+        gemm_minus<T>(h, W + l * ld + l, ld, W + l * ld + f, ld, W + f * ld + l, ld, m - l, n - l,
+                      l - f);
+    }
+}
+template void getrf_rowmajor<double>(oxi_handle_s *, double *, i64, i64, i64, int64_t *, int64_t *, int *, int *);
+template void getrf_rowmajor<float>(oxi_handle_s *, float *, i64, i64, i64, int64_t *, int64_t *, int *, int *);
+
+// Column-major in, column-major out: the C ABI wrapper shared by d/s.
+template <typename T>
+static int getrf_entry(oxi_handle_s *h, i64 m, i64 n, T *dA, i64 lda, int64_t *d_ipiv,
+                       int64_t *h_info) {
+    if (!h || !h_info) return OXI_EINVAL;
+    if (m < 0 || n < 0 || lda < std::max<i64>(1, m)) return OXI_EINVAL;
+    *h_info = 0;
+    if (m == 0 || n == 0) return OXI_OK;
+    if (!dA || !d_ipiv) return OXI_EINVAL;
+    if (leaf_width_for<T>(m) == 0) return OXI_EINVAL;
+    try {
+        OXI_CUDA(cudaSetDevice(h->device));
+        const i64 ld = round_up(n, 32);
+        T *W = (T *)h->work.get((size_t)m * ld * sizeof(T));
+        char *sc = (char *)h->scratch.get(4096);
+        int64_t *d_info = (int64_t *)sc;
+        int *d_nmoves = (int *)(sc + 64);
+        int *d_moves = (int *)(sc + 128);
+        OXI_CUDA(cudaMemsetAsync(d_info, 0, sizeof(int64_t), h->stream));
+        launch_cm_to_rm<T, T>(dA, lda, W, ld, m, n, h->stream);
+        getrf_rowmajor<T>(h, W, ld, m, n, d_ipiv, d_info, d_moves, d_nmoves);
+        launch_rm_to_cm<T, T>(W, ld, dA, lda, m, n, h->stream);
+        int64_t *hi = (int64_t *)h->host_ws.get(64);
+        OXI_CUDA(cudaMemcpyAsync(hi, d_info, sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
+        OXI_CUDA(cudaStreamSynchronize(h->stream));
+        *h_info = hi[0];
+        return hi[0] > 0 ? OXI_ESINGULAR : OXI_OK;
+    } catch (const CudaError &e) {
+        h->last_error = std::string(e.what) + ": " + cudaGetErrorString(e.code);
+        return OXI_ECUDA;
+    }
+}
+
+}  // namespace oxi
+
+extern "C" int oxi_dgetrf(oxi_handle_t h, int64_t m, int64_t n, double *dA, int64_t lda,
+                          int64_t *d_ipiv, int64_t *h_info) {
+    return oxi::getrf_entry<double>(h, m, n, dA, lda, d_ipiv, h_info);
+}
+extern "C" int oxi_sgetrf(oxi_handle_t h, int64_t m, int64_t n, float *dA, int64_t lda,
+                          int64_t *d_ipiv, int64_t *h_info) {
+    return oxi::getrf_entry<float>(h, m, n, dA, lda, d_ipiv, h_info);
+}

@@ -1,0 +1,500 @@
+// Panel-level kernels of the dense LU: layout conversion, the cluster leaf LU,
+// row interchanges, the TRSM leaf and the reference-order GEMM.
+//
+// Storage inside the engine is ROW-major (row i of an m x n matrix is n
+// contiguous elements, leading dimension ld).  Row interchanges -- the laswp of
+// src/lapack/factorizations.jl:82-88 -- then move contiguous row segments, and
+// a panel row (w elements) is one contiguous load.  The C ABI converts from and
+// to the caller's column-major layout at entry and exit.
+#include <cooperative_groups.h>
+#include <climits>
+#include "oxi_internal.h"
+
+namespace cg = cooperative_groups;
+
+namespace oxi {
+
+// ---------------------------------------------------------------------------
+// Layout conversion (32 x 32 tiles through shared memory, conflict-free).
+// ---------------------------------------------------------------------------
+template <typename TS, typename TD>
+__global__ void k_cm_to_rm(const TS *__restrict__ A, i64 lda, TD *__restrict__ W, i64 ldw,
+                           i64 m, i64 n) {
+    __shared__ TD tile[32][33];
+    const i64 i0 = (i64)blockIdx.x * 32, j0 = (i64)blockIdx.y * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+    for (int r = ty; r < 32; r += 8) {             // read column j0+r, rows i0+tx
+        i64 i = i0 + tx, j = j0 + r;
+        if (i < m && j < n) tile[r][tx] = (TD)A[i + j * lda];
+    }
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {  // write row i0+r, columns j0+tx
+        i64 i = i0 + r, j = j0 + tx;
+        if (i < m && j < n) W[i * ldw + j] = tile[tx][r];
+    }
+}
+
+template <typename TS, typename TD>
+__global__ void k_rm_to_cm(const TS *__restrict__ W, i64 ldw, TD *__restrict__ A, i64 lda,
+                           i64 m, i64 n) {
+    __shared__ TD tile[32][33];
+    const i64 i0 = (i64)blockIdx.x * 32, j0 = (i64)blockIdx.y * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    for (int r = ty; r < 32; r += 8) {  // read row i0+r, columns j0+tx
+        i64 i = i0 + r, j = j0 + tx;
+        if (i < m && j < n) tile[r][tx] = (TD)W[i * ldw + j];
+    }
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {  // write column j0+r, rows i0+tx
+        i64 i = i0 + tx, j = j0 + r;
+        if (i < m && j < n) A[i + j * lda] = tile[tx][r];
+    }
+}
+
+template <typename TS, typename TD>
+void launch_cm_to_rm(const TS *A, i64 lda, TD *W, i64 ldw, i64 m, i64 n, cudaStream_t s) {
+    if (m <= 0 || n <= 0) return;
+    dim3 grid((unsigned)((m + 31) / 32), (unsigned)((n + 31) / 32));
+    k_cm_to_rm<TS, TD><<<grid, dim3(32, 8), 0, s>>>(A, lda, W, ldw, m, n);
+    OXI_LAUNCH_CHECK();
+}
+template <typename TS, typename TD>
+void launch_rm_to_cm(const TS *W, i64 ldw, TD *A, i64 lda, i64 m, i64 n, cudaStream_t s) {
+    if (m <= 0 || n <= 0) return;
+    dim3 grid((unsigned)((m + 31) / 32), (unsigned)((n + 31) / 32));
+    k_rm_to_cm<TS, TD><<<grid, dim3(32, 8), 0, s>>>(W, ldw, A, lda, m, n);
+    OXI_LAUNCH_CHECK();
+}
+template void launch_cm_to_rm<double, double>(const double *, i64, double *, i64, i64, i64, cudaStream_t);
+template void launch_cm_to_rm<float, float>(const float *, i64, float *, i64, i64, i64, cudaStream_t);
+template void launch_cm_to_rm<double, float>(const double *, i64, float *, i64, i64, i64, cudaStream_t);
+template void launch_rm_to_cm<double, double>(const double *, i64, double *, i64, i64, i64, cudaStream_t);
+template void launch_rm_to_cm<float, float>(const float *, i64, float *, i64, i64, i64, cudaStream_t);
+template void launch_rm_to_cm<float, double>(const float *, i64, double *, i64, i64, i64, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Leaf LU: one thread-block cluster (1..16 CTAs of LEAF_NT threads) holds the
+// m x W leaf in REGISTERS, R rows per thread (row position i lives in thread
+// g = i mod G, slot k = i / G, G = cluster threads).  Column by column, as the
+// leaf loop of _lu_panel! (src/lapack/factorizations.jl:116-139):
+//   pivot = first row of the largest |a_ij|, i >= j (_lu_pivot, :92-107);
+//   swap rows j and p over the leaf's W columns;
+//   zero pivot -> info (first one), skip the column;
+//   l_ij = a_ij / a_jj (a true division, as the reference);
+//   a_ic = muladd(-l_ij, a_jc, a_ic) for c > j.
+// Per column each CTA reduces its candidate in registers/shared memory and
+// PUSHES it (|value|, position, the whole candidate row) into every CTA's
+// shared memory over DSMEM; one cluster barrier (release/acquire) later every
+// CTA holds all candidates locally and picks the same winner.  The CTA that
+// owns position j also pushes row j, so the two swapped rows never need a
+// second exchange.  Slots are double-buffered by column parity, which is what
+// makes one barrier per column sufficient.  Each row carries the index of the
+// row it started as; at the end a position whose row changed emits a (dst, src)
+// move, the net permutation applied to the other columns by k_rowmoves.
+// ---------------------------------------------------------------------------
+constexpr int LEAF_NT = 256;
+constexpr int LEAF_MAX_CS = 16;
+
+template <typename T, int W, int R>
+__global__ void __launch_bounds__(LEAF_NT, 1)
+k_leaf_lu(T *__restrict__ P, i64 ld, int m, int wact, i64 gofs, int64_t *__restrict__ ipiv,
+          int64_t *__restrict__ info, int *__restrict__ moves, int *__restrict__ nmoves) {
+    cg::cluster_group cl = cg::this_cluster();
+    const int CS = (int)cl.num_blocks();
+    const int cr = (int)cl.block_rank();
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    constexpr int NW = LEAF_NT / 32;
+    const int G = CS * LEAF_NT;
+    const int g = cr * LEAF_NT + t;
+
+    __shared__ T s_cval[2][LEAF_MAX_CS];
+    __shared__ int s_cpos[2][LEAF_MAX_CS];
+    __shared__ int s_cid[2][LEAF_MAX_CS];
+    __shared__ T s_crow[2][LEAF_MAX_CS][W];
+    __shared__ T s_jslot[2][W];
+    __shared__ int s_jslot_id[2];
+    __shared__ T s_wval[NW];
+    __shared__ int s_wpos[NW];
+    __shared__ T s_myrow[W];
+    __shared__ int s_myid;
+    __shared__ T s_jrow[W];
+    __shared__ int s_jid;
+
+    T r[R][W];
+    int id[R];
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        const int i = k * G + g;
+        id[k] = i;
+#pragma unroll
+        for (int c = 0; c < W; ++c) r[k][c] = T(0);
+        if (i < m) {
+            const T *src = P + (i64)i * ld;
+#pragma unroll
+            for (int c = 0; c < W; ++c)
+                if (c < wact) r[k][c] = src[c];
+        }
+    }
+    const int q = m < wact ? m : wact;
+
+#pragma unroll
+    for (int j = 0; j < W; ++j) {
+        if (j >= q) break;
+        const int par = j & 1;
+        // (a) this thread's best candidate in column j
+        T bv = T(-1);
+        int bp = INT_MAX;
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            const int i = k * G + g;
+            if (i >= j && i < m) {
+                const T v = fabs(r[k][j]);
+                if (v > bv) { bv = v; bp = i; }   // slots ascend in i: strict '>' keeps the first
+            }
+        }
+        // (b) warp reduction; ties go to the smaller position
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            const T ov = __shfl_xor_sync(0xffffffffu, bv, off);
+            const int op = __shfl_xor_sync(0xffffffffu, bp, off);
+            if (ov > bv || (ov == bv && op < bp)) { bv = ov; bp = op; }
+        }
+        if (lane == 0) { s_wval[warp] = bv; s_wpos[warp] = bp; }
+        __syncthreads();
+        // (c) CTA candidate (computed redundantly by every thread)
+        T cv = s_wval[0];
+        int cp = s_wpos[0];
+#pragma unroll
+        for (int w = 1; w < NW; ++w) {
+            const T ov = s_wval[w];
+            const int op = s_wpos[w];
+            if (ov > cv || (ov == cv && op < cp)) { cv = ov; cp = op; }
+        }
+        if (cp != INT_MAX && (cp % G) == g) {
+            const int kk = cp / G;
+#pragma unroll
+            for (int k = 0; k < R; ++k)
+                if (k == kk) {
+#pragma unroll
+                    for (int c = 0; c < W; ++c) s_myrow[c] = r[k][c];
+                    s_myid = id[k];
+                }
+        }
+        // position j is always slot 0 of thread j of CTA 0 (j < W <= 32 <= G)
+        const bool own_j = (g == j);
+        if (own_j) {
+#pragma unroll
+            for (int c = 0; c < W; ++c) s_jrow[c] = r[0][c];
+            s_jid = id[0];
+        }
+        __syncthreads();
+        // (d) push the candidate (warp 0) and row j (warp 1 of CTA 0) to every CTA
+        if (warp == 0) {
+            for (int e = lane; e < CS * W; e += 32) {
+                const int dst = e / W, c = e - dst * W;
+                T *rem = cl.map_shared_rank(&s_crow[par][cr][0], dst);
+                rem[c] = s_myrow[c];
+            }
+            if (lane < CS) {
+                *cl.map_shared_rank(&s_cval[par][cr], lane) = cv;
+                *cl.map_shared_rank(&s_cpos[par][cr], lane) = cp;
+                *cl.map_shared_rank(&s_cid[par][cr], lane) = s_myid;
+            }
+        }
+        if (cr == 0 && warp == 1) {
+            for (int e = lane; e < CS * W; e += 32) {
+                const int dst = e / W, c = e - dst * W;
+                T *rem = cl.map_shared_rank(&s_jslot[par][0], dst);
+                rem[c] = s_jrow[c];
+            }
+            if (lane < CS) *cl.map_shared_rank(&s_jslot_id[par], lane) = s_jid;
+        }
+        cl.sync();
+        // (e) winner, identical in every CTA
+        T wv = s_cval[par][0];
+        int wp = s_cpos[par][0], wq = 0;
+        for (int qq = 1; qq < CS; ++qq) {
+            const T ov = s_cval[par][qq];
+            const int op = s_cpos[par][qq];
+            if (ov > wv || (ov == wv && op < wp)) { wv = ov; wp = op; wq = qq; }
+        }
+        const T *prow = (wp == INT_MAX) ? &s_jslot[par][0] : &s_crow[par][wq][0];
+        const int pid = (wp == INT_MAX) ? s_jslot_id[par] : s_cid[par][wq];
+        if (wp == INT_MAX) wp = j;  // no comparable candidate (all NaN): keep row j
+        if (g == 0) ipiv[gofs + j] = gofs + wp + 1;
+        const T d = prow[j];
+        if (d == T(0)) {
+            if (g == 0 && *info == 0) *info = gofs + j + 1;
+            continue;
+        }
+        T u[W];
+#pragma unroll
+        for (int c = 0; c < W; ++c) u[c] = prow[c];
+        // (f) the swap lands in the two owner threads' registers
+        if (wp != j) {
+            if (own_j) {
+#pragma unroll
+                for (int c = 0; c < W; ++c) r[0][c] = u[c];
+                id[0] = pid;
+            }
+            if ((wp % G) == g) {
+                const int kk = wp / G;
+#pragma unroll
+                for (int k = 0; k < R; ++k)
+                    if (k == kk) {
+#pragma unroll
+                        for (int c = 0; c < W; ++c) r[k][c] = s_jslot[par][c];
+                        id[k] = s_jslot_id[par];
+                    }
+            }
+        }
+        // (g) scale the column and apply the rank-1 update below the pivot
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            const int i = k * G + g;
+            if (i > j && i < m) {
+                const T l = r[k][j] / d;
+                r[k][j] = l;
+#pragma unroll
+                for (int c = j + 1; c < W; ++c) r[k][c] = fma(-l, u[c], r[k][c]);
+            }
+        }
+    }
+
+    // store the leaf and emit the moves of the net permutation
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        const int i = k * G + g;
+        if (i < m) {
+            T *dst = P + (i64)i * ld;
+#pragma unroll
+            for (int c = 0; c < W; ++c)
+                if (c < wact) dst[c] = r[k][c];
+            if (id[k] != i) {
+                const int slot = atomicAdd(nmoves, 1);
+                moves[2 * slot] = i;
+                moves[2 * slot + 1] = id[k];
+            }
+        }
+    }
+    // keep every CTA's shared memory alive until all remote pushes have landed
+    cl.sync();
+}
+
+template <typename T> int leaf_width_for(i64 m);
+template <> int leaf_width_for<double>(i64 m) {
+    const i64 cap = (i64)LEAF_MAX_CS * LEAF_NT;
+    if (m <= cap * 2) return 32;
+    if (m <= cap * 4) return 16;
+    if (m <= cap * 8) return 8;
+    if (m <= cap * 16) return 4;
+    return 0;
+}
+template <> int leaf_width_for<float>(i64 m) {
+    const i64 cap = (i64)LEAF_MAX_CS * LEAF_NT;
+    if (m <= cap * 4) return 32;
+    if (m <= cap * 8) return 16;
+    if (m <= cap * 16) return 8;
+    return 0;
+}
+
+template <typename T, int W, int R>
+static void launch_leaf_wr(T *P, i64 ld, i64 m, int w, i64 gofs, int64_t *ipiv, int64_t *info,
+                           int *moves, int *nmoves, cudaStream_t s) {
+    const i64 per_cta = (i64)LEAF_NT * R;
+    int need = (int)((m + per_cta - 1) / per_cta);
+    int cs = 1;  // cluster sizes kept to powers of two
+    while (cs < need) cs <<= 1;
+    auto kern = k_leaf_lu<T, W, R>;
+    if (cs > 8) OXI_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cs);
+    cfg.blockDim = dim3(LEAF_NT);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = cs;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    OXI_CUDA(cudaLaunchKernelEx(&cfg, kern, P, ld, (int)m, w, gofs, ipiv, info, moves, nmoves));
+}
+
+template <typename T>
+void launch_leaf(T *P, i64 ld, i64 m, int w, i64 gofs, int64_t *ipiv, int64_t *info, int *moves,
+                 int *nmoves, int leafw, cudaStream_t s) {
+    const i64 cap = (i64)LEAF_MAX_CS * LEAF_NT;
+    if constexpr (sizeof(T) == 8) {
+        if (leafw == 32) {
+            if (m <= cap) launch_leaf_wr<T, 32, 1>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s);
+            else launch_leaf_wr<T, 32, 2>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s);
+        } else if (leafw == 16) {
+            launch_leaf_wr<T, 16, 4>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s);
+        } else if (leafw == 8) {
+            launch_leaf_wr<T, 8, 8>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s);
+        } else {
+            launch_leaf_wr<T, 4, 16>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s);
+        }
+    } else {
+        if (leafw == 32) {
+            if (m <= cap) launch_leaf_wr<T, 32, 1>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s);
+            else if (m <= 2 * cap) launch_leaf_wr<T, 32, 2>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s);
+            else launch_leaf_wr<T, 32, 4>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s);
+        } else if (leafw == 16) {
+            launch_leaf_wr<T, 16, 8>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s);
+        } else {
+            launch_leaf_wr<T, 8, 16>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s);
+        }
+    }
+}
+template void launch_leaf<double>(double *, i64, i64, int, i64, int64_t *, int64_t *, int *, int *, int, cudaStream_t);
+template void launch_leaf<float>(float *, i64, i64, int, i64, int64_t *, int64_t *, int *, int *, int, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Row moves: W[r0 + dst][c] <- W[r0 + src][c] for every move, all sources read
+// before any destination is written.  One thread per column: the moves of a
+// column are private to its thread, so no synchronisation is needed, and a warp
+// touches 32 contiguous elements of each row (coalesced).
+// ---------------------------------------------------------------------------
+constexpr int MAX_MOVES = 64;
+
+template <typename T>
+__global__ void k_rowmoves(T *__restrict__ W, i64 ld, i64 r0, const int *__restrict__ moves,
+                           const int *__restrict__ nmoves, i64 c_lo, i64 c_hi, i64 skip_lo,
+                           i64 skip_hi) {
+    const i64 c = c_lo + (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= c_hi || (c >= skip_lo && c < skip_hi)) return;
+    const int cnt = min(*nmoves, MAX_MOVES);
+    T tmp[MAX_MOVES];
+    T *base = W + r0 * ld + c;
+#pragma unroll
+    for (int e = 0; e < MAX_MOVES; ++e)
+        if (e < cnt) tmp[e] = base[(i64)moves[2 * e + 1] * ld];
+#pragma unroll
+    for (int e = 0; e < MAX_MOVES; ++e)
+        if (e < cnt) base[(i64)moves[2 * e] * ld] = tmp[e];
+}
+
+template <typename T>
+void launch_rowmoves(T *W, i64 ld, i64 r0, const int *moves, const int *nmoves, i64 c_lo, i64 c_hi,
+                     i64 skip_lo, i64 skip_hi, cudaStream_t s) {
+    if (c_hi <= c_lo) return;
+    const int nt = 128;
+    const i64 cols = c_hi - c_lo;
+    k_rowmoves<T><<<(unsigned)((cols + nt - 1) / nt), nt, 0, s>>>(W, ld, r0, moves, nmoves, c_lo, c_hi,
+                                                                   skip_lo, skip_hi);
+    OXI_LAUNCH_CHECK();
+}
+template void launch_rowmoves<double>(double *, i64, i64, const int *, const int *, i64, i64, i64, i64, cudaStream_t);
+template void launch_rowmoves<float>(float *, i64, i64, const int *, const int *, i64, i64, i64, i64, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// TRSM leaf: B (t x N) <- L^-1 B with L unit lower (t <= 32), row-major.  One
+// thread per right-hand-side column, L staged in shared memory; the order is
+// the reference leaf's (src/blas/level3.jl:309-321): s = b_i, then
+// s = muladd(-L_ip, b_p, s) for p = 1..i-1.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_trsm_leaf(const T *__restrict__ L, i64 ldl, T *__restrict__ B, i64 ldb, int t,
+                            i64 N) {
+    __shared__ T sL[32][33];
+    for (int e = threadIdx.x; e < t * t; e += blockDim.x) {
+        const int i = e / t, p = e - i * t;
+        sL[i][p] = L[(i64)i * ldl + p];
+    }
+    __syncthreads();
+    const i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= N) return;
+    T x[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i)
+        if (i < t) x[i] = B[(i64)i * ldb + c];
+#pragma unroll
+    for (int i = 1; i < 32; ++i) {
+        if (i < t) {
+            T s = x[i];
+#pragma unroll
+            for (int p = 0; p < i; ++p) s = fma(-sL[i][p], x[p], s);
+            x[i] = s;
+        }
+    }
+#pragma unroll
+    for (int i = 1; i < 32; ++i)
+        if (i < t) B[(i64)i * ldb + c] = x[i];
+}
+
+template <typename T>
+void launch_trsm_leaf(const T *L, i64 ldl, T *B, i64 ldb, int t, i64 N, cudaStream_t s) {
+    if (t <= 1 || N <= 0) return;  // a unit 1x1 triangle is the identity
+    const int nt = 128;
+    k_trsm_leaf<T><<<(unsigned)((N + nt - 1) / nt), nt, 0, s>>>(L, ldl, B, ldb, t, N);
+    OXI_LAUNCH_CHECK();
+}
+template void launch_trsm_leaf<double>(const double *, i64, double *, i64, int, i64, cudaStream_t);
+template void launch_trsm_leaf<float>(const float *, i64, float *, i64, int, i64, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Reference-order GEMM: C <- C - A*B, s_ij = sum_p fma(A_ip, B_pj, s) in p order
+// from zero, then C_ij - s_ij -- the arithmetic of src/blas/gemm.jl:286-298 with
+// alpha = -1, beta = 1.  64 x 64 tiles, 16-deep k slabs, 4 x 4 per thread.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_gemm_ref(T *__restrict__ C, i64 ldc, const T *__restrict__ A,
+                                                  i64 lda, const T *__restrict__ B, i64 ldb, i64 M,
+                                                  i64 N, i64 K) {
+    __shared__ T As[16][64 + 1];
+    __shared__ T Bs[16][64 + 1];
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const i64 m0 = (i64)blockIdx.y * 64, n0 = (i64)blockIdx.x * 64;
+    T acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = T(0);
+    for (i64 k0 = 0; k0 < K; k0 += 16) {
+        for (int e = threadIdx.x; e < 64 * 16; e += 256) {
+            const int r = e >> 4, kk = e & 15;   // A: row r, k kk (k contiguous)
+            const i64 gi = m0 + r, gk = k0 + kk;
+            As[kk][r] = (gi < M && gk < K) ? A[gi * lda + gk] : T(0);
+            const int kr = e >> 6, cc = e & 63;  // B: k kr, col cc (n contiguous)
+            const i64 gk2 = k0 + kr, gj = n0 + cc;
+            Bs[kr][cc] = (gk2 < K && gj < N) ? B[gk2 * ldb + gj] : T(0);
+        }
+        __syncthreads();
+        const int kmax = (int)((K - k0) < 16 ? (K - k0) : 16);
+        for (int p = 0; p < kmax; ++p) {
+            T a[4], b[4];
+#pragma unroll
+            for (int x = 0; x < 4; ++x) a[x] = As[p][ty + 16 * x];
+#pragma unroll
+            for (int y = 0; y < 4; ++y) b[y] = Bs[p][tx + 16 * y];
+#pragma unroll
+            for (int x = 0; x < 4; ++x)
+#pragma unroll
+                for (int y = 0; y < 4; ++y) acc[x][y] = fma(a[x], b[y], acc[x][y]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int x = 0; x < 4; ++x)
+#pragma unroll
+        for (int y = 0; y < 4; ++y) {
+            const i64 gi = m0 + ty + 16 * x, gj = n0 + tx + 16 * y;
+            if (gi < M && gj < N) C[gi * ldc + gj] = C[gi * ldc + gj] - acc[x][y];
+        }
+}
+
+template <typename T>
+void launch_gemm_ref(T *C, i64 ldc, const T *A, i64 lda, const T *B, i64 ldb, i64 M, i64 N, i64 K,
+                     cudaStream_t s) {
+    if (M <= 0 || N <= 0 || K <= 0) return;
+    dim3 grid((unsigned)((N + 63) / 64), (unsigned)((M + 63) / 64));
+    k_gemm_ref<T><<<grid, 256, 0, s>>>(C, ldc, A, lda, B, ldb, M, N, K);
+    OXI_LAUNCH_CHECK();
+}
+template void launch_gemm_ref<double>(double *, i64, const double *, i64, const double *, i64, i64, i64, i64, cudaStream_t);
+template void launch_gemm_ref<float>(float *, i64, const float *, i64, const float *, i64, i64, i64, i64, cudaStream_t);
+
+}  // namespace oxi

@@ -1,0 +1,153 @@
+// Internal declarations shared by the translation units of liboxiblas_b200.so.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstddef>
+#include <string>
+#include <vector>
+
+#include "../../include/oxiblas_b200.h"
+
+namespace oxi {
+
+using i64 = int64_t;
+
+// Error plumbing: every CUDA call on the host side goes through OXI_CUDA, which
+// records the message on the handle and returns OXI_ECUDA from the entry point.
+struct CudaError {
+    cudaError_t code;
+    const char *what;
+};
+
+#define OXI_CUDA(expr)                                                                 \
+    do {                                                                               \
+        cudaError_t oxi_e_ = (expr);                                                   \
+        if (oxi_e_ != cudaSuccess) throw ::oxi::CudaError{oxi_e_, #expr};             \
+    } while (0)
+
+#define OXI_LAUNCH_CHECK() OXI_CUDA(cudaGetLastError())
+
+// Device workspace owned by a handle; grows monotonically.
+struct DeviceBuffer {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    void *get(size_t need) {
+        if (need <= bytes) return ptr;
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+        need = (need + 255) & ~size_t(255);
+        OXI_CUDA(cudaMalloc(&ptr, need));
+        bytes = need;
+        return ptr;
+    }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+};
+
+struct PinnedBuffer {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    void *get(size_t need) {
+        if (need <= bytes) return ptr;
+        if (ptr) cudaFreeHost(ptr);
+        ptr = nullptr;
+        bytes = 0;
+        OXI_CUDA(cudaMallocHost(&ptr, need));
+        bytes = need;
+        return ptr;
+    }
+    void release() {
+        if (ptr) cudaFreeHost(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+};
+
+struct Options {
+    i64 blocksize = 128;   // lu_factor default (factorizations.jl:17)
+    int gemm = 0;          // 0 tensor-core engine, 1 reference summation order
+    i64 trsm_leaf = 32;    // recursive TRSM leaf
+    int lookahead = 0;
+};
+
+}  // namespace oxi
+
+struct oxi_handle_s {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    oxi::Options opt;
+    std::string last_error;
+    int sm_count = 148;
+    // workspaces
+    oxi::DeviceBuffer work;      // row-major working matrix
+    oxi::DeviceBuffer scratch;   // small control data (moves, counters, info)
+    oxi::DeviceBuffer solve_ws;  // solve workspace
+    oxi::DeviceBuffer mixed_ws;  // mixed-precision workspace
+    oxi::DeviceBuffer perm_ws;   // row permutation of the last solve
+    oxi::PinnedBuffer host_ws;   // pinned host staging
+};
+
+namespace oxi {
+
+// ---- kernels launched by the drivers (defined in lu_kernels.cu / gemm_*.cu) ----
+
+// Column-major (m x n, lda) -> row-major (m x n, ldw) and back.
+template <typename TS, typename TD>
+void launch_cm_to_rm(const TS *A, i64 lda, TD *W, i64 ldw, i64 m, i64 n, cudaStream_t s);
+template <typename TS, typename TD>
+void launch_rm_to_cm(const TS *W, i64 ldw, TD *A, i64 lda, i64 m, i64 n, cudaStream_t s);
+
+// Leaf LU of the row-major block P (m rows x w columns, ld), one thread-block
+// cluster.  Writes ipiv[gofs + j], *info (first zero pivot, global 1-based), and
+// the (dst, src) row-move list of the net permutation (positions relative to P).
+template <typename T>
+void launch_leaf(T *P, i64 ld, i64 m, int w, i64 gofs, int64_t *ipiv, int64_t *info,
+                 int *moves, int *nmoves, int leafw, cudaStream_t s);
+// Widest leaf width whose register capacity holds m rows.
+template <typename T> int leaf_width_for(i64 m);
+
+// Apply a row-move list (positions relative to row r0) to columns [c_lo, c_hi)
+// of the row-major matrix W, skipping columns [skip_lo, skip_hi).
+template <typename T>
+void launch_rowmoves(T *W, i64 ld, i64 r0, const int *moves, const int *nmoves, i64 c_lo,
+                     i64 c_hi, i64 skip_lo, i64 skip_hi, cudaStream_t s);
+
+// B (t x N, row-major) <- L^-1 B, L unit lower t x t (t <= 32), row-major.
+template <typename T>
+void launch_trsm_leaf(const T *L, i64 ldl, T *B, i64 ldb, int t, i64 N, cudaStream_t s);
+
+// C (M x N) <- C - A (M x K) * B (K x N), all row-major.  Reference order:
+// one FMA chain per output along k, then C - s.
+template <typename T>
+void launch_gemm_ref(T *C, i64 ldc, const T *A, i64 lda, const T *B, i64 ldb, i64 M, i64 N,
+                     i64 K, cudaStream_t s);
+// FP64 tensor-core (DMMA, TMA-fed) version.
+void launch_gemm_dmma(double *C, i64 ldc, const double *A, i64 lda, const double *B, i64 ldb,
+                      i64 M, i64 N, i64 K, cudaStream_t s);
+
+// Host driver: blocked right-looking getrf on a row-major working matrix.
+template <typename T>
+void getrf_rowmajor(oxi_handle_s *h, T *W, i64 ld, i64 m, i64 n, int64_t *d_ipiv,
+                    int64_t *d_info, int *d_moves, int *d_nmoves);
+
+// Driver helpers reused by the mixed-precision and batched paths.
+template <typename T>
+void gemm_minus(oxi_handle_s *h, T *C, i64 ldc, const T *A, i64 lda, const T *B, i64 ldb,
+                i64 M, i64 N, i64 K);
+template <typename T>
+void trsm_lower_unit(oxi_handle_s *h, const T *L, i64 ldl, T *B, i64 ldb, i64 t, i64 N);
+
+// Solve with a device-resident 0-based row permutation (A[perm, :] = L U) and
+// column-major factors; B (n x nrhs, ldb) is overwritten.  *d_err becomes
+// nonzero when a bounded device wait expired.
+template <typename T>
+void getrs_perm(oxi_handle_s *h, char trans, i64 n, i64 nrhs, const T *LU, i64 lda,
+                const int64_t *d_perm, T *B, i64 ldb, int *d_err);
+void perm_from_ipiv(const int64_t *ipiv, i64 q, i64 m, int64_t *perm);
+
+}  // namespace oxi

@@ -1,0 +1,89 @@
+"""The CPU oracle against LAPACK getrf golden vectors and the reference's own
+test properties (CPU only)."""
+import numpy as np
+import pytest
+
+from conftest import bwd, split_lu
+
+
+def test_oracle_matches_lapack_golden(oracle, golden):
+    for name, c in golden.items():
+        A = c["A"]
+        m, n = A.shape
+        F, ipiv, info = oracle.getrf(A, blocksize=c["bs"], check=False)
+        assert info == c["info"], name
+        # test/lapack/lapack_dense.jl:12-14: same partial-pivot choices as getrf
+        if not name.startswith(("singular", "nearly_singular")):
+            assert np.array_equal(ipiv, c["ipiv"]), name
+        if c["lu"] is not None and info == 0:
+            rel = np.linalg.norm(F - c["lu"]) / max(np.linalg.norm(c["lu"]), 1e-300)
+            assert rel < 1e-13, (name, rel)
+        else:
+            assert abs(np.linalg.norm(F) - c["lu_fro"]) <= 1e-12 * c["lu_fro"] or info, name
+        p = oracle.perm_from_ipiv(ipiv, m)
+        L, U = split_lu(F, m, n)
+        assert bwd(L @ U - A[p, :], A) <= 30, name
+
+
+def test_oracle_singular_behaviour(oracle, golden):
+    A = golden["singular_col23_40"]["A"]
+    with pytest.raises(oracle.SingularError) as e:
+        oracle.getrf(A)
+    assert e.value.info == 23
+    _, _, info = oracle.getrf(A, check=False)
+    assert info == 23
+    _, _, info = oracle.getrf(np.zeros((3, 3)), check=False)
+    assert info == 1
+
+
+def test_oracle_solves(oracle):
+    rng = np.random.default_rng(5)
+    for n in (1, 9, 67, 130):
+        A = rng.standard_normal((n, n))
+        F, ipiv, _ = oracle.getrf(A, blocksize=32)
+        b = rng.standard_normal(n)
+        B = rng.standard_normal((n, 3))
+        x = oracle.getrs(F, ipiv, b)
+        X = oracle.getrs(F, ipiv, B)
+        xt = oracle.getrs(F, ipiv, b, "T")
+        c = np.linalg.cond(A)
+        assert bwd((A @ x - b)[:, None], A) <= 30 * c
+        assert bwd(A @ X - B, A) <= 30 * c
+        assert bwd((A.T @ xt - b)[:, None], A) <= 30 * c
+
+
+def test_oracle_mixed_solve(oracle):
+    rng = np.random.default_rng(7)
+    for n in (1, 17, 67):  # test/lapack/factorizations.jl:57-63
+        A = rng.standard_normal((n, n)) + n * np.eye(n)
+        b = rng.standard_normal(n)
+        r = oracle.mixed_solve(A, b)
+        assert r["converged"] and r["iterations"] <= 10
+        assert np.allclose(A @ r["x"], b, rtol=2e-12, atol=2e-12)
+    r = oracle.mixed_solve(A, b, maxiter=0)  # extended_lapack tests: maxiter=0 -> not converged
+    assert r["iterations"] == 0
+
+
+def test_oracle_equilibrate_radix(oracle):
+    rng = np.random.default_rng(11)
+    A = rng.standard_normal((30, 20)) * (10.0 ** rng.uniform(-3, 3, (30, 1)))
+    E, r, c = oracle.equilibrate_radix(A)
+    assert np.all(np.log2(r) == np.round(np.log2(r)))
+    assert np.all(np.log2(c) == np.round(np.log2(c)))
+    assert np.allclose(E * r[:, None] * c[None, :], A, rtol=0, atol=0)
+
+
+def test_oracle_adjoint_matches_finite_differences(oracle):
+    rng = np.random.default_rng(3)
+    n = 12
+    A = rng.standard_normal((n, n)) + n * np.eye(n)
+    b = rng.standard_normal(n)
+    F, ipiv, _ = oracle.getrf(A)
+    x = oracle.getrs(F, ipiv, b)
+    bbar, Abar = oracle.lu_adjoint(F, ipiv, x, x)  # loss 0.5||x||^2 -> xbar = x
+    h = 1e-6
+    for _ in range(4):
+        dA = rng.standard_normal((n, n))
+        f = lambda M: 0.5 * np.sum(np.linalg.solve(M, b) ** 2)
+        fd = (f(A + h * dA) - f(A - h * dA)) / (2 * h)
+        assert abs(fd - np.sum(Abar * dA)) <= 1e-6 * max(1, abs(fd))
