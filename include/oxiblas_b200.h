@@ -57,7 +57,10 @@ enum oxi_option {
     OXI_OPT_BLOCKSIZE = 1,
     OXI_OPT_GEMM = 2,
     OXI_OPT_TRSM_LEAF = 3,
-    OXI_OPT_LOOKAHEAD = 4
+    OXI_OPT_LOOKAHEAD = 4,
+    OXI_OPT_MIXED_BLOCKSIZE = 5, /* panel width of the mixed-precision factor (256) */
+    OXI_OPT_STOP_NORMWISE = 6,   /* 1: the mixed solve stops on the normwise error  */
+    OXI_OPT_GMRES_RESTART = 7    /* GMRES-IR restart length (30)                    */
 };
 int oxi_set_option(oxi_handle_t h, int option, int64_t value);
 int oxi_get_option(oxi_handle_t h, int option, int64_t *value);
@@ -98,6 +101,87 @@ int oxi_sgetrs(oxi_handle_t h, char trans, int64_t n, int64_t nrhs, const float 
 int oxi_dgemm_update(oxi_handle_t h, int64_t m, int64_t n, int64_t k, double *dC,
                      int64_t ldc, const double *dA, int64_t lda, const double *dB,
                      int64_t ldb);
+
+/* ---------------------------------------------------------------------------
+ * Mixed-precision solve: low-precision LU of the radix-equilibrated matrix plus
+ * FP64 iterative refinement.  Replaces mixed_solve / _mixed_precision_impl
+ * (src/lapack/factorizations.jl:425-427, src/lapack/extended_lapack.jl:175-226).
+ *   prec    OXI_PREC_BF16 / OXI_PREC_FP16: FP32 panels, trailing updates on the
+ *           tensor cores with 16-bit operands and FP32 accumulation;
+ *           OXI_PREC_BF16X3: the same with each operand split into two BF16
+ *           terms and three products accumulated (one GEMM over 3K);
+ *           OXI_PREC_FP32: FP32 throughout (the reference's default Low type);
+ *           OXI_PREC_FP64: working-precision factor (lowtype=Float64).
+ *   refine  OXI_REFINE_IR (classical, as the reference), OXI_REFINE_GMRES
+ *           (GMRES-IR), OXI_REFINE_AUTO (IR, switching to GMRES-IR on stagnation).
+ * A (n x n), B and X (n x nrhs, nrhs <= 16) are column-major FP64 device
+ * arrays; X receives the solution.  The stop test compares the componentwise
+ * backward error max_i |r_i| / (|A||x| + |b|)_i (the reference metric) with
+ * rtol, or the normwise one when OXI_OPT_STOP_NORMWISE is set.  A singular low
+ * factor falls back to an FP64 factor (report.fallback, reason FALLBACK).
+ * Returns OXI_OK when converged, OXI_ENOTCONVERGED at maxiter (report filled),
+ * OXI_ENONFINITE for non-finite input, OXI_ESINGULAR when even the FP64 factor
+ * is singular, OXI_EOVERFLOW when a scaled right-hand side overflows.
+ * ------------------------------------------------------------------------- */
+enum oxi_precision {
+    OXI_PREC_FP32 = 0,
+    OXI_PREC_BF16 = 1,
+    OXI_PREC_FP16 = 2,
+    OXI_PREC_FP64 = 3,
+    OXI_PREC_BF16X3 = 4 /* split BF16: A_hi B_hi + A_hi B_lo + A_lo B_hi, BF16 operands */
+};
+enum oxi_refinement { OXI_REFINE_IR = 0, OXI_REFINE_GMRES = 1, OXI_REFINE_AUTO = 2 };
+enum oxi_reason {
+    OXI_REASON_CONVERGED = 0,       /* :converged               */
+    OXI_REASON_ITERATION_LIMIT = 1, /* :iteration_limit         */
+    OXI_REASON_FALLBACK = 2,        /* :working_factor_fallback */
+    OXI_REASON_NONFINITE = 3        /* :nonfinite_iteration     */
+};
+typedef struct oxi_refine_report {
+    int64_t iterations;             /* outer refinement steps (reference `iterations`) */
+    int64_t gmres_iterations;       /* inner GMRES iterations in total */
+    double backward_error;          /* componentwise (reference `backward_error`) */
+    double backward_error_normwise; /* ||b-Ax||_inf / (||A||_inf ||x||_inf + ||b||_inf) */
+    double residual_norm;           /* ||B - A X||_F (reference `residual`) */
+    double factor_ms;               /* equilibration + factorization time */
+    double refine_ms;               /* first solve + refinement time */
+    int64_t info;                   /* first zero pivot of the low-precision factor */
+    int32_t converged;
+    int32_t fallback;
+    int32_t refine_used;            /* oxi_refinement actually used at the end */
+    int32_t reason;                 /* oxi_reason */
+    int32_t low_type;               /* oxi_precision of the factor */
+    int32_t reserved;
+} oxi_refine_report;
+
+/* The mixed path's trailing-update kernel as a standalone call: C <- C - A*B
+ * (column-major FP32) with A and B rounded to prec (OXI_PREC_BF16 / _FP16 /
+ * _BF16X3, FP16
+ * with power-of-two operand scaling) and FP32 accumulation on the tensor cores
+ * (tcgen05); OXI_PREC_FP32 runs the FP32 CUDA-core GEMM.  The low-precision
+ * counterpart of gemm!(C, A, B, -1, 1) (src/blas/gemm.jl:635). */
+int oxi_sgemm_update_lowp(oxi_handle_t h, int prec, int64_t m, int64_t n, int64_t k, float *dC,
+                          int64_t ldc, const float *dA, int64_t lda, const float *dB, int64_t ldb);
+
+int oxi_dgesv_mixed(oxi_handle_t h, int prec, int refine, int64_t n, int64_t nrhs,
+                    const double *dA, int64_t lda, const double *dB, int64_t ldb, double *dX,
+                    int64_t ldx, int maxiter, double rtol, oxi_refine_report *out);
+
+/* ---------------------------------------------------------------------------
+ * Engine instrumentation (no counterpart in the reference, whose benchmarks time
+ * whole calls): kernels launched per handle, and, when enabled, CUDA-event
+ * timing of every launch of each kernel class on the handle's stream together
+ * with its algorithmic flops and bytes.
+ * ------------------------------------------------------------------------- */
+enum oxi_kernel_class {
+    OXI_K_LEAF = 0, OXI_K_ROWMOVES, OXI_K_TRSM_LEAF, OXI_K_GEMM_REF, OXI_K_GEMM_DMMA,
+    OXI_K_GEMM_TC, OXI_K_CONVERT, OXI_K_TRSV, OXI_K_RESIDUAL, OXI_K_OTHER, OXI_K_COUNT
+};
+int oxi_profile_enable(oxi_handle_t h, int on);  /* also clears the records */
+int oxi_profile_read(oxi_handle_t h, int kind, int64_t *launches, double *total_ms,
+                     double *flops, double *bytes);
+int oxi_launch_count(oxi_handle_t h, int64_t *count);
+int oxi_launch_count_reset(oxi_handle_t h);
 
 #ifdef __cplusplus
 }

@@ -10,9 +10,11 @@ from ._lib import (ArgumentError, DimensionMismatch, ExtensionMissing, Handle, S
                    exported_symbols, load)
 from .lu import (LU, colmajor_copy, det, gemm_update, ldiv, ldiv_, ldiv_into, logabsdet, lu, lu_,
                  options)
+from .mixed import gemm_update_lowp, mixed_solve, mixed_solve_device
+from . import synthetic
 
 __all__ = [
     "LU", "lu", "lu_", "ldiv", "ldiv_", "ldiv_into", "det", "logabsdet", "gemm_update", "options",
     "colmajor_copy", "SingularException", "DimensionMismatch", "ArgumentError", "ExtensionMissing",
-    "Handle", "load", "exported_symbols",
+    "Handle", "load", "exported_symbols", "mixed_solve", "mixed_solve_device", "gemm_update_lowp",
 ]

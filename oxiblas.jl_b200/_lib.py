@@ -17,6 +17,7 @@ LIB_PATH = os.path.join(HERE, "liboxiblas_b200.so")
 OXI_OK, OXI_EINVAL, OXI_ESINGULAR, OXI_ENONFINITE, OXI_EOVERFLOW = 0, 1, 2, 3, 4
 OXI_ECUDA, OXI_ETIMEOUT, OXI_ENOMEM, OXI_ENOTCONVERGED = 5, 6, 7, 8
 OPT_BLOCKSIZE, OPT_GEMM, OPT_TRSM_LEAF, OPT_LOOKAHEAD = 1, 2, 3, 4
+OPT_MIXED_BLOCKSIZE, OPT_STOP_NORMWISE, OPT_GMRES_RESTART = 5, 6, 7
 
 
 class SingularException(Exception):
@@ -57,6 +58,15 @@ _SIGS = {
     "oxi_dgetrs": ([_vp, ctypes.c_char, _i64, _i64, _vp, _i64, _vp, _vp, _i64], ctypes.c_int),
     "oxi_sgetrs": ([_vp, ctypes.c_char, _i64, _i64, _vp, _i64, _vp, _vp, _i64], ctypes.c_int),
     "oxi_dgemm_update": ([_vp, _i64, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64], ctypes.c_int),
+    "oxi_sgemm_update_lowp": ([_vp, ctypes.c_int, _i64, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64],
+                              ctypes.c_int),
+    "oxi_profile_enable": ([_vp, ctypes.c_int], ctypes.c_int),
+    "oxi_profile_read": ([_vp, ctypes.c_int, ctypes.POINTER(_i64), ctypes.POINTER(ctypes.c_double),
+                          ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
+    "oxi_launch_count": ([_vp, ctypes.POINTER(_i64)], ctypes.c_int),
+    "oxi_launch_count_reset": ([_vp], ctypes.c_int),
+    "oxi_dgesv_mixed": ([_vp, ctypes.c_int, ctypes.c_int, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64,
+                         ctypes.c_int, ctypes.c_double, _vp], ctypes.c_int),
 }
 
 
@@ -123,6 +133,31 @@ class Handle:
         v = _i64(0)
         self.check(self.lib.oxi_get_option(self.ptr, opt, ctypes.byref(v)))
         return int(v.value)
+
+    KERNEL_CLASSES = ("leaf", "rowmoves", "trsm_leaf", "gemm_ref", "gemm_dmma", "gemm_tc", "convert",
+                      "trsv", "residual", "other")
+
+    def profile(self, on: bool):
+        self.check(self.lib.oxi_profile_enable(self.ptr, 1 if on else 0))
+
+    def profile_read(self):
+        """{class: (timed launches, total ms, flops, bytes)} for the enabled window."""
+        out = {}
+        for k, name in enumerate(self.KERNEL_CLASSES):
+            c, ms, fl, by = _i64(0), ctypes.c_double(0), ctypes.c_double(0), ctypes.c_double(0)
+            self.check(self.lib.oxi_profile_read(self.ptr, k, ctypes.byref(c), ctypes.byref(ms),
+                                                 ctypes.byref(fl), ctypes.byref(by)))
+            if c.value:
+                out[name] = (int(c.value), ms.value, fl.value, by.value)
+        return out
+
+    def launches(self) -> int:
+        v = _i64(0)
+        self.check(self.lib.oxi_launch_count(self.ptr, ctypes.byref(v)))
+        return int(v.value)
+
+    def reset_launches(self):
+        self.check(self.lib.oxi_launch_count_reset(self.ptr))
 
     def check(self, status: int, info: int = 0):
         if status == OXI_OK:

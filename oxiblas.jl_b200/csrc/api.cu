@@ -1,6 +1,11 @@
-// Handle life cycle, options, status strings and the standalone GEMM entry point.
+// Handle life cycle, options, status strings, instrumentation and the
+// standalone GEMM entry points.
 #include <cstring>
 #include "oxi_internal.h"
+
+namespace oxi {
+thread_local Profiler *t_prof = nullptr;
+}
 
 extern "C" {
 
@@ -28,6 +33,7 @@ int oxi_destroy(oxi_handle_t h) {
     h->solve_ws.release();
     h->mixed_ws.release();
     h->perm_ws.release();
+    h->tc_ws.release();
     h->host_ws.release();
     delete h;
     return OXI_OK;
@@ -74,6 +80,17 @@ int oxi_set_option(oxi_handle_t h, int option, int64_t value) {
         case OXI_OPT_LOOKAHEAD:
             h->opt.lookahead = value ? 1 : 0;
             return OXI_OK;
+        case OXI_OPT_MIXED_BLOCKSIZE:
+            if (value < 1) return OXI_EINVAL;
+            h->opt.mixed_blocksize = value;
+            return OXI_OK;
+        case OXI_OPT_STOP_NORMWISE:
+            h->opt.stop_normwise = value ? 1 : 0;
+            return OXI_OK;
+        case OXI_OPT_GMRES_RESTART:
+            if (value < 2 || value > 62) return OXI_EINVAL;
+            h->opt.gmres_restart = (int)value;
+            return OXI_OK;
         default: return OXI_EINVAL;
     }
 }
@@ -85,6 +102,9 @@ int oxi_get_option(oxi_handle_t h, int option, int64_t *value) {
         case OXI_OPT_GEMM: *value = h->opt.gemm; return OXI_OK;
         case OXI_OPT_TRSM_LEAF: *value = h->opt.trsm_leaf; return OXI_OK;
         case OXI_OPT_LOOKAHEAD: *value = h->opt.lookahead; return OXI_OK;
+        case OXI_OPT_MIXED_BLOCKSIZE: *value = h->opt.mixed_blocksize; return OXI_OK;
+        case OXI_OPT_STOP_NORMWISE: *value = h->opt.stop_normwise; return OXI_OK;
+        case OXI_OPT_GMRES_RESTART: *value = h->opt.gmres_restart; return OXI_OK;
         default: return OXI_EINVAL;
     }
 }
@@ -97,6 +117,8 @@ int oxi_dgemm_update(oxi_handle_t h, int64_t m, int64_t n, int64_t k, double *dC
     if (m == 0 || n == 0 || k == 0) return OXI_OK;
     if (!dC || !dA || !dB || ldc < m || lda < m || ldb < k) return OXI_EINVAL;
     try {
+        oxi::ProfGuard pg(&h->prof);
+        OXI_CUDA(cudaSetDevice(h->device));
         oxi::gemm_minus<double>(h, dC, ldc, dB, ldb, dA, lda, n, m, k);
         OXI_CUDA(cudaStreamSynchronize(h->stream));
         return OXI_OK;
@@ -104,6 +126,76 @@ int oxi_dgemm_update(oxi_handle_t h, int64_t m, int64_t n, int64_t k, double *dC
         h->last_error = std::string(e.what) + ": " + cudaGetErrorString(e.code);
         return OXI_ECUDA;
     }
+}
+
+int oxi_sgemm_update_lowp(oxi_handle_t h, int prec, int64_t m, int64_t n, int64_t k, float *dC,
+                          int64_t ldc, const float *dA, int64_t lda, const float *dB, int64_t ldb) {
+    if (!h || m < 0 || n < 0 || k < 0) return OXI_EINVAL;
+    if (prec != OXI_PREC_FP32 && prec != OXI_PREC_BF16 && prec != OXI_PREC_FP16 && prec != OXI_PREC_BF16X3)
+        return OXI_EINVAL;
+    if (m == 0 || n == 0 || k == 0) return OXI_OK;
+    if (!dC || !dA || !dB || ldc < m || lda < m || ldb < k) return OXI_EINVAL;
+    const int saved = h->trailing;
+    try {
+        oxi::ProfGuard pg(&h->prof);
+        OXI_CUDA(cudaSetDevice(h->device));
+        h->trailing = prec;  // OXI_PREC_{FP32,BF16,FP16,BF16X3} == TRAIL_{NATIVE,BF16,FP16,BF16X3}
+        if (prec == OXI_PREC_FP32)
+            oxi::gemm_minus<float>(h, dC, ldc, dB, ldb, dA, lda, n, m, k);
+        else
+            oxi::gemm_trailing_f32(h, dC, ldc, dB, ldb, dA, lda, n, m, k);
+        h->trailing = saved;
+        OXI_CUDA(cudaStreamSynchronize(h->stream));
+        return OXI_OK;
+    } catch (const oxi::CudaError &e) {
+        h->trailing = saved;
+        h->last_error = std::string(e.what) + ": " + cudaGetErrorString(e.code);
+        return OXI_ECUDA;
+    }
+}
+
+int oxi_profile_enable(oxi_handle_t h, int on) {
+    if (!h) return OXI_EINVAL;
+    cudaSetDevice(h->device);
+    cudaStreamSynchronize(h->stream);
+    h->prof.recycle();
+    h->prof.enabled = on != 0;
+    return OXI_OK;
+}
+
+int oxi_profile_read(oxi_handle_t h, int kind, int64_t *launches, double *total_ms, double *flops,
+                     double *bytes) {
+    if (!h || kind < 0 || kind >= oxi::KC_COUNT) return OXI_EINVAL;
+    cudaSetDevice(h->device);
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) return OXI_ECUDA;
+    int64_t cnt = 0;
+    double ms = 0, fl = 0, by = 0;
+    for (auto &r : h->prof.recs) {
+        if (r.kind != kind) continue;
+        float t = 0;
+        if (cudaEventElapsedTime(&t, r.a, r.b) != cudaSuccess) continue;
+        ++cnt;
+        ms += t;
+        fl += r.flops;
+        by += r.bytes;
+    }
+    if (launches) *launches = cnt;
+    if (total_ms) *total_ms = ms;
+    if (flops) *flops = fl;
+    if (bytes) *bytes = by;
+    return OXI_OK;
+}
+
+int oxi_launch_count(oxi_handle_t h, int64_t *count) {
+    if (!h || !count) return OXI_EINVAL;
+    *count = (int64_t)h->prof.launches;
+    return OXI_OK;
+}
+
+int oxi_launch_count_reset(oxi_handle_t h) {
+    if (!h) return OXI_EINVAL;
+    h->prof.launches = 0;
+    return OXI_OK;
 }
 
 }  // extern "C"

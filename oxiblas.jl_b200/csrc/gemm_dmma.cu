@@ -183,6 +183,7 @@ void launch_gemm_dmma(double *C, i64 ldc, const double *A, i64 lda, const double
         attr = true;
     }
     dim3 grid((unsigned)((N + BN - 1) / BN), (unsigned)((M + BM - 1) / BM));
+    ProfScope ps(KC_GEMM_DMMA, s, 2.0 * M * N * K, 8.0 * (2.0 * M * N + M * K + K * N));
     k_gemm_dmma<<<grid, NTHREADS, SMEM_BYTES, s>>>(tmA, tmB, C, ldc, (int)M, (int)N, (int)K);
     OXI_LAUNCH_CHECK();
 }

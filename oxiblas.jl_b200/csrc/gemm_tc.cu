@@ -1,0 +1,390 @@
+// Mixed-precision trailing update on the 5th-generation tensor cores:
+//   C (FP32, row-major) <- C - scale * (A * B^T)
+// A: M x K, B: N x K, both 16-bit (BF16 or FP16) and K-major (K contiguous),
+// accumulated in FP32 in tensor memory (tcgen05.mma kind::f16).
+//
+// CTA tile 128 x 256, k slab 64 (one 128-byte swizzle atom per row), 2-stage
+// TMA -> shared memory ring, 4 warps:
+//   warp 0 lane 0   TMA producer
+//   warp 1 lane 0   MMA issuer (tcgen05.mma, commit -> "stage empty" barrier)
+//   warps 0..3      epilogue: tcgen05.ld 32 lanes x 32 columns at a time, each
+//                   thread owns one row of the tile, C - scale*D written back.
+// Two CTAs per SM (96 KB of shared memory and 256 TMEM columns each) so one
+// CTA's epilogue overlaps the other's loads and MMAs.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include "tma_util.cuh"
+
+namespace oxi {
+
+namespace tc {
+constexpr int BM = 128, BN = 256, BK = 64, STAGES = 2;
+constexpr int A_BYTES = BM * BK * 2;  // 16 KB
+constexpr int B_BYTES = BN * BK * 2;  // 32 KB
+constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
+constexpr int NTHREADS = 128;
+constexpr int TMEM_COLS = 256;
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+}  // namespace tc
+
+__device__ int g_gemm_tc_err;
+
+// UMMA shared-memory descriptor, K-major operand in the 128-byte swizzle
+// layout TMA writes (rows of 128 bytes, 8-row groups 1024 bytes apart).
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t smem_addr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((smem_addr >> 4) & 0x3FFF);  // start address
+    d |= (uint64_t)1 << 16;                       // leading byte offset (unused for SW128 K-major)
+    d |= (uint64_t)(1024 >> 4) << 32;             // stride byte offset: 8 rows x 128 B
+    d |= (uint64_t)1 << 46;                       // descriptor version (sm_100)
+    d |= (uint64_t)2 << 61;                       // SWIZZLE_128B
+    return d;
+}
+
+// Instruction descriptor: D=F32, A/B format (0 F16, 1 BF16), K-major both, M, N.
+__host__ __device__ constexpr uint32_t umma_idesc_f16(int ab_format, int M, int N) {
+    return (1u << 4) | ((uint32_t)ab_format << 7) | ((uint32_t)ab_format << 10) |
+           ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void tc_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+
+template <int AB_FORMAT>
+__global__ void __launch_bounds__(tc::NTHREADS, 2)
+k_gemm_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+          float *__restrict__ C, i64 ldc, int M, int N, int K, float scale,
+          const float *__restrict__ d_scale) {
+    using namespace tc;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~uintptr_t(1023));
+    uint64_t *full = (uint64_t *)(smem + STAGES * STAGE_BYTES);
+    uint64_t *empty = full + STAGES;
+    uint64_t *done = empty + STAGES;
+    uint32_t *tmem_slot = (uint32_t *)(done + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    const int KT = (K + BK - 1) / BK;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(done, 1);
+        fence_barrier_init();
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(tmem_slot)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+        tc_fence_before();
+    }
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        prefetch_tmap(&tmA);
+        prefetch_tmap(&tmB);
+        for (int kt = 0; kt < KT; ++kt) {
+            const int s = kt % STAGES;
+            if (kt >= STAGES && !mbar_wait(&empty[s], ((kt / STAGES) + 1) & 1, &g_gemm_tc_err, 1)) break;
+            uint8_t *sa = smem + s * STAGE_BYTES;
+            mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
+            tma_load_2d(sa, &tmA, &full[s], kt * BK, m0);
+            tma_load_2d(sa + A_BYTES, &tmB, &full[s], kt * BK, n0);
+        }
+    } else if (warp == 1 && lane == 0) {
+        constexpr uint32_t idesc = umma_idesc_f16(AB_FORMAT, BM, BN);
+        bool ok = true;
+        for (int kt = 0; kt < KT && ok; ++kt) {
+            const int s = kt % STAGES;
+            if (!mbar_wait(&full[s], (kt / STAGES) & 1, &g_gemm_tc_err, 2)) { ok = false; break; }
+            tc_fence_after();
+            const uint32_t sa = smem_u32(smem + s * STAGE_BYTES);
+            const uint64_t da = umma_desc_sw128(sa), db = umma_desc_sw128(sa + A_BYTES);
+#pragma unroll
+            for (int k = 0; k < BK / 16; ++k) {
+                const uint64_t adv = (uint64_t)((k * 32) >> 4);  // 16 elements = 32 bytes
+                const uint32_t acc = (kt > 0 || k > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                    " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+                    "l"(da + adv), "l"(db + adv), "r"(idesc), "r"(acc));
+            }
+            asm volatile(
+                "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                    smem_u32(&empty[s]))
+                : "memory");
+        }
+        asm volatile(
+            "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                smem_u32(done))
+            : "memory");
+    }
+    __syncwarp();
+
+    // ---------------- epilogue ----------------
+    const bool have = mbar_wait(done, 0, &g_gemm_tc_err, 3);
+    tc_fence_after();
+    const float sc = d_scale ? scale * (*d_scale) : scale;
+    const int row = m0 + warp * 32 + lane;
+    if (have) {
+#pragma unroll 1
+        for (int c = 0; c < BN / 32; ++c) {
+            uint32_t v[32];
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(c * 32);
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,"
+                "%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                  "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+                  "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]),
+                  "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+                  "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]),
+                  "=r"(v[31])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            const int col0 = n0 + c * 32;
+            if (row < M && col0 < N) {
+                float *cr = C + (i64)row * ldc + col0;
+                if (col0 + 32 <= N && ((((uintptr_t)cr) & 15) == 0)) {
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        float4 x = *(float4 *)(cr + 4 * q);
+                        x.x -= sc * __uint_as_float(v[4 * q + 0]);
+                        x.y -= sc * __uint_as_float(v[4 * q + 1]);
+                        x.z -= sc * __uint_as_float(v[4 * q + 2]);
+                        x.w -= sc * __uint_as_float(v[4 * q + 3]);
+                        *(float4 *)(cr + 4 * q) = x;
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 32; ++j)
+                        if (col0 + j < N) cr[j] -= sc * __uint_as_float(v[j]);
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(TMEM_COLS));
+    }
+}
+
+// ---- operand conversion (FP32 row-major -> 16-bit K-major) ----
+template <typename H> __device__ __forceinline__ H to_half_t(float x);
+template <> __device__ __forceinline__ __nv_bfloat16 to_half_t<__nv_bfloat16>(float x) { return __float2bfloat16_rn(x); }
+template <> __device__ __forceinline__ __half to_half_t<__half>(float x) { return __float2half_rn(x); }
+
+// dst[r][c] = src[r][c] * scale (same orientation): the A operand (L21).
+template <typename H>
+__global__ void k_cvt_rows(const float *__restrict__ src, i64 lds, H *__restrict__ dst, i64 ldd,
+                           int rows, int cols, float scale, const float *__restrict__ d_scale) {
+    const float s = d_scale ? scale * (*d_scale) : scale;
+    const i64 r = blockIdx.y;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < cols; c += gridDim.x * blockDim.x)
+        dst[r * ldd + c] = to_half_t<H>(src[r * lds + c] * s);
+}
+
+// dst[c][r] = src[r][c] * scale (transposed): the B operand (U12 -> N x K).
+template <typename H>
+__global__ void k_cvt_transpose(const float *__restrict__ src, i64 lds, H *__restrict__ dst,
+                                i64 ldd, int rows, int cols, float scale,
+                                const float *__restrict__ d_scale) {
+    __shared__ float tile[32][33];
+    const float s = d_scale ? scale * (*d_scale) : scale;
+    const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    for (int k = ty; k < 32; k += 8) {
+        const int r = r0 + k, c = c0 + tx;
+        tile[k][tx] = (r < rows && c < cols) ? src[(i64)r * lds + c] : 0.f;
+    }
+    __syncthreads();
+    for (int k = ty; k < 32; k += 8) {
+        const int c = c0 + k, r = r0 + tx;
+        if (c < cols && r < rows) dst[(i64)c * ldd + r] = to_half_t<H>(tile[tx][k] * s);
+    }
+}
+
+// Split-BF16 operands: x = hi + lo with hi = bf16(x), lo = bf16(x - hi).  A row
+// becomes [hi | hi | lo] and a B row [hi | lo | hi] along K, so one GEMM over 3K
+// accumulates A_hi B_hi + A_hi B_lo + A_lo B_hi (the A_lo B_lo term, ~2^-16
+// relative, is dropped): FP32-level products from BF16 tensor-core operands.
+__global__ void k_cvt_rows_split3(const float *__restrict__ src, i64 lds, __nv_bfloat16 *__restrict__ dst,
+                                  i64 ldd, int rows, int cols) {
+    const i64 r = blockIdx.y;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < cols; c += gridDim.x * blockDim.x) {
+        const float x = src[r * lds + c];
+        const __nv_bfloat16 hi = __float2bfloat16_rn(x);
+        const __nv_bfloat16 lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+        __nv_bfloat16 *d = dst + r * ldd;
+        d[c] = hi;
+        d[cols + c] = hi;
+        d[2 * cols + c] = lo;
+    }
+}
+__global__ void k_cvt_transpose_split3(const float *__restrict__ src, i64 lds, __nv_bfloat16 *__restrict__ dst,
+                                       i64 ldd, int rows, int cols) {
+    __shared__ float tile[32][33];
+    const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    for (int k = ty; k < 32; k += 8) {
+        const int r = r0 + k, c = c0 + tx;
+        tile[k][tx] = (r < rows && c < cols) ? src[(i64)r * lds + c] : 0.f;
+    }
+    __syncthreads();
+    for (int k = ty; k < 32; k += 8) {
+        const int c = c0 + k, r = r0 + tx;  // dst row c (an N index), K position r
+        if (c < cols && r < rows) {
+            const float x = tile[tx][k];
+            const __nv_bfloat16 hi = __float2bfloat16_rn(x);
+            const __nv_bfloat16 lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+            __nv_bfloat16 *d = dst + (i64)c * ldd;
+            d[r] = hi;
+            d[rows + r] = lo;
+            d[2 * rows + r] = hi;
+        }
+    }
+}
+
+// ---- host ----
+void launch_gemm_tc(int fmt /*0 fp16, 1 bf16*/, float *C, i64 ldc, const void *A16, i64 lda16,
+                    const void *B16, i64 ldb16, i64 M, i64 N, i64 K, float scale,
+                    const float *d_scale, cudaStream_t s) {
+    using namespace tc;
+    if (M <= 0 || N <= 0 || K <= 0) return;
+    CUtensorMap tmA, tmB;
+    const CUtensorMapDataType dt = fmt == 1 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+    make_tmap_2d(&tmA, dt, 2, A16, K, M, lda16, BK, BM, CU_TENSOR_MAP_SWIZZLE_128B);
+    make_tmap_2d(&tmB, dt, 2, B16, K, N, ldb16, BK, BN, CU_TENSOR_MAP_SWIZZLE_128B);
+    dim3 grid((unsigned)((N + BN - 1) / BN), (unsigned)((M + BM - 1) / BM));
+    ProfScope ps(KC_GEMM_TC, s, 2.0 * M * N * K, 8.0 * M * N + 2.0 * (M + N) * K);
+    if (fmt == 1) {
+        static bool attr = false;
+        if (!attr) {
+            OXI_CUDA(cudaFuncSetAttribute(k_gemm_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+            attr = true;
+        }
+        k_gemm_tc<1><<<grid, NTHREADS, SMEM_BYTES, s>>>(tmA, tmB, C, ldc, (int)M, (int)N, (int)K, scale, d_scale);
+    } else {
+        static bool attr = false;
+        if (!attr) {
+            OXI_CUDA(cudaFuncSetAttribute(k_gemm_tc<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+            attr = true;
+        }
+        k_gemm_tc<0><<<grid, NTHREADS, SMEM_BYTES, s>>>(tmA, tmB, C, ldc, (int)M, (int)N, (int)K, scale, d_scale);
+    }
+    OXI_LAUNCH_CHECK();
+}
+
+void launch_cvt_rows16(int fmt, const float *src, i64 lds, void *dst, i64 ldd, i64 rows, i64 cols,
+                       float scale, const float *d_scale, cudaStream_t s) {
+    if (rows <= 0 || cols <= 0) return;
+    dim3 grid((unsigned)std::min<i64>((cols + 255) / 256, 64), (unsigned)rows);
+    ProfScope ps(KC_CONVERT, s, 0.0, 6.0 * rows * cols);
+    if (fmt == 1)
+        k_cvt_rows<__nv_bfloat16><<<grid, 256, 0, s>>>(src, lds, (__nv_bfloat16 *)dst, ldd, (int)rows, (int)cols, scale, d_scale);
+    else
+        k_cvt_rows<__half><<<grid, 256, 0, s>>>(src, lds, (__half *)dst, ldd, (int)rows, (int)cols, scale, d_scale);
+    OXI_LAUNCH_CHECK();
+}
+
+void launch_cvt_transpose16(int fmt, const float *src, i64 lds, void *dst, i64 ldd, i64 rows,
+                            i64 cols, float scale, const float *d_scale, cudaStream_t s) {
+    if (rows <= 0 || cols <= 0) return;
+    dim3 grid((unsigned)((cols + 31) / 32), (unsigned)((rows + 31) / 32));
+    ProfScope ps(KC_CONVERT, s, 0.0, 6.0 * rows * cols);
+    if (fmt == 1)
+        k_cvt_transpose<__nv_bfloat16><<<grid, dim3(32, 8), 0, s>>>(src, lds, (__nv_bfloat16 *)dst, ldd, (int)rows, (int)cols, scale, d_scale);
+    else
+        k_cvt_transpose<__half><<<grid, dim3(32, 8), 0, s>>>(src, lds, (__half *)dst, ldd, (int)rows, (int)cols, scale, d_scale);
+    OXI_LAUNCH_CHECK();
+}
+
+}  // namespace oxi
+
+namespace oxi {
+
+// FP16 operand scaling: L21 has |l| <= 1 under partial pivoting and is scaled by
+// 2^14; U12 is scaled by the power of two that brings max|U12| into [2^14, 2^15),
+// so neither operand overflows FP16 and small entries keep their precision.  The
+// GEMM epilogue multiplies by the inverse of both scales (exact powers of two).
+__global__ void k_absmax_f32(const float *__restrict__ src, i64 lds, int rows, int cols,
+                             unsigned int *__restrict__ out) {
+    float mx = 0.f;
+    const int r = blockIdx.y;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < cols; c += gridDim.x * blockDim.x)
+        mx = fmaxf(mx, fabsf(src[(i64)r * lds + c]));
+    for (int off = 16; off > 0; off >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(mx));
+}
+__global__ void k_fp16_scales(const unsigned int *__restrict__ umax_bits, float *__restrict__ sc) {
+    const float umax = __uint_as_float(*umax_bits);
+    int e = 0;
+    if (umax > 0.f && isfinite(umax)) frexpf(umax, &e);  // umax in [2^(e-1), 2^e)
+    const int su = 15 - e;                                 // umax * 2^su in [2^14, 2^15)
+    sc[0] = ldexpf(1.f, su);                               // U12 scale
+    sc[1] = ldexpf(1.f, -(su + 14));                       // epilogue: 2^-14 * 2^-su
+}
+
+void gemm_trailing_f32(oxi_handle_s *h, float *C, i64 ldc, const float *A, i64 lda, const float *B,
+                       i64 ldb, i64 M, i64 N, i64 K) {
+    if (M <= 0 || N <= 0 || K <= 0) return;
+    if (h->trailing == TRAIL_BF16X3) {
+        const i64 K3 = 3 * K, ldk3 = (K3 + 7) / 8 * 8;
+        char *ws = (char *)h->tc_ws.get((size_t)(M + N) * ldk3 * 2 + 1024);
+        __nv_bfloat16 *A16 = (__nv_bfloat16 *)ws;
+        __nv_bfloat16 *B16 = (__nv_bfloat16 *)(((uintptr_t)(ws + (size_t)M * ldk3 * 2) + 255) & ~uintptr_t(255));
+        cudaStream_t s = h->stream;
+        {
+            ProfScope ps(KC_CONVERT, s, 0.0, 10.0 * (double)M * K);
+            dim3 g((unsigned)std::min<i64>((K + 255) / 256, 64), (unsigned)M);
+            k_cvt_rows_split3<<<g, 256, 0, s>>>(A, lda, A16, ldk3, (int)M, (int)K);
+            OXI_LAUNCH_CHECK();
+        }
+        {
+            ProfScope ps(KC_CONVERT, s, 0.0, 10.0 * (double)N * K);
+            dim3 g((unsigned)((N + 31) / 32), (unsigned)((K + 31) / 32));
+            k_cvt_transpose_split3<<<g, dim3(32, 8), 0, s>>>(B, ldb, B16, ldk3, (int)K, (int)N);
+            OXI_LAUNCH_CHECK();
+        }
+        launch_gemm_tc(1, C, ldc, A16, ldk3, B16, ldk3, M, N, K3, 1.f, nullptr, s);
+        return;
+    }
+    const int fmt = (h->trailing == TRAIL_BF16) ? 1 : 0;
+    const i64 ldk = (K + 7) / 8 * 8;
+    char *ws = (char *)h->tc_ws.get((size_t)(M + N) * ldk * 2 + 1024);
+    void *A16 = ws;
+    void *B16 = ws + (size_t)M * ldk * 2;
+    B16 = (void *)(((uintptr_t)B16 + 255) & ~uintptr_t(255));
+    float *scal = (float *)((char *)h->scratch.get(kScratchBytes) + kScratchScalOff + 1536);
+    cudaStream_t s = h->stream;
+    if (fmt == 1) {
+        launch_cvt_rows16(1, A, lda, A16, ldk, M, K, 1.f, nullptr, s);
+        launch_cvt_transpose16(1, B, ldb, B16, ldk, K, N, 1.f, nullptr, s);
+        launch_gemm_tc(1, C, ldc, A16, ldk, B16, ldk, M, N, K, 1.f, nullptr, s);
+    } else {
+        unsigned int *umax = (unsigned int *)(scal + 4);
+        OXI_CUDA(cudaMemsetAsync(umax, 0, sizeof(unsigned int), s));
+        k_absmax_f32<<<dim3((unsigned)std::min<i64>((N + 255) / 256, 16), (unsigned)K), 256, 0, s>>>(
+            B, ldb, (int)K, (int)N, umax);
+        OXI_LAUNCH_CHECK();
+        k_fp16_scales<<<1, 1, 0, s>>>(umax, scal);
+        OXI_LAUNCH_CHECK();
+        launch_cvt_rows16(0, A, lda, A16, ldk, M, K, 16384.f, nullptr, s);
+        launch_cvt_transpose16(0, B, ldb, B16, ldk, K, N, 1.f, scal, s);
+        launch_gemm_tc(0, C, ldc, A16, ldk, B16, ldk, M, N, K, 1.f, scal + 1, s);
+    }
+}
+
+}  // namespace oxi

@@ -109,6 +109,13 @@ void getrf_rowmajor(oxi_handle_s *h, T *W, i64 ld, i64 m, i64 n, int64_t *d_ipiv
         T *L11 = W + f * ld + f;
         trsm_lower_unit<T>(h, L11, ld, L11 + (l - f), ld, l - f, n - l);
         if (l >= m) continue;
+        if constexpr (sizeof(T) == 4) {
+            if (h->trailing != TRAIL_NATIVE) {
+                gemm_trailing_f32(h, W + l * ld + l, ld, W + l * ld + f, ld, W + f * ld + l, ld,
+                                  m - l, n - l, l - f);
+                continue;
+            }
+        }
         gemm_minus<T>(h, W + l * ld + l, ld, W + l * ld + f, ld, W + f * ld + l, ld, m - l, n - l,
                       l - f);
     }
@@ -127,10 +134,11 @@ static int getrf_entry(oxi_handle_s *h, i64 m, i64 n, T *dA, i64 lda, int64_t *d
     if (!dA || !d_ipiv) return OXI_EINVAL;
     if (leaf_width_for<T>(m) == 0) return OXI_EINVAL;
     try {
+        ProfGuard pg(&h->prof);
         OXI_CUDA(cudaSetDevice(h->device));
         const i64 ld = round_up(n, 32);
         T *W = (T *)h->work.get((size_t)m * ld * sizeof(T));
-        char *sc = (char *)h->scratch.get(4096);
+        char *sc = (char *)h->scratch.get(kScratchBytes);
         int64_t *d_info = (int64_t *)sc;
         int *d_nmoves = (int *)(sc + 64);
         int *d_moves = (int *)(sc + 128);

@@ -319,7 +319,9 @@ static void launch_leaf_wr(T *P, i64 ld, i64 m, int w, i64 gofs, int64_t *ipiv, 
     at[0].val.clusterDim.z = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
+    ProfScope ps(KC_LEAF, s, 0.0, 2.0 * (double)m * w * sizeof(T));
     OXI_CUDA(cudaLaunchKernelEx(&cfg, kern, P, ld, (int)m, w, gofs, ipiv, info, moves, nmoves));
+    count_launch();
 }
 
 template <typename T>
@@ -383,6 +385,7 @@ void launch_rowmoves(T *W, i64 ld, i64 r0, const int *moves, const int *nmoves, 
     if (c_hi <= c_lo) return;
     const int nt = 128;
     const i64 cols = c_hi - c_lo;
+    ProfScope ps(KC_ROWMOVES, s, 0.0, 0.0);
     k_rowmoves<T><<<(unsigned)((cols + nt - 1) / nt), nt, 0, s>>>(W, ld, r0, moves, nmoves, c_lo, c_hi,
                                                                    skip_lo, skip_hi);
     OXI_LAUNCH_CHECK();
@@ -429,6 +432,7 @@ template <typename T>
 void launch_trsm_leaf(const T *L, i64 ldl, T *B, i64 ldb, int t, i64 N, cudaStream_t s) {
     if (t <= 1 || N <= 0) return;  // a unit 1x1 triangle is the identity
     const int nt = 128;
+    ProfScope ps(KC_TRSM_LEAF, s, (double)t * t * N, 2.0 * (double)t * N * sizeof(T));
     k_trsm_leaf<T><<<(unsigned)((N + nt - 1) / nt), nt, 0, s>>>(L, ldl, B, ldb, t, N);
     OXI_LAUNCH_CHECK();
 }
@@ -491,6 +495,7 @@ void launch_gemm_ref(T *C, i64 ldc, const T *A, i64 lda, const T *B, i64 ldb, i6
                      cudaStream_t s) {
     if (M <= 0 || N <= 0 || K <= 0) return;
     dim3 grid((unsigned)((N + 63) / 64), (unsigned)((M + 63) / 64));
+    ProfScope ps(KC_GEMM_REF, s, 2.0 * M * N * K, (double)sizeof(T) * (2.0 * M * N + M * K + K * N));
     k_gemm_ref<T><<<grid, 256, 0, s>>>(C, ldc, A, lda, B, ldb, M, N, K);
     OXI_LAUNCH_CHECK();
 }

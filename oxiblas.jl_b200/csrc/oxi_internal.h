@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "../../include/oxiblas_b200.h"
+#include "profile.h"
 
 namespace oxi {
 
@@ -26,7 +27,19 @@ struct CudaError {
         if (oxi_e_ != cudaSuccess) throw ::oxi::CudaError{oxi_e_, #expr};             \
     } while (0)
 
-#define OXI_LAUNCH_CHECK() OXI_CUDA(cudaGetLastError())
+#define OXI_LAUNCH_CHECK()              \
+    do {                                \
+        ::oxi::count_launch();          \
+        OXI_CUDA(cudaGetLastError());   \
+    } while (0)
+
+// Fixed layout of the handle's small control block (allocated once at this size,
+// so pointers into it stay valid for the whole call).
+constexpr size_t kScratchBytes = 65536;
+constexpr size_t kScratchErrOff = 1024;     // int error words
+constexpr size_t kScratchScalOff = 2048;    // double scalars of the mixed path
+constexpr size_t kScratchTrsvOff = 8192;    // triangular-solve tickets and flags
+constexpr int kTrsvCtlInts = (int)((kScratchBytes - kScratchTrsvOff) / sizeof(int));
 
 // Device workspace owned by a handle; grows monotonically.
 struct DeviceBuffer {
@@ -73,7 +86,14 @@ struct Options {
     int gemm = 0;          // 0 tensor-core engine, 1 reference summation order
     i64 trsm_leaf = 32;    // recursive TRSM leaf
     int lookahead = 0;
+    i64 mixed_blocksize = 256;  // panel width of the mixed-precision factorization
+    int stop_normwise = 0;      // IR stop test: 0 componentwise (reference), 1 normwise
+    int gmres_restart = 30;
+    double gmres_tol = 1e-4;    // inner relative tolerance of GMRES-IR
 };
+
+// Precision of the trailing update inside an FP32 factorization.
+enum TrailingKind { TRAIL_NATIVE = 0, TRAIL_BF16 = 1, TRAIL_FP16 = 2, TRAIL_BF16X3 = 4 };
 
 }  // namespace oxi
 
@@ -90,6 +110,9 @@ struct oxi_handle_s {
     oxi::DeviceBuffer mixed_ws;  // mixed-precision workspace
     oxi::DeviceBuffer perm_ws;   // row permutation of the last solve
     oxi::PinnedBuffer host_ws;   // pinned host staging
+    oxi::DeviceBuffer tc_ws;     // 16-bit GEMM operands
+    int trailing = 0;            // oxi::TrailingKind for getrf_rowmajor<float>
+    oxi::Profiler prof;
 };
 
 namespace oxi {
@@ -130,6 +153,18 @@ void launch_gemm_ref(T *C, i64 ldc, const T *A, i64 lda, const T *B, i64 ldb, i6
 void launch_gemm_dmma(double *C, i64 ldc, const double *A, i64 lda, const double *B, i64 ldb,
                       i64 M, i64 N, i64 K, cudaStream_t s);
 
+// tcgen05 GEMM: C (FP32 row-major) -= scale * A16 * B16^T, 16-bit K-major operands.
+void launch_gemm_tc(int fmt, float *C, i64 ldc, const void *A16, i64 lda16, const void *B16,
+                    i64 ldb16, i64 M, i64 N, i64 K, float scale, const float *d_scale,
+                    cudaStream_t s);
+void launch_cvt_rows16(int fmt, const float *src, i64 lds, void *dst, i64 ldd, i64 rows, i64 cols,
+                       float scale, const float *d_scale, cudaStream_t s);
+void launch_cvt_transpose16(int fmt, const float *src, i64 lds, void *dst, i64 ldd, i64 rows,
+                            i64 cols, float scale, const float *d_scale, cudaStream_t s);
+// C -= A*B for the trailing update of an FP32 factorization in h->trailing precision.
+void gemm_trailing_f32(oxi_handle_s *h, float *C, i64 ldc, const float *A, i64 lda,
+                       const float *B, i64 ldb, i64 M, i64 N, i64 K);
+
 // Host driver: blocked right-looking getrf on a row-major working matrix.
 template <typename T>
 void getrf_rowmajor(oxi_handle_s *h, T *W, i64 ld, i64 m, i64 n, int64_t *d_ipiv,
@@ -149,5 +184,9 @@ template <typename T>
 void getrs_perm(oxi_handle_s *h, char trans, i64 n, i64 nrhs, const T *LU, i64 lda,
                 const int64_t *d_perm, T *B, i64 ldb, int *d_err);
 void perm_from_ipiv(const int64_t *ipiv, i64 q, i64 m, int64_t *perm);
+// L then U solves with ROW-major factors (W, ld), X column-major n x nrhs, in place.
+template <typename T>
+void lu_solve_rowmajor(oxi_handle_s *h, const T *W, i64 ld, i64 n, T *X, i64 ldx, i64 nrhs,
+                       int *d_err);
 
 }  // namespace oxi

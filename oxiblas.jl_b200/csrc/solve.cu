@@ -189,6 +189,7 @@ template <typename T, bool UPPER_A, bool UNIT, bool TRANS>
 static void trsv_launch(const T *A, i64 lda, T *X, i64 ldx, int n, int nrhs, int *ctl, int *err,
                         cudaStream_t s) {
     const int nb = (n + SB - 1) / SB;
+    ProfScope ps(KC_TRSV, s, (double)n * n * nrhs, (double)n * n * sizeof(T) / 2);
     for (int k0 = 0; k0 < nrhs;) {
         const int left = nrhs - k0;
         OXI_CUDA(cudaMemsetAsync(ctl, 0, sizeof(int) * (nb + 1), s));
@@ -238,6 +239,20 @@ void getrs_perm(oxi_handle_s *h, char trans, i64 n, i64 nrhs, const T *LU, i64 l
 template void getrs_perm<double>(oxi_handle_s *, char, i64, i64, const double *, i64, const int64_t *, double *, i64, int *);
 template void getrs_perm<float>(oxi_handle_s *, char, i64, i64, const float *, i64, const int64_t *, float *, i64, int *);
 
+// Row-major factors W are the column-major matrix W^T: L (lower) is then an
+// upper-stored triangle read transposed, U likewise.
+template <typename T>
+void lu_solve_rowmajor(oxi_handle_s *h, const T *W, i64 ld, i64 n, T *X, i64 ldx, i64 nrhs,
+                       int *d_err) {
+    const i64 nb = (n + SB - 1) / SB;
+    if (nb + 1 > kTrsvCtlInts) throw CudaError{cudaErrorInvalidValue, "system too large for the solve control block"};
+    int *ctl = (int *)((char *)h->scratch.get(kScratchBytes) + kScratchTrsvOff);
+    trsv_launch<T, true, true, true>(W, ld, X, ldx, (int)n, (int)nrhs, ctl, d_err, h->stream);
+    trsv_launch<T, false, false, true>(W, ld, X, ldx, (int)n, (int)nrhs, ctl, d_err, h->stream);
+}
+template void lu_solve_rowmajor<float>(oxi_handle_s *, const float *, i64, i64, float *, i64, i64, int *);
+template void lu_solve_rowmajor<double>(oxi_handle_s *, const double *, i64, i64, double *, i64, i64, int *);
+
 // LUFactor.p from the interchange sequence (src/lapack/factorizations.jl:72-75).
 void perm_from_ipiv(const int64_t *ipiv, i64 q, i64 m, int64_t *perm) {
     for (i64 i = 0; i < m; ++i) perm[i] = i;
@@ -259,6 +274,7 @@ static int getrs_entry(oxi_handle_s *h, char trans, i64 n, i64 nrhs, const T *dL
     if (n == 0 || nrhs == 0) return OXI_OK;
     if (!dLU || !d_ipiv || !dB || n >= (1ll << 31)) return OXI_EINVAL;
     try {
+        ProfGuard pg(&h->prof);
         OXI_CUDA(cudaSetDevice(h->device));
         // The interchange sequence is inherently sequential: fold it into the
         // permutation once on the host (n int64 each way).
@@ -268,8 +284,8 @@ static int getrs_entry(oxi_handle_s *h, char trans, i64 n, i64 nrhs, const T *dL
         for (i64 j = 0; j < n; ++j)
             if (ip[j] < 1 || ip[j] > n) return OXI_EINVAL;
         perm_from_ipiv(ip.data(), n, n, perm.data());
-        char *sc = (char *)h->scratch.get(4096);
-        int *d_err = (int *)(sc + 1024);
+        char *sc = (char *)h->scratch.get(kScratchBytes);
+        int *d_err = (int *)(sc + kScratchErrOff);
         int64_t *dperm = (int64_t *)h->perm_ws.get(sizeof(int64_t) * n);
         int64_t *hperm = (int64_t *)h->host_ws.get(sizeof(int64_t) * (n + 8));
         std::copy(perm.begin(), perm.end(), hperm);

@@ -49,9 +49,12 @@ def colmajor_copy(A, dtype=None) -> torch.Tensor:
     t = _as_tensor(A)
     if t.ndim != 2:
         raise DimensionMismatch("matrix expected")
+    dev = _device()
+    if t.device != dev:  # move first (a host transpose would be a slow CPU pass)
+        t = t.to(dev, non_blocking=t.is_pinned())
     if dtype is not None:
         t = t.to(dtype)
-    out = torch.empty((t.shape[1], t.shape[0]), dtype=t.dtype, device=_device())
+    out = torch.empty((t.shape[1], t.shape[0]), dtype=t.dtype, device=dev)
     out.copy_(t.t())
     return out
 
