@@ -350,6 +350,15 @@ def ours(args, ws, rank, local):
                              "peak": peaks.get("bf16_tflops"), "unit": "TFLOP/s",
                              "frac": round(tf / peaks.get("bf16_tflops"), 4)})
     shares = {k: round(v[1] / total_ms, 4) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])}
+    # kernel-class breakdown of one plain FP64 step (diagnostic)
+    h.profile(True)
+    plain_step()
+    pprof = h.profile_read()
+    h.profile(False)
+    ptot = sum(v[1] for v in pprof.values()) or 1.0
+    plain_shares = {k: [round(v[1], 3), v[0]] for k, v in sorted(pprof.items(), key=lambda kv: -kv[1][1])}
+    dmma = pprof.get("gemm_dmma")
+    plain_gemm_tflops = round(dmma[2] / (dmma[1] / 1e3) / 1e12, 2) if dmma else None
 
     # ---- e2e through the public API (host buffers, copies inside the region) ----
     A_host = Acm.t().cpu().pin_memory()  # the user's row-indexed matrix on the host
@@ -407,6 +416,7 @@ def ours(args, ws, rank, local):
                        "factor_ms": round(rep.factor_ms, 3), "refine_ms": round(rep.refine_ms, 3)},
         "ms_per_step_each": [round(x, 3) for x in per_mixed],
         "roofline": roofline, "kernel_time_shares": shares,
+        "plain_fp64_kernel_ms": plain_shares, "plain_fp64_trailing_gemm_tflops": plain_gemm_tflops,
         "cpu_baseline": cpu,
         "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": n * n * 8 + n * 8,
                 "d2h_bytes_per_step": n * 8},

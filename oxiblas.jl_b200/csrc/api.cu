@@ -34,6 +34,8 @@ int oxi_destroy(oxi_handle_t h) {
     h->mixed_ws.release();
     h->perm_ws.release();
     h->tc_ws.release();
+    h->xtag_ws.release();
+    h->rowmap_ws.release();
     h->host_ws.release();
     delete h;
     return OXI_OK;

@@ -67,6 +67,9 @@ struct LuRun {
     i64 ld, m, n, ncols_moved;  // ncols_moved: columns the row moves reach (n, +1 id column)
     int64_t *ipiv, *info;
     int *moves, *nmoves;
+    // panel-level composition (null: each leaf moves every column itself)
+    int *map = nullptr, *list = nullptr, *listcnt = nullptr;
+    i64 pf = 0, pl = 0;  // current panel columns [pf, pl)
 };
 
 // Recursive panel on columns [c0, c0+nc), rows [c0, m).
@@ -81,8 +84,13 @@ static void panel_rec(LuRun<T> &R, i64 c0, i64 nc) {
         OXI_CUDA(cudaMemsetAsync(R.nmoves, 0, sizeof(int), h->stream));
         launch_leaf<T>(R.W + c0 * R.ld + c0, R.ld, mrows, (int)nc, c0, R.ipiv, R.info, R.moves,
                        R.nmoves, leafw, h->stream);
-        launch_rowmoves<T>(R.W, R.ld, c0, R.moves, R.nmoves, 0, R.ncols_moved, c0, c0 + nc,
-                           h->stream);
+        if (R.map) {  // inside the panel now, outside it once per panel
+            launch_rowmoves<T>(R.W, R.ld, c0, R.moves, R.nmoves, R.pf, R.pl, c0, c0 + nc, h->stream);
+            launch_rowmap_apply(R.map, c0 - R.pf, R.moves, R.nmoves, h->stream);
+        } else {
+            launch_rowmoves<T>(R.W, R.ld, c0, R.moves, R.nmoves, 0, R.ncols_moved, c0, c0 + nc,
+                               h->stream);
+        }
         return;
     }
     const i64 hh = split_point(h, nc);
@@ -102,9 +110,28 @@ void getrf_rowmajor(oxi_handle_s *h, T *W, i64 ld, i64 m, i64 n, int64_t *d_ipiv
     LuRun<T> R{h, W, ld, m, n, n, d_ipiv, d_info, d_moves, d_nmoves};
     const i64 q = std::min(m, n);
     const i64 nb = std::max<i64>(h->opt.blocksize, 1);
+    const bool compose = nb > 32 && n > nb;  // worth it when a panel holds several leaves
+    if (compose) {
+        char *ws = (char *)h->rowmap_ws.get(sizeof(int) * (size_t)(m + 4 * nb + 64));
+        R.map = (int *)ws;
+        R.list = R.map + m;
+        R.listcnt = R.list + 4 * nb;
+    }
     for (i64 f = 0; f < q; f += nb) {
         const i64 l = std::min(q, f + nb);
-        panel_rec(R, f, l - f);
+        if (compose) {
+            R.pf = f;
+            R.pl = l;
+            launch_rowmap_init(R.map, m - f, h->stream);
+            panel_rec(R, f, l - f);
+            OXI_CUDA(cudaMemsetAsync(R.listcnt, 0, sizeof(int), h->stream));
+            launch_rowmap_extract(R.map, m - f, R.list, R.listcnt, h->stream);
+            const int maxcnt = (int)std::min<i64>(2 * (l - f), m - f);
+            launch_rowmoves_big<T>(W, ld, f, R.list, R.listcnt, maxcnt, 0, f, h->stream);
+            launch_rowmoves_big<T>(W, ld, f, R.list, R.listcnt, maxcnt, l, R.ncols_moved, h->stream);
+        } else {
+            panel_rec(R, f, l - f);
+        }
         if (l >= n) continue;
         T *L11 = W + f * ld + f;
         trsm_lower_unit<T>(h, L11, ld, L11 + (l - f), ld, l - f, n - l);

@@ -7,7 +7,9 @@
 // a panel row (w elements) is one contiguous load.  The C ABI converts from and
 // to the caller's column-major layout at entry and exit.
 #include <cooperative_groups.h>
+#include <algorithm>
 #include <climits>
+#include <type_traits>
 #include "oxi_internal.h"
 
 namespace cg = cooperative_groups;
@@ -92,7 +94,51 @@ template void launch_rm_to_cm<float, double>(const float *, i64, double *, i64, 
 // row it started as; at the end a position whose row changed emits a (dst, src)
 // move, the net permutation applied to the other columns by k_rowmoves.
 // ---------------------------------------------------------------------------
-constexpr int LEAF_NT = 256;
+// ---------------------------------------------------------------------------
+// Warp arg-max for the pivot search with redux.sync: |v| >= 0 orders like its
+// bit pattern, so the warp maximum is an integer max (FP64: high word, then
+// low word), and the first row among equal maxima is an integer min of the
+// positions -- the reference's "largest |a|, first row on ties".  NaN maps to
+// the smallest key, as a NaN never wins the reference's strict '>' comparison.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t redux_max_u32(uint32_t v) {
+    uint32_t r;
+    asm volatile("redux.sync.max.u32 %0, %1, 0xffffffff;" : "=r"(r) : "r"(v));
+    return r;
+}
+__device__ __forceinline__ uint32_t redux_min_u32(uint32_t v) {
+    uint32_t r;
+    asm volatile("redux.sync.min.u32 %0, %1, 0xffffffff;" : "=r"(r) : "r"(v));
+    return r;
+}
+__device__ __forceinline__ uint64_t pivot_key(float a) {
+    return (a == a) ? (uint64_t)__float_as_uint(fabsf(a)) : 0ull;
+}
+__device__ __forceinline__ uint64_t pivot_key(double a) {
+    return (a == a) ? (uint64_t)__double_as_longlong(fabs(a)) : 0ull;
+}
+// (key, pos) of the warp winner, identical in every lane; pos = INT_MAX when no lane has one.
+template <typename T>
+__device__ __forceinline__ void warp_argmax(uint64_t &key, int &pos) {
+    const uint32_t p = (uint32_t)pos;
+    if constexpr (sizeof(T) == 4) {
+        const uint32_t k = (uint32_t)key;
+        const uint32_t mk = redux_max_u32(p == (uint32_t)INT_MAX ? 0u : k);
+        const uint32_t mp = redux_min_u32(k == mk ? p : (uint32_t)INT_MAX);
+        key = mk;
+        pos = (int)mp;
+    } else {
+        const uint32_t hi = (uint32_t)(key >> 32), lo = (uint32_t)key;
+        const bool valid = p != (uint32_t)INT_MAX;
+        const uint32_t mh = redux_max_u32(valid ? hi : 0u);
+        const uint32_t ml = redux_max_u32(valid && hi == mh ? lo : 0u);
+        const uint32_t mp = redux_min_u32(hi == mh && lo == ml ? p : (uint32_t)INT_MAX);
+        key = ((uint64_t)mh << 32) | ml;
+        pos = (int)mp;
+    }
+}
+
+constexpr int LEAF_NT = 512;
 constexpr int LEAF_MAX_CS = 16;
 
 template <typename T, int W, int R>
@@ -104,24 +150,33 @@ k_leaf_lu(T *__restrict__ P, i64 ld, int m, int wact, i64 gofs, int64_t *__restr
     const int cr = (int)cl.block_rank();
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     constexpr int NW = LEAF_NT / 32;
-    const int G = CS * LEAF_NT;
+    constexpr int VEC = 16 / sizeof(T);  // elements per 16-byte vector
+    const int G = CS * LEAF_NT;  // a power of two: positions split by shift and mask
+    const int lgG = __ffs(G) - 1;
     const int g = cr * LEAF_NT + t;
+    constexpr int LG_NT = (LEAF_NT == 512) ? 9 : (LEAF_NT == 256 ? 8 : 10);
+    static_assert((1 << LG_NT) == LEAF_NT, "LEAF_NT must be a power of two");
 
-    __shared__ T s_cval[2][LEAF_MAX_CS];
+    __shared__ uint64_t s_ckey[2][LEAF_MAX_CS];
     __shared__ int s_cpos[2][LEAF_MAX_CS];
     __shared__ int s_cid[2][LEAF_MAX_CS];
-    __shared__ T s_crow[2][LEAF_MAX_CS][W];
-    __shared__ T s_jslot[2][W];
+    __shared__ __align__(16) T s_crow[2][LEAF_MAX_CS][W];
+    __shared__ __align__(16) T s_jslot[2][W];
     __shared__ int s_jslot_id[2];
-    __shared__ T s_wval[NW];
+    __shared__ uint64_t s_wkey[NW];
     __shared__ int s_wpos[NW];
-    __shared__ T s_myrow[W];
+    __shared__ __align__(16) T s_myrow[W];
     __shared__ int s_myid;
-    __shared__ T s_jrow[W];
+    __shared__ __align__(16) T s_jrow[W];
     __shared__ int s_jid;
+    __shared__ int s_piv[W];   // pivots and info stay on chip until the end: no global
+    __shared__ int s_info;     // store ahead of the per-column cluster barrier
+    if (t == 0) s_info = 0;
 
+    // ---- load: rows of W elements, 16-byte vectors when the row is whole and aligned ----
     T r[R][W];
     int id[R];
+    const bool vec_ok = (wact == W) && ((ld * (i64)sizeof(T)) % 16 == 0) && (((uintptr_t)P) % 16 == 0);
 #pragma unroll
     for (int k = 0; k < R; ++k) {
         const int i = k * G + g;
@@ -130,48 +185,51 @@ k_leaf_lu(T *__restrict__ P, i64 ld, int m, int wact, i64 gofs, int64_t *__restr
         for (int c = 0; c < W; ++c) r[k][c] = T(0);
         if (i < m) {
             const T *src = P + (i64)i * ld;
+            if (vec_ok) {
 #pragma unroll
-            for (int c = 0; c < W; ++c)
-                if (c < wact) r[k][c] = src[c];
+                for (int c = 0; c < W; c += VEC) {
+                    const int4 v = *(const int4 *)(src + c);
+                    const T *vv = (const T *)&v;
+#pragma unroll
+                    for (int u = 0; u < VEC; ++u) r[k][c + u] = vv[u];
+                }
+            } else {
+#pragma unroll
+                for (int c = 0; c < W; ++c)
+                    if (c < wact) r[k][c] = src[c];
+            }
         }
     }
     const int q = m < wact ? m : wact;
 
-#pragma unroll
-    for (int j = 0; j < W; ++j) {
-        if (j >= q) break;
+    // The column loop is kept rolled (one copy of the code, resident in the
+    // instruction cache).  Each row's registers ROTATE by one slot per column:
+    // at step j the active column sits in slot 0, the unfinished columns
+    // j+1..W-1 in slots 1..W-1-j and the finished ones behind them, so every
+    // register index is static and the update is W-1 independent predicated
+    // FMAs.  After W steps the rotation has returned the row to its order.
+#pragma unroll 1
+    for (int j = 0; j < q; ++j) {
         const int par = j & 1;
-        // (a) this thread's best candidate in column j
-        T bv = T(-1);
+        // (a) this thread's best candidate in column j (slot 0)
+        uint64_t bk = 0;
         int bp = INT_MAX;
 #pragma unroll
         for (int k = 0; k < R; ++k) {
             const int i = k * G + g;
-            if (i >= j && i < m) {
-                const T v = fabs(r[k][j]);
-                if (v > bv) { bv = v; bp = i; }   // slots ascend in i: strict '>' keeps the first
-            }
+            const uint64_t key = pivot_key(r[k][0]);
+            if (i >= j && i < m && (bp == INT_MAX || key > bk)) { bk = key; bp = i; }  // slots ascend in i
         }
-        // (b) warp reduction; ties go to the smaller position
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-            const T ov = __shfl_xor_sync(0xffffffffu, bv, off);
-            const int op = __shfl_xor_sync(0xffffffffu, bp, off);
-            if (ov > bv || (ov == bv && op < bp)) { bv = ov; bp = op; }
-        }
-        if (lane == 0) { s_wval[warp] = bv; s_wpos[warp] = bp; }
+        // (b) warp winner
+        warp_argmax<T>(bk, bp);
+        if (lane == 0) { s_wkey[warp] = bk; s_wpos[warp] = bp; }
         __syncthreads();
-        // (c) CTA candidate (computed redundantly by every thread)
-        T cv = s_wval[0];
-        int cp = s_wpos[0];
-#pragma unroll
-        for (int w = 1; w < NW; ++w) {
-            const T ov = s_wval[w];
-            const int op = s_wpos[w];
-            if (ov > cv || (ov == cv && op < cp)) { cv = ov; cp = op; }
-        }
-        if (cp != INT_MAX && (cp % G) == g) {
-            const int kk = cp / G;
+        // (c) CTA winner: every warp reduces the NW warp results
+        uint64_t ck = lane < NW ? s_wkey[lane] : 0ull;
+        int cp = lane < NW ? s_wpos[lane] : INT_MAX;
+        warp_argmax<T>(ck, cp);
+        if (cp != INT_MAX && (cp & (G - 1)) == g) {
+            const int kk = cp >> lgG;
 #pragma unroll
             for (int k = 0; k < R; ++k)
                 if (k == kk) {
@@ -180,8 +238,7 @@ k_leaf_lu(T *__restrict__ P, i64 ld, int m, int wact, i64 gofs, int64_t *__restr
                     s_myid = id[k];
                 }
         }
-        // position j is always slot 0 of thread j of CTA 0 (j < W <= 32 <= G)
-        const bool own_j = (g == j);
+        const bool own_j = (g == j);  // position j: slot 0 of thread j of CTA 0
         if (own_j) {
 #pragma unroll
             for (int c = 0; c < W; ++c) s_jrow[c] = r[0][c];
@@ -192,74 +249,121 @@ k_leaf_lu(T *__restrict__ P, i64 ld, int m, int wact, i64 gofs, int64_t *__restr
         if (warp == 0) {
             for (int e = lane; e < CS * W; e += 32) {
                 const int dst = e / W, c = e - dst * W;
-                T *rem = cl.map_shared_rank(&s_crow[par][cr][0], dst);
-                rem[c] = s_myrow[c];
+                if (dst == cr) s_crow[par][cr][c] = s_myrow[c];
+                else *cl.map_shared_rank(&s_crow[par][cr][c], dst) = s_myrow[c];
             }
             if (lane < CS) {
-                *cl.map_shared_rank(&s_cval[par][cr], lane) = cv;
-                *cl.map_shared_rank(&s_cpos[par][cr], lane) = cp;
-                *cl.map_shared_rank(&s_cid[par][cr], lane) = s_myid;
+                if (lane == cr) {
+                    s_ckey[par][cr] = ck;
+                    s_cpos[par][cr] = cp;
+                    s_cid[par][cr] = s_myid;
+                } else {
+                    *cl.map_shared_rank(&s_ckey[par][cr], lane) = ck;
+                    *cl.map_shared_rank(&s_cpos[par][cr], lane) = cp;
+                    *cl.map_shared_rank(&s_cid[par][cr], lane) = s_myid;
+                }
             }
-        }
-        if (cr == 0 && warp == 1) {
+        } else if (warp == 1 && cr == 0) {
             for (int e = lane; e < CS * W; e += 32) {
                 const int dst = e / W, c = e - dst * W;
-                T *rem = cl.map_shared_rank(&s_jslot[par][0], dst);
-                rem[c] = s_jrow[c];
+                if (dst == 0) s_jslot[par][c] = s_jrow[c];
+                else *cl.map_shared_rank(&s_jslot[par][c], dst) = s_jrow[c];
             }
-            if (lane < CS) *cl.map_shared_rank(&s_jslot_id[par], lane) = s_jid;
+            if (lane < CS) {
+                if (lane == 0) s_jslot_id[par] = s_jid;
+                else *cl.map_shared_rank(&s_jslot_id[par], lane) = s_jid;
+            }
         }
-        cl.sync();
-        // (e) winner, identical in every CTA
-        T wv = s_cval[par][0];
-        int wp = s_cpos[par][0], wq = 0;
-        for (int qq = 1; qq < CS; ++qq) {
-            const T ov = s_cval[par][qq];
-            const int op = s_cpos[par][qq];
-            if (ov > wv || (ov == wv && op < wp)) { wv = ov; wp = op; wq = qq; }
-        }
+        if (CS == 1) __syncthreads();
+        else cl.sync();
+        // (e) winner, identical in every CTA: lanes 0..CS-1 hold one candidate each;
+        // the winning row sits in the slot of the CTA that owns its position
+        uint64_t wk = lane < CS ? s_ckey[par][lane] : 0ull;
+        int wp = lane < CS ? s_cpos[par][lane] : INT_MAX;
+        warp_argmax<T>(wk, wp);
+        const int wq = (wp == INT_MAX) ? 0 : ((wp & (G - 1)) >> LG_NT);
         const T *prow = (wp == INT_MAX) ? &s_jslot[par][0] : &s_crow[par][wq][0];
         const int pid = (wp == INT_MAX) ? s_jslot_id[par] : s_cid[par][wq];
         if (wp == INT_MAX) wp = j;  // no comparable candidate (all NaN): keep row j
-        if (g == 0) ipiv[gofs + j] = gofs + wp + 1;
-        const T d = prow[j];
+        if (t == 0) s_piv[j] = wp;
+        const T d = prow[0];
         if (d == T(0)) {
-            if (g == 0 && *info == 0) *info = gofs + j + 1;
-            continue;
-        }
-        T u[W];
+            // zero pivot: info, no interchange, no elimination (the column is all zero)
+            if (t == 0 && s_info == 0) s_info = j + 1;
+        } else {
+            // the pivot row in registers when they can spare it, else read from shared memory
+            const int live = W - j;  // slots 1..live-1 hold the unfinished columns
+            constexpr bool U_REGS = (W * (R + 1) * (int)sizeof(T) / 4) <= 64;
+            T u[U_REGS ? W : 1];
+            if constexpr (U_REGS) {
 #pragma unroll
-        for (int c = 0; c < W; ++c) u[c] = prow[c];
-        // (f) the swap lands in the two owner threads' registers
-        if (wp != j) {
-            if (own_j) {
+                for (int c = 0; c < W; c += VEC) {
+                    const int4 v = *(const int4 *)(prow + c);
+                    const T *vv = (const T *)&v;
 #pragma unroll
-                for (int c = 0; c < W; ++c) r[0][c] = u[c];
-                id[0] = pid;
+                    for (int e = 0; e < VEC; ++e) u[c + e] = vv[e];
+                }
             }
-            if ((wp % G) == g) {
-                const int kk = wp / G;
+            auto U = [&](int c) -> T {
+                if constexpr (U_REGS) return u[c];
+                else return prow[c];
+            };
+            // the update multiplies by Uz: the pivot row with its finished slots zeroed
+            T uz[U_REGS ? W : 1];
+            if constexpr (U_REGS) {
 #pragma unroll
-                for (int k = 0; k < R; ++k)
-                    if (k == kk) {
+                for (int c = 0; c < W; ++c) uz[c] = (c < live) ? u[c] : T(0);
+            }
+            auto UZ = [&](int c) -> T {
+                if constexpr (U_REGS) return uz[c];
+                else return (c < live) ? prow[c] : T(0);
+            };
+            // (f) the interchange lands in the two owner threads' registers
+            if (wp != j) {
+                if (own_j) {
 #pragma unroll
-                        for (int c = 0; c < W; ++c) r[k][c] = s_jslot[par][c];
-                        id[k] = s_jslot_id[par];
-                    }
+                    for (int c = 0; c < W; ++c) r[0][c] = U(c);
+                    id[0] = pid;
+                }
+                if ((wp & (G - 1)) == g) {
+                    const int kk = wp >> lgG;
+#pragma unroll
+                    for (int k = 0; k < R; ++k)
+                        if (k == kk) {
+#pragma unroll
+                            for (int c = 0; c < W; ++c) r[k][c] = s_jslot[par][c];
+                            id[k] = s_jslot_id[par];
+                        }
+                }
+            }
+            // (g) scale the column and apply the rank-1 update below the pivot
+            // (finished slots see a zero multiplier: fma(-l, 0, a) == a)
+#pragma unroll
+            for (int k = 0; k < R; ++k) {
+                const int i = k * G + g;
+                if (i > j && i < m) {
+                    const T l = r[k][0] / d;
+                    r[k][0] = l;
+#pragma unroll
+                    for (int c = 1; c < W; ++c) r[k][c] = fma(-l, UZ(c), r[k][c]);
+                }
             }
         }
-        // (g) scale the column and apply the rank-1 update below the pivot
+        // (h) rotate: the finished column moves behind the unfinished ones
 #pragma unroll
         for (int k = 0; k < R; ++k) {
-            const int i = k * G + g;
-            if (i > j && i < m) {
-                const T l = r[k][j] / d;
-                r[k][j] = l;
+            const T t0 = r[k][0];
 #pragma unroll
-                for (int c = j + 1; c < W; ++c) r[k][c] = fma(-l, u[c], r[k][c]);
-            }
+            for (int c = 0; c < W - 1; ++c) r[k][c] = r[k][c + 1];
+            r[k][W - 1] = t0;
         }
     }
+    // pivots and info, written once
+    __syncthreads();
+    if (cr == 0 && t < q) ipiv[gofs + t] = gofs + s_piv[t] + 1;
+    if (cr == 0 && t == 0 && s_info != 0 && *info == 0) *info = gofs + s_info;
+    // undo the rotation left by q < W steps (slot s holds column (s + q) mod W)
+    const int rot = q % W;
 
     // store the leaf and emit the moves of the net permutation
 #pragma unroll
@@ -267,9 +371,23 @@ k_leaf_lu(T *__restrict__ P, i64 ld, int m, int wact, i64 gofs, int64_t *__restr
         const int i = k * G + g;
         if (i < m) {
             T *dst = P + (i64)i * ld;
+            if (vec_ok && rot == 0) {
 #pragma unroll
-            for (int c = 0; c < W; ++c)
-                if (c < wact) dst[c] = r[k][c];
+                for (int c = 0; c < W; c += VEC) {
+                    int4 v;
+                    T *vv = (T *)&v;
+#pragma unroll
+                    for (int u = 0; u < VEC; ++u) vv[u] = r[k][c + u];
+                    *(int4 *)(dst + c) = v;
+                }
+            } else {
+#pragma unroll
+                for (int s = 0; s < W; ++s) {
+                    int c = s + rot;
+                    if (c >= W) c -= W;
+                    if (c < wact) dst[c] = r[k][s];
+                }
+            }
             if (id[k] != i) {
                 const int slot = atomicAdd(nmoves, 1);
                 moves[2 * slot] = i;
@@ -278,23 +396,23 @@ k_leaf_lu(T *__restrict__ P, i64 ld, int m, int wact, i64 gofs, int64_t *__restr
         }
     }
     // keep every CTA's shared memory alive until all remote pushes have landed
-    cl.sync();
+    if (CS > 1) cl.sync();
 }
 
 template <typename T> int leaf_width_for(i64 m);
 template <> int leaf_width_for<double>(i64 m) {
-    const i64 cap = (i64)LEAF_MAX_CS * LEAF_NT;
-    if (m <= cap * 2) return 32;
-    if (m <= cap * 4) return 16;
-    if (m <= cap * 8) return 8;
-    if (m <= cap * 16) return 4;
+    const i64 cap = (i64)LEAF_MAX_CS * LEAF_NT;  // rows per slot
+    if (m <= cap * 1) return 32;
+    if (m <= cap * 2) return 16;
+    if (m <= cap * 4) return 8;
+    if (m <= cap * 8) return 4;
     return 0;
 }
 template <> int leaf_width_for<float>(i64 m) {
     const i64 cap = (i64)LEAF_MAX_CS * LEAF_NT;
-    if (m <= cap * 4) return 32;
-    if (m <= cap * 8) return 16;
-    if (m <= cap * 16) return 8;
+    if (m <= cap * 2) return 32;
+    if (m <= cap * 4) return 16;
+    if (m <= cap * 8) return 8;
     return 0;
 }
 
@@ -329,25 +447,18 @@ void launch_leaf(T *P, i64 ld, i64 m, int w, i64 gofs, int64_t *ipiv, int64_t *i
                  int *nmoves, int leafw, cudaStream_t s) {
     const i64 cap = (i64)LEAF_MAX_CS * LEAF_NT;
     if constexpr (sizeof(T) == 8) {
+        if (leafw == 32) launch_leaf_wr<T, 32, 1>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s);
+        else if (leafw == 16) launch_leaf_wr<T, 16, 2>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s);
+        else if (leafw == 8) launch_leaf_wr<T, 8, 4>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s);
+        else launch_leaf_wr<T, 4, 8>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s);
+    } else {
         if (leafw == 32) {
             if (m <= cap) launch_leaf_wr<T, 32, 1>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s);
             else launch_leaf_wr<T, 32, 2>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s);
         } else if (leafw == 16) {
             launch_leaf_wr<T, 16, 4>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s);
-        } else if (leafw == 8) {
+        } else {
             launch_leaf_wr<T, 8, 8>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s);
-        } else {
-            launch_leaf_wr<T, 4, 16>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s);
-        }
-    } else {
-        if (leafw == 32) {
-            if (m <= cap) launch_leaf_wr<T, 32, 1>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s);
-            else if (m <= 2 * cap) launch_leaf_wr<T, 32, 2>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s);
-            else launch_leaf_wr<T, 32, 4>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s);
-        } else if (leafw == 16) {
-            launch_leaf_wr<T, 16, 8>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s);
-        } else {
-            launch_leaf_wr<T, 8, 16>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s);
         }
     }
 }
@@ -361,6 +472,7 @@ template void launch_leaf<float>(float *, i64, i64, int, i64, int64_t *, int64_t
 // touches 32 contiguous elements of each row (coalesced).
 // ---------------------------------------------------------------------------
 constexpr int MAX_MOVES = 64;
+constexpr int MAX_MOVES_LEAF = 64;  // a leaf of <= 32 columns moves at most 64 rows
 
 template <typename T>
 __global__ void k_rowmoves(T *__restrict__ W, i64 ld, i64 r0, const int *__restrict__ moves,
@@ -392,6 +504,123 @@ void launch_rowmoves(T *W, i64 ld, i64 r0, const int *moves, const int *nmoves, 
 }
 template void launch_rowmoves<double>(double *, i64, i64, const int *, const int *, i64, i64, i64, i64, cudaStream_t);
 template void launch_rowmoves<float>(float *, i64, i64, const int *, const int *, i64, i64, i64, i64, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Panel-level composition of the leaves' row permutations.  map[p] = the row
+// (relative to the panel's first row) whose data sits at position p; each
+// leaf's moves compose into it, and at the end of the panel the positions with
+// map[p] != p form one move list for all the columns outside the panel.
+// ---------------------------------------------------------------------------
+__global__ void k_rowmap_init(int *__restrict__ map, int len) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < len) map[p] = p;
+}
+__global__ void k_rowmap_apply(int *__restrict__ map, int offset, const int *__restrict__ moves,
+                               const int *__restrict__ nmoves) {
+    const int e = threadIdx.x;
+    const int cnt = min(*nmoves, MAX_MOVES_LEAF);
+    int v = 0;
+    if (e < cnt) v = map[offset + moves[2 * e + 1]];
+    __syncthreads();
+    if (e < cnt) map[offset + moves[2 * e]] = v;
+}
+__global__ void k_rowmap_extract(const int *__restrict__ map, int len, int *__restrict__ list,
+                                 int *__restrict__ cnt) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= len) return;
+    const int src = map[p];
+    if (src != p) {
+        const int slot = atomicAdd(cnt, 1);
+        list[2 * slot] = p;
+        list[2 * slot + 1] = src;
+    }
+}
+
+// All sources of a CTA's column slab are staged in shared memory before any
+// destination is written, so cycles of the permutation are safe.  Each thread
+// owns one 16-byte vector column of the slab and walks the move list with a
+// stride, 8 independent loads in flight.
+template <typename T, bool VEC>
+__global__ void __launch_bounds__(256) k_rowmoves_big(T *__restrict__ W, i64 ld, i64 r0,
+                                                      const int *__restrict__ list,
+                                                      const int *__restrict__ cnt_ptr, int maxcnt,
+                                                      i64 c_lo, i64 c_hi, int cpc) {
+    extern __shared__ __align__(16) unsigned char rm_smem[];
+    constexpr int V = VEC ? 16 / (int)sizeof(T) : 1;
+    using VT = typename std::conditional<VEC, int4, T>::type;
+    VT *buf = reinterpret_cast<VT *>(rm_smem);
+    const int cnt = min(*cnt_ptr, maxcnt);
+    const i64 cbase = c_lo + (i64)blockIdx.x * cpc;
+    const int cols = (int)((c_hi - cbase) < (i64)cpc ? (c_hi - cbase) : (i64)cpc);
+    if (cols <= 0 || cnt == 0) return;
+    const int nv = cpc / V;                 // vector columns per slab
+    const int v = threadIdx.x % nv, g = threadIdx.x / nv, G = blockDim.x / nv;
+    const bool full = (v + 1) * V <= cols;  // this thread's vector lies inside the slab
+    const bool part = !full && v * V < cols;
+    T *base = W + r0 * ld + cbase + (i64)v * V;
+#pragma unroll 8
+    for (int e = g; e < cnt; e += G) {
+        const T *src = base + (i64)list[2 * e + 1] * ld;
+        if (full) {
+            buf[(i64)e * nv + v] = *reinterpret_cast<const VT *>(src);
+        } else if (part) {
+            T tmp[V];
+            for (int u = 0; u < V; ++u) tmp[u] = (v * V + u < cols) ? src[u] : T(0);
+            buf[(i64)e * nv + v] = *reinterpret_cast<VT *>(tmp);
+        }
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int e = g; e < cnt; e += G) {
+        T *dst = base + (i64)list[2 * e] * ld;
+        if (full) {
+            *reinterpret_cast<VT *>(dst) = buf[(i64)e * nv + v];
+        } else if (part) {
+            const VT val = buf[(i64)e * nv + v];
+            const T *tv = reinterpret_cast<const T *>(&val);
+            for (int u = 0; u < V; ++u)
+                if (v * V + u < cols) dst[u] = tv[u];
+        }
+    }
+}
+
+void launch_rowmap_init(int *map, i64 len, cudaStream_t s) {
+    if (len <= 0) return;
+    k_rowmap_init<<<(unsigned)((len + 255) / 256), 256, 0, s>>>(map, (int)len);
+    OXI_LAUNCH_CHECK();
+}
+void launch_rowmap_apply(int *map, i64 offset, const int *moves, const int *nmoves, cudaStream_t s) {
+    k_rowmap_apply<<<1, MAX_MOVES_LEAF, 0, s>>>(map, (int)offset, moves, nmoves);
+    OXI_LAUNCH_CHECK();
+}
+void launch_rowmap_extract(const int *map, i64 len, int *list, int *cnt, cudaStream_t s) {
+    if (len <= 0) return;
+    k_rowmap_extract<<<(unsigned)((len + 255) / 256), 256, 0, s>>>(map, (int)len, list, cnt);
+    OXI_LAUNCH_CHECK();
+}
+template <typename T>
+void launch_rowmoves_big(T *W, i64 ld, i64 r0, const int *list, const int *cnt, int maxcnt, i64 c_lo,
+                         i64 c_hi, cudaStream_t s) {
+    if (c_hi <= c_lo || maxcnt <= 0) return;
+    const int V = 16 / (int)sizeof(T);
+    const bool vec = ((uintptr_t)W % 16 == 0) && ((ld * (i64)sizeof(T)) % 16 == 0) && (c_lo % V == 0);
+    // slab of 64 columns (FP32) / 32 (FP64): 16 or 8 threads per row, 16 or 32 rows at once
+    int cpc = vec ? 16 * V : 64;
+    while (cpc > V && (size_t)maxcnt * cpc * sizeof(T) > 160 * 1024) cpc /= 2;
+    const size_t smem = (size_t)maxcnt * cpc * sizeof(T);
+    ProfScope ps(KC_ROWMOVES, s, 0.0, 2.0 * maxcnt * (double)(c_hi - c_lo) * sizeof(T));
+    const i64 blocks = (c_hi - c_lo + cpc - 1) / cpc;
+    if (vec) {
+        OXI_CUDA(cudaFuncSetAttribute(k_rowmoves_big<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_rowmoves_big<T, true><<<(unsigned)blocks, 256, smem, s>>>(W, ld, r0, list, cnt, maxcnt, c_lo, c_hi, cpc);
+    } else {
+        OXI_CUDA(cudaFuncSetAttribute(k_rowmoves_big<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_rowmoves_big<T, false><<<(unsigned)blocks, 256, smem, s>>>(W, ld, r0, list, cnt, maxcnt, c_lo, c_hi, cpc);
+    }
+    OXI_LAUNCH_CHECK();
+}
+template void launch_rowmoves_big<double>(double *, i64, i64, const int *, const int *, int, i64, i64, cudaStream_t);
+template void launch_rowmoves_big<float>(float *, i64, i64, const int *, const int *, int, i64, i64, cudaStream_t);
 
 // ---------------------------------------------------------------------------
 // TRSM leaf: B (t x N) <- L^-1 B with L unit lower (t <= 32), row-major.  One

@@ -357,6 +357,7 @@ struct MixedRun {
     int64_t *perm, *ipiv;
     void *W;  // float (low) or double (fallback) row-major factors
     i64 ldw;
+    void *dinvL, *dinvU;  // inverses of the 64 x 64 diagonal blocks of L and U
     bool fallback = false;
     double *scal;  // device scalars (cw/rmax/xmax/bmax per rhs, r^2)
     int *err;      // device error word
@@ -427,12 +428,14 @@ static void precond(MixedRun &M, const double *Rin, i64 ldr, double *Z, i64 ldz,
     if (!M.fallback) {
         k_to_low<float><<<gb, 256, 0, s>>>(Rin, ldr, n, nr, M.rows, M.perm, M.mag, M.low32, M.err);
         OXI_LAUNCH_CHECK();
-        lu_solve_rowmajor<float>(M.h, (const float *)M.W, M.ldw, n, M.low32, n, nr, M.err);
+        lu_solve_rowmajor<float>(M.h, (const float *)M.W, M.ldw, n, M.low32, n, nr, M.err,
+                                 (const float *)M.dinvL, (const float *)M.dinvU);
         k_apply_corr<float><<<gb, 256, 0, s>>>(Z, ldz, n, nr, M.low32, M.mag, M.cols, 0);
     } else {
         k_to_low<double><<<gb, 256, 0, s>>>(Rin, ldr, n, nr, M.rows, M.perm, M.mag, M.low64, M.err);
         OXI_LAUNCH_CHECK();
-        lu_solve_rowmajor<double>(M.h, (const double *)M.W, M.ldw, n, M.low64, n, nr, M.err);
+        lu_solve_rowmajor<double>(M.h, (const double *)M.W, M.ldw, n, M.low64, n, nr, M.err,
+                                  (const double *)M.dinvL, (const double *)M.dinvU);
         k_apply_corr<double><<<gb, 256, 0, s>>>(Z, ldz, n, nr, M.low64, M.mag, M.cols, 0);
     }
     OXI_LAUNCH_CHECK();
@@ -568,7 +571,8 @@ static int dgesv_mixed(oxi_handle_s *h, int prec, int refine, i64 n, i64 nrhs, c
                  o_mag = take(8 * 64), o_low32 = take(4 * n * nrhs), o_low64 = take(8 * n * nrhs),
                  o_perm = take(8 * n), o_ipiv = take(8 * n), o_V = take(8 * n * GM_MAXV),
                  o_gw = take(8 * n), o_gt = take(8 * n), o_gpart = take(8 * 120 * GM_MAXV),
-                 o_gh = take(8 * GM_MAXV), o_gz = take(8 * n);
+                 o_gh = take(8 * GM_MAXV), o_gz = take(8 * n),
+                 o_dinv = take(2 * 8 * (size_t)lu_block_inverse_elems(n));
     char *ws = (char *)h->mixed_ws.get(off);
     M.rows = (double *)(ws + o_rows); M.cols = (double *)(ws + o_cols);
     M.pmax = (double *)(ws + o_pmax); M.psum = (double *)(ws + o_psum);
@@ -578,6 +582,7 @@ static int dgesv_mixed(oxi_handle_s *h, int prec, int refine, i64 n, i64 nrhs, c
     M.perm = (int64_t *)(ws + o_perm); M.ipiv = (int64_t *)(ws + o_ipiv);
     M.V = (double *)(ws + o_V); M.gw = (double *)(ws + o_gw); M.gt = (double *)(ws + o_gt);
     M.gpart = (double *)(ws + o_gpart); M.gh = (double *)(ws + o_gh); M.gz = (double *)(ws + o_gz);
+    const i64 inv_elems = lu_block_inverse_elems(n);
     char *sc = (char *)h->scratch.get(kScratchBytes);
     M.err = (int *)(sc + kScratchErrOff);
     int *nonfinite = M.err + 1;
@@ -640,6 +645,15 @@ static int dgesv_mixed(oxi_handle_s *h, int prec, int refine, i64 n, i64 nrhs, c
             k_equilibrated_rm<double><<<g, dim3(32, 8), 0, s>>>(dA, lda, W, ldw, (int)n, M.rows, M.cols);
             OXI_LAUNCH_CHECK();
             getrf_rowmajor<double>(h, W, ldw, n, n, M.ipiv, d_info, d_moves, d_nmoves);
+        }
+        if (!fp64) {
+            M.dinvL = ws + o_dinv;
+            M.dinvU = (float *)M.dinvL + inv_elems;
+            lu_block_inverses_rowmajor<float>(h, (const float *)M.W, ldw, n, (float *)M.dinvL, (float *)M.dinvU);
+        } else {
+            M.dinvL = ws + o_dinv;
+            M.dinvU = (double *)M.dinvL + inv_elems;
+            lu_block_inverses_rowmajor<double>(h, (const double *)M.W, ldw, n, (double *)M.dinvL, (double *)M.dinvU);
         }
         OXI_CUDA(cudaMemcpyAsync(M.hpiv, d_info, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
         OXI_CUDA(cudaMemcpyAsync(M.hpiv + 8, M.ipiv, sizeof(int64_t) * n, cudaMemcpyDeviceToHost, s));

@@ -111,6 +111,8 @@ struct oxi_handle_s {
     oxi::DeviceBuffer perm_ws;   // row permutation of the last solve
     oxi::PinnedBuffer host_ws;   // pinned host staging
     oxi::DeviceBuffer tc_ws;     // 16-bit GEMM operands
+    oxi::DeviceBuffer xtag_ws;   // tagged solution words of the FP32 triangular solves
+    oxi::DeviceBuffer rowmap_ws; // per-panel row map and composite move list
     int trailing = 0;            // oxi::TrailingKind for getrf_rowmajor<float>
     oxi::Profiler prof;
 };
@@ -139,6 +141,14 @@ template <typename T> int leaf_width_for(i64 m);
 template <typename T>
 void launch_rowmoves(T *W, i64 ld, i64 r0, const int *moves, const int *nmoves, i64 c_lo,
                      i64 c_hi, i64 skip_lo, i64 skip_hi, cudaStream_t s);
+
+// Per-panel composition of the leaves' row permutations (see lu_kernels.cu).
+void launch_rowmap_init(int *map, i64 len, cudaStream_t s);
+void launch_rowmap_apply(int *map, i64 offset, const int *moves, const int *nmoves, cudaStream_t s);
+void launch_rowmap_extract(const int *map, i64 len, int *list, int *cnt, cudaStream_t s);
+template <typename T>
+void launch_rowmoves_big(T *W, i64 ld, i64 r0, const int *list, const int *cnt, int maxcnt, i64 c_lo,
+                         i64 c_hi, cudaStream_t s);
 
 // B (t x N, row-major) <- L^-1 B, L unit lower t x t (t <= 32), row-major.
 template <typename T>
@@ -187,6 +197,10 @@ void perm_from_ipiv(const int64_t *ipiv, i64 q, i64 m, int64_t *perm);
 // L then U solves with ROW-major factors (W, ld), X column-major n x nrhs, in place.
 template <typename T>
 void lu_solve_rowmajor(oxi_handle_s *h, const T *W, i64 ld, i64 n, T *X, i64 ldx, i64 nrhs,
-                       int *d_err);
+                       int *d_err, const T *DinvL = nullptr, const T *DinvU = nullptr);
+// Inverses of the 64 x 64 diagonal blocks of L (unit) and U of row-major factors.
+template <typename T>
+void lu_block_inverses_rowmajor(oxi_handle_s *h, const T *W, i64 ld, i64 n, T *DinvL, T *DinvU);
+i64 lu_block_inverse_elems(i64 n);
 
 }  // namespace oxi

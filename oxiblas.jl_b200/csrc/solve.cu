@@ -11,6 +11,7 @@
 // kernel returns), solves its 64 x 64 diagonal block with warp shuffles, and
 // publishes its rows.  The factor is read once, coalesced: threads run along
 // the contiguous dimension of the factor (rows for L/U, columns for L^T/U^T).
+#include <atomic>
 #include <vector>
 #include "oxi_internal.h"
 #include "tma_util.cuh"
@@ -29,150 +30,305 @@ __device__ __forceinline__ void st_release(int *p, int v) {
     asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// M is the effective triangle: M(r, j) = TRANS ? A[j + r*lda] : A[r + j*lda].
-// LOWER (of M) = (UPPER_A == TRANS).
-template <typename T, bool UPPER_A, bool UNIT, bool TRANS, int NR>
+// M is the effective triangle: ROWACC ? M(r, j) = A[r*lda + j] : M(r, j) = A[r + j*lda].
+// A CTA owns a row block (ticket order); its 8 warps take the solved column
+// blocks round-robin, each lane accumulating two rows, so the off-diagonal
+// products of one block run with 8-way memory parallelism and no cross-lane
+// reductions.  The diagonal block is solved by substitution, or -- when Dinv
+// holds the inverses of the diagonal blocks (computed once per factorization)
+// -- by a 64 x 64 matrix-vector product, which shortens the dependency chain.
+constexpr int TRSV_WARPS = SOLVE_NT / 32;
+
+template <typename T, int NR>
+struct TrsvSmem {
+    T x[TRSV_WARPS][SB][NR];     // per-warp staging of solved blocks
+    T acc[TRSV_WARPS][SB][NR];   // per-warp partial sums
+    T y[SB][NR];                 // right-hand side of the diagonal block
+    T x0[SB][NR];                // the critical block's solution
+    T part[SOLVE_NT / SB][SB][NR];
+    T tile[SB][SB + 1];          // the critical off-diagonal tile, prefetched
+    T diag[SB][SB + 1];          // diagonal block (substitution) or its inverse
+};
+
+__device__ __forceinline__ unsigned long long ld_volatile_u64(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.volatile.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Wait for the tagged word of the current epoch and return its float value.
+__device__ __forceinline__ float tagged_get(const unsigned long long *p, uint32_t epoch, int *err) {
+    unsigned long long w = ld_volatile_u64(p);
+    if ((uint32_t)(w >> 32) != epoch) {
+        const uint64_t t0 = global_ns();
+        uint32_t it = 0;
+        while ((uint32_t)((w = ld_volatile_u64(p)) >> 32) != epoch) {
+            if ((++it & 255) == 0 && global_ns() - t0 > kWaitLimitNs) {
+                atomicExch(err, 3);
+                break;
+            }
+        }
+    }
+    return __uint_as_float((uint32_t)w);
+}
+
+// TAGGED (FP32 only): solved values are also published as 64-bit words
+// (value bits | epoch << 32) in xtag; a consumer spins on the words themselves,
+// so no flag, no fence and no second round trip sit on the dependency chain.
+template <typename T, bool LOWER, bool UNIT, bool ROWACC, int NR, bool INV, bool TAGGED = false>
 __global__ void __launch_bounds__(SOLVE_NT)
-k_trsv(const T *__restrict__ A, i64 lda, T *__restrict__ X, i64 ldx, int n, int *__restrict__ ticket,
-       int *__restrict__ flags, int *__restrict__ err) {
-    constexpr bool LOWER = (UPPER_A == TRANS);
+k_trsv2(const T *__restrict__ A, i64 lda, const T *__restrict__ Dinv, T *__restrict__ X, i64 ldx, int n,
+        int *__restrict__ ticket, int *__restrict__ flags, int *__restrict__ err,
+        unsigned long long *__restrict__ xtag = nullptr, uint32_t epoch = 0) {
+    static_assert(!TAGGED || sizeof(T) == 4, "tagged exchange packs FP32 values");
+    extern __shared__ __align__(16) unsigned char trsv_smem[];
+    TrsvSmem<T, NR> &S = *reinterpret_cast<TrsvSmem<T, NR> *>(trsv_smem);
     __shared__ int s_blk;
-    __shared__ T sx[SB][NR];
-    __shared__ T sD[SB][SB + 1];
-    __shared__ T sred[4][SB][NR];
-    __shared__ int s_abort;
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const int nb = (n + SB - 1) / SB;
-    if (t == 0) { s_blk = atomicAdd(ticket, 1); s_abort = 0; }
+    if (t == 0) s_blk = atomicAdd(ticket, 1);
     __syncthreads();
     const int bi = s_blk;
     if (bi >= nb) return;
     const int b = LOWER ? bi : nb - 1 - bi;
     const int r0 = b * SB;
     const int rows = min(SB, n - r0);
-    auto Mv = [&](int r, int j) -> T { return TRANS ? A[(i64)j + (i64)r * lda] : A[(i64)r + (i64)j * lda]; };
+    auto Mv = [&](int r, int j) -> T {
+        return ROWACC ? A[(i64)r * lda + j] : A[(i64)r + (i64)j * lda];
+    };
 
-    // ---- products with the already-solved blocks ----
-    // !TRANS: thread owns row rr = t % 64 and a quarter of each block's columns.
-    // TRANS : lane owns columns (lane, lane+32) of each block, warp owns 8 rows.
-    T acc[TRANS ? 8 : 1][NR];
-#pragma unroll
-    for (int a = 0; a < (TRANS ? 8 : 1); ++a)
-#pragma unroll
-        for (int k = 0; k < NR; ++k) acc[a][k] = T(0);
+    // ---- prefetch (no dependency on other blocks): diagonal block and critical tile ----
+    const bool has_crit = bi > 0;
+    const int cc = LOWER ? b - 1 : b + 1;  // the last block solved before this one
+    const int cc0 = cc * SB, ccols = has_crit ? min(SB, n - cc0) : 0;
+    for (int e = t; e < SB * SB; e += SOLVE_NT) {
+        // threads run along the contiguous index of the stored factor
+        int r, j;
+        if (ROWACC) { r = e / SB; j = e % SB; } else { r = e % SB; j = e / SB; }
+        if (INV) S.diag[r][j] = Dinv[(i64)b * SB * SB + (i64)r * SB + j];
+        else S.diag[r][j] = (r < rows && j < rows) ? Mv(r0 + r, r0 + j) : T(0);
+        if (has_crit) S.tile[r][j] = (r < rows && j < ccols) ? Mv(r0 + r, cc0 + j) : T(0);
+    }
 
-    for (int step = 0; step < bi; ++step) {
+    // ---- products with the other solved blocks (warps round-robin) ----
+    T acc[2][NR];
+#pragma unroll
+    for (int q = 0; q < 2; ++q)
+#pragma unroll
+        for (int k = 0; k < NR; ++k) acc[q][k] = T(0);
+    for (int step = warp; step < bi - 1; step += TRSV_WARPS) {
         const int c = LOWER ? step : nb - 1 - step;
-        if (t == 0 && ld_acquire(&flags[c]) == 0) {
-            const uint64_t t0 = global_ns();
-            uint32_t it = 0;
-            while (ld_acquire(&flags[c]) == 0) {
-                if ((++it & 255) == 0 && global_ns() - t0 > kWaitLimitNs) {
-                    atomicExch(err, 3);
-                    s_abort = 1;
-                    break;
-                }
-            }
-        }
-        __syncthreads();
-        if (s_abort) return;
         const int c0 = c * SB;
         const int cols = min(SB, n - c0);
-        for (int e = t; e < SB * NR; e += SOLVE_NT) {
-            const int jj = e % SB, k = e / SB;
-            sx[jj][k] = (jj < cols) ? __ldcg(&X[(i64)(c0 + jj) + (i64)k * ldx]) : T(0);
-        }
-        __syncthreads();
-        if (!TRANS) {
-            const int rr = t % SB, jg = t / SB;
-            if (rr < rows) {
-#pragma unroll 4
-                for (int q = 0; q < SB / 4; ++q) {
-                    const int jj = jg * (SB / 4) + q;
-                    if (jj < cols) {
-                        const T a = Mv(r0 + rr, c0 + jj);
-#pragma unroll
-                        for (int k = 0; k < NR; ++k) acc[0][k] = fma(a, sx[jj][k], acc[0][k]);
-                    }
-                }
+        if constexpr (TAGGED) {
+            for (int e = lane; e < SB * NR; e += 32) {
+                const int jj = e % SB, k = e / SB;
+                S.x[warp][jj][k] = (jj < cols) ? (T)tagged_get(&xtag[(i64)(c0 + jj) * NR + k], epoch, err) : T(0);
             }
         } else {
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                const int rr = warp + 8 * i;
-                if (rr < rows) {
-#pragma unroll
-                    for (int hh = 0; hh < 2; ++hh) {
-                        const int jj = lane + 32 * hh;
-                        if (jj < cols) {
-                            const T a = Mv(r0 + rr, c0 + jj);
-#pragma unroll
-                            for (int k = 0; k < NR; ++k) acc[i][k] = fma(a, sx[jj][k], acc[i][k]);
-                        }
+            if (lane == 0 && ld_acquire(&flags[c]) == 0) {
+                const uint64_t t0 = global_ns();
+                uint32_t it = 0;
+                while (ld_acquire(&flags[c]) == 0) {
+                    if ((++it & 255) == 0 && global_ns() - t0 > kWaitLimitNs) {
+                        atomicExch(err, 3);
+                        break;
                     }
                 }
             }
+            __syncwarp();
+            for (int e = lane; e < SB * NR; e += 32) {
+                const int jj = e % SB, k = e / SB;
+                S.x[warp][jj][k] = (jj < cols) ? __ldcg(&X[(i64)(c0 + jj) + (i64)k * ldx]) : T(0);
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int r = lane + 32 * q;
+            if (r >= rows) continue;
+            if (ROWACC) {
+                const T *arow = A + (i64)(r0 + r) * lda + c0;
+                if (cols == SB) {
+#pragma unroll 16
+                    for (int jj = 0; jj < SB; jj += 16 / (int)sizeof(T)) {
+                        T av[16 / sizeof(T)];
+                        *(int4 *)av = *(const int4 *)(arow + jj);
+#pragma unroll
+                        for (int u = 0; u < (int)(16 / sizeof(T)); ++u)
+#pragma unroll
+                            for (int k = 0; k < NR; ++k) acc[q][k] = fma(av[u], S.x[warp][jj + u][k], acc[q][k]);
+                    }
+                } else {
+                    for (int jj = 0; jj < cols; ++jj)
+#pragma unroll
+                        for (int k = 0; k < NR; ++k) acc[q][k] = fma(arow[jj], S.x[warp][jj][k], acc[q][k]);
+                }
+            } else {
+                const T *acol = A + (i64)(r0 + r) + (i64)c0 * lda;
+#pragma unroll 16
+                for (int jj = 0; jj < cols; ++jj) {
+                    const T a = acol[(i64)jj * lda];
+#pragma unroll
+                    for (int k = 0; k < NR; ++k) acc[q][k] = fma(a, S.x[warp][jj][k], acc[q][k]);
+                }
+            }
+        }
+        __syncwarp();
+    }
+#pragma unroll
+    for (int q = 0; q < 2; ++q)
+#pragma unroll
+        for (int k = 0; k < NR; ++k) S.acc[warp][lane + 32 * q][k] = acc[q][k];
+    __syncthreads();
+    for (int e = t; e < SB * NR; e += SOLVE_NT) {
+        const int r = e % SB, k = e / SB;
+        T v = T(0);
+#pragma unroll
+        for (int w = 0; w < TRSV_WARPS; ++w) v += S.acc[w][r][k];
+        S.y[r][k] = (r < rows) ? (X[(i64)(r0 + r) + (i64)k * ldx] - v) : T(0);
+    }
+
+    // ---- critical path: the block solved just before, then the diagonal ----
+    constexpr int SEG = SOLVE_NT / SB, SEGW = SB / SEG;
+    const int pr = t % SB, ps = t / SB;
+    if (has_crit) {
+        if constexpr (TAGGED) {
+            for (int e = t; e < SB * NR; e += SOLVE_NT) {
+                const int jj = e % SB, k = e / SB;
+                S.x0[jj][k] = (jj < ccols) ? (T)tagged_get(&xtag[(i64)(cc0 + jj) * NR + k], epoch, err) : T(0);
+            }
+        } else {
+            if (t == 0 && ld_acquire(&flags[cc]) == 0) {
+                const uint64_t t0 = global_ns();
+                uint32_t it = 0;
+                while (ld_acquire(&flags[cc]) == 0) {
+                    if ((++it & 255) == 0 && global_ns() - t0 > kWaitLimitNs) {
+                        atomicExch(err, 3);
+                        break;
+                    }
+                }
+            }
+            __syncthreads();
+            for (int e = t; e < SB * NR; e += SOLVE_NT) {
+                const int jj = e % SB, k = e / SB;
+                S.x0[jj][k] = (jj < ccols) ? __ldcg(&X[(i64)(cc0 + jj) + (i64)k * ldx]) : T(0);
+            }
         }
         __syncthreads();
-    }
-
-    // ---- right-hand side of the diagonal block: y = b - acc ----
-    if (!TRANS) {
-        const int rr = t % SB, jg = t / SB;
+        T pv[NR];
 #pragma unroll
-        for (int k = 0; k < NR; ++k) sred[jg][rr][k] = acc[0][k];
+        for (int k = 0; k < NR; ++k) pv[k] = T(0);
+#pragma unroll
+        for (int jj = 0; jj < SEGW; ++jj) {
+            const T a = S.tile[pr][ps * SEGW + jj];
+#pragma unroll
+            for (int k = 0; k < NR; ++k) pv[k] = fma(a, S.x0[ps * SEGW + jj][k], pv[k]);
+        }
+#pragma unroll
+        for (int k = 0; k < NR; ++k) S.part[ps][pr][k] = pv[k];
+        __syncthreads();
+        for (int e = t; e < SB * NR; e += SOLVE_NT) {
+            const int r = e % SB, k = e / SB;
+            T v = T(0);
+#pragma unroll
+            for (int q = 0; q < SEG; ++q) v += S.part[q][r][k];
+            S.y[r][k] -= v;
+        }
+    }
+    __syncthreads();
+
+    if (INV) {
+        // x_b = Dinv_b y, split over SEG column segments
+        T pv[NR];
+#pragma unroll
+        for (int k = 0; k < NR; ++k) pv[k] = T(0);
+#pragma unroll
+        for (int jj = 0; jj < SEGW; ++jj) {
+            const T a = S.diag[pr][ps * SEGW + jj];
+#pragma unroll
+            for (int k = 0; k < NR; ++k) pv[k] = fma(a, S.y[ps * SEGW + jj][k], pv[k]);
+        }
+#pragma unroll
+        for (int k = 0; k < NR; ++k) S.part[ps][pr][k] = pv[k];
+        __syncthreads();
+        for (int e = t; e < SB * NR; e += SOLVE_NT) {
+            const int r = e % SB, k = e / SB;
+            if (r >= rows) continue;
+            T v = T(0);
+#pragma unroll
+            for (int q = 0; q < SEG; ++q) v += S.part[q][r][k];
+            X[(i64)(r0 + r) + (i64)k * ldx] = v;
+            if constexpr (TAGGED)
+                xtag[(i64)(r0 + r) * NR + k] = ((unsigned long long)epoch << 32) | __float_as_uint((float)v);
+        }
     } else {
+        // substitution on the diagonal block: warp k takes right-hand side k
+        for (int k = warp; k < NR; k += TRSV_WARPS) {
+            T y[2];
 #pragma unroll
-        for (int i = 0; i < 8; ++i)
+            for (int q = 0; q < 2; ++q) y[q] = S.y[lane + 32 * q][k];
+            for (int st = 0; st < rows; ++st) {
+                const int p = LOWER ? st : rows - 1 - st;
+                const int hp = p >> 5, lp = p & 31;
+                const T yp = __shfl_sync(0xffffffffu, hp ? y[1] : y[0], lp);
+                const T xp = UNIT ? yp : yp / S.diag[p][p];
+                if (lane == lp) { if (hp) y[1] = xp; else y[0] = xp; }
 #pragma unroll
-            for (int k = 0; k < NR; ++k) {
-                T v = acc[i][k];
-#pragma unroll
-                for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-                if (lane == 0) sred[0][warp + 8 * i][k] = v;
+                for (int q = 0; q < 2; ++q) {
+                    const int r = lane + 32 * q;
+                    const bool below = LOWER ? (r > p) : (r < p);
+                    if (below && r < rows) y[q] = fma(-S.diag[r][p], xp, y[q]);
+                }
             }
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int r = lane + 32 * q;
+                if (r < rows) {
+                    X[(i64)(r0 + r) + (i64)k * ldx] = y[q];
+                    if constexpr (TAGGED)
+                        xtag[(i64)(r0 + r) * NR + k] =
+                            ((unsigned long long)epoch << 32) | __float_as_uint((float)y[q]);
+                }
+            }
+        }
     }
-    // diagonal block of M into shared memory
-    for (int e = t; e < SB * SB; e += SOLVE_NT) {
-        int r, j;
-        if (!TRANS) { r = e % SB; j = e / SB; } else { j = e % SB; r = e / SB; }
-        sD[r][j] = (r < rows && j < rows) ? Mv(r0 + r, r0 + j) : T(0);
+    if constexpr (!TAGGED) {
+        __threadfence();
+        __syncthreads();
+        if (t == 0) st_release(&flags[b], 1);
     }
-    __syncthreads();
+}
 
-    // ---- diagonal solve: warp k handles right-hand side k ----
-    for (int k = warp; k < NR; k += SOLVE_NT / 32) {
-        T y[2];
-#pragma unroll
-        for (int hh = 0; hh < 2; ++hh) {
-            const int r = lane + 32 * hh;
-            T s = T(0);
-            if (!TRANS) s = sred[0][r][k] + sred[1][r][k] + sred[2][r][k] + sred[3][r][k];
-            else s = sred[0][r][k];
-            y[hh] = (r < rows) ? (X[(i64)(r0 + r) + (i64)k * ldx] - s) : T(0);
-        }
-        for (int step = 0; step < rows; ++step) {
-            const int p = LOWER ? step : rows - 1 - step;
-            const int hp = p >> 5, lp = p & 31;
-            T yp = __shfl_sync(0xffffffffu, hp ? y[1] : y[0], lp);
-            const T xp = UNIT ? yp : yp / sD[p][p];
-            if (lane == lp) { if (hp) y[1] = xp; else y[0] = xp; }
-#pragma unroll
-            for (int hh = 0; hh < 2; ++hh) {
-                const int r = lane + 32 * hh;
-                const bool below = LOWER ? (r > p) : (r < p);
-                if (below && r < rows) y[hh] = fma(-sD[r][p], xp, y[hh]);
-            }
-        }
-#pragma unroll
-        for (int hh = 0; hh < 2; ++hh) {
-            const int r = lane + 32 * hh;
-            if (r < rows) X[(i64)(r0 + r) + (i64)k * ldx] = y[hh];
-        }
+// Inverses of the SB x SB diagonal blocks of the effective triangle M (unit or
+// not), row-major per block: one CTA per block, thread j solves M x = e_j.
+template <typename T, bool LOWER, bool UNIT, bool ROWACC>
+__global__ void __launch_bounds__(SB) k_tri_inv_blocks(const T *__restrict__ A, i64 lda, int n,
+                                                       T *__restrict__ Dinv) {
+    extern __shared__ __align__(16) unsigned char inv_smem[];
+    T(*sM)[SB + 1] = reinterpret_cast<T(*)[SB + 1]>(inv_smem);
+    T(*sX)[SB + 1] = reinterpret_cast<T(*)[SB + 1]>(inv_smem + sizeof(T) * SB * (SB + 1));
+    const int b = blockIdx.x, r0 = b * SB, rows = min(SB, n - r0);
+    const int j = threadIdx.x;
+    for (int r = 0; r < SB; ++r) {
+        T v = T(0);
+        if (r < rows && j < rows) v = ROWACC ? A[(i64)(r0 + r) * lda + r0 + j] : A[(i64)(r0 + r) + (i64)(r0 + j) * lda];
+        if (r >= rows || j >= rows) v = (r == j) ? T(1) : T(0);  // pad with the identity
+        sM[r][j] = v;
     }
-    __threadfence();
     __syncthreads();
-    if (t == 0) st_release(&flags[b], 1);
+    for (int st = 0; st < SB; ++st) {
+        const int i = LOWER ? st : SB - 1 - st;
+        T s = (i == j) ? T(1) : T(0);
+        if (LOWER) {
+            for (int p = 0; p < i; ++p) s = fma(-sM[i][p], sX[p][j], s);
+        } else {
+            for (int p = i + 1; p < SB; ++p) s = fma(-sM[i][p], sX[p][j], s);
+        }
+        sX[i][j] = UNIT ? s : s / sM[i][i];
+    }
+    __syncthreads();
+    for (int r = 0; r < SB; ++r) Dinv[(i64)b * SB * SB + (i64)r * SB + j] = sX[r][j];
 }
 
 template <typename T>
@@ -185,9 +341,15 @@ __global__ void k_gather_rows(const T *__restrict__ B, i64 ldb, const int64_t *_
     else X[perm[i] + (i64)k * ldx] = B[i + (i64)k * ldb];
 }
 
+// UPPER_A / TRANS describe the stored factor as in LAPACK (column-major A,
+// op(A) = A or A^T); ROWACC access of the same memory is the transposed view.
+static std::atomic<uint32_t> g_trsv_epoch{0};  // tags of the FP32 exchange words
+
 template <typename T, bool UPPER_A, bool UNIT, bool TRANS>
 static void trsv_launch(const T *A, i64 lda, T *X, i64 ldx, int n, int nrhs, int *ctl, int *err,
-                        cudaStream_t s) {
+                        cudaStream_t s, const T *Dinv = nullptr,
+                        unsigned long long *xtag = nullptr) {
+    constexpr bool LOWER = (UPPER_A == TRANS);
     const int nb = (n + SB - 1) / SB;
     ProfScope ps(KC_TRSV, s, (double)n * n * nrhs, (double)n * n * sizeof(T) / 2);
     for (int k0 = 0; k0 < nrhs;) {
@@ -195,18 +357,47 @@ static void trsv_launch(const T *A, i64 lda, T *X, i64 ldx, int n, int nrhs, int
         OXI_CUDA(cudaMemsetAsync(ctl, 0, sizeof(int) * (nb + 1), s));
         int *ticket = ctl, *flags = ctl + 1;
         T *Xk = X + (i64)k0 * ldx;
-        if (left >= 4) {
-            k_trsv<T, UPPER_A, UNIT, TRANS, 4><<<nb, SOLVE_NT, 0, s>>>(A, lda, Xk, ldx, n, ticket, flags, err);
-            k0 += 4;
-        } else if (left >= 2) {
-            k_trsv<T, UPPER_A, UNIT, TRANS, 2><<<nb, SOLVE_NT, 0, s>>>(A, lda, Xk, ldx, n, ticket, flags, err);
-            k0 += 2;
-        } else {
-            k_trsv<T, UPPER_A, UNIT, TRANS, 1><<<nb, SOLVE_NT, 0, s>>>(A, lda, Xk, ldx, n, ticket, flags, err);
-            k0 += 1;
-        }
+#define OXI_TRSV_GO(NRV)                                                                              \
+    do {                                                                                             \
+        const int smem = (int)sizeof(TrsvSmem<T, NRV>);                                             \
+        const uint32_t ep = ++g_trsv_epoch;                                                          \
+        if (Dinv) {                                                                                  \
+            if constexpr (sizeof(T) == 4) {                                                          \
+                if (xtag) {                                                                          \
+                    auto kern = k_trsv2<T, LOWER, UNIT, TRANS, NRV, true, true>;                     \
+                    OXI_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)); \
+                    kern<<<nb, SOLVE_NT, smem, s>>>(A, lda, Dinv, Xk, ldx, n, ticket, flags, err, xtag, ep); \
+                    k0 += NRV;                                                                       \
+                    break;                                                                           \
+                }                                                                                    \
+            }                                                                                        \
+            auto kern = k_trsv2<T, LOWER, UNIT, TRANS, NRV, true>;                                   \
+            OXI_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)); \
+            kern<<<nb, SOLVE_NT, smem, s>>>(A, lda, Dinv, Xk, ldx, n, ticket, flags, err, nullptr, 0u); \
+        } else {                                                                                     \
+            auto kern = k_trsv2<T, LOWER, UNIT, TRANS, NRV, false>;                                  \
+            OXI_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)); \
+            kern<<<nb, SOLVE_NT, smem, s>>>(A, lda, Dinv, Xk, ldx, n, ticket, flags, err, nullptr, 0u); \
+        }                                                                                            \
+        k0 += NRV;                                                                                   \
+    } while (0)
+        if (left >= 4) OXI_TRSV_GO(4);
+        else if (left >= 2) OXI_TRSV_GO(2);
+        else OXI_TRSV_GO(1);
+#undef OXI_TRSV_GO
         OXI_LAUNCH_CHECK();
     }
+}
+
+template <typename T, bool UPPER_A, bool UNIT, bool TRANS>
+static void tri_inv_launch(const T *A, i64 lda, int n, T *Dinv, cudaStream_t s) {
+    constexpr bool LOWER = (UPPER_A == TRANS);
+    const int nb = (n + SB - 1) / SB;
+    const int smem = 2 * (int)sizeof(T) * SB * (SB + 1);
+    OXI_CUDA(cudaFuncSetAttribute(k_tri_inv_blocks<T, LOWER, UNIT, TRANS>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    k_tri_inv_blocks<T, LOWER, UNIT, TRANS><<<nb, SB, smem, s>>>(A, lda, n, Dinv);
+    OXI_LAUNCH_CHECK();
 }
 
 // Solve with device-resident permutation `perm` (0-based, A[perm,:] = L U).
@@ -240,18 +431,38 @@ template void getrs_perm<double>(oxi_handle_s *, char, i64, i64, const double *,
 template void getrs_perm<float>(oxi_handle_s *, char, i64, i64, const float *, i64, const int64_t *, float *, i64, int *);
 
 // Row-major factors W are the column-major matrix W^T: L (lower) is then an
-// upper-stored triangle read transposed, U likewise.
+// upper-stored triangle read transposed, U likewise.  Dinv (optional): the
+// inverses of the 64 x 64 diagonal blocks of L and of U, from
+// lu_block_inverses_rowmajor.
 template <typename T>
 void lu_solve_rowmajor(oxi_handle_s *h, const T *W, i64 ld, i64 n, T *X, i64 ldx, i64 nrhs,
-                       int *d_err) {
+                       int *d_err, const T *DinvL, const T *DinvU) {
     const i64 nb = (n + SB - 1) / SB;
     if (nb + 1 > kTrsvCtlInts) throw CudaError{cudaErrorInvalidValue, "system too large for the solve control block"};
     int *ctl = (int *)((char *)h->scratch.get(kScratchBytes) + kScratchTrsvOff);
-    trsv_launch<T, true, true, true>(W, ld, X, ldx, (int)n, (int)nrhs, ctl, d_err, h->stream);
-    trsv_launch<T, false, false, true>(W, ld, X, ldx, (int)n, (int)nrhs, ctl, d_err, h->stream);
+    unsigned long long *xtag = nullptr;
+    if (sizeof(T) == 4 && DinvL && DinvU) {
+        const size_t need = sizeof(unsigned long long) * (size_t)n * 4;
+        if (h->xtag_ws.bytes < need) {  // fresh words: epoch 0 never matches a launch
+            xtag = (unsigned long long *)h->xtag_ws.get(need);
+            OXI_CUDA(cudaMemsetAsync(xtag, 0, h->xtag_ws.bytes, h->stream));
+        }
+        xtag = (unsigned long long *)h->xtag_ws.get(need);
+    }
+    trsv_launch<T, true, true, true>(W, ld, X, ldx, (int)n, (int)nrhs, ctl, d_err, h->stream, DinvL, xtag);
+    trsv_launch<T, false, false, true>(W, ld, X, ldx, (int)n, (int)nrhs, ctl, d_err, h->stream, DinvU, xtag);
 }
-template void lu_solve_rowmajor<float>(oxi_handle_s *, const float *, i64, i64, float *, i64, i64, int *);
-template void lu_solve_rowmajor<double>(oxi_handle_s *, const double *, i64, i64, double *, i64, i64, int *);
+template void lu_solve_rowmajor<float>(oxi_handle_s *, const float *, i64, i64, float *, i64, i64, int *, const float *, const float *);
+template void lu_solve_rowmajor<double>(oxi_handle_s *, const double *, i64, i64, double *, i64, i64, int *, const double *, const double *);
+
+template <typename T>
+void lu_block_inverses_rowmajor(oxi_handle_s *h, const T *W, i64 ld, i64 n, T *DinvL, T *DinvU) {
+    tri_inv_launch<T, true, true, true>(W, ld, (int)n, DinvL, h->stream);
+    tri_inv_launch<T, false, false, true>(W, ld, (int)n, DinvU, h->stream);
+}
+template void lu_block_inverses_rowmajor<float>(oxi_handle_s *, const float *, i64, i64, float *, float *);
+template void lu_block_inverses_rowmajor<double>(oxi_handle_s *, const double *, i64, i64, double *, double *);
+i64 lu_block_inverse_elems(i64 n) { return ((n + SB - 1) / SB) * (i64)SB * SB; }
 
 // LUFactor.p from the interchange sequence (src/lapack/factorizations.jl:72-75).
 void perm_from_ipiv(const int64_t *ipiv, i64 q, i64 m, int64_t *perm) {
