@@ -36,6 +36,10 @@ int oxi_destroy(oxi_handle_t h) {
     h->tc_ws.release();
     h->xtag_ws.release();
     h->rowmap_ws.release();
+    h->gcache.reset();
+    if (h->aux_stream) cudaStreamDestroy(h->aux_stream);
+    if (h->aux_fork) cudaEventDestroy(h->aux_fork);
+    if (h->aux_join) cudaEventDestroy(h->aux_join);
     h->host_ws.release();
     delete h;
     return OXI_OK;
@@ -93,6 +97,10 @@ int oxi_set_option(oxi_handle_t h, int option, int64_t value) {
             if (value < 2 || value > 62) return OXI_EINVAL;
             h->opt.gmres_restart = (int)value;
             return OXI_OK;
+        case OXI_OPT_GRAPHS:
+            h->opt.graphs = value ? 1 : 0;
+            if (!value) h->gcache.reset();
+            return OXI_OK;
         default: return OXI_EINVAL;
     }
 }
@@ -107,6 +115,7 @@ int oxi_get_option(oxi_handle_t h, int option, int64_t *value) {
         case OXI_OPT_MIXED_BLOCKSIZE: *value = h->opt.mixed_blocksize; return OXI_OK;
         case OXI_OPT_STOP_NORMWISE: *value = h->opt.stop_normwise; return OXI_OK;
         case OXI_OPT_GMRES_RESTART: *value = h->opt.gmres_restart; return OXI_OK;
+        case OXI_OPT_GRAPHS: *value = h->opt.graphs; return OXI_OK;
         default: return OXI_EINVAL;
     }
 }
@@ -158,6 +167,7 @@ int oxi_sgemm_update_lowp(oxi_handle_t h, int prec, int64_t m, int64_t n, int64_
 
 int oxi_profile_enable(oxi_handle_t h, int on) {
     if (!h) return OXI_EINVAL;
+    h->gcache.reset();  // profiled launches are recorded individually
     cudaSetDevice(h->device);
     cudaStreamSynchronize(h->stream);
     h->prof.recycle();

@@ -145,7 +145,9 @@ k_gemm_dmma(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUt
         if (lane == 0) mbar_arrive(&empty[s]);
     }
 
-    // epilogue: C -= acc
+    // epilogue: C -= acc.  The eight C pairs of a row are loaded before any is
+    // used so their round trips overlap (16-byte accesses when aligned).
+    const bool vec2 = ((ldc & 1) == 0) && ((((uintptr_t)C) & 15) == 0);
 #pragma unroll
     for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
@@ -153,11 +155,27 @@ k_gemm_dmma(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUt
             const int r = m0 + wm * 32 + mt * 16 + gid + 8 * h;
             if (r >= M) continue;
             double *crow = C + (i64)r * ldc;
+            double2 cv[4];
 #pragma unroll
             for (int nt = 0; nt < 4; ++nt) {
                 const int c = n0 + wn * 32 + nt * 8 + 2 * tig;
-                if (c < N) crow[c] = crow[c] - acc[mt][nt][2 * h];
-                if (c + 1 < N) crow[c + 1] = crow[c + 1] - acc[mt][nt][2 * h + 1];
+                if (c + 1 < N && vec2) cv[nt] = __ldcs((const double2 *)(crow + c));
+                else {
+                    cv[nt].x = (c < N) ? crow[c] : 0.0;
+                    cv[nt].y = (c + 1 < N) ? crow[c + 1] : 0.0;
+                }
+            }
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt) {
+                const int c = n0 + wn * 32 + nt * 8 + 2 * tig;
+                double2 v;
+                v.x = cv[nt].x - acc[mt][nt][2 * h];
+                v.y = cv[nt].y - acc[mt][nt][2 * h + 1];
+                if (c + 1 < N && vec2) __stcs((double2 *)(crow + c), v);
+                else {
+                    if (c < N) crow[c] = v.x;
+                    if (c + 1 < N) crow[c + 1] = v.y;
+                }
             }
         }
 }

@@ -3,14 +3,10 @@
 // A: M x K, B: N x K, both 16-bit (BF16 or FP16) and K-major (K contiguous),
 // accumulated in FP32 in tensor memory (tcgen05.mma kind::f16).
 //
-// CTA tile 128 x 256, k slab 64 (one 128-byte swizzle atom per row), 2-stage
-// TMA -> shared memory ring, 4 warps:
-//   warp 0 lane 0   TMA producer
-//   warp 1 lane 0   MMA issuer (tcgen05.mma, commit -> "stage empty" barrier)
-//   warps 0..3      epilogue: tcgen05.ld 32 lanes x 32 columns at a time, each
-//                   thread owns one row of the tile, C - scale*D written back.
-// Two CTAs per SM (96 KB of shared memory and 256 TMEM columns each) so one
-// CTA's epilogue overlaps the other's loads and MMAs.
+// Tile 128 x 256, k slab 64 (one 128-byte swizzle atom per row), a 2-stage TMA
+// ring for the operands, the whole FP32 C tile (128 KB) in shared memory, and
+// two TMEM accumulators so that a tile's epilogue overlaps the next tile's MMAs
+// (see k_gemm_tc).
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include "tma_util.cuh"
@@ -22,9 +18,13 @@ constexpr int BM = 128, BN = 256, BK = 64, STAGES = 2;
 constexpr int A_BYTES = BM * BK * 2;  // 16 KB
 constexpr int B_BYTES = BN * BK * 2;  // 32 KB
 constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
-constexpr int NTHREADS = 128;
-constexpr int TMEM_COLS = 256;
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+constexpr int CBOX_COLS = 32;                    // one 128-byte swizzle atom per row
+constexpr int NCBOX = BN / CBOX_COLS;            // 8 boxes across the tile
+constexpr int CBOX_BYTES = BM * CBOX_COLS * 4;   // 16 KB
+constexpr int C_BYTES = NCBOX * CBOX_BYTES;      // 128 KB: the whole FP32 C tile
+constexpr int NTHREADS = 256;
+constexpr int TMEM_COLS = 256;  // per accumulator buffer (two buffers)
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + C_BYTES + 1024 + 256;
 }  // namespace tc
 
 __device__ int g_gemm_tc_err;
@@ -53,36 +53,79 @@ __device__ __forceinline__ void tc_fence_after() {
 __device__ __forceinline__ void tc_fence_before() {
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
 }
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap *tm, const void *src, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%2, %3}], [%1];" ::"l"(
+            (uint64_t)tm),
+        "r"(smem_u32(src)), "r"(x), "r"(y)
+        : "memory");
+}
 
+// Bounded wait that also gives up when another role of the CTA has aborted.
+__device__ __forceinline__ bool mbar_wait_ab(uint64_t *bar, uint32_t parity, int code,
+                                             volatile int *abort_flag) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    for (;;) {
+        for (int it = 0; it < 256; ++it)
+            if (mbar_try_wait(bar, parity)) return true;
+        if (*abort_flag) return false;
+        if (global_ns() - t0 > kWaitLimitNs) break;
+    }
+    atomicExch(&g_gemm_tc_err, code);
+    *abort_flag = 1;
+    return false;
+}
+
+// Persistent, warp-specialised tcgen05 GEMM (one CTA per SM, tiles strided by
+// the grid):
+//   warp 0 lane 0   operand producer: A/B slabs by TMA into a 2-stage ring
+//   warp 1 lane 0   MMA issuer into one of two 256-column TMEM accumulators
+//   warp 2 lane 0   C producer: the tile's FP32 C (eight 32-column boxes, 128-byte
+//                   swizzle) by TMA, once the previous tile has been stored
+//   warps 4..7      epilogue warpgroup: TMEM -> registers, C - scale*D in shared
+//                   memory, TMA store -- overlapping the next tile's MMAs
 template <int AB_FORMAT>
-__global__ void __launch_bounds__(tc::NTHREADS, 2)
+__global__ void __launch_bounds__(256, 1)
 k_gemm_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-          float *__restrict__ C, i64 ldc, int M, int N, int K, float scale,
+          const __grid_constant__ CUtensorMap tmC, int M, int N, int K, float scale,
           const float *__restrict__ d_scale) {
     using namespace tc;
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~uintptr_t(1023));
-    uint64_t *full = (uint64_t *)(smem + STAGES * STAGE_BYTES);
+    uint8_t *sC = smem + STAGES * STAGE_BYTES;
+    uint64_t *full = (uint64_t *)(sC + C_BYTES);
     uint64_t *empty = full + STAGES;
-    uint64_t *done = empty + STAGES;
-    uint32_t *tmem_slot = (uint32_t *)(done + 1);
+    uint64_t *tfull = empty + STAGES;  // [2]
+    uint64_t *tempty = tfull + 2;      // [2]
+    uint64_t *cfull = tempty + 2;
+    uint64_t *cempty = cfull + 1;
+    uint32_t *tmem_slot = (uint32_t *)(cempty + 1);
+    volatile int *abort_flag = (volatile int *)(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
     const int KT = (K + BK - 1) / BK;
+    const int tilesN = (N + BN - 1) / BN, tilesM = (M + BM - 1) / BM;
+    const int ntiles = tilesM * tilesN;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
-        mbar_init(done, 1);
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&tfull[b], 1);
+            mbar_init(&tempty[b], 4);
+        }
+        mbar_init(cfull, 1);
+        mbar_init(cempty, 1);
+        *abort_flag = 0;
         fence_barrier_init();
     }
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                          smem_u32(tmem_slot)),
-                     "r"(TMEM_COLS));
+                     "r"(2 * TMEM_COLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
         tc_fence_before();
     }
@@ -93,91 +136,132 @@ k_gemm_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
     if (warp == 0 && lane == 0) {
         prefetch_tmap(&tmA);
         prefetch_tmap(&tmB);
-        for (int kt = 0; kt < KT; ++kt) {
-            const int s = kt % STAGES;
-            if (kt >= STAGES && !mbar_wait(&empty[s], ((kt / STAGES) + 1) & 1, &g_gemm_tc_err, 1)) break;
-            uint8_t *sa = smem + s * STAGE_BYTES;
-            mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
-            tma_load_2d(sa, &tmA, &full[s], kt * BK, m0);
-            tma_load_2d(sa + A_BYTES, &tmB, &full[s], kt * BK, n0);
+        int kb = 0;
+        for (int tile = blockIdx.x; tile < ntiles && !*abort_flag; tile += gridDim.x) {
+            const int m0 = (tile / tilesN) * BM, n0 = (tile % tilesN) * BN;
+            for (int kt = 0; kt < KT; ++kt, ++kb) {
+                const int s = kb % STAGES;
+                if (kb >= STAGES && !mbar_wait_ab(&empty[s], ((kb / STAGES) + 1) & 1, 1, abort_flag)) break;
+                uint8_t *sa = smem + s * STAGE_BYTES;
+                mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
+                tma_load_2d(sa, &tmA, &full[s], kt * BK, m0);
+                tma_load_2d(sa + A_BYTES, &tmB, &full[s], kt * BK, n0);
+            }
         }
     } else if (warp == 1 && lane == 0) {
         constexpr uint32_t idesc = umma_idesc_f16(AB_FORMAT, BM, BN);
-        bool ok = true;
-        for (int kt = 0; kt < KT && ok; ++kt) {
-            const int s = kt % STAGES;
-            if (!mbar_wait(&full[s], (kt / STAGES) & 1, &g_gemm_tc_err, 2)) { ok = false; break; }
+        int kb = 0, li = 0;
+        for (int tile = blockIdx.x; tile < ntiles && !*abort_flag; tile += gridDim.x, ++li) {
+            const int b = li & 1;
+            if (li >= 2 && !mbar_wait_ab(&tempty[b], ((li >> 1) + 1) & 1, 2, abort_flag)) break;
             tc_fence_after();
-            const uint32_t sa = smem_u32(smem + s * STAGE_BYTES);
-            const uint64_t da = umma_desc_sw128(sa), db = umma_desc_sw128(sa + A_BYTES);
+            const uint32_t dacc = tmem + (uint32_t)(b * TMEM_COLS);
+            for (int kt = 0; kt < KT; ++kt, ++kb) {
+                const int s = kb % STAGES;
+                if (!mbar_wait_ab(&full[s], (kb / STAGES) & 1, 3, abort_flag)) break;
+                tc_fence_after();
+                const uint32_t sa = smem_u32(smem + s * STAGE_BYTES);
+                const uint64_t da = umma_desc_sw128(sa), db = umma_desc_sw128(sa + A_BYTES);
 #pragma unroll
-            for (int k = 0; k < BK / 16; ++k) {
-                const uint64_t adv = (uint64_t)((k * 32) >> 4);  // 16 elements = 32 bytes
-                const uint32_t acc = (kt > 0 || k > 0) ? 1u : 0u;
+                for (int k = 0; k < BK / 16; ++k) {
+                    const uint64_t adv = (uint64_t)((k * 32) >> 4);  // 16 elements = 32 bytes
+                    const uint32_t acc = (kt > 0 || k > 0) ? 1u : 0u;
+                    asm volatile(
+                        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(dacc),
+                        "l"(da + adv), "l"(db + adv), "r"(idesc), "r"(acc));
+                }
                 asm volatile(
-                    "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-                    " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
-                    "l"(da + adv), "l"(db + adv), "r"(idesc), "r"(acc));
+                    "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                        smem_u32(&empty[s]))
+                    : "memory");
             }
             asm volatile(
                 "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                    smem_u32(&empty[s]))
+                    smem_u32(&tfull[b]))
                 : "memory");
         }
-        asm volatile(
-            "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                smem_u32(done))
-            : "memory");
-    }
-    __syncwarp();
-
-    // ---------------- epilogue ----------------
-    const bool have = mbar_wait(done, 0, &g_gemm_tc_err, 3);
-    tc_fence_after();
-    const float sc = d_scale ? scale * (*d_scale) : scale;
-    const int row = m0 + warp * 32 + lane;
-    if (have) {
-#pragma unroll 1
-        for (int c = 0; c < BN / 32; ++c) {
-            uint32_t v[32];
-            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(c * 32);
+    } else if (warp == 2 && lane == 0) {
+        prefetch_tmap(&tmC);
+        int li = 0;
+        for (int tile = blockIdx.x; tile < ntiles && !*abort_flag; tile += gridDim.x, ++li) {
+            const int m0 = (tile / tilesN) * BM, n0 = (tile % tilesN) * BN;
+            if (li >= 1 && !mbar_wait_ab(cempty, (li - 1) & 1, 4, abort_flag)) break;
+            mbar_arrive_expect_tx(cfull, C_BYTES);
+#pragma unroll
+            for (int bx = 0; bx < NCBOX; ++bx)
+                tma_load_2d(sC + bx * CBOX_BYTES, &tmC, cfull, n0 + bx * CBOX_COLS, m0);
+        }
+    } else if (warp >= 4) {
+        const int ew = warp - 4;          // TMEM lane quadrant of this warp
+        const int r = ew * 32 + lane;     // tile row owned by this thread
+        const float sc = d_scale ? scale * (*d_scale) : scale;
+        int li = 0;
+        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++li) {
+            const int m0 = (tile / tilesN) * BM, n0 = (tile % tilesN) * BN;
+            const int b = li & 1;
+            const bool ok = mbar_wait_ab(&tfull[b], (li >> 1) & 1, 5, abort_flag) &&
+                            mbar_wait_ab(cfull, li & 1, 6, abort_flag);
+            // uniform decision across the epilogue warpgroup (it meets at a named barrier)
+            uint32_t all_ok;
             asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,"
-                "%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
-                  "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
-                  "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]),
-                  "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
-                  "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]),
-                  "=r"(v[31])
-                : "r"(taddr));
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            const int col0 = n0 + c * 32;
-            if (row < M && col0 < N) {
-                float *cr = C + (i64)row * ldc + col0;
-                if (col0 + 32 <= N && ((((uintptr_t)cr) & 15) == 0)) {
+                "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n"
+                " bar.red.and.pred q, 1, 128, p;\n selp.u32 %0, 1, 0, q;\n}\n"
+                : "=r"(all_ok)
+                : "r"((uint32_t)ok)
+                : "memory");
+            if (!all_ok) break;
+            tc_fence_after();
+            const uint32_t base = tmem + (uint32_t)(b * TMEM_COLS) + ((uint32_t)(ew * 32) << 16);
+#pragma unroll 1
+            for (int c = 0; c < NCBOX; ++c) {
+                uint32_t v[32];
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,"
+                    "%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                      "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+                      "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]),
+                      "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+                      "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]),
+                      "=r"(v[31])
+                    : "r"(base + (uint32_t)(c * 32)));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                uint8_t *rowp = sC + c * CBOX_BYTES + r * 128;
 #pragma unroll
-                    for (int q = 0; q < 8; ++q) {
-                        float4 x = *(float4 *)(cr + 4 * q);
-                        x.x -= sc * __uint_as_float(v[4 * q + 0]);
-                        x.y -= sc * __uint_as_float(v[4 * q + 1]);
-                        x.z -= sc * __uint_as_float(v[4 * q + 2]);
-                        x.w -= sc * __uint_as_float(v[4 * q + 3]);
-                        *(float4 *)(cr + 4 * q) = x;
-                    }
-                } else {
-#pragma unroll
-                    for (int j = 0; j < 32; ++j)
-                        if (col0 + j < N) cr[j] -= sc * __uint_as_float(v[j]);
+                for (int q = 0; q < 8; ++q) {
+                    float4 *p4 = (float4 *)(rowp + ((q ^ (r & 7)) << 4));  // 128-byte swizzle
+                    float4 x = *p4;
+                    x.x -= sc * __uint_as_float(v[4 * q + 0]);
+                    x.y -= sc * __uint_as_float(v[4 * q + 1]);
+                    x.z -= sc * __uint_as_float(v[4 * q + 2]);
+                    x.w -= sc * __uint_as_float(v[4 * q + 3]);
+                    *p4 = x;
                 }
             }
+            // the accumulator buffer is drained: the MMA warp may reuse it
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&tempty[b]);
+            fence_proxy_async();  // shared-memory writes -> visible to the TMA (async proxy)
+            asm volatile("bar.sync 1, 128;" ::: "memory");
+            if (ew == 0 && lane == 0) {
+#pragma unroll
+                for (int bx = 0; bx < NCBOX; ++bx)
+                    tma_store_2d(&tmC, sC + bx * CBOX_BYTES, n0 + bx * CBOX_COLS, m0);
+                asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+                asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+                mbar_arrive(cempty);  // the C buffer may be refilled
+            }
         }
+        if (ew == 0 && lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
     }
     tc_fence_before();
     __syncthreads();
     if (warp == 1) {
+        tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
-                     "r"(TMEM_COLS));
+                     "r"(2 * TMEM_COLS));
     }
 }
 
@@ -263,11 +347,20 @@ void launch_gemm_tc(int fmt /*0 fp16, 1 bf16*/, float *C, i64 ldc, const void *A
                     const float *d_scale, cudaStream_t s) {
     using namespace tc;
     if (M <= 0 || N <= 0 || K <= 0) return;
-    CUtensorMap tmA, tmB;
+    CUtensorMap tmA, tmB, tmC;
     const CUtensorMapDataType dt = fmt == 1 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
     make_tmap_2d(&tmA, dt, 2, A16, K, M, lda16, BK, BM, CU_TENSOR_MAP_SWIZZLE_128B);
     make_tmap_2d(&tmB, dt, 2, B16, K, N, ldb16, BK, BN, CU_TENSOR_MAP_SWIZZLE_128B);
-    dim3 grid((unsigned)((N + BN - 1) / BN), (unsigned)((M + BM - 1) / BM));
+    make_tmap_2d(&tmC, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, C, N, M, ldc, CBOX_COLS, BM,
+                 CU_TENSOR_MAP_SWIZZLE_128B);
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        OXI_CUDA(cudaGetDevice(&dev));
+        OXI_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    }
+    const i64 tiles = ((N + BN - 1) / BN) * ((M + BM - 1) / BM);
+    dim3 grid((unsigned)std::min<i64>(tiles, sms));
     ProfScope ps(KC_GEMM_TC, s, 2.0 * M * N * K, 8.0 * M * N + 2.0 * (M + N) * K);
     if (fmt == 1) {
         static bool attr = false;
@@ -275,14 +368,14 @@ void launch_gemm_tc(int fmt /*0 fp16, 1 bf16*/, float *C, i64 ldc, const void *A
             OXI_CUDA(cudaFuncSetAttribute(k_gemm_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
             attr = true;
         }
-        k_gemm_tc<1><<<grid, NTHREADS, SMEM_BYTES, s>>>(tmA, tmB, C, ldc, (int)M, (int)N, (int)K, scale, d_scale);
+        k_gemm_tc<1><<<grid, NTHREADS, SMEM_BYTES, s>>>(tmA, tmB, tmC, (int)M, (int)N, (int)K, scale, d_scale);
     } else {
         static bool attr = false;
         if (!attr) {
             OXI_CUDA(cudaFuncSetAttribute(k_gemm_tc<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
             attr = true;
         }
-        k_gemm_tc<0><<<grid, NTHREADS, SMEM_BYTES, s>>>(tmA, tmB, C, ldc, (int)M, (int)N, (int)K, scale, d_scale);
+        k_gemm_tc<0><<<grid, NTHREADS, SMEM_BYTES, s>>>(tmA, tmB, tmC, (int)M, (int)N, (int)K, scale, d_scale);
     }
     OXI_LAUNCH_CHECK();
 }
@@ -340,6 +433,15 @@ __global__ void k_fp16_scales(const unsigned int *__restrict__ umax_bits, float 
 void gemm_trailing_f32(oxi_handle_s *h, float *C, i64 ldc, const float *A, i64 lda, const float *B,
                        i64 ldb, i64 M, i64 N, i64 K) {
     if (M <= 0 || N <= 0 || K <= 0) return;
+    if (((uintptr_t)C % 16) != 0 || (ldc * 4) % 16 != 0) {
+        // the C tile travels by TMA: stage an unaligned C through an aligned copy
+        const i64 ldp = (N + 3) / 4 * 4;
+        float *Cp = (float *)h->solve_ws.get(sizeof(float) * (size_t)M * ldp);
+        OXI_CUDA(cudaMemcpy2DAsync(Cp, ldp * 4, C, ldc * 4, N * 4, M, cudaMemcpyDeviceToDevice, h->stream));
+        gemm_trailing_f32(h, Cp, ldp, A, lda, B, ldb, M, N, K);
+        OXI_CUDA(cudaMemcpy2DAsync(C, ldc * 4, Cp, ldp * 4, N * 4, M, cudaMemcpyDeviceToDevice, h->stream));
+        return;
+    }
     if (h->trailing == TRAIL_BF16X3) {
         const i64 K3 = 3 * K, ldk3 = (K3 + 7) / 8 * 8;
         char *ws = (char *)h->tc_ws.get((size_t)(M + N) * ldk3 * 2 + 1024);

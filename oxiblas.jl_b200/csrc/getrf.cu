@@ -31,11 +31,10 @@ template <typename T>
 void gemm_minus(oxi_handle_s *h, T *C, i64 ldc, const T *A, i64 lda, const T *B, i64 ldb, i64 M,
                 i64 N, i64 K) {
     if (M <= 0 || N <= 0 || K <= 0) return;
-    if constexpr (sizeof(T) == 8) {
-        if (h->opt.gemm == 0) {
-            launch_gemm_dmma(C, ldc, A, lda, B, ldb, M, N, K, h->stream);
-            return;
-        }
+    if (h->opt.gemm == 0) {
+        if constexpr (sizeof(T) == 8) launch_gemm_dmma(C, ldc, A, lda, B, ldb, M, N, K, h->stream);
+        else launch_gemm_simt<T>(C, ldc, A, lda, B, ldb, M, N, K, h->stream);
+        return;
     }
     launch_gemm_ref<T>(C, ldc, A, lda, B, ldb, M, N, K, h->stream);
 }
@@ -47,9 +46,13 @@ template void gemm_minus<float>(oxi_handle_s *, float *, i64, const float *, i64
 template <typename T>
 void trsm_lower_unit(oxi_handle_s *h, const T *L, i64 ldl, T *B, i64 ldb, i64 t, i64 N) {
     if (t <= 1 || N <= 0) return;
+    if (h->opt.gemm == 0 && t <= 256) {  // tensor-core engine: one fused launch
+        launch_trsm_fused<T>(L, ldl, B, ldb, (int)t, N, h->stream);
+        return;
+    }
     const i64 leaf = std::min<i64>(std::max<i64>(h->opt.trsm_leaf, 1), 32);
     if (t <= leaf) {
-        launch_trsm_leaf<T>(L, ldl, B, ldb, (int)t, N, h->stream);
+        launch_trsm_leaf<T>(L, ldl, B, ldb, (int)t, N, h->stream, h->opt.gemm == 1);
         return;
     }
     const i64 t1 = split_point(h, t);
@@ -150,6 +153,80 @@ void getrf_rowmajor(oxi_handle_s *h, T *W, i64 ld, i64 m, i64 n, int64_t *d_ipiv
 template void getrf_rowmajor<double>(oxi_handle_s *, double *, i64, i64, i64, int64_t *, int64_t *, int *, int *);
 template void getrf_rowmajor<float>(oxi_handle_s *, float *, i64, i64, i64, int64_t *, int64_t *, int *, int *);
 
+template <typename T>
+void getrf_rowmajor_cached(oxi_handle_s *h, T *W, i64 ld, i64 m, i64 n, int64_t *d_ipiv,
+                           int64_t *d_info, int *d_moves, int *d_nmoves) {
+    // The legacy default stream cannot be captured: run on the handle's own
+    // stream, ordered after and before the caller's work through events.
+    if (h->stream == nullptr && h->opt.graphs && !h->prof.enabled) {
+        if (!h->aux_stream) {
+            OXI_CUDA(cudaStreamCreateWithFlags(&h->aux_stream, cudaStreamNonBlocking));
+            OXI_CUDA(cudaEventCreateWithFlags(&h->aux_fork, cudaEventDisableTiming));
+            OXI_CUDA(cudaEventCreateWithFlags(&h->aux_join, cudaEventDisableTiming));
+        }
+        OXI_CUDA(cudaEventRecord(h->aux_fork, nullptr));
+        OXI_CUDA(cudaStreamWaitEvent(h->aux_stream, h->aux_fork, 0));
+        h->stream = h->aux_stream;
+        try {
+            getrf_rowmajor_cached<T>(h, W, ld, m, n, d_ipiv, d_info, d_moves, d_nmoves);
+        } catch (...) {
+            h->stream = nullptr;
+            throw;
+        }
+        h->stream = nullptr;
+        OXI_CUDA(cudaEventRecord(h->aux_join, h->aux_stream));
+        OXI_CUDA(cudaStreamWaitEvent(nullptr, h->aux_join, 0));
+        return;
+    }
+    auto &gc = h->gcache;
+    const uint64_t key[12] = {sizeof(T), (uint64_t)(uintptr_t)W, (uint64_t)ld, (uint64_t)m, (uint64_t)n,
+                              (uint64_t)(uintptr_t)d_ipiv, (uint64_t)(uintptr_t)d_info,
+                              (uint64_t)(uintptr_t)d_moves, (uint64_t)h->opt.blocksize,
+                              (uint64_t)h->opt.gemm | ((uint64_t)h->opt.trsm_leaf << 8) |
+                                  ((uint64_t)h->trailing << 16),
+                              (uint64_t)(uintptr_t)h->stream,
+                              (uint64_t)(uintptr_t)h->rowmap_ws.ptr ^ (uint64_t)(uintptr_t)h->tc_ws.ptr};
+    const bool usable = h->opt.graphs && !h->prof.enabled;
+    const bool same = gc.seen > 0 && std::memcmp(gc.key, key, sizeof(key)) == 0;
+    if (usable && same && gc.valid) {
+        OXI_CUDA(cudaGraphLaunch(gc.exec, h->stream));
+        return;
+    }
+    if (usable && same && gc.seen >= 1) {
+        // second occurrence: capture this run and keep it
+        gc.reset();
+        cudaStreamCaptureStatus st;
+        OXI_CUDA(cudaStreamIsCapturing(h->stream, &st));
+        if (st == cudaStreamCaptureStatusNone && h->stream != nullptr) {
+            OXI_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+            try {
+                getrf_rowmajor<T>(h, W, ld, m, n, d_ipiv, d_info, d_moves, d_nmoves);
+            } catch (...) {
+                cudaGraph_t g;
+                cudaStreamEndCapture(h->stream, &g);
+                if (g) cudaGraphDestroy(g);
+                throw;
+            }
+            OXI_CUDA(cudaStreamEndCapture(h->stream, &gc.graph));
+            OXI_CUDA(cudaGraphInstantiate(&gc.exec, gc.graph, 0));
+            std::memcpy(gc.key, key, sizeof(key));
+            gc.valid = true;
+            gc.seen = 2;
+            OXI_CUDA(cudaGraphLaunch(gc.exec, h->stream));
+            return;
+        }
+    }
+    // first occurrence (or graphs off): direct launches, remember the key
+    if (!same) {
+        gc.reset();
+        std::memcpy(gc.key, key, sizeof(key));
+    }
+    gc.seen = std::max(gc.seen, 1);
+    getrf_rowmajor<T>(h, W, ld, m, n, d_ipiv, d_info, d_moves, d_nmoves);
+}
+template void getrf_rowmajor_cached<double>(oxi_handle_s *, double *, i64, i64, i64, int64_t *, int64_t *, int *, int *);
+template void getrf_rowmajor_cached<float>(oxi_handle_s *, float *, i64, i64, i64, int64_t *, int64_t *, int *, int *);
+
 // Column-major in, column-major out: the C ABI wrapper shared by d/s.
 template <typename T>
 static int getrf_entry(oxi_handle_s *h, i64 m, i64 n, T *dA, i64 lda, int64_t *d_ipiv,
@@ -171,7 +248,7 @@ static int getrf_entry(oxi_handle_s *h, i64 m, i64 n, T *dA, i64 lda, int64_t *d
         int *d_moves = (int *)(sc + 128);
         OXI_CUDA(cudaMemsetAsync(d_info, 0, sizeof(int64_t), h->stream));
         launch_cm_to_rm<T, T>(dA, lda, W, ld, m, n, h->stream);
-        getrf_rowmajor<T>(h, W, ld, m, n, d_ipiv, d_info, d_moves, d_nmoves);
+        getrf_rowmajor_cached<T>(h, W, ld, m, n, d_ipiv, d_info, d_moves, d_nmoves);
         launch_rm_to_cm<T, T>(W, ld, dA, lda, m, n, h->stream);
         int64_t *hi = (int64_t *)h->host_ws.get(64);
         OXI_CUDA(cudaMemcpyAsync(hi, d_info, sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));

@@ -657,16 +657,143 @@ __global__ void k_trsm_leaf(const T *__restrict__ L, i64 ldl, T *__restrict__ B,
         if (i < t) B[(i64)i * ldb + c] = x[i];
 }
 
+// Column-oriented (right-looking) leaf for the tensor-core engine: once x_p is
+// final, x_i -= L_ip x_p for all i > p -- t-p independent FMAs per step instead
+// of one dependent chain per row.  One right-hand-side column per thread.
 template <typename T>
-void launch_trsm_leaf(const T *L, i64 ldl, T *B, i64 ldb, int t, i64 N, cudaStream_t s) {
+__global__ void k_trsm_leaf_col(const T *__restrict__ L, i64 ldl, T *__restrict__ B, i64 ldb, int t,
+                                i64 N) {
+    __shared__ T sL[32][33];
+    for (int e = threadIdx.x; e < t * t; e += blockDim.x) {
+        const int i = e / t, p = e - i * t;
+        sL[i][p] = L[(i64)i * ldl + p];
+    }
+    __syncthreads();
+    const i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= N) return;
+    T x[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i)
+        if (i < t) x[i] = B[(i64)i * ldb + c];
+#pragma unroll
+    for (int p = 0; p < 31; ++p) {
+        if (p + 1 < t) {
+            const T xp = x[p];
+#pragma unroll
+            for (int i = p + 1; i < 32; ++i)
+                if (i < t) x[i] = fma(-sL[i][p], xp, x[i]);
+        }
+    }
+#pragma unroll
+    for (int i = 1; i < 32; ++i)
+        if (i < t) B[(i64)i * ldb + c] = x[i];
+}
+
+template <typename T>
+void launch_trsm_leaf(const T *L, i64 ldl, T *B, i64 ldb, int t, i64 N, cudaStream_t s,
+                      bool ref_order) {
     if (t <= 1 || N <= 0) return;  // a unit 1x1 triangle is the identity
     const int nt = 128;
     ProfScope ps(KC_TRSM_LEAF, s, (double)t * t * N, 2.0 * (double)t * N * sizeof(T));
-    k_trsm_leaf<T><<<(unsigned)((N + nt - 1) / nt), nt, 0, s>>>(L, ldl, B, ldb, t, N);
+    if (ref_order) {
+        k_trsm_leaf<T><<<(unsigned)((N + nt - 1) / nt), nt, 0, s>>>(L, ldl, B, ldb, t, N);
+    } else {
+        k_trsm_leaf_col<T><<<(unsigned)((N + nt - 1) / nt), nt, 0, s>>>(L, ldl, B, ldb, t, N);
+    }
     OXI_LAUNCH_CHECK();
 }
-template void launch_trsm_leaf<double>(const double *, i64, double *, i64, int, i64, cudaStream_t);
-template void launch_trsm_leaf<float>(const float *, i64, float *, i64, int, i64, cudaStream_t);
+// ---------------------------------------------------------------------------
+// Fused blocked TRSM (tensor-core engine): B (t x N) <- L^-1 B for a unit lower
+// L with t <= 256, one CTA per 32-column strip of B kept in shared memory for
+// the whole solve.  Block row I: X_I -= sum_{J<I} L_IJ X_J (L blocks staged
+// through shared memory), then the 32 x 32 diagonal block by warp-shuffle
+// substitution (lane = row, one warp per 4 columns).  One launch replaces the
+// recursive halving's leaves and GEMMs.
+// ---------------------------------------------------------------------------
+constexpr int TF_TB = 32, TF_CW = 32, TF_TMAX = 256;
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_trsm_fused(const T *__restrict__ L, i64 ldl, T *__restrict__ B,
+                                                    i64 ldb, int t, i64 N) {
+    extern __shared__ __align__(16) unsigned char tf_smem[];
+    T(*X)[TF_CW + 1] = reinterpret_cast<T(*)[TF_CW + 1]>(tf_smem);
+    T(*Lb)[TF_TB + 1] = reinterpret_cast<T(*)[TF_TB + 1]>(tf_smem + sizeof(T) * TF_TMAX * (TF_CW + 1));
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const i64 c0 = (i64)blockIdx.x * TF_CW;
+    const int cols = (int)((N - c0) < TF_CW ? (N - c0) : TF_CW);
+    for (int e = tid; e < t * TF_CW; e += 256) {
+        const int i = e / TF_CW, c = e % TF_CW;
+        X[i][c] = (c < cols) ? B[(i64)i * ldb + c0 + c] : T(0);
+    }
+    __syncthreads();
+    const int nblk = (t + TF_TB - 1) / TF_TB;
+    const int r = tid >> 3, cq = (tid & 7) * 4;  // update mapping: row r, 4 columns
+    for (int I = 0; I < nblk; ++I) {
+        const int r0 = I * TF_TB, rows = min(TF_TB, t - r0);
+        if (I > 0) {
+            T acc[4] = {T(0), T(0), T(0), T(0)};
+            for (int J = 0; J < I; ++J) {
+                const int p0 = J * TF_TB;
+                for (int e = tid; e < TF_TB * TF_TB; e += 256) {
+                    const int rr = e / TF_TB, pp = e % TF_TB;
+                    Lb[rr][pp] = (rr < rows) ? L[(i64)(r0 + rr) * ldl + p0 + pp] : T(0);
+                }
+                __syncthreads();
+#pragma unroll 8
+                for (int p = 0; p < TF_TB; ++p) {
+                    const T l = Lb[r][p];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) acc[q] = fma(l, X[p0 + p][cq + q], acc[q]);
+                }
+                __syncthreads();
+            }
+            if (r < rows) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) X[r0 + r][cq + q] -= acc[q];
+            }
+        }
+        // diagonal block
+        for (int e = tid; e < TF_TB * TF_TB; e += 256) {
+            const int rr = e / TF_TB, pp = e % TF_TB;
+            Lb[rr][pp] = (rr < rows && pp < rows) ? L[(i64)(r0 + rr) * ldl + r0 + pp] : T(0);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int c = warp * 4 + q;
+            T x = (lane < rows) ? X[r0 + lane][c] : T(0);
+            for (int p = 0; p < rows - 1; ++p) {
+                const T xp = __shfl_sync(0xffffffffu, x, p);
+                if (lane > p) x = fma(-Lb[lane][p], xp, x);
+            }
+            if (lane < rows) X[r0 + lane][c] = x;
+        }
+        __syncthreads();
+    }
+    for (int e = tid; e < t * TF_CW; e += 256) {
+        const int i = e / TF_CW, c = e % TF_CW;
+        if (c < cols) B[(i64)i * ldb + c0 + c] = X[i][c];
+    }
+}
+
+template <typename T>
+void launch_trsm_fused(const T *L, i64 ldl, T *B, i64 ldb, int t, i64 N, cudaStream_t s) {
+    if (t <= 1 || N <= 0) return;
+    const size_t smem = sizeof(T) * ((size_t)TF_TMAX * (TF_CW + 1) + TF_TB * (TF_TB + 1));
+    static bool attr = false;
+    if (!attr) {
+        OXI_CUDA(cudaFuncSetAttribute(k_trsm_fused<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr = true;
+    }
+    ProfScope ps(KC_TRSM_LEAF, s, (double)t * t * N, 2.0 * (double)t * N * sizeof(T));
+    k_trsm_fused<T><<<(unsigned)((N + TF_CW - 1) / TF_CW), 256, smem, s>>>(L, ldl, B, ldb, t, N);
+    OXI_LAUNCH_CHECK();
+}
+template void launch_trsm_fused<double>(const double *, i64, double *, i64, int, i64, cudaStream_t);
+template void launch_trsm_fused<float>(const float *, i64, float *, i64, int, i64, cudaStream_t);
+
+template void launch_trsm_leaf<double>(const double *, i64, double *, i64, int, i64, cudaStream_t, bool);
+template void launch_trsm_leaf<float>(const float *, i64, float *, i64, int, i64, cudaStream_t, bool);
 
 // ---------------------------------------------------------------------------
 // Reference-order GEMM: C <- C - A*B, s_ij = sum_p fma(A_ip, B_pj, s) in p order
@@ -728,6 +855,109 @@ void launch_gemm_ref(T *C, i64 ldc, const T *A, i64 lda, const T *B, i64 ldb, i6
     k_gemm_ref<T><<<grid, 256, 0, s>>>(C, ldc, A, lda, B, ldb, M, N, K);
     OXI_LAUNCH_CHECK();
 }
+// ---------------------------------------------------------------------------
+// Register-blocked CUDA-core GEMM for the FP32 panel (C <- C - A*B, row-major):
+// 128 x BN tile, 16-deep k slabs double-buffered through registers, 8 x (BN/16)
+// outputs per thread (strided so shared-memory reads broadcast or are
+// conflict-free).
+// ---------------------------------------------------------------------------
+template <typename T, int BN>
+__global__ void __launch_bounds__(256) k_gemm_simt(T *__restrict__ C, i64 ldc, const T *__restrict__ A,
+                                                   i64 lda, const T *__restrict__ B, i64 ldb, i64 M,
+                                                   i64 N, i64 K) {
+    constexpr int BM = 128, BK = 16, TN = BN / 16;
+    __shared__ T As[2][BK][BM + 4];
+    __shared__ T Bs[2][BK][BN + 4];
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const i64 m0 = (i64)blockIdx.y * BM, n0 = (i64)blockIdx.x * BN;
+    T acc[8][TN];
+#pragma unroll
+    for (int a = 0; a < 8; ++a)
+#pragma unroll
+        for (int b = 0; b < TN; ++b) acc[a][b] = T(0);
+    constexpr int AL = BM * BK / 256, BL = BK * BN / 256;
+    T ra[AL], rb[BL];
+    auto gload = [&](i64 k0) {
+#pragma unroll
+        for (int q = 0; q < AL; ++q) {
+            const int e = threadIdx.x + q * 256;
+            const int r = e / BK, kk = e % BK;
+            const i64 gi = m0 + r, gk = k0 + kk;
+            ra[q] = (gi < M && gk < K) ? A[gi * lda + gk] : T(0);
+        }
+#pragma unroll
+        for (int q = 0; q < BL; ++q) {
+            const int e = threadIdx.x + q * 256;
+            const int kr = e / BN, cc = e % BN;
+            const i64 gk = k0 + kr, gj = n0 + cc;
+            rb[q] = (gk < K && gj < N) ? B[gk * ldb + gj] : T(0);
+        }
+    };
+    auto sstore = [&](int buf) {
+#pragma unroll
+        for (int q = 0; q < AL; ++q) {
+            const int e = threadIdx.x + q * 256;
+            As[buf][e % BK][e / BK] = ra[q];
+        }
+#pragma unroll
+        for (int q = 0; q < BL; ++q) {
+            const int e = threadIdx.x + q * 256;
+            Bs[buf][e / BN][e % BN] = rb[q];
+        }
+    };
+    gload(0);
+    sstore(0);
+    __syncthreads();
+    int buf = 0;
+    for (i64 k0 = 0; k0 < K; k0 += BK) {
+        const bool more = k0 + BK < K;
+        if (more) gload(k0 + BK);
+#pragma unroll
+        for (int p = 0; p < BK; ++p) {
+            T a[8], b[TN];
+#pragma unroll
+            for (int x = 0; x < 8; ++x) a[x] = As[buf][p][ty + 16 * x];
+#pragma unroll
+            for (int y = 0; y < TN; ++y) b[y] = Bs[buf][p][tx + 16 * y];
+#pragma unroll
+            for (int x = 0; x < 8; ++x)
+#pragma unroll
+                for (int y = 0; y < TN; ++y) acc[x][y] = fma(a[x], b[y], acc[x][y]);
+        }
+        if (more) {
+            sstore(buf ^ 1);
+            __syncthreads();
+            buf ^= 1;
+        }
+    }
+#pragma unroll
+    for (int x = 0; x < 8; ++x) {
+        const i64 gi = m0 + ty + 16 * x;
+        if (gi >= M) continue;
+#pragma unroll
+        for (int y = 0; y < TN; ++y) {
+            const i64 gj = n0 + tx + 16 * y;
+            if (gj < N) C[gi * ldc + gj] -= acc[x][y];
+        }
+    }
+}
+
+template <typename T>
+void launch_gemm_simt(T *C, i64 ldc, const T *A, i64 lda, const T *B, i64 ldb, i64 M, i64 N, i64 K,
+                      cudaStream_t s) {
+    if (M <= 0 || N <= 0 || K <= 0) return;
+    ProfScope ps(KC_GEMM_REF, s, 2.0 * M * N * K, (double)sizeof(T) * (2.0 * M * N + M * K + K * N));
+    if (N <= 64) {
+        dim3 grid((unsigned)((N + 63) / 64), (unsigned)((M + 127) / 128));
+        k_gemm_simt<T, 64><<<grid, 256, 0, s>>>(C, ldc, A, lda, B, ldb, M, N, K);
+    } else {
+        dim3 grid((unsigned)((N + 127) / 128), (unsigned)((M + 127) / 128));
+        k_gemm_simt<T, 128><<<grid, 256, 0, s>>>(C, ldc, A, lda, B, ldb, M, N, K);
+    }
+    OXI_LAUNCH_CHECK();
+}
+template void launch_gemm_simt<float>(float *, i64, const float *, i64, const float *, i64, i64, i64, i64, cudaStream_t);
+
 template void launch_gemm_ref<double>(double *, i64, const double *, i64, const double *, i64, i64, i64, i64, cudaStream_t);
 template void launch_gemm_ref<float>(float *, i64, const float *, i64, const float *, i64, i64, i64, i64, cudaStream_t);
 

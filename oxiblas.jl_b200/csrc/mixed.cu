@@ -26,7 +26,7 @@
 namespace oxi {
 
 namespace {
-constexpr int RS = 8;        // column chunks of the split residual / GEMV
+constexpr int RS = 16;       // column chunks of the split residual / GEMV
 constexpr int NRMAX = 4;     // right-hand sides per residual pass
 inline i64 rup(i64 x, i64 a) { return (x + a - 1) / a * a; }
 }  // namespace
@@ -145,9 +145,9 @@ __global__ void k_resid_part(const double *__restrict__ A, i64 lda, int n, const
 #pragma unroll
     for (int k = 0; k < NR; ++k) { ax[k] = 0.0; den[k] = 0.0; }
     const double *a = A + i;
-#pragma unroll 4
+#pragma unroll 16
     for (int j = j0; j < j1; ++j) {
-        const double v = a[(i64)j * lda];
+        const double v = __ldcs(&a[(i64)j * lda]);
 #pragma unroll
         for (int k = 0; k < NR; ++k) {
             if (k < nr) {
@@ -631,7 +631,7 @@ static int dgesv_mixed(oxi_handle_s *h, int prec, int refine, i64 n, i64 nrhs, c
             h->opt.blocksize = h->opt.mixed_blocksize;
             h->trailing = prec;
             try {
-                getrf_rowmajor<float>(h, W, ldw, n, n, M.ipiv, d_info, d_moves, d_nmoves);
+                getrf_rowmajor_cached<float>(h, W, ldw, n, n, M.ipiv, d_info, d_moves, d_nmoves);
             } catch (...) {
                 h->opt.blocksize = saved_bs;
                 h->trailing = saved_tr;
@@ -644,7 +644,7 @@ static int dgesv_mixed(oxi_handle_s *h, int prec, int refine, i64 n, i64 nrhs, c
             M.W = W;
             k_equilibrated_rm<double><<<g, dim3(32, 8), 0, s>>>(dA, lda, W, ldw, (int)n, M.rows, M.cols);
             OXI_LAUNCH_CHECK();
-            getrf_rowmajor<double>(h, W, ldw, n, n, M.ipiv, d_info, d_moves, d_nmoves);
+            getrf_rowmajor_cached<double>(h, W, ldw, n, n, M.ipiv, d_info, d_moves, d_nmoves);
         }
         if (!fp64) {
             M.dinvL = ws + o_dinv;

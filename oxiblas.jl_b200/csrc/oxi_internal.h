@@ -88,6 +88,7 @@ struct Options {
     int lookahead = 0;
     i64 mixed_blocksize = 256;  // panel width of the mixed-precision factorization
     int stop_normwise = 0;      // IR stop test: 0 componentwise (reference), 1 normwise
+    int graphs = 1;             // replay repeated factorizations as CUDA graphs
     int gmres_restart = 30;
     double gmres_tol = 1e-4;    // inner relative tolerance of GMRES-IR
 };
@@ -115,6 +116,25 @@ struct oxi_handle_s {
     oxi::DeviceBuffer rowmap_ws; // per-panel row map and composite move list
     int trailing = 0;            // oxi::TrailingKind for getrf_rowmajor<float>
     oxi::Profiler prof;
+    cudaStream_t aux_stream = nullptr;      // capturable stream used when the caller's is legacy
+    cudaEvent_t aux_fork = nullptr, aux_join = nullptr;
+    // CUDA graph of the last factorization (replayed when the same shape and
+    // buffers come back)
+    struct GraphCache {
+        bool valid = false;
+        int seen = 0;
+        uint64_t key[12] = {};
+        cudaGraphExec_t exec = nullptr;
+        cudaGraph_t graph = nullptr;
+        void reset() {
+            if (exec) cudaGraphExecDestroy(exec);
+            if (graph) cudaGraphDestroy(graph);
+            exec = nullptr;
+            graph = nullptr;
+            valid = false;
+            seen = 0;
+        }
+    } gcache;
 };
 
 namespace oxi {
@@ -152,7 +172,15 @@ void launch_rowmoves_big(T *W, i64 ld, i64 r0, const int *list, const int *cnt, 
 
 // B (t x N, row-major) <- L^-1 B, L unit lower t x t (t <= 32), row-major.
 template <typename T>
-void launch_trsm_leaf(const T *L, i64 ldl, T *B, i64 ldb, int t, i64 N, cudaStream_t s);
+void launch_trsm_leaf(const T *L, i64 ldl, T *B, i64 ldb, int t, i64 N, cudaStream_t s,
+                      bool ref_order);
+// Fused blocked TRSM, unit lower L with t <= 256 (one launch).
+template <typename T>
+void launch_trsm_fused(const T *L, i64 ldl, T *B, i64 ldb, int t, i64 N, cudaStream_t s);
+// FP32 register-blocked CUDA-core GEMM (any summation order).
+template <typename T>
+void launch_gemm_simt(T *C, i64 ldc, const T *A, i64 lda, const T *B, i64 ldb, i64 M, i64 N, i64 K,
+                      cudaStream_t s);
 
 // C (M x N) <- C - A (M x K) * B (K x N), all row-major.  Reference order:
 // one FMA chain per output along k, then C - s.
@@ -174,6 +202,12 @@ void launch_cvt_transpose16(int fmt, const float *src, i64 lds, void *dst, i64 l
 // C -= A*B for the trailing update of an FP32 factorization in h->trailing precision.
 void gemm_trailing_f32(oxi_handle_s *h, float *C, i64 ldc, const float *A, i64 lda,
                        const float *B, i64 ldb, i64 M, i64 N, i64 K);
+
+// getrf_rowmajor through the handle's graph cache (same shape, buffers and
+// options: replay; second occurrence: capture; otherwise direct launches).
+template <typename T>
+void getrf_rowmajor_cached(oxi_handle_s *h, T *W, i64 ld, i64 m, i64 n, int64_t *d_ipiv,
+                           int64_t *d_info, int *d_moves, int *d_nmoves);
 
 // Host driver: blocked right-looking getrf on a row-major working matrix.
 template <typename T>
