@@ -85,12 +85,20 @@ static void panel_rec(LuRun<T> &R, i64 c0, i64 nc) {
     if (leafw == 0) throw CudaError{cudaErrorInvalidValue, "panel taller than the leaf capacity"};
     if (nc <= leafw) {
         OXI_CUDA(cudaMemsetAsync(R.nmoves, 0, sizeof(int), h->stream));
-        launch_leaf<T>(R.W + c0 * R.ld + c0, R.ld, mrows, (int)nc, c0, R.ipiv, R.info, R.moves,
-                       R.nmoves, leafw, h->stream);
-        if (R.map) {  // inside the panel now, outside it once per panel
-            launch_rowmoves<T>(R.W, R.ld, c0, R.moves, R.nmoves, R.pf, R.pl, c0, c0 + nc, h->stream);
-            launch_rowmap_apply(R.map, c0 - R.pf, R.moves, R.nmoves, h->stream);
+        if (R.map) {  // inside the panel by the leaf itself, outside it once per panel
+            LeafPanel pn;
+            pn.left_n = (int)(c0 - R.pf);
+            pn.nother = (int)((c0 - R.pf) + (R.pl - c0 - nc));
+            pn.pc_lo = (int)R.pf;
+            pn.right_lo = (int)(c0 + nc);
+            pn.leaf_c0 = (int)c0;
+            pn.map = R.map;
+            pn.map_off = (int)(c0 - R.pf);
+            launch_leaf<T>(R.W + c0 * R.ld + c0, R.ld, mrows, (int)nc, c0, R.ipiv, R.info, R.moves,
+                           R.nmoves, leafw, h->stream, pn);
         } else {
+            launch_leaf<T>(R.W + c0 * R.ld + c0, R.ld, mrows, (int)nc, c0, R.ipiv, R.info, R.moves,
+                           R.nmoves, leafw, h->stream);
             launch_rowmoves<T>(R.W, R.ld, c0, R.moves, R.nmoves, 0, R.ncols_moved, c0, c0 + nc,
                                h->stream);
         }

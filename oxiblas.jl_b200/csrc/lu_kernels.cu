@@ -140,11 +140,13 @@ __device__ __forceinline__ void warp_argmax(uint64_t &key, int &pos) {
 
 constexpr int LEAF_NT = 512;
 constexpr int LEAF_MAX_CS = 16;
+constexpr int LEAF_MOVE_ELEMS = 32;  // (moved rows x other panel columns) per thread, at most
 
 template <typename T, int W, int R>
 __global__ void __launch_bounds__(LEAF_NT, 1)
 k_leaf_lu(T *__restrict__ P, i64 ld, int m, int wact, i64 gofs, int64_t *__restrict__ ipiv,
-          int64_t *__restrict__ info, int *__restrict__ moves, int *__restrict__ nmoves) {
+          int64_t *__restrict__ info, int *__restrict__ moves, int *__restrict__ nmoves,
+          LeafPanel pn) {
     cg::cluster_group cl = cg::this_cluster();
     const int CS = (int)cl.num_blocks();
     const int cr = (int)cl.block_rank();
@@ -395,6 +397,48 @@ k_leaf_lu(T *__restrict__ P, i64 ld, int m, int wact, i64 gofs, int64_t *__restr
             }
         }
     }
+    if (pn.nother > 0 || pn.map) {
+        // The leaf's row interchanges on the panel's other columns, and on the
+        // panel row map, done here rather than by separate launches: read every
+        // moved row segment, meet at a cluster barrier, write.
+        __threadfence();
+        if (CS > 1) cl.sync(); else __syncthreads();
+        const int cnt = min(*(volatile int *)nmoves, 2 * W);
+        const int tot = cnt * pn.nother;
+        T vals[LEAF_MOVE_ELEMS];
+        int mapv[R];
+#pragma unroll
+        for (int q = 0; q < LEAF_MOVE_ELEMS; ++q) {
+            const int e = g + q * G;
+            if (e < tot) {
+                const int mv = e / pn.nother, oc = e - mv * pn.nother;
+                const int col = oc < pn.left_n ? pn.pc_lo + oc : pn.right_lo + (oc - pn.left_n);
+                const int src = __ldcg(&moves[2 * mv + 1]);
+                vals[q] = P[(i64)src * ld + (col - pn.leaf_c0)];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            const int i = k * G + g;
+            mapv[k] = (pn.map && i < m && id[k] != i) ? pn.map[pn.map_off + id[k]] : 0;
+        }
+        if (CS > 1) cl.sync(); else __syncthreads();
+#pragma unroll
+        for (int q = 0; q < LEAF_MOVE_ELEMS; ++q) {
+            const int e = g + q * G;
+            if (e < tot) {
+                const int mv = e / pn.nother, oc = e - mv * pn.nother;
+                const int col = oc < pn.left_n ? pn.pc_lo + oc : pn.right_lo + (oc - pn.left_n);
+                const int dst = __ldcg(&moves[2 * mv]);
+                P[(i64)dst * ld + (col - pn.leaf_c0)] = vals[q];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            const int i = k * G + g;
+            if (pn.map && i < m && id[k] != i) pn.map[pn.map_off + i] = mapv[k];
+        }
+    }
     // keep every CTA's shared memory alive until all remote pushes have landed
     if (CS > 1) cl.sync();
 }
@@ -418,7 +462,7 @@ template <> int leaf_width_for<float>(i64 m) {
 
 template <typename T, int W, int R>
 static void launch_leaf_wr(T *P, i64 ld, i64 m, int w, i64 gofs, int64_t *ipiv, int64_t *info,
-                           int *moves, int *nmoves, cudaStream_t s) {
+                           int *moves, int *nmoves, cudaStream_t s, LeafPanel pn) {
     const i64 per_cta = (i64)LEAF_NT * R;
     int need = (int)((m + per_cta - 1) / per_cta);
     int cs = 1;  // cluster sizes kept to powers of two
@@ -437,33 +481,35 @@ static void launch_leaf_wr(T *P, i64 ld, i64 m, int w, i64 gofs, int64_t *ipiv, 
     at[0].val.clusterDim.z = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
+    if ((i64)pn.nother * 2 * W > (i64)LEAF_MOVE_ELEMS * cs * LEAF_NT)
+        throw CudaError{cudaErrorInvalidValue, "panel too wide for the in-leaf row moves"};
     ProfScope ps(KC_LEAF, s, 0.0, 2.0 * (double)m * w * sizeof(T));
-    OXI_CUDA(cudaLaunchKernelEx(&cfg, kern, P, ld, (int)m, w, gofs, ipiv, info, moves, nmoves));
+    OXI_CUDA(cudaLaunchKernelEx(&cfg, kern, P, ld, (int)m, w, gofs, ipiv, info, moves, nmoves, pn));
     count_launch();
 }
 
 template <typename T>
 void launch_leaf(T *P, i64 ld, i64 m, int w, i64 gofs, int64_t *ipiv, int64_t *info, int *moves,
-                 int *nmoves, int leafw, cudaStream_t s) {
+                 int *nmoves, int leafw, cudaStream_t s, LeafPanel pn) {
     const i64 cap = (i64)LEAF_MAX_CS * LEAF_NT;
     if constexpr (sizeof(T) == 8) {
-        if (leafw == 32) launch_leaf_wr<T, 32, 1>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s);
-        else if (leafw == 16) launch_leaf_wr<T, 16, 2>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s);
-        else if (leafw == 8) launch_leaf_wr<T, 8, 4>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s);
-        else launch_leaf_wr<T, 4, 8>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s);
+        if (leafw == 32) launch_leaf_wr<T, 32, 1>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s, pn);
+        else if (leafw == 16) launch_leaf_wr<T, 16, 2>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s, pn);
+        else if (leafw == 8) launch_leaf_wr<T, 8, 4>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s, pn);
+        else launch_leaf_wr<T, 4, 8>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s, pn);
     } else {
         if (leafw == 32) {
-            if (m <= cap) launch_leaf_wr<T, 32, 1>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s);
-            else launch_leaf_wr<T, 32, 2>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s);
+            if (m <= cap) launch_leaf_wr<T, 32, 1>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s, pn);
+            else launch_leaf_wr<T, 32, 2>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s, pn);
         } else if (leafw == 16) {
-            launch_leaf_wr<T, 16, 4>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s);
+            launch_leaf_wr<T, 16, 4>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s, pn);
         } else {
-            launch_leaf_wr<T, 8, 8>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s);
+            launch_leaf_wr<T, 8, 8>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s, pn);
         }
     }
 }
-template void launch_leaf<double>(double *, i64, i64, int, i64, int64_t *, int64_t *, int *, int *, int, cudaStream_t);
-template void launch_leaf<float>(float *, i64, i64, int, i64, int64_t *, int64_t *, int *, int *, int, cudaStream_t);
+template void launch_leaf<double>(double *, i64, i64, int, i64, int64_t *, int64_t *, int *, int *, int, cudaStream_t, LeafPanel);
+template void launch_leaf<float>(float *, i64, i64, int, i64, int64_t *, int64_t *, int *, int *, int, cudaStream_t, LeafPanel);
 
 // ---------------------------------------------------------------------------
 // Row moves: W[r0 + dst][c] <- W[r0 + src][c] for every move, all sources read
@@ -712,12 +758,16 @@ void launch_trsm_leaf(const T *L, i64 ldl, T *B, i64 ldb, int t, i64 N, cudaStre
 // ---------------------------------------------------------------------------
 constexpr int TF_TB = 32, TF_CW = 32, TF_TMAX = 256;
 
+// Right-looking: for each 32-row block J, solve its 32 x 32 diagonal block by
+// warp-shuffle substitution (lane = row, one warp per 4 columns), then update all
+// rows below with that block's solution in one pass (L column block staged in
+// shared memory, 7 x 4 outputs per thread).
 template <typename T>
 __global__ void __launch_bounds__(256) k_trsm_fused(const T *__restrict__ L, i64 ldl, T *__restrict__ B,
                                                     i64 ldb, int t, i64 N) {
     extern __shared__ __align__(16) unsigned char tf_smem[];
     T(*X)[TF_CW + 1] = reinterpret_cast<T(*)[TF_CW + 1]>(tf_smem);
-    T(*Lb)[TF_TB + 1] = reinterpret_cast<T(*)[TF_TB + 1]>(tf_smem + sizeof(T) * TF_TMAX * (TF_CW + 1));
+    T(*Lc)[TF_TB + 1] = reinterpret_cast<T(*)[TF_TB + 1]>(tf_smem + sizeof(T) * TF_TMAX * (TF_CW + 1));
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const i64 c0 = (i64)blockIdx.x * TF_CW;
     const int cols = (int)((N - c0) < TF_CW ? (N - c0) : TF_CW);
@@ -725,48 +775,57 @@ __global__ void __launch_bounds__(256) k_trsm_fused(const T *__restrict__ L, i64
         const int i = e / TF_CW, c = e % TF_CW;
         X[i][c] = (c < cols) ? B[(i64)i * ldb + c0 + c] : T(0);
     }
-    __syncthreads();
     const int nblk = (t + TF_TB - 1) / TF_TB;
-    const int r = tid >> 3, cq = (tid & 7) * 4;  // update mapping: row r, 4 columns
-    for (int I = 0; I < nblk; ++I) {
-        const int r0 = I * TF_TB, rows = min(TF_TB, t - r0);
-        if (I > 0) {
-            T acc[4] = {T(0), T(0), T(0), T(0)};
-            for (int J = 0; J < I; ++J) {
-                const int p0 = J * TF_TB;
-                for (int e = tid; e < TF_TB * TF_TB; e += 256) {
-                    const int rr = e / TF_TB, pp = e % TF_TB;
-                    Lb[rr][pp] = (rr < rows) ? L[(i64)(r0 + rr) * ldl + p0 + pp] : T(0);
-                }
-                __syncthreads();
-#pragma unroll 8
-                for (int p = 0; p < TF_TB; ++p) {
-                    const T l = Lb[r][p];
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) acc[q] = fma(l, X[p0 + p][cq + q], acc[q]);
-                }
-                __syncthreads();
-            }
-            if (r < rows) {
-#pragma unroll
-                for (int q = 0; q < 4; ++q) X[r0 + r][cq + q] -= acc[q];
-            }
-        }
-        // diagonal block
-        for (int e = tid; e < TF_TB * TF_TB; e += 256) {
+    const int cq = (tid & 7) * 4, rq = tid >> 3;  // update mapping: rows rq + 32 q, columns cq..cq+3
+    for (int J = 0; J < nblk; ++J) {
+        const int j0 = J * TF_TB, jrows = min(TF_TB, t - j0);
+        const int rb = j0 + jrows, nrem = t - rb;  // rows below the block
+        // stage L[j0.., j0..j0+31] (diagonal block first, then the rows below)
+        for (int e = tid; e < (t - j0) * TF_TB; e += 256) {
             const int rr = e / TF_TB, pp = e % TF_TB;
-            Lb[rr][pp] = (rr < rows && pp < rows) ? L[(i64)(r0 + rr) * ldl + r0 + pp] : T(0);
+            Lc[rr][pp] = (pp < jrows) ? L[(i64)(j0 + rr) * ldl + j0 + pp] : T(0);
         }
         __syncthreads();
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int c = warp * 4 + q;
-            T x = (lane < rows) ? X[r0 + lane][c] : T(0);
-            for (int p = 0; p < rows - 1; ++p) {
+            T x = (lane < jrows) ? X[j0 + lane][c] : T(0);
+            for (int p = 0; p < jrows - 1; ++p) {
                 const T xp = __shfl_sync(0xffffffffu, x, p);
-                if (lane > p) x = fma(-Lb[lane][p], xp, x);
+                if (lane > p) x = fma(-Lc[lane][p], xp, x);
             }
-            if (lane < rows) X[r0 + lane][c] = x;
+            if (lane < jrows) X[j0 + lane][c] = x;
+        }
+        __syncthreads();
+        if (nrem > 0) {
+            T acc[7][4];
+#pragma unroll
+            for (int q = 0; q < 7; ++q)
+#pragma unroll
+                for (int u = 0; u < 4; ++u) acc[q][u] = T(0);
+#pragma unroll 4
+            for (int p = 0; p < jrows; ++p) {
+                const T x0 = X[j0 + p][cq], x1 = X[j0 + p][cq + 1], x2 = X[j0 + p][cq + 2], x3 = X[j0 + p][cq + 3];
+#pragma unroll
+                for (int q = 0; q < 7; ++q) {
+                    const int r = rq + 32 * q;
+                    if (r < nrem) {
+                        const T l = Lc[TF_TB + r][p];
+                        acc[q][0] = fma(l, x0, acc[q][0]);
+                        acc[q][1] = fma(l, x1, acc[q][1]);
+                        acc[q][2] = fma(l, x2, acc[q][2]);
+                        acc[q][3] = fma(l, x3, acc[q][3]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 7; ++q) {
+                const int r = rq + 32 * q;
+                if (r < nrem) {
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) X[rb + r][cq + u] -= acc[q][u];
+                }
+            }
         }
         __syncthreads();
     }
@@ -779,7 +838,7 @@ __global__ void __launch_bounds__(256) k_trsm_fused(const T *__restrict__ L, i64
 template <typename T>
 void launch_trsm_fused(const T *L, i64 ldl, T *B, i64 ldb, int t, i64 N, cudaStream_t s) {
     if (t <= 1 || N <= 0) return;
-    const size_t smem = sizeof(T) * ((size_t)TF_TMAX * (TF_CW + 1) + TF_TB * (TF_TB + 1));
+    const size_t smem = sizeof(T) * ((size_t)TF_TMAX * (TF_CW + 1) + (size_t)TF_TMAX * (TF_TB + 1));
     static bool attr = false;
     if (!attr) {
         OXI_CUDA(cudaFuncSetAttribute(k_trsm_fused<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

@@ -133,36 +133,50 @@ __global__ void k_check_finite(const double *__restrict__ B, i64 ldb, int n, int
 // ---------------------------------------------------------------------------
 // FP64 residual R = B - A X (or product Y = A X) with the componentwise error
 // ---------------------------------------------------------------------------
+// Each thread owns two adjacent rows (one 16-byte load per column when the
+// column base is 16-byte aligned); columns split into RS chunks.
 template <int NR>
 __global__ void k_resid_part(const double *__restrict__ A, i64 lda, int n, const double *__restrict__ X,
                              i64 ldx, int nr, double *__restrict__ pax, double *__restrict__ pden) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
     const int s = blockIdx.y;
     if (i >= n) return;
     const int chunk = (n + RS - 1) / RS;
     const int j0 = s * chunk, j1 = min(n, j0 + chunk);
-    double ax[NR], den[NR];
+    const bool two = i + 1 < n;
+    const bool vec = two && ((lda & 1) == 0) && ((((uintptr_t)(A + i)) & 15) == 0);
+    double ax[2][NR], den[2][NR];
 #pragma unroll
-    for (int k = 0; k < NR; ++k) { ax[k] = 0.0; den[k] = 0.0; }
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int k = 0; k < NR; ++k) { ax[h][k] = 0.0; den[h][k] = 0.0; }
     const double *a = A + i;
-#pragma unroll 16
+#pragma unroll 8
     for (int j = j0; j < j1; ++j) {
-        const double v = __ldcs(&a[(i64)j * lda]);
+        double2 v;
+        if (vec) v = __ldcs((const double2 *)(a + (i64)j * lda));
+        else { v.x = a[(i64)j * lda]; v.y = two ? a[(i64)j * lda + 1] : 0.0; }
 #pragma unroll
         for (int k = 0; k < NR; ++k) {
             if (k < nr) {
                 const double x = __ldg(&X[j + (i64)k * ldx]);
-                ax[k] = fma(v, x, ax[k]);
-                den[k] = fma(fabs(v), fabs(x), den[k]);
+                ax[0][k] = fma(v.x, x, ax[0][k]);
+                ax[1][k] = fma(v.y, x, ax[1][k]);
+                den[0][k] = fma(fabs(v.x), fabs(x), den[0][k]);
+                den[1][k] = fma(fabs(v.y), fabs(x), den[1][k]);
             }
         }
     }
 #pragma unroll
-    for (int k = 0; k < NR; ++k)
-        if (k < nr) {
-            pax[((i64)s * NR + k) * n + i] = ax[k];
-            if (pden) pden[((i64)s * NR + k) * n + i] = den[k];
-        }
+    for (int h = 0; h < 2; ++h) {
+        if (h == 1 && !two) break;
+#pragma unroll
+        for (int k = 0; k < NR; ++k)
+            if (k < nr) {
+                pax[((i64)s * NR + k) * n + i + h] = ax[h][k];
+                if (pden) pden[((i64)s * NR + k) * n + i + h] = den[h][k];
+            }
+    }
 }
 
 // mode 0: R = B - sum(pax), errors into scal[k*4 + {0 cw, 1 rmax, 2 xmax, 3 bmax}], scal[64+k] += r^2
@@ -380,7 +394,7 @@ static void residual(MixedRun &M, const double *Xin, double *Rout, std::vector<d
     ProfScope ps(KC_RESIDUAL, s, 2.0 * (double)n * n * nrhs, 8.0 * (double)n * n);
     for (int k0 = 0; k0 < nrhs; k0 += NRMAX) {
         const int nr = std::min(NRMAX, nrhs - k0);
-        dim3 g1(blocks_for(n, 128), RS);
+        dim3 g1(blocks_for((n + 1) / 2, 128), RS);
         k_resid_part<NRMAX><<<g1, 128, 0, s>>>(M.A, M.lda, n, Xin + (i64)k0 * M.ldx, M.ldx, nr, M.pax, M.pden);
         OXI_LAUNCH_CHECK();
         dim3 g2(blocks_for(n), nr);
@@ -409,7 +423,7 @@ static void residual(MixedRun &M, const double *Xin, double *Rout, std::vector<d
 static void matvec(MixedRun &M, const double *x, double *y) {
     cudaStream_t s = M.s;
     const int n = (int)M.n;
-    dim3 g1(blocks_for(n, 128), RS);
+    dim3 g1(blocks_for((n + 1) / 2, 128), RS);
     k_resid_part<NRMAX><<<g1, 128, 0, s>>>(M.A, M.lda, n, x, n, 1, M.pax, nullptr);
     OXI_LAUNCH_CHECK();
     k_resid_final<<<dim3(blocks_for(n), 1), 256, 0, s>>>(nullptr, 0, y, n, nullptr, 0, n, 1, 0, M.pax,

@@ -150,9 +150,17 @@ void launch_rm_to_cm(const TS *W, i64 ldw, TD *A, i64 lda, i64 m, i64 n, cudaStr
 // Leaf LU of the row-major block P (m rows x w columns, ld), one thread-block
 // cluster.  Writes ipiv[gofs + j], *info (first zero pivot, global 1-based), and
 // the (dst, src) row-move list of the net permutation (positions relative to P).
+// In-leaf application of the leaf's row interchanges to the rest of its panel
+// (columns [pc_lo, pc_lo + left_n) and [right_lo, right_lo + nother - left_n),
+// absolute) and to the panel row map (map[map_off + position]); nother = 0 and
+// map = null switch it off.
+struct LeafPanel {
+    int nother = 0, left_n = 0, pc_lo = 0, right_lo = 0, leaf_c0 = 0, map_off = 0;
+    int *map = nullptr;
+};
 template <typename T>
 void launch_leaf(T *P, i64 ld, i64 m, int w, i64 gofs, int64_t *ipiv, int64_t *info,
-                 int *moves, int *nmoves, int leafw, cudaStream_t s);
+                 int *moves, int *nmoves, int leafw, cudaStream_t s, LeafPanel pn = LeafPanel());
 // Widest leaf width whose register capacity holds m rows.
 template <typename T> int leaf_width_for(i64 m);
 
