@@ -111,6 +111,9 @@ k_trsv2(const T *__restrict__ A, i64 lda, const T *__restrict__ Dinv, T *__restr
     }
 
     // ---- products with the other solved blocks (warps round-robin) ----
+    // 16-byte row loads only when every row start is 16-byte aligned (the
+    // caller's lda need not be even).
+    const bool vec_rows = ROWACC && ((lda * (i64)sizeof(T)) % 16 == 0) && ((((uintptr_t)A) & 15) == 0);
     T acc[2][NR];
 #pragma unroll
     for (int q = 0; q < 2; ++q)
@@ -149,7 +152,7 @@ k_trsv2(const T *__restrict__ A, i64 lda, const T *__restrict__ Dinv, T *__restr
             if (r >= rows) continue;
             if (ROWACC) {
                 const T *arow = A + (i64)(r0 + r) * lda + c0;
-                if (cols == SB) {
+                if (cols == SB && vec_rows) {
 #pragma unroll 16
                     for (int jj = 0; jj < SB; jj += 16 / (int)sizeof(T)) {
                         T av[16 / sizeof(T)];

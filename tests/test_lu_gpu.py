@@ -178,3 +178,20 @@ def test_float32_lu(pkg, oracle):
         b = rng.standard_normal(n).astype(np.float32)
         x = _np(F.solve(torch.from_numpy(b)))
         assert np.linalg.norm(A @ x - b) / (np.linalg.norm(A) * np.linalg.norm(x)) < 1e-5
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_transposed_solve_unaligned_leading_dimension(pkg, dtype):
+    """ldiv!(transpose(F), B) when lda * sizeof(T) is not a multiple of 16: the
+    transposed triangular solves read the factor along rows, so their row
+    starts are not 16-byte aligned (n = 331, 333 odd; n = 258 for FP32)."""
+    rng = np.random.default_rng(6)
+    for n in (258, 331, 333):
+        A = (rng.standard_normal((n, n)) + 4 * np.eye(n)).astype(dtype)
+        B = rng.standard_normal((n, 3)).astype(dtype)
+        F = pkg.lu(torch.from_numpy(A))
+        r = 1e-9 if dtype == np.float64 else 2e-3
+        ref64 = A.astype(np.float64)
+        for Fv, M in ((F, ref64), (F.T, ref64.T), (F.H, ref64.T)):
+            X = _np(pkg.ldiv(Fv, torch.from_numpy(B))).astype(np.float64)
+            assert np.allclose(X, np.linalg.solve(M, B.astype(np.float64)), rtol=r, atol=r), (n, dtype)
