@@ -32,7 +32,8 @@ enum oxi_status {
     OXI_ECUDA = 5,       /* CUDA runtime error                                        */
     OXI_ETIMEOUT = 6,    /* a bounded device-side wait expired                         */
     OXI_ENOMEM = 7,      /* workspace allocation failed                                */
-    OXI_ENOTCONVERGED = 8 /* refinement stopped at maxiter (report still filled)      */
+    OXI_ENOTCONVERGED = 8, /* refinement stopped at maxiter (report still filled)     */
+    OXI_ESCRATCH = 9       /* size beyond the fixed scratch of oxi_dgetrs_noalloc       */
 };
 
 typedef struct oxi_handle_s *oxi_handle_t;
@@ -94,6 +95,30 @@ int oxi_dgetrs(oxi_handle_t h, char trans, int64_t n, int64_t nrhs, const double
                int64_t lda, const int64_t *d_ipiv, double *dB, int64_t ldb);
 int oxi_sgetrs(oxi_handle_t h, char trans, int64_t n, int64_t nrhs, const float *dLU,
                int64_t lda, const int64_t *d_ipiv, float *dB, int64_t ldb);
+
+/* ---------------------------------------------------------------------------
+ * oxi_dgetrs_noalloc: oxi_dgetrs that allocates nothing.  It has no counterpart
+ * in the reference; it exists for callers that cannot allocate device memory
+ * at solve time (a process whose device memory is held by its own pool
+ * allocator, or a latency-bound loop that cudaFree's implicit device-wide
+ * synchronisation would stall).  Same arguments, results and status codes as
+ * oxi_dgetrs, but no handle: work runs on `stream` (cudaStream_t as void*,
+ * NULL = legacy default stream) of the current device.
+ * Its scratch (permutation, solve vector, control words) is one file-scope
+ * device array of OXI_NOALLOC_SCRATCH_BYTES per device.  Limits:
+ * n <= OXI_NOALLOC_MAX_N and n * nrhs <= OXI_NOALLOC_MAX_ELEMS, else
+ * OXI_ESCRATCH (nothing is launched).  The first call on a device resolves
+ * the array's address and loads the kernels it uses; make that first call
+ * before any stream capture.  Every call shares the array and leaves its
+ * contents behind: calls that overlap on the GPU (two streams, two host
+ * threads) race and must be serialised by the caller.  It calls no cudaMalloc,
+ * cudaFree or allocating library routine.  The call synchronises `stream`.
+ * ------------------------------------------------------------------------- */
+#define OXI_NOALLOC_SCRATCH_BYTES (8 << 20)
+#define OXI_NOALLOC_MAX_N 65536
+#define OXI_NOALLOC_MAX_ELEMS 917504 /* (8 MiB - 1 MiB) / sizeof(double) */
+int oxi_dgetrs_noalloc(void *stream, char trans, int64_t n, int64_t nrhs, const double *dLU,
+                       int64_t lda, const int64_t *d_ipiv, double *dB, int64_t ldb);
 
 /* ---------------------------------------------------------------------------
  * Trailing-update GEMM as a standalone kernel: C <- C - A*B (column-major),

@@ -16,6 +16,7 @@ LIB_PATH = os.path.join(HERE, "liboxiblas_b200.so")
 
 OXI_OK, OXI_EINVAL, OXI_ESINGULAR, OXI_ENONFINITE, OXI_EOVERFLOW = 0, 1, 2, 3, 4
 OXI_ECUDA, OXI_ETIMEOUT, OXI_ENOMEM, OXI_ENOTCONVERGED = 5, 6, 7, 8
+OXI_ESCRATCH = 9
 OPT_BLOCKSIZE, OPT_GEMM, OPT_TRSM_LEAF, OPT_LOOKAHEAD = 1, 2, 3, 4
 OPT_MIXED_BLOCKSIZE, OPT_STOP_NORMWISE, OPT_GMRES_RESTART = 5, 6, 7
 
@@ -57,6 +58,7 @@ _SIGS = {
     "oxi_sgetrf": ([_vp, _i64, _i64, _vp, _i64, _vp, ctypes.POINTER(_i64)], ctypes.c_int),
     "oxi_dgetrs": ([_vp, ctypes.c_char, _i64, _i64, _vp, _i64, _vp, _vp, _i64], ctypes.c_int),
     "oxi_sgetrs": ([_vp, ctypes.c_char, _i64, _i64, _vp, _i64, _vp, _vp, _i64], ctypes.c_int),
+    "oxi_dgetrs_noalloc": ([_vp, ctypes.c_char, _i64, _i64, _vp, _i64, _vp, _vp, _i64], ctypes.c_int),
     "oxi_dgemm_update": ([_vp, _i64, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64], ctypes.c_int),
     "oxi_sgemm_update_lowp": ([_vp, ctypes.c_int, _i64, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64],
                               ctypes.c_int),

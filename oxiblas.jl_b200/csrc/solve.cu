@@ -12,6 +12,7 @@
 // publishes its rows.  The factor is read once, coalesced: threads run along
 // the contiguous dimension of the factor (rows for L/U, columns for L^T/U^T).
 #include <atomic>
+#include <mutex>
 #include <vector>
 #include "oxi_internal.h"
 #include "tma_util.cuh"
@@ -516,7 +517,147 @@ static int getrs_entry(oxi_handle_s *h, char trans, i64 n, i64 nrhs, const T *dL
     }
 }
 
+// ---------------------------------------------------------------------------
+// No-allocation FP64 getrs.  Its scratch is one file-scope device array:
+//   [0, 4)        timeout word of the triangular solves (cleared every call)
+//   [4, 8)        invalid-pivot flag (cleared every call)
+//   [256, 4356)   tickets + per-block flags of k_trsv2 (cleared per launch)
+//   [8 KiB, +8n)  0-based permutation, int64 (written whole every call)
+//   [1 MiB, 8 MiB) the solve vector X, n x nrhs (written before it is read)
+constexpr i64 kNaScratchBytes = OXI_NOALLOC_SCRATCH_BYTES;
+constexpr i64 kNaCtlOff = 256, kNaPermOff = 8192, kNaXOff = 1 << 20;
+constexpr i64 kNaMaxN = OXI_NOALLOC_MAX_N;
+constexpr i64 kNaMaxElems = OXI_NOALLOC_MAX_ELEMS;
+static_assert(kNaMaxElems * (i64)sizeof(double) == kNaScratchBytes - kNaXOff, "X region");
+static_assert(kNaPermOff + 8 * kNaMaxN <= kNaXOff, "permutation region");
+static_assert(kNaCtlOff + 4 * (kNaMaxN / SB + 1) <= kNaPermOff, "control region");
+constexpr int kNaMaxDevices = 64;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaScratchBytes];
+
+// The interchange sequence folded into a permutation (as perm_from_ipiv) on the
+// device: all threads check the pivots and seed the identity, then one thread
+// applies the n swaps in shared memory (16-bit rows, n <= 65536), eight pivots
+// fetched ahead at a time.  An out-of-range pivot sets *bad and writes nothing.
+__global__ void __launch_bounds__(1024) k_perm_from_ipiv_na(const int64_t *__restrict__ ipiv, int n,
+                                                            int64_t *__restrict__ perm, int *__restrict__ bad) {
+    extern __shared__ uint16_t s_perm[];
+    int badl = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const int64_t p = ipiv[i];
+        badl |= (p < 1 || p > n);
+        s_perm[i] = (uint16_t)i;
+    }
+    if (__syncthreads_or(badl)) {
+        if (threadIdx.x == 0) *bad = 1;
+        return;
+    }
+    if (threadIdx.x == 0) {
+        for (int j0 = 0; j0 < n; j0 += 8) {
+            int p[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) p[u] = (j0 + u < n) ? (int)ipiv[j0 + u] - 1 : j0 + u;
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                if (j0 + u >= n) break;
+                const uint16_t a = s_perm[j0 + u], b = s_perm[p[u]];
+                s_perm[j0 + u] = b;
+                s_perm[p[u]] = a;
+            }
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) perm[i] = s_perm[i];
+}
+
+template <bool UPPER_A, bool UNIT, bool TRANS>
+static void na_load_trsv(cudaFuncAttributes *fa) {
+    constexpr bool LOWER = (UPPER_A == TRANS);
+    OXI_CUDA(cudaFuncGetAttributes(fa, k_trsv2<double, LOWER, UNIT, TRANS, 1, false>));
+    OXI_CUDA(cudaFuncGetAttributes(fa, k_trsv2<double, LOWER, UNIT, TRANS, 2, false>));
+    OXI_CUDA(cudaFuncGetAttributes(fa, k_trsv2<double, LOWER, UNIT, TRANS, 4, false>));
+}
+
+// Once per device, with that device current: the array's address, and the
+// kernels of this path loaded (so no later call loads a module).
+static char *noalloc_scratch(int dev) {
+    static std::atomic<char *> ptrs[kNaMaxDevices];
+    static std::mutex mu;
+    char *p = ptrs[dev].load(std::memory_order_acquire);
+    if (p) return p;
+    std::lock_guard<std::mutex> lk(mu);
+    p = ptrs[dev].load(std::memory_order_acquire);
+    if (p) return p;
+    void *sym = nullptr;
+    OXI_CUDA(cudaGetSymbolAddress(&sym, g_noalloc_scratch));
+    OXI_CUDA(cudaFuncSetAttribute(k_perm_from_ipiv_na, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(sizeof(uint16_t) * kNaMaxN)));
+    cudaFuncAttributes fa;
+    OXI_CUDA(cudaFuncGetAttributes(&fa, k_gather_rows<double>));
+    na_load_trsv<false, true, false>(&fa);
+    na_load_trsv<true, false, false>(&fa);
+    na_load_trsv<true, false, true>(&fa);
+    na_load_trsv<false, true, true>(&fa);
+    p = (char *)sym;
+    ptrs[dev].store(p, std::memory_order_release);
+    return p;
+}
+
+static int getrs_noalloc(cudaStream_t s, char trans, i64 n, i64 nrhs, const double *dLU, i64 lda,
+                         const int64_t *d_ipiv, double *dB, i64 ldb) {
+    if (trans == 'C') trans = 'T';
+    if (trans != 'N' && trans != 'T') return OXI_EINVAL;
+    if (n < 0 || nrhs < 0 || lda < std::max<i64>(1, n) || ldb < std::max<i64>(1, n)) return OXI_EINVAL;
+    if (n == 0 || nrhs == 0) return OXI_OK;
+    if (!dLU || !d_ipiv || !dB) return OXI_EINVAL;
+    if (n > kNaMaxN || nrhs > kNaMaxElems || n * nrhs > kNaMaxElems) return OXI_ESCRATCH;
+    try {
+        int dev = 0;
+        OXI_CUDA(cudaGetDevice(&dev));
+        if (dev < 0 || dev >= kNaMaxDevices) return OXI_EINVAL;
+        char *sc = noalloc_scratch(dev);
+        int *err = (int *)sc, *bad = err + 1, *ctl = (int *)(sc + kNaCtlOff);
+        int64_t *perm = (int64_t *)(sc + kNaPermOff);
+        double *X = (double *)(sc + kNaXOff);
+        int hflags[2] = {0, 0};
+        OXI_CUDA(cudaMemsetAsync(sc, 0, sizeof(hflags), s));
+        k_perm_from_ipiv_na<<<1, 1024, sizeof(uint16_t) * n, s>>>(d_ipiv, (int)n, perm, bad);
+        OXI_LAUNCH_CHECK();
+        OXI_CUDA(cudaMemcpyAsync(hflags, sc, sizeof(hflags), cudaMemcpyDeviceToHost, s));
+        OXI_CUDA(cudaStreamSynchronize(s));
+        if (hflags[1]) return OXI_EINVAL;  // B untouched, as oxi_dgetrs
+        const i64 tot = n * nrhs;
+        const int nt = 256;
+        const unsigned gb = (unsigned)((tot + nt - 1) / nt);
+        if (trans == 'N') {
+            k_gather_rows<double><<<gb, nt, 0, s>>>(dB, ldb, perm, X, n, (int)n, (int)nrhs, 0);
+            OXI_LAUNCH_CHECK();
+            trsv_launch<double, false, true, false>(dLU, lda, X, n, (int)n, (int)nrhs, ctl, err, s);
+            trsv_launch<double, true, false, false>(dLU, lda, X, n, (int)n, (int)nrhs, ctl, err, s);
+            OXI_CUDA(cudaMemcpy2DAsync(dB, ldb * sizeof(double), X, n * sizeof(double), n * sizeof(double),
+                                       nrhs, cudaMemcpyDeviceToDevice, s));
+        } else {
+            OXI_CUDA(cudaMemcpy2DAsync(X, n * sizeof(double), dB, ldb * sizeof(double), n * sizeof(double),
+                                       nrhs, cudaMemcpyDeviceToDevice, s));
+            trsv_launch<double, true, false, true>(dLU, lda, X, n, (int)n, (int)nrhs, ctl, err, s);
+            trsv_launch<double, false, true, true>(dLU, lda, X, n, (int)n, (int)nrhs, ctl, err, s);
+            k_gather_rows<double><<<gb, nt, 0, s>>>(X, n, perm, dB, ldb, (int)n, (int)nrhs, 1);
+            OXI_LAUNCH_CHECK();
+        }
+        OXI_CUDA(cudaMemcpyAsync(hflags, sc, sizeof(int), cudaMemcpyDeviceToHost, s));
+        OXI_CUDA(cudaStreamSynchronize(s));
+        return hflags[0] ? OXI_ETIMEOUT : OXI_OK;
+    } catch (const CudaError &) {
+        return OXI_ECUDA;
+    }
+}
+
 }  // namespace oxi
+
+extern "C" int oxi_dgetrs_noalloc(void *stream, char trans, int64_t n, int64_t nrhs, const double *dLU,
+                                  int64_t lda, const int64_t *d_ipiv, double *dB, int64_t ldb) {
+    return oxi::getrs_noalloc((cudaStream_t)stream, trans, n, nrhs, dLU, lda, d_ipiv, dB, ldb);
+}
 
 extern "C" int oxi_dgetrs(oxi_handle_t h, char trans, int64_t n, int64_t nrhs, const double *dLU,
                           int64_t lda, const int64_t *d_ipiv, double *dB, int64_t ldb) {
