@@ -1,6 +1,9 @@
 #!/usr/bin/env python
-"""Benchmark: n=16384 solve time, BF16-LU + FP64 iterative refinement vs plain
-FP64 LU, at equal (FP64-level) backward error, on one B200 per rank.
+"""Benchmark: n=16384 solve time, 16-bit tensor-core LU + FP64 iterative
+refinement vs plain FP64 LU, at equal (FP64-level) backward error, on one B200
+per rank.  The default low precision is split FP16 (fp16x3: power-of-two
+scaled FP16 operands, hi/lo split, three products per K on the tensor cores,
+FP32 panels); split BF16 (bf16x3) is timed beside it on the same system.
 
 One step = one solve of a seeded synthetic system A x = b with A = U diag(s) V^T
 (Haar U, V; s log-uniform on [1e-4, 1], kappa ~ 1e4; n = 16384, one right-hand
@@ -39,10 +42,15 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=16384)
     ap.add_argument("--kappa", type=float, default=1e4)
-    ap.add_argument("--prec", default="bf16x3", choices=["bf16x3", "bf16", "fp16", "fp32"])
+    ap.add_argument("--prec", default="fp16x3", choices=["fp16x3", "bf16x3", "bf16", "fp16", "fp32"])
     ap.add_argument("--refine", default="auto", choices=["ir", "gmres", "auto"])
     ap.add_argument("--tol", type=float, default=1e-14)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--workload", default="solve", choices=["solve", "batched", "adjoint"],
+                    help="solve: the headline n=16384 metric (default); batched: 4096 uneven small "
+                         "LU solves in one launch; adjoint: rrule of x = A \\ b at n=2048")
+    ap.add_argument("--count", type=int, default=4096, help="batched: number of problems")
+    ap.add_argument("--no-autotune", action="store_true", help="batched: keep the default tuning")
     return ap.parse_args()
 
 
@@ -304,6 +312,20 @@ def ours(args, ws, rank, local):
     st, rep = mixed_step()  # verification of the final state (untimed)
     ms_mixed = max_over_ranks(ws, tot_mixed / args.steps)
 
+    # ---- the split-BF16 variant, same system, for comparison ----
+    alt = {}
+    if args.prec != "bf16x3":
+        def bf_step():
+            return pkg.mixed_solve_device(Acm, Bcm, Xcm, n, 1, maxiter=30, rtol=args.tol, precision="bf16x3",
+                                          refine=args.refine, normwise=True)
+        for _ in range(2):
+            bf_step()
+        tot_bf, _ = timed(bf_step, max(1, min(args.steps, 3)))
+        st_bf, rep_bf = bf_step()
+        alt["bf16x3"] = {"ms": round(max_over_ranks(ws, tot_bf / max(1, min(args.steps, 3))), 3),
+                         "iterations": int(rep_bf.iterations), "converged": bool(rep_bf.converged)}
+        mixed_step()  # leave the default precision's answer in Xcm
+
     # ---- timed: plain FP64 ----
     ksteps_plain = max(1, min(args.steps, 3))
     tot_plain, per_plain = timed(plain_step, ksteps_plain)
@@ -415,6 +437,7 @@ def ours(args, ws, rank, local):
                        "refine_used": ("ir", "gmres", "auto")[rep.refine_used],
                        "factor_ms": round(rep.factor_ms, 3), "refine_ms": round(rep.refine_ms, 3)},
         "ms_per_step_each": [round(x, 3) for x in per_mixed],
+        "other_precisions": alt,
         "roofline": roofline, "kernel_time_shares": shares,
         "plain_fp64_kernel_ms": plain_shares, "plain_fp64_trailing_gemm_tflops": plain_gemm_tflops,
         "cpu_baseline": cpu,
@@ -427,12 +450,177 @@ def ours(args, ws, rank, local):
         print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# Secondary workloads (not the headline line): batched uneven LU, adjoint
+# ---------------------------------------------------------------------------
+def _timed_each(stream, fn, steps, pre=None):
+    import torch
+    out = []
+    for _ in range(steps):
+        if pre:
+            pre()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        out.append(e0.elapsed_time(e1))
+    return out
+
+
+def batched_workload(args, ws, rank, local):
+    """4096 independent FP64 systems, n ~ U{16..256}, A = N(0,1) + n I, 1..8 RHS:
+    FP32 factor + FP64 refinement (componentwise 1e-13) vs plain FP64, each one
+    persistent launch over all problems."""
+    import numpy as np
+    import torch
+    import __graft_entry__ as E
+    pkg = E.load_package()
+    dev = torch.device("cuda", local)
+    rng = np.random.default_rng(20261104 + rank)
+    count = args.count
+    orders = rng.integers(16, 257, size=count)
+    k = rng.integers(1, 9, size=count)
+    P = pkg.BatchedLU(orders, k, device=dev)
+    g = torch.Generator(device=dev).manual_seed(20261104 + rank)
+    P.poolA.normal_(generator=g)
+    P.poolB.normal_(generator=g)
+    diag = np.concatenate([P._offA[i] + np.arange(n) * (n + 1) for i, n in enumerate(orders)])
+    dshift = np.concatenate([np.full(n, float(n)) for n in orders])
+    P.poolA[torch.from_numpy(diag).to(dev)] += torch.from_numpy(dshift).to(dev)
+    A0, B0 = P.poolA.clone(), P.poolB.clone()
+    tune = None
+    if not args.no_autotune:
+        tune = {"fp32": pkg.batched_autotune(orders, "fp32", nrhs=4)[:2],
+                "fp64": pkg.batched_autotune(orders, "fp64", nrhs=4)[:2]}
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(args.warmup):
+        rep = P.gesv("fp32", maxiter=10, rtol=1e-13)
+    h = pkg.Handle.get()
+    h.reset_launches()
+    with Clocks(local) as ck:
+        t_mixed = _timed_each(stream, lambda: P.gesv("fp32", maxiter=10, rtol=1e-13), args.steps)
+    launches = h.launches() // max(1, args.steps)
+    clocks = ck.summary()
+    rep = P.gesv("fp32", maxiter=10, rtol=1e-13)
+
+    def restore():
+        P.poolA.copy_(A0)
+        P.poolB.copy_(B0)
+
+    for _ in range(max(1, args.warmup)):
+        restore()
+        P.gesv("fp64")
+    t_plain = _timed_each(stream, lambda: P.gesv("fp64"), args.steps, pre=restore)
+    ms_mixed = max_over_ranks(ws, statistics.median(t_mixed))
+    ms_plain = max_over_ranks(ws, statistics.median(t_plain))
+    flops = float(np.sum(2.0 / 3.0 * orders.astype(float) ** 3 + 2.0 * orders.astype(float) ** 2 * k))
+    # plain FP64: read A, write LU, read B, write X once (algorithmic bytes)
+    bytes_plain = float(np.sum(16.0 * orders.astype(float) ** 2 + 16.0 * orders * k))
+    # check a sample of the plain answers against the untouched copy
+    restore()
+    Bref = B0.clone()
+    P.gesv("fp64")
+    worst = 0.0
+    for i in range(0, count, max(1, count // 64)):
+        n, kk = int(orders[i]), int(k[i])
+        Ai = A0[P._offA[i]:P._offA[i] + n * n].view(n, n).t()
+        Bi = Bref[P._offB[i]:P._offB[i] + n * kk].view(kk, n).t()
+        Xi = P.B(i)
+        R = Bi - Ai @ Xi
+        den = Ai.abs() @ Xi.abs() + Bi.abs()
+        worst = max(worst, float((R.abs() / den).max()))
+    line = {
+        "metric": "batched uneven LU+solve time: 4096 FP64 systems, n~U{16..256}, 1-8 RHS",
+        "value": round(ms_mixed, 3), "unit": "ms", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms_mixed, 3), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": f"batched uneven LU, {count} problems, n~U{{16..256}}, N(0,1)+nI, "
+                               "nrhs~U{1..8}; one persistent graph-replayed launch",
+                   "l2": "pools (≈0.8 GB) larger than L2", "parallelism": f"replicas{ws}"},
+        "plain_fp64_ms": round(ms_plain, 3),
+        "speedup_vs_plain_fp64": round(ms_plain / ms_mixed, 3),
+        "tflops": {"mixed": round(flops / ms_mixed / 1e9, 3), "plain_fp64": round(flops / ms_plain / 1e9, 3)},
+        "plain_fp64_hbm_gbs": round(bytes_plain / ms_plain / 1e6, 1),
+        "refinement": {"max_iterations": int(rep["iterations"].max()),
+                       "mean_iterations": round(float(rep["iterations"].mean()), 3),
+                       "max_backward_error": float(rep["backward_error"].max())},
+        "plain_fp64_max_backward_error_sample": worst,
+        "tuning": tune, "gpu_launches_per_step": launches, "clocks": clocks,
+        "ms_each": {"mixed": [round(x, 3) for x in t_mixed], "plain_fp64": [round(x, 3) for x in t_plain]},
+    }
+    if not args.no_cpu and rank == 0 and ws == 1:
+        orc = E.load_oracle()
+        sample = list(range(0, count, 16))
+        An = A0.cpu().numpy()
+        Bn = B0.cpu().numpy()
+        t0 = time.perf_counter()
+        for i in sample:
+            n, kk = int(orders[i]), int(k[i])
+            Ai = An[P._offA[i]:P._offA[i] + n * n].reshape(n, n).T
+            Bi = Bn[P._offB[i]:P._offB[i] + n * kk].reshape(kk, n).T
+            F, ip, _ = orc.getrf(Ai, check=False)
+            orc.getrs(F, ip, Bi)
+        t_s = time.perf_counter() - t0
+        fs = float(np.sum(2.0 / 3.0 * orders[sample].astype(float) ** 3))
+        ft = float(np.sum(2.0 / 3.0 * orders.astype(float) ** 3))
+        line["cpu_baseline"] = {"value": round(t_s * ft / fs * 1e3, 1), "unit": "ms", "cores": orc.num_threads(),
+                                "kind": "port",
+                                "sample": f"oracle FP64 getrf+getrs on every 16th problem ({len(sample)}), "
+                                          "extrapolated by LU flops"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def adjoint_workload(args, ws, rank, local):
+    """rrule of x = A \\ b, n = 2048, kappa 1e3: pullback time with the stored factors."""
+    import torch
+    import __graft_entry__ as E
+    pkg = E.load_package()
+    dev = torch.device("cuda", local)
+    n = 2048
+    A = pkg.synthetic.kappa_matrix(n, 1e3, seed=4242 + rank, device=dev)
+    g = torch.Generator(device=dev).manual_seed(4243 + rank)
+    b = torch.randn(n, dtype=torch.float64, device=dev, generator=g)
+    F = pkg.lu(A)
+    x = F.solve(b)
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(args.warmup):
+        pkg.lu_adjoint(F, x, x)
+    t = _timed_each(stream, lambda: pkg.lu_adjoint(F, x, x), args.steps)
+
+    def fwd_bwd():
+        A1 = A.clone().requires_grad_()
+        xx = pkg.solve(A1, b)
+        (0.5 * (xx * xx).sum()).backward()
+
+    for _ in range(args.warmup):
+        fwd_bwd()
+    t2 = _timed_each(stream, fwd_bwd, args.steps)
+    ms = max_over_ranks(ws, statistics.median(t))
+    line = {"metric": "adjoint of x = A\\b (n=2048, kappa 1e3): pullback time with stored LU factors",
+            "value": round(ms, 4), "unit": "ms", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms, 4), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "rrule x = A\\b, n=2048, sigma log-uniform [1e-3, 1], loss 0.5||x||^2",
+                       "parallelism": f"replicas{ws}"},
+            "forward_plus_backward_ms": round(max_over_ranks(ws, statistics.median(t2)), 4),
+            "abar_write_gbs": round(8.0 * n * n / (ms / 1e3) / 1e9, 1)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     ws, rank, local = dist_setup(args)
     try:
         if args.impl == "reference":
             reference_arm(args, ws, rank)
+        elif args.workload == "batched":
+            batched_workload(args, ws, rank, local)
+        elif args.workload == "adjoint":
+            adjoint_workload(args, ws, rank, local)
         else:
             ours(args, ws, rank, local)
     finally:

@@ -121,6 +121,22 @@ int oxi_dgetrs_noalloc(void *stream, char trans, int64_t n, int64_t nrhs, const 
                        int64_t lda, const int64_t *d_ipiv, double *dB, int64_t ldb);
 
 /* ---------------------------------------------------------------------------
+ * Adjoint of X = A \ B (reverse-mode rule, e.g. a ChainRulesCore rrule or a
+ * torch.autograd.Function backward) with the factors of oxi_dgetrf reused:
+ *   Bbar = A^-T Xbar     (the transposed solve of ldiv!(transpose(F), B),
+ *                         src/api/linalg_api.jl:176-184; solve_transposed,
+ *                         src/lapack/expert_refinement.jl:2-23)
+ *   Abar = -Bbar X^T     (n x n, written in one pass)
+ * X, Xbar, Bbar: n x nrhs column-major; Bbar may be Xbar itself (same ldb),
+ * not X.  nrhs = 0 gives Abar = 0.  The reference has no differentiation rule;
+ * this entry point is the one its rrule would call.
+ * ------------------------------------------------------------------------- */
+int oxi_dlu_adjoint(oxi_handle_t h, int64_t n, int64_t nrhs, const double *dLU, int64_t lda,
+                    const int64_t *d_ipiv, const double *dX, int64_t ldx, const double *dXbar,
+                    int64_t ldxbar, double *dBbar, int64_t ldbbar, double *dAbar,
+                    int64_t ldabar);
+
+/* ---------------------------------------------------------------------------
  * Trailing-update GEMM as a standalone kernel: C <- C - A*B (column-major),
  * the gemm!(C, A, B, -1, 1) call of src/lapack/factorizations.jl:69
  * (src/blas/gemm.jl:635).
@@ -135,8 +151,9 @@ int oxi_dgemm_update(oxi_handle_t h, int64_t m, int64_t n, int64_t k, double *dC
  * (src/lapack/factorizations.jl:425-427, src/lapack/extended_lapack.jl:175-226).
  *   prec    OXI_PREC_BF16 / OXI_PREC_FP16: FP32 panels, trailing updates on the
  *           tensor cores with 16-bit operands and FP32 accumulation;
- *           OXI_PREC_BF16X3: the same with each operand split into two BF16
- *           terms and three products accumulated (one GEMM over 3K);
+ *           OXI_PREC_BF16X3 / OXI_PREC_FP16X3: the same with each operand split
+ *           into two BF16 (FP16, scaled) terms and three products accumulated
+ *           (one GEMM over 3K);
  *           OXI_PREC_FP32: FP32 throughout (the reference's default Low type);
  *           OXI_PREC_FP64: working-precision factor (lowtype=Float64).
  *   refine  OXI_REFINE_IR (classical, as the reference), OXI_REFINE_GMRES
@@ -155,7 +172,9 @@ enum oxi_precision {
     OXI_PREC_BF16 = 1,
     OXI_PREC_FP16 = 2,
     OXI_PREC_FP64 = 3,
-    OXI_PREC_BF16X3 = 4 /* split BF16: A_hi B_hi + A_hi B_lo + A_lo B_hi, BF16 operands */
+    OXI_PREC_BF16X3 = 4, /* split BF16: A_hi B_hi + A_hi B_lo + A_lo B_hi, BF16 operands */
+    OXI_PREC_FP16X3 = 5  /* split FP16, power-of-two scaled: the same three products with
+                            FP16 operands (about 22 significant bits instead of 16) */
 };
 enum oxi_refinement { OXI_REFINE_IR = 0, OXI_REFINE_GMRES = 1, OXI_REFINE_AUTO = 2 };
 enum oxi_reason {
@@ -183,7 +202,7 @@ typedef struct oxi_refine_report {
 
 /* The mixed path's trailing-update kernel as a standalone call: C <- C - A*B
  * (column-major FP32) with A and B rounded to prec (OXI_PREC_BF16 / _FP16 /
- * _BF16X3, FP16
+ * _BF16X3 / _FP16X3, FP16
  * with power-of-two operand scaling) and FP32 accumulation on the tensor cores
  * (tcgen05); OXI_PREC_FP32 runs the FP32 CUDA-core GEMM.  The low-precision
  * counterpart of gemm!(C, A, B, -1, 1) (src/blas/gemm.jl:635). */
@@ -193,6 +212,48 @@ int oxi_sgemm_update_lowp(oxi_handle_t h, int prec, int64_t m, int64_t n, int64_
 int oxi_dgesv_mixed(oxi_handle_t h, int prec, int refine, int64_t n, int64_t nrhs,
                     const double *dA, int64_t lda, const double *dB, int64_t ldb, double *dX,
                     int64_t ldx, int maxiter, double rtol, oxi_refine_report *out);
+
+/* ---------------------------------------------------------------------------
+ * Batched LU of many independent small matrices of uneven orders (1..256), in
+ * one persistent launch that takes matrices from a size-bucketed work queue
+ * (replayed as a CUDA graph when the same call repeats).  The reference
+ * factors one matrix per lu call (src/lapack/factorizations.jl:17-77); its
+ * batching pattern is gemm_batched! (src/blas/batched.jl:4-49), an outer loop
+ * over independent problems.  Per matrix the results are those of lu/ldiv!
+ * (pivots with the reference's rule, factors in place, LAPACK 1-based ipiv).
+ * All array arguments are DEVICE arrays of `count` entries; d_A[i] (column-
+ * major, leading dimension d_lda[i] >= n) etc. point to each problem.
+ * d_info[i]: 0, the first zero pivot (> 0), -1 for bad arguments of that
+ * problem, -2 for non-finite input (mixed).  The call synchronises once and
+ * returns OXI_EINVAL / OXI_ENONFINITE / OXI_ESINGULAR / OXI_ENOTCONVERGED if
+ * any problem had that outcome (d_info tells which), else OXI_OK.
+ * ------------------------------------------------------------------------- */
+int oxi_dgetrf_batched_uneven(oxi_handle_t h, int64_t count, const int32_t *d_n, double *const *d_A,
+                              const int64_t *d_lda, int64_t *const *d_ipiv, int32_t *d_info);
+/* Factor and solve (1..8 right-hand sides each, d_nrhs[i] <= 8):
+ *   prec OXI_PREC_FP64: plain FP64 LU in place (A -> factors, B -> X, as
+ *        LAPACK dgesv); d_X, d_ldx, d_iters, d_berr unused (may be NULL).
+ *   prec OXI_PREC_FP32: FP32 LU of the radix-equilibrated matrix plus FP64
+ *        iterative refinement (mixed_solve, src/lapack/extended_lapack.jl:
+ *        175-226) to componentwise backward error <= rtol or maxiter steps; A
+ *        and B are left intact, X receives the solution, d_iters / d_berr
+ *        (nullable) the steps and the final backward error per problem.
+ * d_ipiv (nullable; entries nullable): pivots of each factor. */
+int oxi_dgesv_batched_uneven(oxi_handle_t h, int prec, int64_t count, const int32_t *d_n,
+                             const int32_t *d_nrhs, double *const *d_A, const int64_t *d_lda,
+                             int64_t *const *d_ipiv, double *const *d_B, const int64_t *d_ldb,
+                             double *const *d_X, const int64_t *d_ldx, int32_t *d_info,
+                             int32_t *d_iters, double *d_berr, int maxiter, double rtol);
+/* Autotuner: times candidate panel widths per size bucket (orders 32b+1..32b+32)
+ * and shared-memory thresholds (orders up to n_smem keep the working matrix on
+ * chip) for prec (OXI_PREC_FP64 or OXI_PREC_FP32) on synthetic matrices
+ * (N(0,1) + n I) of the host-given orders h_n with nrhs right-hand sides, and
+ * keeps the fastest in the handle.  *best_ms (nullable): its time. */
+int oxi_batched_autotune(oxi_handle_t h, int prec, int64_t count, const int32_t *h_n, int32_t nrhs,
+                         double *best_ms);
+/* Current tuning (defaults when untuned) and explicit setting (a saved table). */
+int oxi_batched_get_tuning(oxi_handle_t h, int prec, int32_t *n_smem, int32_t *nb /* [8] */);
+int oxi_batched_set_tuning(oxi_handle_t h, int prec, int32_t n_smem, const int32_t *nb /* [8] */);
 
 /* ---------------------------------------------------------------------------
  * Engine instrumentation (no counterpart in the reference, whose benchmarks time

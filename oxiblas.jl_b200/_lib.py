@@ -59,6 +59,16 @@ _SIGS = {
     "oxi_dgetrs": ([_vp, ctypes.c_char, _i64, _i64, _vp, _i64, _vp, _vp, _i64], ctypes.c_int),
     "oxi_sgetrs": ([_vp, ctypes.c_char, _i64, _i64, _vp, _i64, _vp, _vp, _i64], ctypes.c_int),
     "oxi_dgetrs_noalloc": ([_vp, ctypes.c_char, _i64, _i64, _vp, _i64, _vp, _vp, _i64], ctypes.c_int),
+    "oxi_dlu_adjoint": ([_vp, _i64, _i64, _vp, _i64, _vp, _vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64],
+                        ctypes.c_int),
+    "oxi_dgetrf_batched_uneven": ([_vp, _i64, _vp, _vp, _vp, _vp, _vp], ctypes.c_int),
+    "oxi_dgesv_batched_uneven": ([_vp, ctypes.c_int, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                  _vp, _vp, ctypes.c_int, ctypes.c_double], ctypes.c_int),
+    "oxi_batched_autotune": ([_vp, ctypes.c_int, _i64, _vp, ctypes.c_int32, ctypes.POINTER(ctypes.c_double)],
+                             ctypes.c_int),
+    "oxi_batched_get_tuning": ([_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)],
+                               ctypes.c_int),
+    "oxi_batched_set_tuning": ([_vp, ctypes.c_int, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)], ctypes.c_int),
     "oxi_dgemm_update": ([_vp, _i64, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64], ctypes.c_int),
     "oxi_sgemm_update_lowp": ([_vp, ctypes.c_int, _i64, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64],
                               ctypes.c_int),

@@ -1,10 +1,24 @@
 // Handle life cycle, options, status strings, instrumentation and the
 // standalone GEMM entry points.
 #include <cstring>
+#include <mutex>
+#include <set>
+#include <tuple>
 #include "oxi_internal.h"
 
 namespace oxi {
 thread_local Profiler *t_prof = nullptr;
+
+void set_max_dyn_smem(const void *func, int bytes) {
+    static std::mutex mu;
+    static std::set<std::tuple<const void *, int, int>> done;
+    int dev = 0;
+    OXI_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(mu);
+    if (done.count(std::make_tuple(func, dev, bytes))) return;
+    OXI_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    done.insert(std::make_tuple(func, dev, bytes));
+}
 }
 
 extern "C" {
@@ -37,6 +51,9 @@ int oxi_destroy(oxi_handle_t h) {
     h->xtag_ws.release();
     h->rowmap_ws.release();
     h->gcache.reset();
+    h->bgraph.reset();
+    h->batch_ctl.release();
+    h->batch_wsp.release();
     if (h->aux_stream) cudaStreamDestroy(h->aux_stream);
     if (h->aux_fork) cudaEventDestroy(h->aux_fork);
     if (h->aux_join) cudaEventDestroy(h->aux_join);
@@ -102,7 +119,10 @@ int oxi_set_option(oxi_handle_t h, int option, int64_t value) {
             return OXI_OK;
         case OXI_OPT_GRAPHS:
             h->opt.graphs = value ? 1 : 0;
-            if (!value) h->gcache.reset();
+            if (!value) {
+                h->gcache.reset();
+                h->bgraph.reset();
+            }
             return OXI_OK;
         default: return OXI_EINVAL;
     }
@@ -145,7 +165,8 @@ int oxi_dgemm_update(oxi_handle_t h, int64_t m, int64_t n, int64_t k, double *dC
 int oxi_sgemm_update_lowp(oxi_handle_t h, int prec, int64_t m, int64_t n, int64_t k, float *dC,
                           int64_t ldc, const float *dA, int64_t lda, const float *dB, int64_t ldb) {
     if (!h || m < 0 || n < 0 || k < 0) return OXI_EINVAL;
-    if (prec != OXI_PREC_FP32 && prec != OXI_PREC_BF16 && prec != OXI_PREC_FP16 && prec != OXI_PREC_BF16X3)
+    if (prec != OXI_PREC_FP32 && prec != OXI_PREC_BF16 && prec != OXI_PREC_FP16 && prec != OXI_PREC_BF16X3 &&
+        prec != OXI_PREC_FP16X3)
         return OXI_EINVAL;
     if (m == 0 || n == 0 || k == 0) return OXI_OK;
     if (!dC || !dA || !dB || ldc < m || lda < m || ldb < k) return OXI_EINVAL;
@@ -153,7 +174,7 @@ int oxi_sgemm_update_lowp(oxi_handle_t h, int prec, int64_t m, int64_t n, int64_
     try {
         oxi::ProfGuard pg(&h->prof);
         OXI_CUDA(cudaSetDevice(h->device));
-        h->trailing = prec;  // OXI_PREC_{FP32,BF16,FP16,BF16X3} == TRAIL_{NATIVE,BF16,FP16,BF16X3}
+        h->trailing = prec;  // OXI_PREC_{FP32,BF16,FP16,BF16X3,FP16X3} == TRAIL_{NATIVE,...,FP16X3}
         if (prec == OXI_PREC_FP32)
             oxi::gemm_minus<float>(h, dC, ldc, dB, ldb, dA, lda, n, m, k);
         else
@@ -171,6 +192,7 @@ int oxi_sgemm_update_lowp(oxi_handle_t h, int prec, int64_t m, int64_t n, int64_
 int oxi_profile_enable(oxi_handle_t h, int on) {
     if (!h) return OXI_EINVAL;
     h->gcache.reset();  // profiled launches are recorded individually
+    h->bgraph.reset();
     cudaSetDevice(h->device);
     cudaStreamSynchronize(h->stream);
     h->prof.recycle();

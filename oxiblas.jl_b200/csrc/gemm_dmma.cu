@@ -194,12 +194,7 @@ void launch_gemm_dmma(double *C, i64 ldc, const double *A, i64 lda, const double
                  CU_TENSOR_MAP_SWIZZLE_128B);
     make_tmap_2d(&tmB, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, B, N, K, ldb, 8, BK,
                  CU_TENSOR_MAP_SWIZZLE_NONE);
-    static bool attr = false;
-    if (!attr) {
-        OXI_CUDA(cudaFuncSetAttribute(k_gemm_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      SMEM_BYTES));
-        attr = true;
-    }
+    set_max_dyn_smem((const void *)k_gemm_dmma, SMEM_BYTES);
     dim3 grid((unsigned)((N + BN - 1) / BN), (unsigned)((M + BM - 1) / BM));
     ProfScope ps(KC_GEMM_DMMA, s, 2.0 * M * N * K, 8.0 * (2.0 * M * N + M * K + K * N));
     k_gemm_dmma<<<grid, NTHREADS, SMEM_BYTES, s>>>(tmA, tmB, C, ldc, (int)M, (int)N, (int)K);

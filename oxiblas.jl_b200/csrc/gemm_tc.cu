@@ -300,26 +300,36 @@ __global__ void k_cvt_transpose(const float *__restrict__ src, i64 lds, H *__res
     }
 }
 
-// Split-BF16 operands: x = hi + lo with hi = bf16(x), lo = bf16(x - hi).  A row
-// becomes [hi | hi | lo] and a B row [hi | lo | hi] along K, so one GEMM over 3K
-// accumulates A_hi B_hi + A_hi B_lo + A_lo B_hi (the A_lo B_lo term, ~2^-16
-// relative, is dropped): FP32-level products from BF16 tensor-core operands.
-__global__ void k_cvt_rows_split3(const float *__restrict__ src, i64 lds, __nv_bfloat16 *__restrict__ dst,
-                                  i64 ldd, int rows, int cols) {
+// Split operands: x = hi + lo with hi = H(x s), lo = H(x s - hi) (s: the operand's
+// power-of-two scale, 1 for BF16).  A row becomes [hi | hi | lo] and a B row
+// [hi | lo | hi] along K, so one GEMM over 3K accumulates A_hi B_hi + A_hi B_lo
+// + A_lo B_hi; the dropped A_lo B_lo term is ~2^-16 (BF16) or ~2^-22 (FP16)
+// relative.  FP32-accumulated products from 16-bit tensor-core operands.
+template <typename H>
+__device__ __forceinline__ float from_half_t(H x);
+template <> __device__ __forceinline__ float from_half_t<__nv_bfloat16>(__nv_bfloat16 x) { return __bfloat162float(x); }
+template <> __device__ __forceinline__ float from_half_t<__half>(__half x) { return __half2float(x); }
+
+template <typename H>
+__global__ void k_cvt_rows_split3(const float *__restrict__ src, i64 lds, H *__restrict__ dst, i64 ldd, int rows,
+                                  int cols, float scale, const float *__restrict__ d_scale) {
+    const float sc = d_scale ? scale * (*d_scale) : scale;
     const i64 r = blockIdx.y;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < cols; c += gridDim.x * blockDim.x) {
-        const float x = src[r * lds + c];
-        const __nv_bfloat16 hi = __float2bfloat16_rn(x);
-        const __nv_bfloat16 lo = __float2bfloat16_rn(x - __bfloat162float(hi));
-        __nv_bfloat16 *d = dst + r * ldd;
+        const float x = src[r * lds + c] * sc;
+        const H hi = to_half_t<H>(x);
+        const H lo = to_half_t<H>(x - from_half_t<H>(hi));
+        H *d = dst + r * ldd;
         d[c] = hi;
         d[cols + c] = hi;
         d[2 * cols + c] = lo;
     }
 }
-__global__ void k_cvt_transpose_split3(const float *__restrict__ src, i64 lds, __nv_bfloat16 *__restrict__ dst,
-                                       i64 ldd, int rows, int cols) {
+template <typename H>
+__global__ void k_cvt_transpose_split3(const float *__restrict__ src, i64 lds, H *__restrict__ dst, i64 ldd,
+                                       int rows, int cols, float scale, const float *__restrict__ d_scale) {
     __shared__ float tile[32][33];
+    const float sc = d_scale ? scale * (*d_scale) : scale;
     const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
     const int tx = threadIdx.x, ty = threadIdx.y;
     for (int k = ty; k < 32; k += 8) {
@@ -330,10 +340,10 @@ __global__ void k_cvt_transpose_split3(const float *__restrict__ src, i64 lds, _
     for (int k = ty; k < 32; k += 8) {
         const int c = c0 + k, r = r0 + tx;  // dst row c (an N index), K position r
         if (c < cols && r < rows) {
-            const float x = tile[tx][k];
-            const __nv_bfloat16 hi = __float2bfloat16_rn(x);
-            const __nv_bfloat16 lo = __float2bfloat16_rn(x - __bfloat162float(hi));
-            __nv_bfloat16 *d = dst + (i64)c * ldd;
+            const float x = tile[tx][k] * sc;
+            const H hi = to_half_t<H>(x);
+            const H lo = to_half_t<H>(x - from_half_t<H>(hi));
+            H *d = dst + (i64)c * ldd;
             d[r] = hi;
             d[rows + r] = lo;
             d[2 * rows + r] = hi;
@@ -363,18 +373,10 @@ void launch_gemm_tc(int fmt /*0 fp16, 1 bf16*/, float *C, i64 ldc, const void *A
     dim3 grid((unsigned)std::min<i64>(tiles, sms));
     ProfScope ps(KC_GEMM_TC, s, 2.0 * M * N * K, 8.0 * M * N + 2.0 * (M + N) * K);
     if (fmt == 1) {
-        static bool attr = false;
-        if (!attr) {
-            OXI_CUDA(cudaFuncSetAttribute(k_gemm_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
-            attr = true;
-        }
+        set_max_dyn_smem((const void *)k_gemm_tc<1>, SMEM_BYTES);
         k_gemm_tc<1><<<grid, NTHREADS, SMEM_BYTES, s>>>(tmA, tmB, tmC, (int)M, (int)N, (int)K, scale, d_scale);
     } else {
-        static bool attr = false;
-        if (!attr) {
-            OXI_CUDA(cudaFuncSetAttribute(k_gemm_tc<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
-            attr = true;
-        }
+        set_max_dyn_smem((const void *)k_gemm_tc<0>, SMEM_BYTES);
         k_gemm_tc<0><<<grid, NTHREADS, SMEM_BYTES, s>>>(tmA, tmB, tmC, (int)M, (int)N, (int)K, scale, d_scale);
     }
     OXI_LAUNCH_CHECK();
@@ -442,25 +444,48 @@ void gemm_trailing_f32(oxi_handle_s *h, float *C, i64 ldc, const float *A, i64 l
         OXI_CUDA(cudaMemcpy2DAsync(C, ldc * 4, Cp, ldp * 4, N * 4, M, cudaMemcpyDeviceToDevice, h->stream));
         return;
     }
-    if (h->trailing == TRAIL_BF16X3) {
+    if (h->trailing == TRAIL_BF16X3 || h->trailing == TRAIL_FP16X3) {
+        const bool f16 = h->trailing == TRAIL_FP16X3;
         const i64 K3 = 3 * K, ldk3 = (K3 + 7) / 8 * 8;
         char *ws = (char *)h->tc_ws.get((size_t)(M + N) * ldk3 * 2 + 1024);
-        __nv_bfloat16 *A16 = (__nv_bfloat16 *)ws;
-        __nv_bfloat16 *B16 = (__nv_bfloat16 *)(((uintptr_t)(ws + (size_t)M * ldk3 * 2) + 255) & ~uintptr_t(255));
+        void *A16 = ws;
+        void *B16 = (void *)(((uintptr_t)(ws + (size_t)M * ldk3 * 2) + 255) & ~uintptr_t(255));
         cudaStream_t s = h->stream;
+        float *scal = nullptr;
+        if (f16) {  // the FP16 operand scales (see k_fp16_scales)
+            scal = (float *)((char *)h->scratch.get(kScratchBytes) + kScratchScalOff + 1536);
+            unsigned int *umax = (unsigned int *)(scal + 4);
+            OXI_CUDA(cudaMemsetAsync(umax, 0, sizeof(unsigned int), s));
+            k_absmax_f32<<<dim3((unsigned)std::min<i64>((N + 255) / 256, 16), (unsigned)K), 256, 0, s>>>(
+                B, ldb, (int)K, (int)N, umax);
+            OXI_LAUNCH_CHECK();
+            k_fp16_scales<<<1, 1, 0, s>>>(umax, scal);
+            OXI_LAUNCH_CHECK();
+        }
         {
             ProfScope ps(KC_CONVERT, s, 0.0, 10.0 * (double)M * K);
             dim3 g((unsigned)std::min<i64>((K + 255) / 256, 64), (unsigned)M);
-            k_cvt_rows_split3<<<g, 256, 0, s>>>(A, lda, A16, ldk3, (int)M, (int)K);
+            if (f16)
+                k_cvt_rows_split3<__half><<<g, 256, 0, s>>>(A, lda, (__half *)A16, ldk3, (int)M, (int)K, 16384.f,
+                                                            nullptr);
+            else
+                k_cvt_rows_split3<__nv_bfloat16><<<g, 256, 0, s>>>(A, lda, (__nv_bfloat16 *)A16, ldk3, (int)M,
+                                                                   (int)K, 1.f, nullptr);
             OXI_LAUNCH_CHECK();
         }
         {
             ProfScope ps(KC_CONVERT, s, 0.0, 10.0 * (double)N * K);
             dim3 g((unsigned)((N + 31) / 32), (unsigned)((K + 31) / 32));
-            k_cvt_transpose_split3<<<g, dim3(32, 8), 0, s>>>(B, ldb, B16, ldk3, (int)K, (int)N);
+            if (f16)
+                k_cvt_transpose_split3<__half><<<g, dim3(32, 8), 0, s>>>(B, ldb, (__half *)B16, ldk3, (int)K,
+                                                                         (int)N, 1.f, scal);
+            else
+                k_cvt_transpose_split3<__nv_bfloat16><<<g, dim3(32, 8), 0, s>>>(B, ldb, (__nv_bfloat16 *)B16, ldk3,
+                                                                                (int)K, (int)N, 1.f, nullptr);
             OXI_LAUNCH_CHECK();
         }
-        launch_gemm_tc(1, C, ldc, A16, ldk3, B16, ldk3, M, N, K3, 1.f, nullptr, s);
+        if (f16) launch_gemm_tc(0, C, ldc, A16, ldk3, B16, ldk3, M, N, K3, 1.f, scal + 1, s);
+        else launch_gemm_tc(1, C, ldc, A16, ldk3, B16, ldk3, M, N, K3, 1.f, nullptr, s);
         return;
     }
     const int fmt = (h->trailing == TRAIL_BF16) ? 1 : 0;

@@ -654,13 +654,15 @@ void launch_rowmoves_big(T *W, i64 ld, i64 r0, const int *list, const int *cnt, 
     int cpc = vec ? 16 * V : 64;
     while (cpc > V && (size_t)maxcnt * cpc * sizeof(T) > 160 * 1024) cpc /= 2;
     const size_t smem = (size_t)maxcnt * cpc * sizeof(T);
+    constexpr int kMaxSmem = 200 * 1024;  // the kernel's one limit (see set_max_dyn_smem)
+    if (smem > (size_t)kMaxSmem) throw CudaError{cudaErrorInvalidValue, "panel too wide for the row moves"};
     ProfScope ps(KC_ROWMOVES, s, 0.0, 2.0 * maxcnt * (double)(c_hi - c_lo) * sizeof(T));
     const i64 blocks = (c_hi - c_lo + cpc - 1) / cpc;
     if (vec) {
-        OXI_CUDA(cudaFuncSetAttribute(k_rowmoves_big<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        set_max_dyn_smem((const void *)k_rowmoves_big<T, true>, kMaxSmem);
         k_rowmoves_big<T, true><<<(unsigned)blocks, 256, smem, s>>>(W, ld, r0, list, cnt, maxcnt, c_lo, c_hi, cpc);
     } else {
-        OXI_CUDA(cudaFuncSetAttribute(k_rowmoves_big<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        set_max_dyn_smem((const void *)k_rowmoves_big<T, false>, kMaxSmem);
         k_rowmoves_big<T, false><<<(unsigned)blocks, 256, smem, s>>>(W, ld, r0, list, cnt, maxcnt, c_lo, c_hi, cpc);
     }
     OXI_LAUNCH_CHECK();
@@ -839,11 +841,7 @@ template <typename T>
 void launch_trsm_fused(const T *L, i64 ldl, T *B, i64 ldb, int t, i64 N, cudaStream_t s) {
     if (t <= 1 || N <= 0) return;
     const size_t smem = sizeof(T) * ((size_t)TF_TMAX * (TF_CW + 1) + (size_t)TF_TMAX * (TF_TB + 1));
-    static bool attr = false;
-    if (!attr) {
-        OXI_CUDA(cudaFuncSetAttribute(k_trsm_fused<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr = true;
-    }
+    set_max_dyn_smem((const void *)k_trsm_fused<T>, (int)smem);
     ProfScope ps(KC_TRSM_LEAF, s, (double)t * t * N, 2.0 * (double)t * N * sizeof(T));
     k_trsm_fused<T><<<(unsigned)((N + TF_CW - 1) / TF_CW), 256, smem, s>>>(L, ldl, B, ldb, t, N);
     OXI_LAUNCH_CHECK();

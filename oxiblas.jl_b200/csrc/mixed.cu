@@ -21,6 +21,7 @@
 #include <cmath>
 #include <vector>
 #include "oxi_internal.h"
+#include "scaling.cuh"
 #include "tma_util.cuh"
 
 namespace oxi {
@@ -30,17 +31,6 @@ constexpr int RS = 16;       // column chunks of the split residual / GEMV
 constexpr int NRMAX = 4;     // right-hand sides per residual pass
 inline i64 rup(i64 x, i64 a) { return (x + a - 1) / a * a; }
 }  // namespace
-
-// 2^round(log2 v) clamped to Float64's exponent range (equilibrate's radix
-// scale).  log2 v = e + log2 f with v = f 2^e, f in [0.5, 1): it rounds to e
-// exactly when f >= 2^-1/2 (an irrational bound, so no ties arise).
-__device__ __forceinline__ double radix_scale(double v) {
-    int e;
-    const double f = frexp(v, &e);
-    int r = (f >= 0.70710678118654757) ? e : e - 1;
-    r = max(-1022, min(1023, r));
-    return ldexp(1.0, r);
-}
 
 __device__ __forceinline__ void atomic_max_nonneg(double *addr, double v) {
     // non-negative doubles order like their bit patterns; NaN is mapped to +Inf
@@ -245,14 +235,6 @@ __global__ void k_scaled_absmax(const double *__restrict__ R, i64 ldr, int n, in
     if (!isfinite(mx)) mx = INFINITY;
     for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
     if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&mag[k], mx);
-}
-
-// power of two 2^exponent(m) (Julia's exponent: floor(log2 m)), 0 for m == 0
-__device__ __forceinline__ double binary_scale(double m) {
-    if (m == 0.0) return 0.0;
-    int e;
-    frexp(m, &e);
-    return ldexp(1.0, e - 1);
 }
 
 // low[i, k] = T((R[perm[i], k] / rows[perm[i]]) / mag_k): scale, round, permute
@@ -779,7 +761,7 @@ extern "C" int oxi_dgesv_mixed(oxi_handle_t h, int prec, int refine, int64_t n, 
     if (!h) return OXI_EINVAL;
     if (out) *out = oxi_refine_report{};
     if (n < 0 || nrhs < 0 || maxiter < 0 || !(rtol >= 0) || !std::isfinite(rtol)) return OXI_EINVAL;
-    if (prec < OXI_PREC_FP32 || prec > OXI_PREC_BF16X3 || refine < 0 || refine > OXI_REFINE_AUTO)
+    if (prec < OXI_PREC_FP32 || prec > OXI_PREC_FP16X3 || refine < 0 || refine > OXI_REFINE_AUTO)
         return OXI_EINVAL;
     if (n == 0 || nrhs == 0) return OXI_OK;
     if (!dA || !dB || !dX || lda < n || ldb < n || ldx < n || nrhs > 16) return OXI_EINVAL;

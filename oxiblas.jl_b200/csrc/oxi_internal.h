@@ -94,7 +94,7 @@ struct Options {
 };
 
 // Precision of the trailing update inside an FP32 factorization.
-enum TrailingKind { TRAIL_NATIVE = 0, TRAIL_BF16 = 1, TRAIL_FP16 = 2, TRAIL_BF16X3 = 4 };
+enum TrailingKind { TRAIL_NATIVE = 0, TRAIL_BF16 = 1, TRAIL_FP16 = 2, TRAIL_BF16X3 = 4, TRAIL_FP16X3 = 5 };
 
 }  // namespace oxi
 
@@ -135,9 +135,36 @@ struct oxi_handle_s {
             seen = 0;
         }
     } gcache;
+    // batched small LU: tuning per mode (0 FP64, 1 FP32 factor + FP64 refinement),
+    // queue/status block, per-CTA FP32 working matrices, graph of the last call
+    struct BatchTune {
+        bool tuned = false;
+        int n_smem = 0;
+        int nb[8] = {};
+    } btune[2];
+    oxi::DeviceBuffer batch_ctl, batch_wsp;
+    struct BatchGraph {
+        std::vector<uint64_t> key;
+        int seen = 0;
+        cudaGraphExec_t exec = nullptr;
+        cudaGraph_t graph = nullptr;
+        void reset() {
+            if (exec) cudaGraphExecDestroy(exec);
+            if (graph) cudaGraphDestroy(graph);
+            exec = nullptr;
+            graph = nullptr;
+            seen = 0;
+            key.clear();
+        }
+    } bgraph;
 };
 
 namespace oxi {
+
+// Raise a kernel's dynamic shared-memory limit to `bytes`, once per device
+// (the attribute belongs to the device's context).  A kernel keeps ONE limit,
+// its largest use, so launches captured in a CUDA graph never see it lowered.
+void set_max_dyn_smem(const void *func, int bytes);
 
 // ---- kernels launched by the drivers (defined in lu_kernels.cu / gemm_*.cu) ----
 

@@ -6,6 +6,7 @@ src/lapack/extended_lapack.jl:175-226).
 precision : "fp32" (the reference's default Low = Float32), "bf16" / "fp16"
             (FP32 panels, tensor-core trailing updates with 16-bit operands),
             "bf16x3" (split-BF16 operands, three products accumulated in FP32),
+            "fp16x3" (split-FP16 operands, power-of-two scaled, the same three products),
             "fp64" (working-precision factor).
 refine    : "ir" (classical, the reference's loop), "gmres" (GMRES-IR),
             "auto" (IR, switching to GMRES-IR when it stagnates).
@@ -26,7 +27,7 @@ from ._lib import (ArgumentError, DimensionMismatch, Handle, SingularException, 
                    OXI_ENONFINITE, OXI_ENOTCONVERGED, OXI_ESINGULAR, OXI_OK)
 from .lu import colmajor_copy, _as_tensor
 
-PREC = {"fp32": 0, "bf16": 1, "fp16": 2, "fp64": 3, "bf16x3": 4}
+PREC = {"fp32": 0, "bf16": 1, "fp16": 2, "fp64": 3, "bf16x3": 4, "fp16x3": 5}
 REFINE = {"ir": 0, "gmres": 1, "auto": 2}
 REASONS = ("converged", "iteration_limit", "working_factor_fallback", "nonfinite_iteration")
 

@@ -13,7 +13,7 @@ def _np(t):
     return t.detach().cpu().numpy()
 
 
-@pytest.mark.parametrize("prec", ["bf16", "fp16", "bf16x3", "fp32"])
+@pytest.mark.parametrize("prec", ["bf16", "fp16", "bf16x3", "fp16x3", "fp32"])
 def test_lowp_trailing_gemm(pkg, prec):
     torch.manual_seed(1)
     for (m, n, k) in ((128, 256, 64), (300, 517, 256), (2048, 1024, 256), (1000, 77, 40)):
@@ -27,12 +27,12 @@ def test_lowp_trailing_gemm(pkg, prec):
             tol = 1e-5
         else:  # scaled FP16, split BF16 and FP32 against the exact product
             ref = C.double() - A.double() @ B.double()
-            tol = {"fp16": 5e-3, "bf16x3": 5e-5, "fp32": 1e-5}[prec]
+            tol = {"fp16": 5e-3, "bf16x3": 5e-5, "fp16x3": 1e-5, "fp32": 1e-5}[prec]
         err = (C2.double() - ref).abs().max().item() / ref.abs().max().item()
         assert err < tol, (prec, m, n, k, err)
 
 
-@pytest.mark.parametrize("prec", ["fp32", "bf16", "fp16", "fp64", "bf16x3"])
+@pytest.mark.parametrize("prec", ["fp32", "bf16", "fp16", "fp64", "bf16x3", "fp16x3"])
 def test_mixed_solve_reference_cases(pkg, prec):
     rng = np.random.default_rng(7)
     for n in (1, 17, 67, 300):
@@ -77,6 +77,8 @@ def test_mixed_low_precision_pivot_loss_falls_back(pkg):
 
 @pytest.mark.parametrize("prec,refine,n,kappa", [("bf16x3", "ir", 1024, 1e4),
                                                  ("bf16x3", "auto", 1024, 1e4),
+                                                 ("fp16x3", "ir", 1024, 1e4),
+                                                 ("fp16x3", "auto", 2048, 1e4),
                                                  ("fp16", "gmres", 1024, 1e4),
                                                  ("fp32", "ir", 1024, 1e4),
                                                  ("bf16", "gmres", 512, 1e2)])
