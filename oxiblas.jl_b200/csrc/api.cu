@@ -9,6 +9,26 @@
 namespace oxi {
 thread_local Profiler *t_prof = nullptr;
 
+void queue_wait_errors(oxi_handle_s *h, int *hdst) {
+    int *a[3] = {leaf_wait_err_addr(), dmma_wait_err_addr(), tc_wait_err_addr()};
+    for (int i = 0; i < 3; ++i)
+        OXI_CUDA(cudaMemcpyAsync(hdst + i, a[i], sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+}
+
+int check_wait_errors(oxi_handle_s *h, const int *hsrc) {
+    int *a[3] = {leaf_wait_err_addr(), dmma_wait_err_addr(), tc_wait_err_addr()};
+    bool any = false;
+    for (int i = 0; i < 3; ++i)
+        if (hsrc[i]) {
+            any = true;
+            OXI_CUDA(cudaMemsetAsync(a[i], 0, sizeof(int), h->stream));
+        }
+    if (!any) return OXI_OK;
+    OXI_CUDA(cudaStreamSynchronize(h->stream));
+    h->last_error = "a bounded device wait timed out (leaf exchange / GEMM pipeline); results are void";
+    return OXI_ETIMEOUT;
+}
+
 void set_max_dyn_smem(const void *func, int bytes) {
     static std::mutex mu;
     static std::set<std::tuple<const void *, int, int>> done;
@@ -154,8 +174,10 @@ int oxi_dgemm_update(oxi_handle_t h, int64_t m, int64_t n, int64_t k, double *dC
         oxi::ProfGuard pg(&h->prof);
         OXI_CUDA(cudaSetDevice(h->device));
         oxi::gemm_minus<double>(h, dC, ldc, dB, ldb, dA, lda, n, m, k);
+        int *he = (int *)h->host_ws.get(64);
+        oxi::queue_wait_errors(h, he);
         OXI_CUDA(cudaStreamSynchronize(h->stream));
-        return OXI_OK;
+        return oxi::check_wait_errors(h, he);
     } catch (const oxi::CudaError &e) {
         h->last_error = std::string(e.what) + ": " + cudaGetErrorString(e.code);
         return OXI_ECUDA;
@@ -180,8 +202,10 @@ int oxi_sgemm_update_lowp(oxi_handle_t h, int prec, int64_t m, int64_t n, int64_
         else
             oxi::gemm_trailing_f32(h, dC, ldc, dB, ldb, dA, lda, n, m, k);
         h->trailing = saved;
+        int *he = (int *)h->host_ws.get(64);
+        oxi::queue_wait_errors(h, he);
         OXI_CUDA(cudaStreamSynchronize(h->stream));
-        return OXI_OK;
+        return oxi::check_wait_errors(h, he);
     } catch (const oxi::CudaError &e) {
         h->trailing = saved;
         h->last_error = std::string(e.what) + ": " + cudaGetErrorString(e.code);

@@ -52,6 +52,12 @@ constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barrier
 
 __device__ int g_gemm_dmma_err;
 
+int *dmma_wait_err_addr() {
+    void *p = nullptr;
+    OXI_CUDA(cudaGetSymbolAddress(&p, g_gemm_dmma_err));
+    return (int *)p;
+}
+
 __global__ void __launch_bounds__(NTHREADS, 2)
 k_gemm_dmma(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
             double *__restrict__ C, i64 ldc, int M, int N, int K) {

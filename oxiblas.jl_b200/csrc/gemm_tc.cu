@@ -29,6 +29,12 @@ constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + C_BYTES + 1024 + 256;
 
 __device__ int g_gemm_tc_err;
 
+int *tc_wait_err_addr() {
+    void *p = nullptr;
+    OXI_CUDA(cudaGetSymbolAddress(&p, g_gemm_tc_err));
+    return (int *)p;
+}
+
 // UMMA shared-memory descriptor, K-major operand in the 128-byte swizzle
 // layout TMA writes (rows of 128 bytes, 8-row groups 1024 bytes apart).
 __device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t smem_addr) {

@@ -260,8 +260,11 @@ static int getrf_entry(oxi_handle_s *h, i64 m, i64 n, T *dA, i64 lda, int64_t *d
         launch_rm_to_cm<T, T>(W, ld, dA, lda, m, n, h->stream);
         int64_t *hi = (int64_t *)h->host_ws.get(64);
         OXI_CUDA(cudaMemcpyAsync(hi, d_info, sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
+        queue_wait_errors(h, (int *)(hi + 2));
         OXI_CUDA(cudaStreamSynchronize(h->stream));
         *h_info = hi[0];
+        const int we = check_wait_errors(h, (const int *)(hi + 2));
+        if (we != OXI_OK) return we;
         return hi[0] > 0 ? OXI_ESINGULAR : OXI_OK;
     } catch (const CudaError &e) {
         h->last_error = std::string(e.what) + ": " + cudaGetErrorString(e.code);

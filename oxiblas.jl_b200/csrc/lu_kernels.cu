@@ -11,6 +11,7 @@
 #include <climits>
 #include <type_traits>
 #include "oxi_internal.h"
+#include "tma_util.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -86,11 +87,12 @@ template void launch_rm_to_cm<float, double>(const float *, i64, double *, i64, 
 //   a_ic = muladd(-l_ij, a_jc, a_ic) for c > j.
 // Per column each CTA reduces its candidate in registers/shared memory and
 // PUSHES it (|value|, position, the whole candidate row) into every CTA's
-// shared memory over DSMEM; one cluster barrier (release/acquire) later every
-// CTA holds all candidates locally and picks the same winner.  The CTA that
-// owns position j also pushes row j, so the two swapped rows never need a
-// second exchange.  Slots are double-buffered by column parity, which is what
-// makes one barrier per column sufficient.  Each row carries the index of the
+// shared memory with st.async, each store completing its bytes on the
+// receiver's mbarrier; a CTA waits on its own barrier until all candidates
+// have landed and picks the same winner as every other CTA.  The CTA that owns
+// position j also pushes row j, so the two swapped rows never need a second
+// exchange.  Slots are double-buffered by column parity, which is what makes
+// one exchange per column sufficient.  Each row carries the index of the
 // row it started as; at the end a position whose row changed emits a (dst, src)
 // move, the net permutation applied to the other columns by k_rowmoves.
 // ---------------------------------------------------------------------------
@@ -142,6 +144,8 @@ constexpr int LEAF_NT = 512;
 constexpr int LEAF_MAX_CS = 16;
 constexpr int LEAF_MOVE_ELEMS = 32;  // (moved rows x other panel columns) per thread, at most
 
+__device__ int g_leaf_err;  // a leaf exchange wait that timed out (read by the host after a call)
+
 template <typename T, int W, int R>
 __global__ void __launch_bounds__(LEAF_NT, 1)
 k_leaf_lu(T *__restrict__ P, i64 ld, int m, int wact, i64 gofs, int64_t *__restrict__ ipiv,
@@ -159,12 +163,11 @@ k_leaf_lu(T *__restrict__ P, i64 ld, int m, int wact, i64 gofs, int64_t *__restr
     constexpr int LG_NT = (LEAF_NT == 512) ? 9 : (LEAF_NT == 256 ? 8 : 10);
     static_assert((1 << LG_NT) == LEAF_NT, "LEAF_NT must be a power of two");
 
-    __shared__ uint64_t s_ckey[2][LEAF_MAX_CS];
-    __shared__ int s_cpos[2][LEAF_MAX_CS];
-    __shared__ int s_cid[2][LEAF_MAX_CS];
+    __shared__ __align__(16) uint4 s_cmeta[2][LEAF_MAX_CS];  // per CTA: {key lo, key hi, position, row id}
     __shared__ __align__(16) T s_crow[2][LEAF_MAX_CS][W];
     __shared__ __align__(16) T s_jslot[2][W];
-    __shared__ int s_jslot_id[2];
+    __shared__ __align__(16) uint4 s_jmeta[2];               // {row id of position j, 0, 0, 0}
+    __shared__ __align__(8) uint64_t s_xbar[2];              // exchange barriers, by column parity
     __shared__ uint64_t s_wkey[NW];
     __shared__ int s_wpos[NW];
     __shared__ __align__(16) T s_myrow[W];
@@ -172,8 +175,17 @@ k_leaf_lu(T *__restrict__ P, i64 ld, int m, int wact, i64 gofs, int64_t *__restr
     __shared__ __align__(16) T s_jrow[W];
     __shared__ int s_jid;
     __shared__ int s_piv[W];   // pivots and info stay on chip until the end: no global
-    __shared__ int s_info;     // store ahead of the per-column cluster barrier
-    if (t == 0) s_info = 0;
+    __shared__ int s_info;     // store ahead of the per-column exchange
+    if (t == 0) {
+        s_info = 0;
+        mbar_init(&s_xbar[0], 1);
+        mbar_init(&s_xbar[1], 1);
+        fence_barrier_init();
+    }
+    // every CTA's exchange barriers exist before any CTA pushes into them
+    if (CS > 1) cl.sync();
+    else __syncthreads();
+    bool dead = false;  // an exchange that timed out: stop waiting (g_leaf_err reports it)
 
     // ---- load: rows of W elements, 16-byte vectors when the row is whole and aligned ----
     T r[R][W];
@@ -247,45 +259,64 @@ k_leaf_lu(T *__restrict__ P, i64 ld, int m, int wact, i64 gofs, int64_t *__restr
             s_jid = id[0];
         }
         __syncthreads();
-        // (d) push the candidate (warp 0) and row j (warp 1 of CTA 0) to every CTA
-        if (warp == 0) {
-            for (int e = lane; e < CS * W; e += 32) {
-                const int dst = e / W, c = e - dst * W;
-                if (dst == cr) s_crow[par][cr][c] = s_myrow[c];
-                else *cl.map_shared_rank(&s_crow[par][cr][c], dst) = s_myrow[c];
+        // (d) every CTA's candidate (warp 0) and row j (warp 1 of CTA 0) into every
+        // CTA's slots of this parity.  Across CTAs each 16-byte store completes its
+        // bytes on the receiver's exchange barrier (st.async), and each CTA waits
+        // only on its own barrier: no cluster-wide barrier per column.  A slot is
+        // rewritten two columns later, after its receiver has pushed the column in
+        // between, i.e. after it finished reading the slot.
+        if (CS == 1) {
+            if (warp == 0) {
+                for (int c = lane; c < W; c += 32) s_crow[par][0][c] = s_myrow[c];
+                if (lane == 0)
+                    s_cmeta[par][0] = make_uint4((uint32_t)ck, (uint32_t)(ck >> 32), (uint32_t)cp, (uint32_t)s_myid);
+            } else if (warp == 1) {
+                for (int c = lane; c < W; c += 32) s_jslot[par][c] = s_jrow[c];
+                if (lane == 0) s_jmeta[par] = make_uint4((uint32_t)s_jid, 0u, 0u, 0u);
             }
-            if (lane < CS) {
-                if (lane == cr) {
-                    s_ckey[par][cr] = ck;
-                    s_cpos[par][cr] = cp;
-                    s_cid[par][cr] = s_myid;
-                } else {
-                    *cl.map_shared_rank(&s_ckey[par][cr], lane) = ck;
-                    *cl.map_shared_rank(&s_cpos[par][cr], lane) = cp;
-                    *cl.map_shared_rank(&s_cid[par][cr], lane) = s_myid;
+            __syncthreads();
+        } else {
+            constexpr int NCH = W * (int)sizeof(T) / 16;  // 16-byte chunks of a row
+            if (t == 0) mbar_arrive_expect_tx(&s_xbar[par], (uint32_t)((CS + 1) * 16 * (1 + NCH)));
+            if (warp == 0) {
+                for (int e = lane; e < CS * (1 + NCH); e += 32) {
+                    const int dst = e / (1 + NCH), q = e - dst * (1 + NCH);
+                    const uint32_t rbar = cluster_map_u32(&s_xbar[par], dst);
+                    if (q == 0)
+                        st_async_v4(cluster_map_u32(&s_cmeta[par][cr], dst),
+                                    make_uint4((uint32_t)ck, (uint32_t)(ck >> 32), (uint32_t)cp, (uint32_t)s_myid),
+                                    rbar);
+                    else
+                        st_async_v4(cluster_map_u32(&s_crow[par][cr][0], dst) + 16u * (q - 1),
+                                    reinterpret_cast<const uint4 *>(s_myrow)[q - 1], rbar);
+                }
+            } else if (warp == 1 && cr == 0) {
+                for (int e = lane; e < CS * (1 + NCH); e += 32) {
+                    const int dst = e / (1 + NCH), q = e - dst * (1 + NCH);
+                    const uint32_t rbar = cluster_map_u32(&s_xbar[par], dst);
+                    if (q == 0)
+                        st_async_v4(cluster_map_u32(&s_jmeta[par], dst), make_uint4((uint32_t)s_jid, 0u, 0u, 0u),
+                                    rbar);
+                    else
+                        st_async_v4(cluster_map_u32(&s_jslot[par][0], dst) + 16u * (q - 1),
+                                    reinterpret_cast<const uint4 *>(s_jrow)[q - 1], rbar);
                 }
             }
-        } else if (warp == 1 && cr == 0) {
-            for (int e = lane; e < CS * W; e += 32) {
-                const int dst = e / W, c = e - dst * W;
-                if (dst == 0) s_jslot[par][c] = s_jrow[c];
-                else *cl.map_shared_rank(&s_jslot[par][c], dst) = s_jrow[c];
-            }
-            if (lane < CS) {
-                if (lane == 0) s_jslot_id[par] = s_jid;
-                else *cl.map_shared_rank(&s_jslot_id[par], lane) = s_jid;
-            }
+            if (!dead && !mbar_wait(&s_xbar[par], (uint32_t)((j >> 1) & 1), &g_leaf_err, 1)) dead = true;
         }
-        if (CS == 1) __syncthreads();
-        else cl.sync();
         // (e) winner, identical in every CTA: lanes 0..CS-1 hold one candidate each;
         // the winning row sits in the slot of the CTA that owns its position
-        uint64_t wk = lane < CS ? s_ckey[par][lane] : 0ull;
-        int wp = lane < CS ? s_cpos[par][lane] : INT_MAX;
+        uint64_t wk = 0ull;
+        int wp = INT_MAX;
+        if (lane < CS) {
+            const uint4 mv = s_cmeta[par][lane];
+            wk = ((uint64_t)mv.y << 32) | mv.x;
+            wp = (int)mv.z;
+        }
         warp_argmax<T>(wk, wp);
         const int wq = (wp == INT_MAX) ? 0 : ((wp & (G - 1)) >> LG_NT);
         const T *prow = (wp == INT_MAX) ? &s_jslot[par][0] : &s_crow[par][wq][0];
-        const int pid = (wp == INT_MAX) ? s_jslot_id[par] : s_cid[par][wq];
+        const int pid = (wp == INT_MAX) ? (int)s_jmeta[par].x : (int)s_cmeta[par][wq].w;
         if (wp == INT_MAX) wp = j;  // no comparable candidate (all NaN): keep row j
         if (t == 0) s_piv[j] = wp;
         const T d = prow[0];
@@ -334,7 +365,7 @@ k_leaf_lu(T *__restrict__ P, i64 ld, int m, int wact, i64 gofs, int64_t *__restr
                         if (k == kk) {
 #pragma unroll
                             for (int c = 0; c < W; ++c) r[k][c] = s_jslot[par][c];
-                            id[k] = s_jslot_id[par];
+                            id[k] = (int)s_jmeta[par].x;
                         }
                 }
             }
@@ -441,6 +472,12 @@ k_leaf_lu(T *__restrict__ P, i64 ld, int m, int wact, i64 gofs, int64_t *__restr
     }
     // keep every CTA's shared memory alive until all remote pushes have landed
     if (CS > 1) cl.sync();
+}
+
+int *leaf_wait_err_addr() {
+    void *p = nullptr;
+    OXI_CUDA(cudaGetSymbolAddress(&p, g_leaf_err));
+    return (int *)p;
 }
 
 template <typename T> int leaf_width_for(i64 m);

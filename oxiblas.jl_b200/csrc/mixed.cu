@@ -27,7 +27,7 @@
 namespace oxi {
 
 namespace {
-constexpr int RS = 16;       // column chunks of the split residual / GEMV
+constexpr int RS = 32;       // column chunks of the split residual / GEMV
 constexpr int NRMAX = 4;     // right-hand sides per residual pass
 inline i64 rup(i64 x, i64 a) { return (x + a - 1) / a * a; }
 }  // namespace
@@ -769,7 +769,12 @@ extern "C" int oxi_dgesv_mixed(oxi_handle_t h, int prec, int refine, int64_t n, 
     try {
         oxi::ProfGuard pg(&h->prof);
         OXI_CUDA(cudaSetDevice(h->device));
-        return oxi::dgesv_mixed(h, prec, refine, n, nrhs, dA, lda, dB, ldb, dX, ldx, maxiter, rtol, out);
+        const int st = oxi::dgesv_mixed(h, prec, refine, n, nrhs, dA, lda, dB, ldb, dX, ldx, maxiter, rtol, out);
+        int *he = (int *)h->host_ws.get(64);
+        oxi::queue_wait_errors(h, he);
+        OXI_CUDA(cudaStreamSynchronize(h->stream));
+        const int we = oxi::check_wait_errors(h, he);
+        return we != OXI_OK ? we : st;
     } catch (const oxi::CudaError &e) {
         h->last_error = std::string(e.what) + ": " + cudaGetErrorString(e.code);
         return OXI_ECUDA;

@@ -161,6 +161,17 @@ struct oxi_handle_s {
 
 namespace oxi {
 
+// Device error words of the kernels with bounded waits (one per translation
+// unit).  A non-zero word means a wait timed out and that call's results are
+// void.  queue_wait_errors enqueues their copies into hdst[0..2] (pinned host
+// memory) on the handle's stream; after the stream is idle, check_wait_errors
+// returns OXI_ETIMEOUT if any was set (and clears the words), else OXI_OK.
+int *leaf_wait_err_addr();
+int *dmma_wait_err_addr();
+int *tc_wait_err_addr();
+void queue_wait_errors(oxi_handle_s *h, int *hdst);
+int check_wait_errors(oxi_handle_s *h, const int *hsrc);
+
 // Raise a kernel's dynamic shared-memory limit to `bytes`, once per device
 // (the attribute belongs to the device's context).  A kernel keeps ONE limit,
 // its largest use, so launches captured in a CUDA graph never see it lowered.
