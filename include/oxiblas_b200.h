@@ -62,8 +62,12 @@ enum oxi_option {
     OXI_OPT_MIXED_BLOCKSIZE = 5, /* panel width of the mixed-precision factor (256) */
     OXI_OPT_STOP_NORMWISE = 6,   /* 1: the mixed solve stops on the normwise error  */
     OXI_OPT_GMRES_RESTART = 7,   /* GMRES-IR restart length (30)                    */
-    OXI_OPT_GRAPHS = 8           /* 1 (default): a factorization repeated with the same
+    OXI_OPT_GRAPHS = 8,          /* 1 (default): a factorization repeated with the same
                                     shape and workspace replays as a CUDA graph      */
+    OXI_OPT_TOURNAMENT = 9       /* 1: the mixed solve's FP32 factor picks each 32-column
+                                    leaf's pivots by tournament (TSLU); 0 (default):
+                                    partial pivoting, the reference's rule (faster on
+                                    B200, see oxiblas.jl_b200/csrc/tslu.cu)           */
 };
 int oxi_set_option(oxi_handle_t h, int option, int64_t value);
 int oxi_get_option(oxi_handle_t h, int option, int64_t *value);

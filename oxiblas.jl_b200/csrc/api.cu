@@ -70,6 +70,7 @@ int oxi_destroy(oxi_handle_t h) {
     h->tc_ws.release();
     h->xtag_ws.release();
     h->rowmap_ws.release();
+    h->tslu_ws.release();
     h->gcache.reset();
     h->bgraph.reset();
     h->batch_ctl.release();
@@ -144,6 +145,9 @@ int oxi_set_option(oxi_handle_t h, int option, int64_t value) {
                 h->bgraph.reset();
             }
             return OXI_OK;
+        case OXI_OPT_TOURNAMENT:
+            h->opt.tournament = value ? 1 : 0;
+            return OXI_OK;
         default: return OXI_EINVAL;
     }
 }
@@ -159,6 +163,7 @@ int oxi_get_option(oxi_handle_t h, int option, int64_t *value) {
         case OXI_OPT_STOP_NORMWISE: *value = h->opt.stop_normwise; return OXI_OK;
         case OXI_OPT_GMRES_RESTART: *value = h->opt.gmres_restart; return OXI_OK;
         case OXI_OPT_GRAPHS: *value = h->opt.graphs; return OXI_OK;
+        case OXI_OPT_TOURNAMENT: *value = h->opt.tournament; return OXI_OK;
         default: return OXI_EINVAL;
     }
 }

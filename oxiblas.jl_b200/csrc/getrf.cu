@@ -81,10 +81,23 @@ static void panel_rec(LuRun<T> &R, i64 c0, i64 nc) {
     oxi_handle_s *h = R.h;
     const i64 mrows = R.m - c0;
     if (mrows <= 0 || nc <= 0) return;
-    const int leafw = leaf_width_for<T>(mrows);
+    // FP32 inside the mixed solve: tournament-pivoting leaves (32 columns at any height)
+    const bool ts = (sizeof(T) == 4) && h->tslu && tslu_applicable(mrows);
+    const int leafw = ts ? 32 : leaf_width_for<T>(mrows);
     if (leafw == 0) throw CudaError{cudaErrorInvalidValue, "panel taller than the leaf capacity"};
     if (nc <= leafw) {
         OXI_CUDA(cudaMemsetAsync(R.nmoves, 0, sizeof(int), h->stream));
+        auto leaf = [&](LeafPanel pn) {
+            if constexpr (sizeof(T) == 4) {
+                if (ts) {
+                    launch_tslu_leaf(h, R.W + c0 * R.ld + c0, R.ld, mrows, (int)nc, c0, R.ipiv, R.info, R.moves,
+                                     R.nmoves, h->stream, pn);
+                    return;
+                }
+            }
+            launch_leaf<T>(R.W + c0 * R.ld + c0, R.ld, mrows, (int)nc, c0, R.ipiv, R.info, R.moves, R.nmoves,
+                           leafw, h->stream, pn);
+        };
         if (R.map) {  // inside the panel by the leaf itself, outside it once per panel
             LeafPanel pn;
             pn.left_n = (int)(c0 - R.pf);
@@ -94,11 +107,9 @@ static void panel_rec(LuRun<T> &R, i64 c0, i64 nc) {
             pn.leaf_c0 = (int)c0;
             pn.map = R.map;
             pn.map_off = (int)(c0 - R.pf);
-            launch_leaf<T>(R.W + c0 * R.ld + c0, R.ld, mrows, (int)nc, c0, R.ipiv, R.info, R.moves,
-                           R.nmoves, leafw, h->stream, pn);
+            leaf(pn);
         } else {
-            launch_leaf<T>(R.W + c0 * R.ld + c0, R.ld, mrows, (int)nc, c0, R.ipiv, R.info, R.moves,
-                           R.nmoves, leafw, h->stream);
+            leaf(LeafPanel());
             launch_rowmoves<T>(R.W, R.ld, c0, R.moves, R.nmoves, 0, R.ncols_moved, c0, c0 + nc,
                                h->stream);
         }
@@ -191,9 +202,10 @@ void getrf_rowmajor_cached(oxi_handle_s *h, T *W, i64 ld, i64 m, i64 n, int64_t 
                               (uint64_t)(uintptr_t)d_ipiv, (uint64_t)(uintptr_t)d_info,
                               (uint64_t)(uintptr_t)d_moves, (uint64_t)h->opt.blocksize,
                               (uint64_t)h->opt.gemm | ((uint64_t)h->opt.trsm_leaf << 8) |
-                                  ((uint64_t)h->trailing << 16),
+                                  ((uint64_t)h->trailing << 16) | ((uint64_t)h->tslu << 24),
                               (uint64_t)(uintptr_t)h->stream,
-                              (uint64_t)(uintptr_t)h->rowmap_ws.ptr ^ (uint64_t)(uintptr_t)h->tc_ws.ptr};
+                              (uint64_t)(uintptr_t)h->rowmap_ws.ptr ^ (uint64_t)(uintptr_t)h->tc_ws.ptr ^
+                                  ((uint64_t)(uintptr_t)h->tslu_ws.ptr << 1)};
     const bool usable = h->opt.graphs && !h->prof.enabled;
     const bool same = gc.seen > 0 && std::memcmp(gc.key, key, sizeof(key)) == 0;
     if (usable && same && gc.valid) {

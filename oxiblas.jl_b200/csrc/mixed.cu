@@ -626,15 +626,18 @@ static int dgesv_mixed(oxi_handle_s *h, int prec, int refine, i64 n, i64 nrhs, c
             const int saved_tr = h->trailing;
             h->opt.blocksize = h->opt.mixed_blocksize;
             h->trailing = prec;
+            h->tslu = h->opt.tournament;
             try {
                 getrf_rowmajor_cached<float>(h, W, ldw, n, n, M.ipiv, d_info, d_moves, d_nmoves);
             } catch (...) {
                 h->opt.blocksize = saved_bs;
                 h->trailing = saved_tr;
+                h->tslu = 0;
                 throw;
             }
             h->opt.blocksize = saved_bs;
             h->trailing = saved_tr;
+            h->tslu = 0;
         } else {
             double *W = (double *)h->work.get((size_t)n * ldw * sizeof(double));
             M.W = W;

@@ -89,6 +89,7 @@ struct Options {
     i64 mixed_blocksize = 256;  // panel width of the mixed-precision factorization
     int stop_normwise = 0;      // IR stop test: 0 componentwise (reference), 1 normwise
     int graphs = 1;             // replay repeated factorizations as CUDA graphs
+    int tournament = 0;         // mixed solve: tournament pivoting in the FP32 leaves (off: slower, see tslu.cu)
     int gmres_restart = 30;
     double gmres_tol = 1e-4;    // inner relative tolerance of GMRES-IR
 };
@@ -114,6 +115,8 @@ struct oxi_handle_s {
     oxi::DeviceBuffer tc_ws;     // 16-bit GEMM operands
     oxi::DeviceBuffer xtag_ws;   // tagged solution words of the FP32 triangular solves
     oxi::DeviceBuffer rowmap_ws; // per-panel row map and composite move list
+    oxi::DeviceBuffer tslu_ws;   // tournament-pivoting tree of the FP32 leaves
+    int tslu = 0;                // 1 inside the mixed solve's FP32 factor: tournament leaves
     int trailing = 0;            // oxi::TrailingKind for getrf_rowmajor<float>
     oxi::Profiler prof;
     cudaStream_t aux_stream = nullptr;      // capturable stream used when the caller's is legacy
@@ -196,6 +199,13 @@ struct LeafPanel {
     int nother = 0, left_n = 0, pc_lo = 0, right_lo = 0, leaf_c0 = 0, map_off = 0;
     int *map = nullptr;
 };
+
+// Tournament-pivoting leaf (FP32, mixed solve only): same contract as
+// launch_leaf (pivots, info, moves, in-panel moves through pn).
+bool tslu_applicable(i64 m);
+void launch_tslu_leaf(oxi_handle_s *h, float *P, i64 ld, i64 m, int w, i64 gofs, int64_t *ipiv, int64_t *info,
+                      int *moves, int *nmoves, cudaStream_t s, LeafPanel pn);
+
 template <typename T>
 void launch_leaf(T *P, i64 ld, i64 m, int w, i64 gofs, int64_t *ipiv, int64_t *info,
                  int *moves, int *nmoves, int leafw, cudaStream_t s, LeafPanel pn = LeafPanel());

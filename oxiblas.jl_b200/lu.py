@@ -24,7 +24,7 @@ import numpy as np
 import torch
 
 from ._lib import (ArgumentError, DimensionMismatch, Handle, SingularException, OPT_BLOCKSIZE,
-                   OPT_GEMM, OPT_LOOKAHEAD, OPT_TRSM_LEAF, OXI_ESINGULAR)
+                   OPT_GEMM, OPT_LOOKAHEAD, OPT_TOURNAMENT, OPT_TRSM_LEAF, OXI_ESINGULAR)
 
 _KIND = {torch.float64: "d", torch.float32: "s"}
 
@@ -60,18 +60,20 @@ def colmajor_copy(A, dtype=None) -> torch.Tensor:
 
 
 @contextlib.contextmanager
-def options(blocksize=None, gemm=None, trsm_leaf=None, lookahead=None):
+def options(blocksize=None, gemm=None, trsm_leaf=None, lookahead=None, tournament=None):
     """Temporarily set engine options on this thread's handle.
 
-    blocksize : lu_factor(...; blocksize) (reference default 128)
-    gemm      : "tensor" (DMMA/tcgen05 engine, default) or "reference"
-                (one FMA chain per dot product, the reference GEMM's order)
-    trsm_leaf : leaf size of the recursive TRSM (reference 8; engine default 32)
+    blocksize  : lu_factor(...; blocksize) (reference default 128)
+    gemm       : "tensor" (DMMA/tcgen05 engine, default) or "reference"
+                 (one FMA chain per dot product, the reference GEMM's order)
+    trsm_leaf  : leaf size of the recursive TRSM (reference 8; engine default 32)
+    tournament : mixed solve only -- True: tournament pivoting in the FP32
+                 factor's leaves; False (default): partial pivoting
     """
     h = Handle.get()
     saved = []
     for opt, val in ((OPT_BLOCKSIZE, blocksize), (OPT_GEMM, gemm), (OPT_TRSM_LEAF, trsm_leaf),
-                     (OPT_LOOKAHEAD, lookahead)):
+                     (OPT_LOOKAHEAD, lookahead), (OPT_TOURNAMENT, tournament)):
         if val is None:
             continue
         if opt == OPT_GEMM:

@@ -95,3 +95,29 @@ def test_mixed_conditioned_reaches_fp64_backward_error(pkg, oracle, prec, refine
     assert oracle.normwise_backward_error(An, x, bn) <= 1e-14
     xo = np.linalg.solve(An, bn)
     assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= kappa * 1e-13
+
+
+@pytest.mark.parametrize("n", [129, 300, 1500, 4100])
+def test_tournament_and_partial_pivoting_leaves_both_converge(pkg, oracle, n):
+    """The mixed solve's FP32 factor with tournament-pivoting leaves (an option)
+    and with the partial-pivoting leaves (default): both reach FP64 backward
+    error, with similar iteration counts (the factor is a preconditioner for
+    refinement)."""
+    A = pkg.synthetic.kappa_matrix(n, 1e3, seed=21)
+    g = torch.Generator(device="cuda").manual_seed(22)
+    b = torch.randn(n, dtype=torch.float64, device="cuda", generator=g)
+    its = {}
+    for tour in (True, False):
+        with pkg.options(tournament=tour):
+            r = pkg.mixed_solve(A, b, precision="fp32", refine="ir", rtol=1e-14, normwise=True, maxiter=30)
+        assert r["converged"], (tour, {k: v for k, v in r.items() if k != "x"})
+        assert oracle.normwise_backward_error(_np(A), _np(r["x"]), _np(b)) <= 1e-14
+        its[tour] = r["iterations"]
+    assert its[True] <= its[False] + 2, its
+    # a pivoting-hungry matrix (no diagonal dominance) through the 16-bit path
+    rng = np.random.default_rng(23)
+    An = rng.standard_normal((n, n))
+    with pkg.options(tournament=True):
+        r = pkg.mixed_solve(An, rng.standard_normal(n), precision="fp16x3", refine="auto", rtol=1e-14,
+                            normwise=True, maxiter=30)
+    assert r["converged"], {k: v for k, v in r.items() if k != "x"}
