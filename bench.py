@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--refine", default="auto", choices=["ir", "gmres", "auto"])
     ap.add_argument("--tol", type=float, default=1e-14)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--lookahead", type=int, default=None,
+                    help="1: overlap each panel with the previous trailing update (both arms)")
     ap.add_argument("--workload", default="solve", choices=["solve", "batched", "adjoint"],
                     help="solve: the headline n=16384 metric (default); batched: 4096 uneven small "
                          "LU solves in one launch; adjoint: rrule of x = A \\ b at n=2048")
@@ -258,6 +260,8 @@ def ours(args, ws, rank, local):
     Bcm = b.reshape(1, n).contiguous()
     Xcm = torch.zeros_like(Bcm)
     h = pkg.Handle.get()
+    if args.lookahead is not None:
+        h.set_option(4, args.lookahead)  # OXI_OPT_LOOKAHEAD, for the mixed and the plain arm
     stream = torch.cuda.current_stream(dev)
 
     def mixed_step():
@@ -429,7 +433,7 @@ def ours(args, ws, rank, local):
         "config": {"workload": WORKLOAD, "n": n, "nrhs": 1, "kappa": args.kappa,
                    "precision": args.prec, "refine": args.refine, "stop": f"normwise<={args.tol}",
                    "l2": "inputs larger than L2 (2.1 GB matrix), no flush",
-                   "parallelism": f"replicas{ws}"},
+                   "lookahead": int(args.lookahead or 0), "parallelism": f"replicas{ws}"},
         "plain_fp64_ms": round(ms_plain, 3),
         "speedup_vs_plain_fp64": round(ms_plain / ms_mixed, 3),
         "backward_error_normwise": {"mixed": nw_mixed, "plain_fp64": nw_plain},

@@ -68,6 +68,7 @@ int oxi_destroy(oxi_handle_t h) {
     h->mixed_ws.release();
     h->perm_ws.release();
     h->tc_ws.release();
+    h->tc_ws2.release();
     h->xtag_ws.release();
     h->rowmap_ws.release();
     h->tslu_ws.release();
@@ -76,6 +77,9 @@ int oxi_destroy(oxi_handle_t h) {
     h->batch_ctl.release();
     h->batch_wsp.release();
     if (h->aux_stream) cudaStreamDestroy(h->aux_stream);
+    if (h->la_stream) cudaStreamDestroy(h->la_stream);
+    if (h->la_fork) cudaEventDestroy(h->la_fork);
+    if (h->la_join) cudaEventDestroy(h->la_join);
     if (h->aux_fork) cudaEventDestroy(h->aux_fork);
     if (h->aux_join) cudaEventDestroy(h->aux_join);
     h->host_ws.release();
@@ -126,6 +130,7 @@ int oxi_set_option(oxi_handle_t h, int option, int64_t value) {
             return OXI_OK;
         case OXI_OPT_LOOKAHEAD:
             h->opt.lookahead = value ? 1 : 0;
+            h->gcache.reset();
             return OXI_OK;
         case OXI_OPT_MIXED_BLOCKSIZE:
             if (value < 1) return OXI_EINVAL;

@@ -360,7 +360,7 @@ __global__ void k_cvt_transpose_split3(const float *__restrict__ src, i64 lds, H
 // ---- host ----
 void launch_gemm_tc(int fmt /*0 fp16, 1 bf16*/, float *C, i64 ldc, const void *A16, i64 lda16,
                     const void *B16, i64 ldb16, i64 M, i64 N, i64 K, float scale,
-                    const float *d_scale, cudaStream_t s) {
+                    const float *d_scale, cudaStream_t s, int max_ctas) {
     using namespace tc;
     if (M <= 0 || N <= 0 || K <= 0) return;
     CUtensorMap tmA, tmB, tmC;
@@ -376,7 +376,7 @@ void launch_gemm_tc(int fmt /*0 fp16, 1 bf16*/, float *C, i64 ldc, const void *A
         OXI_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     }
     const i64 tiles = ((N + BN - 1) / BN) * ((M + BM - 1) / BM);
-    dim3 grid((unsigned)std::min<i64>(tiles, sms));
+    dim3 grid((unsigned)std::min<i64>(tiles, max_ctas > 0 ? std::min(max_ctas, sms) : sms));
     ProfScope ps(KC_GEMM_TC, s, 2.0 * M * N * K, 8.0 * M * N + 2.0 * (M + N) * K);
     if (fmt == 1) {
         set_max_dyn_smem((const void *)k_gemm_tc<1>, SMEM_BYTES);
@@ -453,13 +453,14 @@ void gemm_trailing_f32(oxi_handle_s *h, float *C, i64 ldc, const float *A, i64 l
     if (h->trailing == TRAIL_BF16X3 || h->trailing == TRAIL_FP16X3) {
         const bool f16 = h->trailing == TRAIL_FP16X3;
         const i64 K3 = 3 * K, ldk3 = (K3 + 7) / 8 * 8;
-        char *ws = (char *)h->tc_ws.get((size_t)(M + N) * ldk3 * 2 + 1024);
+        DeviceBuffer &tcw = h->tc_slot ? h->tc_ws2 : h->tc_ws;
+        char *ws = (char *)tcw.get((size_t)(M + N) * ldk3 * 2 + 1024);
         void *A16 = ws;
         void *B16 = (void *)(((uintptr_t)(ws + (size_t)M * ldk3 * 2) + 255) & ~uintptr_t(255));
         cudaStream_t s = h->stream;
         float *scal = nullptr;
         if (f16) {  // the FP16 operand scales (see k_fp16_scales)
-            scal = (float *)((char *)h->scratch.get(kScratchBytes) + kScratchScalOff + 1536);
+            scal = (float *)((char *)h->scratch.get(kScratchBytes) + kScratchScalOff + 1536 + 256 * h->tc_slot);
             unsigned int *umax = (unsigned int *)(scal + 4);
             OXI_CUDA(cudaMemsetAsync(umax, 0, sizeof(unsigned int), s));
             k_absmax_f32<<<dim3((unsigned)std::min<i64>((N + 255) / 256, 16), (unsigned)K), 256, 0, s>>>(
@@ -490,22 +491,23 @@ void gemm_trailing_f32(oxi_handle_s *h, float *C, i64 ldc, const float *A, i64 l
                                                                                 (int)K, (int)N, 1.f, nullptr);
             OXI_LAUNCH_CHECK();
         }
-        if (f16) launch_gemm_tc(0, C, ldc, A16, ldk3, B16, ldk3, M, N, K3, 1.f, scal + 1, s);
-        else launch_gemm_tc(1, C, ldc, A16, ldk3, B16, ldk3, M, N, K3, 1.f, nullptr, s);
+        if (f16) launch_gemm_tc(0, C, ldc, A16, ldk3, B16, ldk3, M, N, K3, 1.f, scal + 1, s, h->gemm_ctas);
+        else launch_gemm_tc(1, C, ldc, A16, ldk3, B16, ldk3, M, N, K3, 1.f, nullptr, s, h->gemm_ctas);
         return;
     }
     const int fmt = (h->trailing == TRAIL_BF16) ? 1 : 0;
     const i64 ldk = (K + 7) / 8 * 8;
-    char *ws = (char *)h->tc_ws.get((size_t)(M + N) * ldk * 2 + 1024);
+    DeviceBuffer &tcw = h->tc_slot ? h->tc_ws2 : h->tc_ws;
+    char *ws = (char *)tcw.get((size_t)(M + N) * ldk * 2 + 1024);
     void *A16 = ws;
     void *B16 = ws + (size_t)M * ldk * 2;
     B16 = (void *)(((uintptr_t)B16 + 255) & ~uintptr_t(255));
-    float *scal = (float *)((char *)h->scratch.get(kScratchBytes) + kScratchScalOff + 1536);
+    float *scal = (float *)((char *)h->scratch.get(kScratchBytes) + kScratchScalOff + 1536 + 256 * h->tc_slot);
     cudaStream_t s = h->stream;
     if (fmt == 1) {
         launch_cvt_rows16(1, A, lda, A16, ldk, M, K, 1.f, nullptr, s);
         launch_cvt_transpose16(1, B, ldb, B16, ldk, K, N, 1.f, nullptr, s);
-        launch_gemm_tc(1, C, ldc, A16, ldk, B16, ldk, M, N, K, 1.f, nullptr, s);
+        launch_gemm_tc(1, C, ldc, A16, ldk, B16, ldk, M, N, K, 1.f, nullptr, s, h->gemm_ctas);
     } else {
         unsigned int *umax = (unsigned int *)(scal + 4);
         OXI_CUDA(cudaMemsetAsync(umax, 0, sizeof(unsigned int), s));
@@ -516,7 +518,7 @@ void gemm_trailing_f32(oxi_handle_s *h, float *C, i64 ldc, const float *A, i64 l
         OXI_LAUNCH_CHECK();
         launch_cvt_rows16(0, A, lda, A16, ldk, M, K, 16384.f, nullptr, s);
         launch_cvt_transpose16(0, B, ldb, B16, ldk, K, N, 1.f, scal, s);
-        launch_gemm_tc(0, C, ldc, A16, ldk, B16, ldk, M, N, K, 1.f, scal + 1, s);
+        launch_gemm_tc(0, C, ldc, A16, ldk, B16, ldk, M, N, K, 1.f, scal + 1, s, h->gemm_ctas);
     }
 }
 

@@ -139,34 +139,84 @@ void getrf_rowmajor(oxi_handle_s *h, T *W, i64 ld, i64 m, i64 n, int64_t *d_ipiv
         R.list = R.map + m;
         R.listcnt = R.list + 4 * nb;
     }
-    for (i64 f = 0; f < q; f += nb) {
-        const i64 l = std::min(q, f + nb);
-        if (compose) {
-            R.pf = f;
-            R.pl = l;
-            launch_rowmap_init(R.map, m - f, h->stream);
-            panel_rec(R, f, l - f);
-            OXI_CUDA(cudaMemsetAsync(R.listcnt, 0, sizeof(int), h->stream));
-            launch_rowmap_extract(R.map, m - f, R.list, R.listcnt, h->stream);
-            const int maxcnt = (int)std::min<i64>(2 * (l - f), m - f);
-            launch_rowmoves_big<T>(W, ld, f, R.list, R.listcnt, maxcnt, 0, f, h->stream);
-            launch_rowmoves_big<T>(W, ld, f, R.list, R.listcnt, maxcnt, l, R.ncols_moved, h->stream);
-        } else {
-            panel_rec(R, f, l - f);
-        }
-        if (l >= n) continue;
-        T *L11 = W + f * ld + f;
-        trsm_lower_unit<T>(h, L11, ld, L11 + (l - f), ld, l - f, n - l);
-        if (l >= m) continue;
+    // Lookahead (the reference's threaded lookahead, src/lapack/factorizations.jl:41-70):
+    // after panel k the next panel's columns are updated first; the rest of the
+    // trailing update runs on a second stream, concurrently with the next panel's
+    // factorization, which touches only its own columns.  Its row moves and U12
+    // solve, which do touch the other columns, wait for that update.
+    // Applied where the trailing update is the persistent tensor-core GEMM, whose
+    // CTA count can leave SMs to the panel; the FP64 DMMA update fills every SM
+    // and delays the panel's cluster instead (measured: no gain), so FP64 runs
+    // the plain schedule.
+    bool la = h->opt.lookahead && compose;
+    if constexpr (sizeof(T) == 8) la = false;
+    else if (h->trailing == TRAIL_NATIVE) la = false;
+    cudaStream_t sA = h->stream;
+    if (la && !h->la_stream) {
+        OXI_CUDA(cudaStreamCreateWithFlags(&h->la_stream, cudaStreamNonBlocking));
+        OXI_CUDA(cudaEventCreateWithFlags(&h->la_fork, cudaEventDisableTiming));
+        OXI_CUDA(cudaEventCreateWithFlags(&h->la_join, cudaEventDisableTiming));
+    }
+    bool b_pending = false;
+    auto update = [&](i64 f, i64 l, i64 c0, i64 c1) {  // W[l:m, c0:c1] -= L21 U12[:, c0:c1]
         if constexpr (sizeof(T) == 4) {
             if (h->trailing != TRAIL_NATIVE) {
-                gemm_trailing_f32(h, W + l * ld + l, ld, W + l * ld + f, ld, W + f * ld + l, ld,
-                                  m - l, n - l, l - f);
-                continue;
+                gemm_trailing_f32(h, W + l * ld + c0, ld, W + l * ld + f, ld, W + f * ld + c0, ld, m - l, c1 - c0,
+                                  l - f);
+                return;
             }
         }
-        gemm_minus<T>(h, W + l * ld + l, ld, W + l * ld + f, ld, W + f * ld + l, ld, m - l, n - l,
-                      l - f);
+        gemm_minus<T>(h, W + l * ld + c0, ld, W + l * ld + f, ld, W + f * ld + c0, ld, m - l, c1 - c0, l - f);
+    };
+    try {
+        for (i64 f = 0; f < q; f += nb) {
+            const i64 l = std::min(q, f + nb);
+            if (compose) {
+                R.pf = f;
+                R.pl = l;
+                launch_rowmap_init(R.map, m - f, sA);
+                panel_rec(R, f, l - f);
+                OXI_CUDA(cudaMemsetAsync(R.listcnt, 0, sizeof(int), sA));
+                launch_rowmap_extract(R.map, m - f, R.list, R.listcnt, sA);
+                if (b_pending) {  // the previous trailing update reads L21 and writes the columns moved now
+                    OXI_CUDA(cudaStreamWaitEvent(sA, h->la_join, 0));
+                    b_pending = false;
+                }
+                const int maxcnt = (int)std::min<i64>(2 * (l - f), m - f);
+                launch_rowmoves_big<T>(W, ld, f, R.list, R.listcnt, maxcnt, 0, f, sA);
+                launch_rowmoves_big<T>(W, ld, f, R.list, R.listcnt, maxcnt, l, R.ncols_moved, sA);
+            } else {
+                panel_rec(R, f, l - f);
+            }
+            if (l >= n) continue;
+            T *L11 = W + f * ld + f;
+            trsm_lower_unit<T>(h, L11, ld, L11 + (l - f), ld, l - f, n - l);
+            if (l >= m) continue;
+            const i64 l2 = std::min(n, l + nb);  // the next panel's columns
+            if (la && l2 < n) {
+                update(f, l, l, l2);
+                OXI_CUDA(cudaEventRecord(h->la_fork, sA));
+                OXI_CUDA(cudaStreamWaitEvent(h->la_stream, h->la_fork, 0));
+                // second stream: its own operand buffers, and SMs left free for the panel
+                h->stream = h->la_stream;
+                h->tc_slot = 1;
+                h->gemm_ctas = std::max(1, h->sm_count - 24);
+                update(f, l, l2, n);
+                h->stream = sA;
+                h->tc_slot = 0;
+                h->gemm_ctas = 0;
+                OXI_CUDA(cudaEventRecord(h->la_join, h->la_stream));
+                b_pending = true;
+            } else {
+                update(f, l, l, n);
+            }
+        }
+        if (b_pending) OXI_CUDA(cudaStreamWaitEvent(sA, h->la_join, 0));
+    } catch (...) {
+        h->stream = sA;
+        h->tc_slot = 0;
+        h->gemm_ctas = 0;
+        throw;
     }
 }
 template void getrf_rowmajor<double>(oxi_handle_s *, double *, i64, i64, i64, int64_t *, int64_t *, int *, int *);
@@ -202,7 +252,8 @@ void getrf_rowmajor_cached(oxi_handle_s *h, T *W, i64 ld, i64 m, i64 n, int64_t 
                               (uint64_t)(uintptr_t)d_ipiv, (uint64_t)(uintptr_t)d_info,
                               (uint64_t)(uintptr_t)d_moves, (uint64_t)h->opt.blocksize,
                               (uint64_t)h->opt.gemm | ((uint64_t)h->opt.trsm_leaf << 8) |
-                                  ((uint64_t)h->trailing << 16) | ((uint64_t)h->tslu << 24),
+                                  ((uint64_t)h->trailing << 16) | ((uint64_t)h->tslu << 24) |
+                                  ((uint64_t)h->opt.lookahead << 32),
                               (uint64_t)(uintptr_t)h->stream,
                               (uint64_t)(uintptr_t)h->rowmap_ws.ptr ^ (uint64_t)(uintptr_t)h->tc_ws.ptr ^
                                   ((uint64_t)(uintptr_t)h->tslu_ws.ptr << 1)};

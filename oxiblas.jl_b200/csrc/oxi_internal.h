@@ -85,7 +85,7 @@ struct Options {
     i64 blocksize = 128;   // lu_factor default (factorizations.jl:17)
     int gemm = 0;          // 0 tensor-core engine, 1 reference summation order
     i64 trsm_leaf = 32;    // recursive TRSM leaf
-    int lookahead = 0;
+    int lookahead = 1;          // overlap panel k+1 with the trailing update of panel k
     i64 mixed_blocksize = 256;  // panel width of the mixed-precision factorization
     int stop_normwise = 0;      // IR stop test: 0 componentwise (reference), 1 normwise
     int graphs = 1;             // replay repeated factorizations as CUDA graphs
@@ -113,6 +113,11 @@ struct oxi_handle_s {
     oxi::DeviceBuffer perm_ws;   // row permutation of the last solve
     oxi::PinnedBuffer host_ws;   // pinned host staging
     oxi::DeviceBuffer tc_ws;     // 16-bit GEMM operands
+    oxi::DeviceBuffer tc_ws2;    // the same for a second, concurrent trailing update
+    int tc_slot = 0;             // which of the two operand buffers (and scale slots) to use
+    int gemm_ctas = 0;           // > 0: cap on the persistent tensor-core GEMM's CTAs
+    cudaStream_t la_stream = nullptr;        // lookahead: the trailing update's stream
+    cudaEvent_t la_fork = nullptr, la_join = nullptr;
     oxi::DeviceBuffer xtag_ws;   // tagged solution words of the FP32 triangular solves
     oxi::DeviceBuffer rowmap_ws; // per-panel row map and composite move list
     oxi::DeviceBuffer tslu_ws;   // tournament-pivoting tree of the FP32 leaves
@@ -250,7 +255,7 @@ void launch_gemm_dmma(double *C, i64 ldc, const double *A, i64 lda, const double
 // tcgen05 GEMM: C (FP32 row-major) -= scale * A16 * B16^T, 16-bit K-major operands.
 void launch_gemm_tc(int fmt, float *C, i64 ldc, const void *A16, i64 lda16, const void *B16,
                     i64 ldb16, i64 M, i64 N, i64 K, float scale, const float *d_scale,
-                    cudaStream_t s);
+                    cudaStream_t s, int max_ctas = 0);
 void launch_cvt_rows16(int fmt, const float *src, i64 lds, void *dst, i64 ldd, i64 rows, i64 cols,
                        float scale, const float *d_scale, cudaStream_t s);
 void launch_cvt_transpose16(int fmt, const float *src, i64 lds, void *dst, i64 ldd, i64 rows,

@@ -195,3 +195,22 @@ def test_transposed_solve_unaligned_leading_dimension(pkg, dtype):
         for Fv, M in ((F, ref64), (F.T, ref64.T), (F.H, ref64.T)):
             X = _np(pkg.ldiv(Fv, torch.from_numpy(B))).astype(np.float64)
             assert np.allclose(X, np.linalg.solve(M, B.astype(np.float64)), rtol=r, atol=r), (n, dtype)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_lookahead_gives_identical_factors(pkg, oracle, dtype):
+    """OXI_OPT_LOOKAHEAD on or off leaves getrf's pivots and factors bit-identical
+    (for FP64 and native FP32 the option keeps the plain schedule), and the
+    pivots match the oracle's."""
+    rng = np.random.default_rng(41)
+    for n, bs in ((1000, 128), (1537, 64)):
+        A = rng.standard_normal((n, n)).astype(dtype)
+        with pkg.options(lookahead=0):
+            F0 = pkg.lu(torch.from_numpy(A), blocksize=bs)
+        with pkg.options(lookahead=1):
+            F1 = pkg.lu(torch.from_numpy(A), blocksize=bs)
+        assert torch.equal(F0.ipiv, F1.ipiv)
+        assert torch.equal(F0.factors, F1.factors)
+        if dtype == np.float64:
+            _, ipo, _ = oracle.getrf(A, blocksize=bs)
+            assert np.array_equal(_np(F1.ipiv), ipo)

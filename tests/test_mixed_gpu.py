@@ -121,3 +121,21 @@ def test_tournament_and_partial_pivoting_leaves_both_converge(pkg, oracle, n):
         r = pkg.mixed_solve(An, rng.standard_normal(n), precision="fp16x3", refine="auto", rtol=1e-14,
                             normwise=True, maxiter=30)
     assert r["converged"], {k: v for k, v in r.items() if k != "x"}
+
+
+@pytest.mark.parametrize("prec", ["fp16x3", "fp32"])
+def test_mixed_with_lookahead(pkg, oracle, prec):
+    n = 2100
+    A = pkg.synthetic.kappa_matrix(n, 1e4, seed=31)
+    g = torch.Generator(device="cuda").manual_seed(32)
+    b = torch.randn(n, dtype=torch.float64, device="cuda", generator=g)
+    with pkg.options(lookahead=0):
+        r0 = pkg.mixed_solve(A, b, precision=prec, refine="auto", rtol=1e-14, normwise=True, maxiter=30)
+    with pkg.options(lookahead=1):
+        r1 = pkg.mixed_solve(A, b, precision=prec, refine="auto", rtol=1e-14, normwise=True, maxiter=30)
+        r2 = pkg.mixed_solve(A, b, precision=prec, refine="auto", rtol=1e-14, normwise=True, maxiter=30)
+    for r in (r0, r1, r2):
+        assert r["converged"]
+        assert oracle.normwise_backward_error(_np(A), _np(r["x"]), _np(b)) <= 1e-14
+    assert torch.equal(r1["x"], r2["x"])  # the graph replay of the lookahead schedule
+    assert r1["iterations"] == r0["iterations"]
