@@ -76,7 +76,7 @@ template void launch_rm_to_cm<float, float>(const float *, i64, float *, i64, i6
 template void launch_rm_to_cm<float, double>(const float *, i64, double *, i64, i64, i64, cudaStream_t);
 
 // ---------------------------------------------------------------------------
-// Leaf LU: one thread-block cluster (1..16 CTAs of LEAF_NT threads) holds the
+// Leaf LU: one thread-block cluster (1..16 CTAs of NT = 256 or 512 threads) holds the
 // m x W leaf in REGISTERS, R rows per thread (row position i lives in thread
 // g = i mod G, slot k = i / G, G = cluster threads).  Column by column, as the
 // leaf loop of _lu_panel! (src/lapack/factorizations.jl:116-139):
@@ -142,12 +142,11 @@ __device__ __forceinline__ void warp_argmax(uint64_t &key, int &pos) {
 
 constexpr int LEAF_NT = 512;
 constexpr int LEAF_MAX_CS = 16;
-constexpr int LEAF_MOVE_ELEMS = 32;  // (moved rows x other panel columns) per thread, at most
 
 __device__ int g_leaf_err;  // a leaf exchange wait that timed out (read by the host after a call)
 
-template <typename T, int W, int R>
-__global__ void __launch_bounds__(LEAF_NT, 1)
+template <typename T, int W, int R, int NT>
+__global__ void __launch_bounds__(NT, 1)
 k_leaf_lu(T *__restrict__ P, i64 ld, int m, int wact, i64 gofs, int64_t *__restrict__ ipiv,
           int64_t *__restrict__ info, int *__restrict__ moves, int *__restrict__ nmoves,
           LeafPanel pn) {
@@ -155,13 +154,14 @@ k_leaf_lu(T *__restrict__ P, i64 ld, int m, int wact, i64 gofs, int64_t *__restr
     const int CS = (int)cl.num_blocks();
     const int cr = (int)cl.block_rank();
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    constexpr int NW = LEAF_NT / 32;
+    constexpr int NW = NT / 32;
+    constexpr int MOVE_ELEMS = 16384 / NT;  // (moved rows x other panel columns) per thread, at most
     constexpr int VEC = 16 / sizeof(T);  // elements per 16-byte vector
-    const int G = CS * LEAF_NT;  // a power of two: positions split by shift and mask
+    const int G = CS * NT;  // a power of two: positions split by shift and mask
     const int lgG = __ffs(G) - 1;
-    const int g = cr * LEAF_NT + t;
-    constexpr int LG_NT = (LEAF_NT == 512) ? 9 : (LEAF_NT == 256 ? 8 : 10);
-    static_assert((1 << LG_NT) == LEAF_NT, "LEAF_NT must be a power of two");
+    const int g = cr * NT + t;
+    constexpr int LG_NT = (NT == 512) ? 9 : (NT == 256 ? 8 : 10);
+    static_assert((1 << LG_NT) == NT, "NT must be 256 or 512");
 
     __shared__ __align__(16) uint4 s_cmeta[2][LEAF_MAX_CS];  // per CTA: {key lo, key hi, position, row id}
     __shared__ __align__(16) T s_crow[2][LEAF_MAX_CS][W];
@@ -436,10 +436,10 @@ k_leaf_lu(T *__restrict__ P, i64 ld, int m, int wact, i64 gofs, int64_t *__restr
         if (CS > 1) cl.sync(); else __syncthreads();
         const int cnt = min(*(volatile int *)nmoves, 2 * W);
         const int tot = cnt * pn.nother;
-        T vals[LEAF_MOVE_ELEMS];
+        T vals[MOVE_ELEMS];
         int mapv[R];
 #pragma unroll
-        for (int q = 0; q < LEAF_MOVE_ELEMS; ++q) {
+        for (int q = 0; q < MOVE_ELEMS; ++q) {
             const int e = g + q * G;
             if (e < tot) {
                 const int mv = e / pn.nother, oc = e - mv * pn.nother;
@@ -455,7 +455,7 @@ k_leaf_lu(T *__restrict__ P, i64 ld, int m, int wact, i64 gofs, int64_t *__restr
         }
         if (CS > 1) cl.sync(); else __syncthreads();
 #pragma unroll
-        for (int q = 0; q < LEAF_MOVE_ELEMS; ++q) {
+        for (int q = 0; q < MOVE_ELEMS; ++q) {
             const int e = g + q * G;
             if (e < tot) {
                 const int mv = e / pn.nother, oc = e - mv * pn.nother;
@@ -497,18 +497,18 @@ template <> int leaf_width_for<float>(i64 m) {
     return 0;
 }
 
-template <typename T, int W, int R>
+template <typename T, int W, int R, int NT = LEAF_NT>
 static void launch_leaf_wr(T *P, i64 ld, i64 m, int w, i64 gofs, int64_t *ipiv, int64_t *info,
                            int *moves, int *nmoves, cudaStream_t s, LeafPanel pn) {
-    const i64 per_cta = (i64)LEAF_NT * R;
+    const i64 per_cta = (i64)NT * R;
     int need = (int)((m + per_cta - 1) / per_cta);
     int cs = 1;  // cluster sizes kept to powers of two
     while (cs < need) cs <<= 1;
-    auto kern = k_leaf_lu<T, W, R>;
+    auto kern = k_leaf_lu<T, W, R, NT>;
     if (cs > 8) OXI_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(cs);
-    cfg.blockDim = dim3(LEAF_NT);
+    cfg.blockDim = dim3(NT);
     cfg.dynamicSmemBytes = 0;
     cfg.stream = s;
     cudaLaunchAttribute at[1];
@@ -518,7 +518,7 @@ static void launch_leaf_wr(T *P, i64 ld, i64 m, int w, i64 gofs, int64_t *ipiv, 
     at[0].val.clusterDim.z = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    if ((i64)pn.nother * 2 * W > (i64)LEAF_MOVE_ELEMS * cs * LEAF_NT)
+    if ((i64)pn.nother * 2 * W > (i64)16384 * cs)
         throw CudaError{cudaErrorInvalidValue, "panel too wide for the in-leaf row moves"};
     ProfScope ps(KC_LEAF, s, 0.0, 2.0 * (double)m * w * sizeof(T));
     OXI_CUDA(cudaLaunchKernelEx(&cfg, kern, P, ld, (int)m, w, gofs, ipiv, info, moves, nmoves, pn));
@@ -529,6 +529,9 @@ template <typename T>
 void launch_leaf(T *P, i64 ld, i64 m, int w, i64 gofs, int64_t *ipiv, int64_t *info, int *moves,
                  int *nmoves, int leafw, cudaStream_t s, LeafPanel pn) {
     const i64 cap = (i64)LEAF_MAX_CS * LEAF_NT;
+    // FP32 32-wide leaves up to 8192 rows: 256 threads x 2 rows (about 15% faster per
+    // column than 512 x 1: half the warps repeat the per-column work); FP64 keeps
+    // 512 x 1 (its 2-row variant needs 254 registers and measured slower)
     if constexpr (sizeof(T) == 8) {
         if (leafw == 32) launch_leaf_wr<T, 32, 1>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s, pn);
         else if (leafw == 16) launch_leaf_wr<T, 16, 2>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s, pn);
@@ -536,7 +539,7 @@ void launch_leaf(T *P, i64 ld, i64 m, int w, i64 gofs, int64_t *ipiv, int64_t *i
         else launch_leaf_wr<T, 4, 8>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s, pn);
     } else {
         if (leafw == 32) {
-            if (m <= cap) launch_leaf_wr<T, 32, 1>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s, pn);
+            if (m <= cap) launch_leaf_wr<T, 32, 2, 256>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s, pn);
             else launch_leaf_wr<T, 32, 2>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s, pn);
         } else if (leafw == 16) {
             launch_leaf_wr<T, 16, 4>(P, ld, m, w, gofs, ipiv, info, moves, nmoves, s, pn);
