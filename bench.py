@@ -48,9 +48,15 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--lookahead", type=int, default=None,
                     help="1: overlap each panel with the previous trailing update (both arms)")
-    ap.add_argument("--workload", default="solve", choices=["solve", "batched", "adjoint"],
-                    help="solve: the headline n=16384 metric (default); batched: 4096 uneven small "
-                         "LU solves in one launch; adjoint: rrule of x = A \\ b at n=2048")
+    ap.add_argument("--workload", default="solve",
+                    choices=["solve", "config2", "config5", "batched", "adjoint"],
+                    help="solve: the headline n=16384 metric (default); config2: n=8192, 16 RHS, "
+                         "kappa 1e4; config5: n=32768, kappa 1e6, rows scaled 10^U(-3,3), FP16 + "
+                         "GMRES-IR; batched: 4096 uneven small LU solves in one launch; adjoint: rrule "
+                         "of x = A \\ b at n=2048")
+    ap.add_argument("--nrhs", type=int, default=1)
+    ap.add_argument("--row-scale", type=float, default=0.0, help="rows scaled by 10^U(-d, d)")
+    ap.add_argument("--alt", default="bf16x3", help="comma-separated precisions timed beside --prec")
     ap.add_argument("--count", type=int, default=4096, help="batched: number of problems")
     ap.add_argument("--no-autotune", action="store_true", help="batched: keep the default tuning")
     return ap.parse_args()
@@ -242,7 +248,7 @@ def reference_arm(args, ws, rank):
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
-def ours(args, ws, rank, local):
+def ours(args, ws, rank, local, metric=METRIC, workload=WORKLOAD):
     import numpy as np
     import torch
     import __graft_entry__ as E
@@ -251,13 +257,14 @@ def ours(args, ws, rank, local):
     n = args.n
     dev = torch.device("cuda", local)
     seed = 20261104 + 7919 * rank
-    A = pkg.synthetic.kappa_matrix(n, args.kappa, seed=seed, device=dev)
+    nrhs = args.nrhs
+    A = pkg.synthetic.kappa_matrix(n, args.kappa, seed=seed, device=dev, row_scale_decades=args.row_scale)
     g = torch.Generator(device=dev).manual_seed(seed + 1)
-    b = torch.randn(n, dtype=torch.float64, device=dev, generator=g)
+    b = torch.randn(n, nrhs, dtype=torch.float64, device=dev, generator=g)
     Acm = A.t().contiguous()  # column-major A
     del A
     torch.cuda.empty_cache()
-    Bcm = b.reshape(1, n).contiguous()
+    Bcm = b.t().contiguous()  # (nrhs, n): column-major B
     Xcm = torch.zeros_like(Bcm)
     h = pkg.Handle.get()
     if args.lookahead is not None:
@@ -265,13 +272,13 @@ def ours(args, ws, rank, local):
     stream = torch.cuda.current_stream(dev)
 
     def mixed_step():
-        st, rep = pkg.mixed_solve_device(Acm, Bcm, Xcm, n, 1, maxiter=30, rtol=args.tol,
+        st, rep = pkg.mixed_solve_device(Acm, Bcm, Xcm, n, nrhs, maxiter=30, rtol=args.tol,
                                          precision=args.prec, refine=args.refine, normwise=True)
         return st, rep
 
     # plain FP64 LU + solve through the C ABI (lu! on a copy, then ldiv!)
     work = torch.empty_like(Acm)
-    xplain = torch.empty(n, dtype=torch.float64, device=dev)
+    xplain = torch.empty(n, nrhs, dtype=torch.float64, device=dev)
 
     def plain_step():
         work.copy_(Acm)
@@ -316,18 +323,20 @@ def ours(args, ws, rank, local):
     st, rep = mixed_step()  # verification of the final state (untimed)
     ms_mixed = max_over_ranks(ws, tot_mixed / args.steps)
 
-    # ---- the split-BF16 variant, same system, for comparison ----
+    # ---- other low precisions on the same system, for comparison ----
     alt = {}
-    if args.prec != "bf16x3":
-        def bf_step():
-            return pkg.mixed_solve_device(Acm, Bcm, Xcm, n, 1, maxiter=30, rtol=args.tol, precision="bf16x3",
+    for ap_ in [a for a in args.alt.split(",") if a and a != args.prec]:
+        def alt_step(prec=ap_):
+            return pkg.mixed_solve_device(Acm, Bcm, Xcm, n, nrhs, maxiter=30, rtol=args.tol, precision=prec,
                                           refine=args.refine, normwise=True)
         for _ in range(2):
-            bf_step()
-        tot_bf, _ = timed(bf_step, max(1, min(args.steps, 3)))
-        st_bf, rep_bf = bf_step()
-        alt["bf16x3"] = {"ms": round(max_over_ranks(ws, tot_bf / max(1, min(args.steps, 3))), 3),
-                         "iterations": int(rep_bf.iterations), "converged": bool(rep_bf.converged)}
+            alt_step()
+        ka = max(1, min(args.steps, 3))
+        tot_a, _ = timed(alt_step, ka)
+        st_a, rep_a = alt_step()
+        alt[ap_] = {"ms": round(max_over_ranks(ws, tot_a / ka), 3), "iterations": int(rep_a.iterations),
+                    "gmres_iterations": int(rep_a.gmres_iterations), "converged": bool(rep_a.converged)}
+    if alt:
         mixed_step()  # leave the default precision's answer in Xcm
 
     # ---- timed: plain FP64 ----
@@ -336,13 +345,14 @@ def ours(args, ws, rank, local):
     ms_plain = max_over_ranks(ws, tot_plain / ksteps_plain)
 
     # backward errors of both answers (FP64, in the harness)
-    def normwise(x):
+    def normwise(x):  # max over right-hand sides of ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf)
         r = b - (Acm.t() @ x)
         an = Acm.t().abs().sum(dim=1).max()
-        return float(r.abs().max() / (an * x.abs().max() + b.abs().max()))
+        return float((r.abs().amax(dim=0) / (an * x.abs().amax(dim=0) + b.abs().amax(dim=0))).max())
 
-    nw_mixed = normwise(Xcm[0])
+    nw_mixed = normwise(Xcm.t())
     nw_plain = normwise(xplain)
+    fwd_vs_plain = float((Xcm.t() - xplain).abs().max() / xplain.abs().max())
 
     # ---- profiled pass (same steps) for the roofline of the dominant kernel ----
     h.profile(True)
@@ -388,7 +398,7 @@ def ours(args, ws, rank, local):
 
     # ---- e2e through the public API (host buffers, copies inside the region) ----
     A_host = Acm.t().cpu().pin_memory()  # the user's row-indexed matrix on the host
-    b_host = b.cpu().pin_memory()
+    b_host = (b[:, 0] if nrhs == 1 else b).cpu().pin_memory()
     ke = max(1, min(args.steps, 3))
     barrier(ws)
     torch.cuda.synchronize()
@@ -408,15 +418,15 @@ def ours(args, ws, rank, local):
 
     # ---- CPU baseline (rank 0, N=1) ----
     cpu = None
-    if rank == 0 and ws == 1 and not args.no_cpu:
+    if rank == 0 and ws == 1 and not args.no_cpu and metric == METRIC:
         A32 = np.asfortranarray(Acm.t().float().cpu().numpy())
         t_lu, t_prefix, frac, cores = cpu_mixed_estimate(A32, n, panels=3)
         del A32
         A64 = np.asfortranarray(Acm.t().cpu().numpy())
-        x0 = Xcm[0].cpu().numpy()
+        x0 = Xcm[0].cpu().numpy()  # first right-hand side
         t0 = time.perf_counter()
         import __graft_entry__ as E2
-        E2.load_oracle().refinement_residual(A64, x0, b.cpu().numpy())
+        E2.load_oracle().refinement_residual(A64, x0, b[:, 0].cpu().numpy())
         t_res = time.perf_counter() - t0
         del A64
         cpu_ms = (t_lu + 3 * t_res) * 1e3
@@ -426,17 +436,19 @@ def ours(args, ws, rank, local):
                           f"full-size FP64 residual ({t_res*1e3:.0f} ms): the reference's mixed_solve")}
 
     line = {
-        "metric": METRIC, "value": round(ms_mixed, 3), "unit": "ms", "n_gpus": ws,
+        "metric": metric, "value": round(ms_mixed, 3), "unit": "ms", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_mixed, 3),
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": f"{args.prec}+f32+f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "n": n, "nrhs": 1, "kappa": args.kappa,
+        "config": {"workload": workload, "n": n, "nrhs": nrhs, "kappa": args.kappa,
+                   "row_scale_decades": args.row_scale,
                    "precision": args.prec, "refine": args.refine, "stop": f"normwise<={args.tol}",
                    "l2": "inputs larger than L2 (2.1 GB matrix), no flush",
                    "lookahead": int(args.lookahead or 0), "parallelism": f"replicas{ws}"},
         "plain_fp64_ms": round(ms_plain, 3),
         "speedup_vs_plain_fp64": round(ms_plain / ms_mixed, 3),
         "backward_error_normwise": {"mixed": nw_mixed, "plain_fp64": nw_plain},
+        "forward_error_vs_plain_fp64": fwd_vs_plain,
         "refinement": {"iterations": int(rep.iterations), "gmres_iterations": int(rep.gmres_iterations),
                        "refine_used": ("ir", "gmres", "auto")[rep.refine_used],
                        "factor_ms": round(rep.factor_ms, 3), "refine_ms": round(rep.refine_ms, 3)},
@@ -445,8 +457,8 @@ def ours(args, ws, rank, local):
         "roofline": roofline, "kernel_time_shares": shares,
         "plain_fp64_kernel_ms": plain_shares, "plain_fp64_trailing_gemm_tflops": plain_gemm_tflops,
         "cpu_baseline": cpu,
-        "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": n * n * 8 + n * 8,
-                "d2h_bytes_per_step": n * 8},
+        "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": n * n * 8 + n * nrhs * 8,
+                "d2h_bytes_per_step": n * nrhs * 8},
         "gpu_launches": launches,
         "clocks": clocks,
     }
@@ -625,6 +637,20 @@ def main():
             batched_workload(args, ws, rank, local)
         elif args.workload == "adjoint":
             adjoint_workload(args, ws, rank, local)
+        elif args.workload == "config2":
+            args.n, args.nrhs, args.kappa = 8192, 16, 1e4
+            ours(args, ws, rank, local,
+                 metric="n=8192 16-RHS solve time: 16-bit tensor-core LU + FP64 IR vs plain FP64 LU "
+                        "at equal backward error (kappa 1e4)",
+                 workload="dense LU solve n=8192 kappa~1e4 nrhs=16 (Haar U, V; sigma log-uniform)")
+        elif args.workload == "config5":
+            args.n, args.nrhs, args.kappa, args.row_scale = 32768, 1, 1e6, 3.0
+            if args.alt == "bf16x3":  # single-pass FP16 + GMRES-IR (the configuration's form) beside it
+                args.alt = "fp16"
+            ours(args, ws, rank, local,
+                 metric="n=32768 solve time, kappa 1e6 and rows scaled 10^U(-3,3): FP16 tensor-core LU + "
+                        "FP64 GMRES-IR vs plain FP64 LU at equal backward error",
+                 workload="dense LU solve n=32768 kappa~1e6, row scaling 10^U(-3,3), nrhs=1")
         else:
             ours(args, ws, rank, local)
     finally:

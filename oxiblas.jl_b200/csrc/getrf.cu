@@ -72,6 +72,7 @@ struct LuRun {
     int *moves, *nmoves;
     // panel-level composition (null: each leaf moves every column itself)
     int *map = nullptr, *list = nullptr, *listcnt = nullptr;
+    int *list2 = nullptr, *listcnt2 = nullptr;  // lookahead: the odd panels' move list
     i64 pf = 0, pl = 0;  // current panel columns [pf, pl)
 };
 
@@ -134,10 +135,12 @@ void getrf_rowmajor(oxi_handle_s *h, T *W, i64 ld, i64 m, i64 n, int64_t *d_ipiv
     const i64 nb = std::max<i64>(h->opt.blocksize, 1);
     const bool compose = nb > 32 && n > nb;  // worth it when a panel holds several leaves
     if (compose) {
-        char *ws = (char *)h->rowmap_ws.get(sizeof(int) * (size_t)(m + 4 * nb + 64));
+        char *ws = (char *)h->rowmap_ws.get(sizeof(int) * (size_t)(m + 8 * nb + 128));
         R.map = (int *)ws;
         R.list = R.map + m;
         R.listcnt = R.list + 4 * nb;
+        R.list2 = R.listcnt + 64;
+        R.listcnt2 = R.list2 + 4 * nb;
     }
     // Lookahead (the reference's threaded lookahead, src/lapack/factorizations.jl:41-70):
     // after panel k the next panel's columns are updated first; the rest of the
@@ -169,47 +172,62 @@ void getrf_rowmajor(oxi_handle_s *h, T *W, i64 ld, i64 m, i64 n, int64_t *d_ipiv
         gemm_minus<T>(h, W + l * ld + c0, ld, W + l * ld + f, ld, W + f * ld + c0, ld, m - l, c1 - c0, l - f);
     };
     try {
-        for (i64 f = 0; f < q; f += nb) {
+        for (i64 f = 0, k = 0; f < q; f += nb, ++k) {
             const i64 l = std::min(q, f + nb);
+            const i64 l2 = std::min(n, l + nb);  // the next panel's columns
+            const bool split = la && l < n && l < m && l2 < n;
+            int *list = R.list, *listcnt = R.listcnt;
+            if (la && (k & 1)) {  // the second stream may still read the previous panel's list
+                list = R.list2;
+                listcnt = R.listcnt2;
+            }
+            const int maxcnt = (int)std::min<i64>(2 * (l - f), m - f);
             if (compose) {
                 R.pf = f;
                 R.pl = l;
                 launch_rowmap_init(R.map, m - f, sA);
                 panel_rec(R, f, l - f);
-                OXI_CUDA(cudaMemsetAsync(R.listcnt, 0, sizeof(int), sA));
-                launch_rowmap_extract(R.map, m - f, R.list, R.listcnt, sA);
+                OXI_CUDA(cudaMemsetAsync(listcnt, 0, sizeof(int), sA));
+                launch_rowmap_extract(R.map, m - f, list, listcnt, sA);
                 if (b_pending) {  // the previous trailing update reads L21 and writes the columns moved now
                     OXI_CUDA(cudaStreamWaitEvent(sA, h->la_join, 0));
                     b_pending = false;
                 }
-                const int maxcnt = (int)std::min<i64>(2 * (l - f), m - f);
-                launch_rowmoves_big<T>(W, ld, f, R.list, R.listcnt, maxcnt, 0, f, sA);
-                launch_rowmoves_big<T>(W, ld, f, R.list, R.listcnt, maxcnt, l, R.ncols_moved, sA);
+                if (!split) {
+                    launch_rowmoves_big<T>(W, ld, f, list, listcnt, maxcnt, 0, f, sA);
+                    launch_rowmoves_big<T>(W, ld, f, list, listcnt, maxcnt, l, R.ncols_moved, sA);
+                }
             } else {
                 panel_rec(R, f, l - f);
             }
             if (l >= n) continue;
             T *L11 = W + f * ld + f;
-            trsm_lower_unit<T>(h, L11, ld, L11 + (l - f), ld, l - f, n - l);
-            if (l >= m) continue;
-            const i64 l2 = std::min(n, l + nb);  // the next panel's columns
-            if (la && l2 < n) {
-                update(f, l, l, l2);
-                OXI_CUDA(cudaEventRecord(h->la_fork, sA));
-                OXI_CUDA(cudaStreamWaitEvent(h->la_stream, h->la_fork, 0));
-                // second stream: its own operand buffers, and SMs left free for the panel
-                h->stream = h->la_stream;
-                h->tc_slot = 1;
-                h->gemm_ctas = std::max(1, h->sm_count - 24);
-                update(f, l, l2, n);
-                h->stream = sA;
-                h->tc_slot = 0;
-                h->gemm_ctas = 0;
-                OXI_CUDA(cudaEventRecord(h->la_join, h->la_stream));
-                b_pending = true;
-            } else {
+            if (!split) {
+                trsm_lower_unit<T>(h, L11, ld, L11 + (l - f), ld, l - f, n - l);
+                if (l >= m) continue;
                 update(f, l, l, n);
+                continue;
             }
+            // the next panel's columns now, on this stream ...
+            launch_rowmoves_big<T>(W, ld, f, list, listcnt, maxcnt, l, l2, sA);
+            trsm_lower_unit<T>(h, L11, ld, L11 + (l - f), ld, l - f, l2 - l);
+            update(f, l, l, l2);
+            OXI_CUDA(cudaEventRecord(h->la_fork, sA));
+            OXI_CUDA(cudaStreamWaitEvent(h->la_stream, h->la_fork, 0));
+            // ... everything else on the second stream: its own operand buffers, and
+            // SMs left free for the next panel's cluster
+            h->stream = h->la_stream;
+            h->tc_slot = 1;
+            h->gemm_ctas = std::max(1, h->sm_count - 24);
+            launch_rowmoves_big<T>(W, ld, f, list, listcnt, maxcnt, 0, f, h->stream);
+            launch_rowmoves_big<T>(W, ld, f, list, listcnt, maxcnt, l2, R.ncols_moved, h->stream);
+            trsm_lower_unit<T>(h, L11, ld, W + f * ld + l2, ld, l - f, n - l2);
+            update(f, l, l2, n);
+            h->stream = sA;
+            h->tc_slot = 0;
+            h->gemm_ctas = 0;
+            OXI_CUDA(cudaEventRecord(h->la_join, h->la_stream));
+            b_pending = true;
         }
         if (b_pending) OXI_CUDA(cudaStreamWaitEvent(sA, h->la_join, 0));
     } catch (...) {
@@ -219,6 +237,7 @@ void getrf_rowmajor(oxi_handle_s *h, T *W, i64 ld, i64 m, i64 n, int64_t *d_ipiv
         throw;
     }
 }
+
 template void getrf_rowmajor<double>(oxi_handle_s *, double *, i64, i64, i64, int64_t *, int64_t *, int *, int *);
 template void getrf_rowmajor<float>(oxi_handle_s *, float *, i64, i64, i64, int64_t *, int64_t *, int *, int *);
 

@@ -29,6 +29,7 @@ namespace oxi {
 namespace {
 constexpr int RS = 32;       // column chunks of the split residual / GEMV
 constexpr int NRMAX = 4;     // right-hand sides per residual pass
+constexpr int NCMAX = 16;    // right-hand sides per correction solve (one triangular-solve launch each)
 inline i64 rup(i64 x, i64 a) { return (x + a - 1) / a * a; }
 }  // namespace
 
@@ -682,8 +683,8 @@ static int dgesv_mixed(oxi_handle_s *h, int prec, int refine, i64 n, i64 nrhs, c
     // ---- 4-5. first solve and refinement ----
     const int nr_i = (int)nrhs;
     auto correct_all = [&](const double *Rin, i64 ldr, int add) {
-        for (int k0 = 0; k0 < nr_i; k0 += NRMAX) {
-            const int nr = std::min(NRMAX, nr_i - k0);
+        for (int k0 = 0; k0 < nr_i; k0 += NCMAX) {
+            const int nr = std::min(NCMAX, nr_i - k0);
             if (!add) {
                 precond(M, Rin + (i64)k0 * ldr, ldr, dX + (i64)k0 * ldx, ldx, nr);
             } else {

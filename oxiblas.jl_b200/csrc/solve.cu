@@ -385,7 +385,18 @@ static void trsv_launch(const T *A, i64 lda, T *X, i64 ldx, int n, int nrhs, int
         }                                                                                            \
         k0 += NRV;                                                                                   \
     } while (0)
-        if (left >= 4) OXI_TRSV_GO(4);
+        // several right-hand sides per launch read the factor once for all of them
+        // (FP32 up to 16 columns, FP64 up to 8: the staging fits shared memory)
+        bool wide = false;
+        if constexpr (sizeof(T) == 4) {
+            if (left >= 16) {
+                OXI_TRSV_GO(16);
+                wide = true;
+            }
+        }
+        if (wide) {
+        } else if (left >= 8) OXI_TRSV_GO(8);
+        else if (left >= 4) OXI_TRSV_GO(4);
         else if (left >= 2) OXI_TRSV_GO(2);
         else OXI_TRSV_GO(1);
 #undef OXI_TRSV_GO
@@ -446,7 +457,7 @@ void lu_solve_rowmajor(oxi_handle_s *h, const T *W, i64 ld, i64 n, T *X, i64 ldx
     int *ctl = (int *)((char *)h->scratch.get(kScratchBytes) + kScratchTrsvOff);
     unsigned long long *xtag = nullptr;
     if (sizeof(T) == 4 && DinvL && DinvU) {
-        const size_t need = sizeof(unsigned long long) * (size_t)n * 4;
+        const size_t need = sizeof(unsigned long long) * (size_t)n * 16;  // NR <= 16 words per row
         if (h->xtag_ws.bytes < need) {  // fresh words: epoch 0 never matches a launch
             xtag = (unsigned long long *)h->xtag_ws.get(need);
             OXI_CUDA(cudaMemsetAsync(xtag, 0, h->xtag_ws.bytes, h->stream));
