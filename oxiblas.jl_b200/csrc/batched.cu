@@ -105,6 +105,9 @@ struct Misc {
     int red_i[2][bt::NW];
     double red_m[bt::NW][bt::MAXRHS];
     int piv[bt::NMAX];   // pivot row (0-based, within the matrix) of each column
+    int rowat[bt::NMAX]; // a panel's net permutation: position p holds row rowat[p]
+    int mvpos[2 * bt::NBMAX];
+    int nmv;
     int perm[bt::NMAX];  // net permutation: row i of L U is row perm[i] of A
     double rows[bt::NMAX], cols[bt::NMAX];
     int item, info, bad;
@@ -203,15 +206,55 @@ __device__ void lu_blocked(T *W, int ldw, int n, int nb, bool in_smem, T *sP, T 
         }
         // interchanges on the other columns, then U12 = L11^-1 A12
         const int c2 = k + jb;
+        if (!in_smem) {
+            // global working matrix: the panel's net permutation once, every moved
+            // row of the other columns staged in shared memory (sU), then written
+            // back -- one round trip instead of jb dependent swaps per column
+            for (int p = k + threadIdx.x; p < n; p += NT) S.rowat[p] = p;
+            if (threadIdx.x == 0) S.nmv = 0;
+            __syncthreads();
+            if (threadIdx.x == 0)
+                for (int j = 0; j < jb; ++j) {
+                    const int a = k + j, b = S.piv[k + j];
+                    const int t = S.rowat[a];
+                    S.rowat[a] = S.rowat[b];
+                    S.rowat[b] = t;
+                }
+            __syncthreads();
+            for (int p = k + threadIdx.x; p < n; p += NT)
+                if (S.rowat[p] != p) S.mvpos[atomicAdd(&S.nmv, 1)] = p;
+            __syncthreads();
+            const int nmv = S.nmv;  // <= 2 jb
+            if (nmv > 0) {
+                const int ccap = (nb * NMAX) / nmv;  // columns per pass (>= 128)
+                for (int cb = 0; cb < n; cb += ccap) {
+                    const int cn = min(ccap, n - cb);
+                    for (int e = threadIdx.x; e < nmv * cn; e += NT) {
+                        const int mv = e / cn, c = cb + e % cn;
+                        if (c >= k && c < c2) continue;
+                        sU[mv * ccap + (c - cb)] = W[S.rowat[S.mvpos[mv]] + (i64)c * ldw];
+                    }
+                    __syncthreads();
+                    for (int e = threadIdx.x; e < nmv * cn; e += NT) {
+                        const int mv = e / cn, c = cb + e % cn;
+                        if (c >= k && c < c2) continue;
+                        W[S.mvpos[mv] + (i64)c * ldw] = sU[mv * ccap + (c - cb)];
+                    }
+                    __syncthreads();
+                }
+            }
+        }
         for (int c = threadIdx.x; c < n; c += NT) {
             if (c >= k && c < c2) continue;
             T *wc = W + (i64)c * ldw;
-            for (int j = 0; j < jb; ++j) {
-                const int p = S.piv[k + j];
-                if (p != k + j) {
-                    const T t = wc[k + j];
-                    wc[k + j] = wc[p];
-                    wc[p] = t;
+            if (in_smem) {
+                for (int j = 0; j < jb; ++j) {
+                    const int p = S.piv[k + j];
+                    if (p != k + j) {
+                        const T t = wc[k + j];
+                        wc[k + j] = wc[p];
+                        wc[p] = t;
+                    }
                 }
             }
             if (c >= c2) {
@@ -318,6 +361,72 @@ __device__ void warp_lu_solve(const T *W, int ldw, int n, T (&y)[bt::NQ]) {
             if (i < j) y[q] = fma(-col[i], xj, y[q]);
         }
     }
+}
+
+// The whole CTA solves L U y = z for the right-hand sides held by its active
+// warps (y distributed as in warp_lu_solve), the factor read from global
+// memory in chunks of cw columns staged in shared memory (cw * NMAX elements),
+// so each dependent step reads shared memory, not L2.  Every thread calls it.
+template <typename T>
+__device__ void block_lu_solve(const T *W, int ldw, int n, T *stage, int cw, bool active, T (&y)[bt::NQ]) {
+    using namespace bt;
+    const int lane = threadIdx.x & 31;
+    for (int j0 = 0; j0 < n; j0 += cw) {  // forward, unit lower
+        const int jn = min(cw, n - j0);
+        __syncthreads();
+        for (int e = threadIdx.x; e < jn * n; e += NT) {
+            const int j = e / n, r = e - j * n;
+            stage[r + j * NMAX] = W[r + (i64)(j0 + j) * ldw];
+        }
+        __syncthreads();
+        if (active) {
+            for (int jj = 0; jj < jn; ++jj) {
+                const int j = j0 + jj, qj = j >> 5, lj = j & 31;
+                T src = y[0];
+#pragma unroll
+                for (int q = 1; q < NQ; ++q)
+                    if (q == qj) src = y[q];
+                const T yj = __shfl_sync(0xffffffffu, src, lj);
+                const T *col = stage + jj * NMAX;
+#pragma unroll
+                for (int q = 0; q < NQ; ++q) {
+                    const int i = lane + 32 * q;
+                    if (i > j && i < n) y[q] = fma(-col[i], yj, y[q]);
+                }
+            }
+        }
+    }
+    for (int j1 = n; j1 > 0; j1 -= cw) {  // backward, upper
+        const int j0 = max(0, j1 - cw), jn = j1 - j0;
+        __syncthreads();
+        for (int e = threadIdx.x; e < jn * n; e += NT) {
+            const int j = e / n, r = e - j * n;
+            stage[r + j * NMAX] = W[r + (i64)(j0 + j) * ldw];
+        }
+        __syncthreads();
+        if (active) {
+            for (int j = j1 - 1; j >= j0; --j) {
+                const int qj = j >> 5, lj = j & 31;
+                T src = y[0];
+#pragma unroll
+                for (int q = 1; q < NQ; ++q)
+                    if (q == qj) src = y[q];
+                const T *col = stage + (j - j0) * NMAX;
+                const T xj = __shfl_sync(0xffffffffu, src, lj) / col[j];
+                if (lane == lj) {
+#pragma unroll
+                    for (int q = 0; q < NQ; ++q)
+                        if (q == qj) y[q] = xj;
+                }
+#pragma unroll
+                for (int q = 0; q < NQ; ++q) {
+                    const int i = lane + 32 * q;
+                    if (i < j) y[q] = fma(-col[i], xj, y[q]);
+                }
+            }
+        }
+    }
+    __syncthreads();
 }
 
 __device__ __forceinline__ int bucket_of(int n) { return (n - 1) >> 5; }
@@ -501,48 +610,62 @@ __global__ void __launch_bounds__(bt::NT, 2) k_lu_batched(const __grid_constant_
         __syncthreads();
 
         if constexpr (sizeof(T) == 8) {
-            // plain solve in place in B
-            for (int r = warp; r < nr; r += NW) {
-                double *b = B + (i64)r * ldb;
+            // plain solve in place in B: warp r takes right-hand side r (nr <= 8 warps)
+            {
+                const bool active = warp < nr;
+                double *b = active ? B + (i64)warp * ldb : nullptr;
                 T y[NQ];
 #pragma unroll
                 for (int q = 0; q < NQ; ++q) {
                     const int i = lane + 32 * q;
-                    y[q] = (i < n) ? (T)b[S.perm[i]] : T(0);
+                    y[q] = (active && i < n) ? (T)b[S.perm[i]] : T(0);
                 }
                 __syncwarp();
-                warp_lu_solve<T>(W, ldw, n, y);
+                if (in_smem) {
+                    if (active) warp_lu_solve<T>(W, ldw, n, y);
+                } else {
+                    block_lu_solve<T>(W, ldw, n, sP, nb, active, y);
+                }
+                if (active) {
 #pragma unroll
-                for (int q = 0; q < NQ; ++q) {
-                    const int i = lane + 32 * q;
-                    if (i < n) b[i] = y[q];
+                    for (int q = 0; q < NQ; ++q) {
+                        const int i = lane + 32 * q;
+                        if (i < n) b[i] = y[q];
+                    }
                 }
             }
             __syncthreads();
         } else {
             // correction of each right-hand side by its warp: sX (+)= C (LU)^-1 P (R^-1 r / s) s
             auto correct = [&](bool add) {
-                for (int r = warp; r < nr; r += NW) {
-                    const double *rr = sR + r * NMAX;
+                const bool active = warp < nr;  // warp r takes right-hand side r
+                double sc = 0.0;
+                T y[NQ];
+#pragma unroll
+                for (int q = 0; q < NQ; ++q) y[q] = T(0);
+                if (active) {
+                    const double *rr = sR + warp * NMAX;
                     double mx = 0.0;
                     for (int i = lane; i < n; i += 32) mx = fmax(mx, fabs(rr[i] / S.rows[i]));
 #pragma unroll
                     for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
-                    if (!isfinite(mx)) mx = INFINITY;
-                    const double sc = isfinite(mx) ? binary_scale(mx) : 0.0;
-                    T y[NQ];
+                    sc = isfinite(mx) ? binary_scale(mx) : 0.0;
 #pragma unroll
                     for (int q = 0; q < NQ; ++q) {
                         const int i = lane + 32 * q;
-                        T v = T(0);
                         if (i < n && sc != 0.0) {
                             const int p = S.perm[i];
-                            v = (T)((rr[p] / S.rows[p]) / sc);
+                            y[q] = (T)((rr[p] / S.rows[p]) / sc);
                         }
-                        y[q] = v;
                     }
-                    warp_lu_solve<T>(W, ldw, n, y);
-                    double *xx = sX + r * NMAX;
+                }
+                if (in_smem) {
+                    if (active) warp_lu_solve<T>(W, ldw, n, y);
+                } else {
+                    block_lu_solve<T>(W, ldw, n, sP, nb, active, y);
+                }
+                if (active) {
+                    double *xx = sX + warp * NMAX;
 #pragma unroll
                     for (int q = 0; q < NQ; ++q) {
                         const int i = lane + 32 * q;
@@ -653,7 +776,9 @@ static int batch_grid(oxi_handle_s *h, int mode, int smem, int count) {
     const void *kern = (mode == MODE_MIXED) ? (const void *)k_lu_batched<float> : (const void *)k_lu_batched<double>;
     int optin = 0;
     OXI_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
-    const int limit = optin - (int)sizeof(Misc);
+    cudaFuncAttributes fa;
+    OXI_CUDA(cudaFuncGetAttributes(&fa, kern));
+    const int limit = optin - (int)fa.sharedSizeBytes;  // the kernel's own static shared memory
     if (smem > limit) throw CudaError{cudaErrorInvalidValue, "batched tuning exceeds shared memory"};
     set_max_dyn_smem(kern, limit);
     int per_sm = 0;
@@ -840,7 +965,7 @@ static float time_batched(oxi_handle_s *h, BatchDesc d, const int (&nb)[bt::NBUC
     const int smem = batch_smem_layout(d.mode == MODE_MIXED ? 4 : 8, d.mode, n_smem, d.nbmax, &d);
     int optin = 0;
     OXI_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
-    if (smem + (int)sizeof(Misc) > optin) return INFINITY;
+    if (smem + (int)sizeof(Misc) + 256 > optin) return INFINITY;  // static part: Misc plus alignment
     const int grid = batch_grid(h, d.mode, smem, d.count);
     if (d.mode == MODE_MIXED) d.wsp = (float *)h->batch_wsp.get(sizeof(float) * (size_t)NMAX * NMAX * grid);
     cudaEvent_t e0, e1;
@@ -1022,7 +1147,7 @@ extern "C" int oxi_batched_set_tuning(oxi_handle_t h, int prec, int32_t n_smem, 
     int optin = 0;
     if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device) != cudaSuccess)
         return OXI_ECUDA;
-    if (smem + (int)sizeof(oxi::Misc) > optin) return OXI_EINVAL;
+    if (smem + (int)sizeof(oxi::Misc) + 256 > optin) return OXI_EINVAL;
     auto &tn = h->btune[prec == OXI_PREC_FP64 ? 0 : 1];
     tn.tuned = true;
     tn.n_smem = n_smem;
