@@ -140,6 +140,31 @@ __device__ __forceinline__ void warp_argmax(uint64_t &key, int &pos) {
     }
 }
 
+// A row of W elements between registers and 16-byte-aligned shared memory.
+template <typename T, int W>
+__device__ __forceinline__ void store_row(T *dst, const T (&v)[W]) {
+    constexpr int VEC = 16 / sizeof(T);
+#pragma unroll
+    for (int c = 0; c < W; c += VEC) {
+        int4 x;
+        T *xx = (T *)&x;
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) xx[e] = v[c + e];
+        *(int4 *)(dst + c) = x;
+    }
+}
+template <typename T, int W>
+__device__ __forceinline__ void load_row(T (&v)[W], const T *src) {
+    constexpr int VEC = 16 / sizeof(T);
+#pragma unroll
+    for (int c = 0; c < W; c += VEC) {
+        const int4 x = *(const int4 *)(src + c);
+        const T *xx = (const T *)&x;
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) v[c + e] = xx[e];
+    }
+}
+
 constexpr int LEAF_NT = 512;
 constexpr int LEAF_MAX_CS = 16;
 
@@ -247,60 +272,65 @@ k_leaf_lu(T *__restrict__ P, i64 ld, int m, int wact, i64 gofs, int64_t *__restr
 #pragma unroll
             for (int k = 0; k < R; ++k)
                 if (k == kk) {
-#pragma unroll
-                    for (int c = 0; c < W; ++c) s_myrow[c] = r[k][c];
-                    s_myid = id[k];
+                    if (CS == 1) {  // a single CTA stages straight into the slots it reads
+                        store_row<T, W>(&s_crow[par][0][0], r[k]);
+                        s_cmeta[par][0] = make_uint4((uint32_t)ck, (uint32_t)(ck >> 32), (uint32_t)cp, (uint32_t)id[k]);
+                    } else {
+                        store_row<T, W>(s_myrow, r[k]);
+                        s_myid = id[k];
+                    }
                 }
         }
+        if (CS == 1 && t == 0 && cp == INT_MAX) s_cmeta[par][0] = make_uint4(0u, 0u, (uint32_t)INT_MAX, 0u);
         const bool own_j = (g == j);  // position j: slot 0 of thread j of CTA 0
         if (own_j) {
-#pragma unroll
-            for (int c = 0; c < W; ++c) s_jrow[c] = r[0][c];
-            s_jid = id[0];
+            if (CS == 1) {
+                store_row<T, W>(&s_jslot[par][0], r[0]);
+                s_jmeta[par] = make_uint4((uint32_t)id[0], 0u, 0u, 0u);
+            } else {
+                store_row<T, W>(s_jrow, r[0]);
+                s_jid = id[0];
+            }
         }
         __syncthreads();
-        // (d) every CTA's candidate (warp 0) and row j (warp 1 of CTA 0) into every
-        // CTA's slots of this parity.  Across CTAs each 16-byte store completes its
-        // bytes on the receiver's exchange barrier (st.async), and each CTA waits
-        // only on its own barrier: no cluster-wide barrier per column.  A slot is
+        // (d) every CTA's candidate and, from CTA 0, row j into every CTA's slots
+        // of this parity.  Across CTAs each 16-byte store completes its bytes on
+        // the receiver's exchange barrier (st.async), and each CTA waits only on
+        // its own barrier: no cluster-wide barrier per column.  A slot is
         // rewritten two columns later, after its receiver has pushed the column in
         // between, i.e. after it finished reading the slot.
-        if (CS == 1) {
-            if (warp == 0) {
-                for (int c = lane; c < W; c += 32) s_crow[par][0][c] = s_myrow[c];
-                if (lane == 0)
-                    s_cmeta[par][0] = make_uint4((uint32_t)ck, (uint32_t)(ck >> 32), (uint32_t)cp, (uint32_t)s_myid);
-            } else if (warp == 1) {
-                for (int c = lane; c < W; c += 32) s_jslot[par][c] = s_jrow[c];
-                if (lane == 0) s_jmeta[par] = make_uint4((uint32_t)s_jid, 0u, 0u, 0u);
-            }
-            __syncthreads();
-        } else {
-            constexpr int NCH = W * (int)sizeof(T) / 16;  // 16-byte chunks of a row
-            if (t == 0) mbar_arrive_expect_tx(&s_xbar[par], (uint32_t)((CS + 1) * 16 * (1 + NCH)));
-            if (warp == 0) {
-                for (int e = lane; e < CS * (1 + NCH); e += 32) {
-                    const int dst = e / (1 + NCH), q = e - dst * (1 + NCH);
-                    const uint32_t rbar = cluster_map_u32(&s_xbar[par], dst);
-                    if (q == 0)
-                        st_async_v4(cluster_map_u32(&s_cmeta[par][cr], dst),
-                                    make_uint4((uint32_t)ck, (uint32_t)(ck >> 32), (uint32_t)cp, (uint32_t)s_myid),
-                                    rbar);
-                    else
-                        st_async_v4(cluster_map_u32(&s_crow[par][cr][0], dst) + 16u * (q - 1),
-                                    reinterpret_cast<const uint4 *>(s_myrow)[q - 1], rbar);
+        if (CS > 1) {
+            constexpr int PER = 1 + W * (int)sizeof(T) / 16;  // stores per row: meta + 16-byte chunks
+            const int npush = CS * PER;                          // this CTA's candidate, to every CTA
+            if (t == 0) mbar_arrive_expect_tx(&s_xbar[par], (uint32_t)((CS + 1) * 16 * PER));
+            // One 16-byte store per thread, spread over the CTA's warps so that no
+            // warp issues more than one round: the candidate on threads
+            // 0..npush-1 and, in CTA 0, row j on the next npush.
+            const int nall = (cr == 0) ? 2 * npush : npush;
+            for (int e = t; e < nall; e += NT) {
+                const bool jr = e >= npush;
+                const int ee = jr ? e - npush : e;
+                const int dst = ee / PER, qq = ee - dst * PER;
+                uint4 v;
+                uint32_t raddr;
+                if (!jr) {
+                    if (qq == 0) {
+                        v = make_uint4((uint32_t)ck, (uint32_t)(ck >> 32), (uint32_t)cp, (uint32_t)s_myid);
+                        raddr = cluster_map_u32(&s_cmeta[par][cr], dst);
+                    } else {
+                        v = reinterpret_cast<const uint4 *>(s_myrow)[qq - 1];
+                        raddr = cluster_map_u32(&s_crow[par][cr][0], dst) + 16u * (qq - 1);
+                    }
+                } else {
+                    if (qq == 0) {
+                        v = make_uint4((uint32_t)s_jid, 0u, 0u, 0u);
+                        raddr = cluster_map_u32(&s_jmeta[par], dst);
+                    } else {
+                        v = reinterpret_cast<const uint4 *>(s_jrow)[qq - 1];
+                        raddr = cluster_map_u32(&s_jslot[par][0], dst) + 16u * (qq - 1);
+                    }
                 }
-            } else if (warp == 1 && cr == 0) {
-                for (int e = lane; e < CS * (1 + NCH); e += 32) {
-                    const int dst = e / (1 + NCH), q = e - dst * (1 + NCH);
-                    const uint32_t rbar = cluster_map_u32(&s_xbar[par], dst);
-                    if (q == 0)
-                        st_async_v4(cluster_map_u32(&s_jmeta[par], dst), make_uint4((uint32_t)s_jid, 0u, 0u, 0u),
-                                    rbar);
-                    else
-                        st_async_v4(cluster_map_u32(&s_jslot[par][0], dst) + 16u * (q - 1),
-                                    reinterpret_cast<const uint4 *>(s_jrow)[q - 1], rbar);
-                }
+                st_async_v4(raddr, v, cluster_map_u32(&s_xbar[par], dst));
             }
             if (!dead && !mbar_wait(&s_xbar[par], (uint32_t)((j >> 1) & 1), &g_leaf_err, 1)) dead = true;
         }
@@ -324,38 +354,12 @@ k_leaf_lu(T *__restrict__ P, i64 ld, int m, int wact, i64 gofs, int64_t *__restr
             // zero pivot: info, no interchange, no elimination (the column is all zero)
             if (t == 0 && s_info == 0) s_info = j + 1;
         } else {
-            // the pivot row in registers when they can spare it, else read from shared memory
             const int live = W - j;  // slots 1..live-1 hold the unfinished columns
-            constexpr bool U_REGS = (W * (R + 1) * (int)sizeof(T) / 4) <= 64;
-            T u[U_REGS ? W : 1];
-            if constexpr (U_REGS) {
-#pragma unroll
-                for (int c = 0; c < W; c += VEC) {
-                    const int4 v = *(const int4 *)(prow + c);
-                    const T *vv = (const T *)&v;
-#pragma unroll
-                    for (int e = 0; e < VEC; ++e) u[c + e] = vv[e];
-                }
-            }
-            auto U = [&](int c) -> T {
-                if constexpr (U_REGS) return u[c];
-                else return prow[c];
-            };
-            // the update multiplies by Uz: the pivot row with its finished slots zeroed
-            T uz[U_REGS ? W : 1];
-            if constexpr (U_REGS) {
-#pragma unroll
-                for (int c = 0; c < W; ++c) uz[c] = (c < live) ? u[c] : T(0);
-            }
-            auto UZ = [&](int c) -> T {
-                if constexpr (U_REGS) return uz[c];
-                else return (c < live) ? prow[c] : T(0);
-            };
             // (f) the interchange lands in the two owner threads' registers
             if (wp != j) {
                 if (own_j) {
 #pragma unroll
-                    for (int c = 0; c < W; ++c) r[0][c] = U(c);
+                    for (int c = 0; c < W; ++c) r[0][c] = prow[c];
                     id[0] = pid;
                 }
                 if ((wp & (G - 1)) == g) {
@@ -363,22 +367,30 @@ k_leaf_lu(T *__restrict__ P, i64 ld, int m, int wact, i64 gofs, int64_t *__restr
 #pragma unroll
                     for (int k = 0; k < R; ++k)
                         if (k == kk) {
-#pragma unroll
-                            for (int c = 0; c < W; ++c) r[k][c] = s_jslot[par][c];
+                            load_row<T, W>(r[k], &s_jslot[par][0]);
                             id[k] = (int)s_jmeta[par].x;
                         }
                 }
             }
-            // (g) scale the column and apply the rank-1 update below the pivot
-            // (finished slots see a zero multiplier: fma(-l, 0, a) == a)
+            // (g) scale the column and apply the rank-1 update below the pivot to
+            // the unfinished slots (the compare is uniform across the warp).  FP32
+            // multiplies finished slots by a zero instead of skipping them
+            // (fma(-l, 0, a) == a for finite l), FP64 predicates each slot: the
+            // faster form measured for each
 #pragma unroll
             for (int k = 0; k < R; ++k) {
                 const int i = k * G + g;
                 if (i > j && i < m) {
                     const T l = r[k][0] / d;
                     r[k][0] = l;
+                    if constexpr (sizeof(T) == 4) {
 #pragma unroll
-                    for (int c = 1; c < W; ++c) r[k][c] = fma(-l, UZ(c), r[k][c]);
+                        for (int c = 1; c < W; ++c) r[k][c] = fma(-l, (c < live) ? prow[c] : T(0), r[k][c]);
+                    } else {
+#pragma unroll
+                        for (int c = 1; c < W; ++c)
+                            if (c < live) r[k][c] = fma(-l, prow[c], r[k][c]);
+                    }
                 }
             }
         }
