@@ -89,6 +89,13 @@ class Clocks:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            # nvidia-smi's start-up takes host CPU for a few hundred ms: let it
+            # settle (first sample written) so it does not slow the timed steps'
+            # host-side launches
+            t0 = time.time()
+            while time.time() - t0 < 3.0 and os.path.getsize(self.path) == 0:
+                time.sleep(0.05)
+            time.sleep(0.2)
         except (OSError, FileNotFoundError):
             self.proc = None
         return self

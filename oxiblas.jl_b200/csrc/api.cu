@@ -78,6 +78,9 @@ int oxi_destroy(oxi_handle_t h) {
     h->batch_wsp.release();
     if (h->aux_stream) cudaStreamDestroy(h->aux_stream);
     if (h->la_stream) cudaStreamDestroy(h->la_stream);
+    if (h->la_main) cudaStreamDestroy(h->la_main);
+    if (h->la_in) cudaEventDestroy(h->la_in);
+    if (h->la_out) cudaEventDestroy(h->la_out);
     if (h->la_fork) cudaEventDestroy(h->la_fork);
     if (h->la_join) cudaEventDestroy(h->la_join);
     if (h->aux_fork) cudaEventDestroy(h->aux_fork);

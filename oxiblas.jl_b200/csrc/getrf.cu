@@ -133,7 +133,9 @@ void getrf_rowmajor(oxi_handle_s *h, T *W, i64 ld, i64 m, i64 n, int64_t *d_ipiv
     LuRun<T> R{h, W, ld, m, n, n, d_ipiv, d_info, d_moves, d_nmoves};
     const i64 q = std::min(m, n);
     const i64 nb = std::max<i64>(h->opt.blocksize, 1);
-    const bool compose = nb > 32 && n > nb;  // worth it when a panel holds several leaves
+    // worth it when a panel holds several leaves; the leaf itself moves the rows
+    // of panels up to LEAF_MAX_OTHER columns wider than a leaf
+    const bool compose = nb > 32 && n > nb && nb <= LEAF_MAX_OTHER;
     if (compose) {
         char *ws = (char *)h->rowmap_ws.get(sizeof(int) * (size_t)(m + 8 * nb + 128));
         R.map = (int *)ws;
@@ -154,12 +156,27 @@ void getrf_rowmajor(oxi_handle_s *h, T *W, i64 ld, i64 m, i64 n, int64_t *d_ipiv
     bool la = h->opt.lookahead && compose;
     if constexpr (sizeof(T) == 8) la = false;
     else if (h->trailing == TRAIL_NATIVE) la = false;
-    cudaStream_t sA = h->stream;
+    // With lookahead the panels run on a stream of the highest priority and the
+    // trailing update on one of the lowest: when SMs free up, the block scheduler
+    // serves the panel's kernels (the leaf's 16-CTA cluster needs 16 SMs of one
+    // GPC) before the update's.
+    const cudaStream_t caller = h->stream;
     if (la && !h->la_stream) {
-        OXI_CUDA(cudaStreamCreateWithFlags(&h->la_stream, cudaStreamNonBlocking));
+        int lo = 0, hi = 0;
+        OXI_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+        OXI_CUDA(cudaStreamCreateWithPriority(&h->la_stream, cudaStreamNonBlocking, lo));
+        OXI_CUDA(cudaStreamCreateWithPriority(&h->la_main, cudaStreamNonBlocking, hi));
         OXI_CUDA(cudaEventCreateWithFlags(&h->la_fork, cudaEventDisableTiming));
         OXI_CUDA(cudaEventCreateWithFlags(&h->la_join, cudaEventDisableTiming));
+        OXI_CUDA(cudaEventCreateWithFlags(&h->la_in, cudaEventDisableTiming));
+        OXI_CUDA(cudaEventCreateWithFlags(&h->la_out, cudaEventDisableTiming));
     }
+    if (la) {
+        OXI_CUDA(cudaEventRecord(h->la_in, caller));
+        OXI_CUDA(cudaStreamWaitEvent(h->la_main, h->la_in, 0));
+        h->stream = h->la_main;
+    }
+    cudaStream_t sA = h->stream;
     bool b_pending = false;
     auto update = [&](i64 f, i64 l, i64 c0, i64 c1) {  // W[l:m, c0:c1] -= L21 U12[:, c0:c1]
         if constexpr (sizeof(T) == 4) {
@@ -230,8 +247,13 @@ void getrf_rowmajor(oxi_handle_s *h, T *W, i64 ld, i64 m, i64 n, int64_t *d_ipiv
             b_pending = true;
         }
         if (b_pending) OXI_CUDA(cudaStreamWaitEvent(sA, h->la_join, 0));
+        if (la) {
+            OXI_CUDA(cudaEventRecord(h->la_out, sA));
+            OXI_CUDA(cudaStreamWaitEvent(caller, h->la_out, 0));
+        }
+        h->stream = caller;
     } catch (...) {
-        h->stream = sA;
+        h->stream = caller;
         h->tc_slot = 0;
         h->gemm_ctas = 0;
         throw;
@@ -298,7 +320,7 @@ void getrf_rowmajor_cached(oxi_handle_s *h, T *W, i64 ld, i64 m, i64 n, int64_t 
                 throw;
             }
             OXI_CUDA(cudaStreamEndCapture(h->stream, &gc.graph));
-            OXI_CUDA(cudaGraphInstantiate(&gc.exec, gc.graph, 0));
+            OXI_CUDA(cudaGraphInstantiate(&gc.exec, gc.graph, cudaGraphInstantiateFlagUseNodePriority));
             std::memcpy(gc.key, key, sizeof(key));
             gc.valid = true;
             gc.seen = 2;

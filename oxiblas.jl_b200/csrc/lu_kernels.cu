@@ -180,7 +180,10 @@ k_leaf_lu(T *__restrict__ P, i64 ld, int m, int wact, i64 gofs, int64_t *__restr
     const int cr = (int)cl.block_rank();
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     constexpr int NW = NT / 32;
-    constexpr int MOVE_ELEMS = 16384 / NT;  // (moved rows x other panel columns) per thread, at most
+    // in-leaf row moves: at most 2W moved rows, over at least 8 warps; at most
+    // LEAF_MAX_OTHER other panel columns, in 32-column chunks
+    constexpr int MOVE_PW = (2 * W + NW - 1) / NW;
+    constexpr int MOVE_CH = LEAF_MAX_OTHER / 32;
     constexpr int VEC = 16 / sizeof(T);  // elements per 16-byte vector
     const int G = CS * NT;  // a power of two: positions split by shift and mask
     const int lgG = __ffs(G) - 1;
@@ -447,17 +450,27 @@ k_leaf_lu(T *__restrict__ P, i64 ld, int m, int wact, i64 gofs, int64_t *__restr
         __threadfence();
         if (CS > 1) cl.sync(); else __syncthreads();
         const int cnt = min(*(volatile int *)nmoves, 2 * W);
-        const int tot = cnt * pn.nother;
-        T vals[MOVE_ELEMS];
+        // One warp per moved row (warps of the whole cluster, in turn), one lane
+        // per column of each 32-column chunk: no division, and the leaf's rows are
+        // stored, so their registers are free for the staged values.
+        const int gw = cr * NW + warp, nwc = CS * NW;
+        const int nother = pn.nother;
+        T vals[MOVE_PW][MOVE_CH];
+        int dsts[MOVE_PW];
         int mapv[R];
 #pragma unroll
-        for (int q = 0; q < MOVE_ELEMS; ++q) {
-            const int e = g + q * G;
-            if (e < tot) {
-                const int mv = e / pn.nother, oc = e - mv * pn.nother;
-                const int col = oc < pn.left_n ? pn.pc_lo + oc : pn.right_lo + (oc - pn.left_n);
+        for (int mi = 0; mi < MOVE_PW; ++mi) {
+            const int mv = gw + mi * nwc;
+            dsts[mi] = -1;
+            if (mv < cnt) {
                 const int src = __ldcg(&moves[2 * mv + 1]);
-                vals[q] = P[(i64)src * ld + (col - pn.leaf_c0)];
+                dsts[mi] = __ldcg(&moves[2 * mv]);
+                const T *srow = P + (i64)src * ld - pn.leaf_c0;
+#pragma unroll
+                for (int ci = 0; ci < MOVE_CH; ++ci) {
+                    const int oc = ci * 32 + lane;
+                    if (oc < nother) vals[mi][ci] = srow[oc < pn.left_n ? pn.pc_lo + oc : pn.right_lo + (oc - pn.left_n)];
+                }
             }
         }
 #pragma unroll
@@ -467,13 +480,14 @@ k_leaf_lu(T *__restrict__ P, i64 ld, int m, int wact, i64 gofs, int64_t *__restr
         }
         if (CS > 1) cl.sync(); else __syncthreads();
 #pragma unroll
-        for (int q = 0; q < MOVE_ELEMS; ++q) {
-            const int e = g + q * G;
-            if (e < tot) {
-                const int mv = e / pn.nother, oc = e - mv * pn.nother;
-                const int col = oc < pn.left_n ? pn.pc_lo + oc : pn.right_lo + (oc - pn.left_n);
-                const int dst = __ldcg(&moves[2 * mv]);
-                P[(i64)dst * ld + (col - pn.leaf_c0)] = vals[q];
+        for (int mi = 0; mi < MOVE_PW; ++mi) {
+            if (dsts[mi] >= 0) {
+                T *drow = P + (i64)dsts[mi] * ld - pn.leaf_c0;
+#pragma unroll
+                for (int ci = 0; ci < MOVE_CH; ++ci) {
+                    const int oc = ci * 32 + lane;
+                    if (oc < nother) drow[oc < pn.left_n ? pn.pc_lo + oc : pn.right_lo + (oc - pn.left_n)] = vals[mi][ci];
+                }
             }
         }
 #pragma unroll
@@ -530,7 +544,7 @@ static void launch_leaf_wr(T *P, i64 ld, i64 m, int w, i64 gofs, int64_t *ipiv, 
     at[0].val.clusterDim.z = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    if ((i64)pn.nother * 2 * W > (i64)16384 * cs)
+    if (pn.nother > LEAF_MAX_OTHER)
         throw CudaError{cudaErrorInvalidValue, "panel too wide for the in-leaf row moves"};
     ProfScope ps(KC_LEAF, s, 0.0, 2.0 * (double)m * w * sizeof(T));
     OXI_CUDA(cudaLaunchKernelEx(&cfg, kern, P, ld, (int)m, w, gofs, ipiv, info, moves, nmoves, pn));

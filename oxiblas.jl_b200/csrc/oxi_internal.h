@@ -117,6 +117,8 @@ struct oxi_handle_s {
     int tc_slot = 0;             // which of the two operand buffers (and scale slots) to use
     int gemm_ctas = 0;           // > 0: cap on the persistent tensor-core GEMM's CTAs
     cudaStream_t la_stream = nullptr;        // lookahead: the trailing update's stream
+    cudaStream_t la_main = nullptr;          // lookahead: the panels' stream (highest priority)
+    cudaEvent_t la_in = nullptr, la_out = nullptr;  // caller's stream -> la_main -> caller's stream
     cudaEvent_t la_fork = nullptr, la_join = nullptr;
     oxi::DeviceBuffer xtag_ws;   // tagged solution words of the FP32 triangular solves
     oxi::DeviceBuffer rowmap_ws; // per-panel row map and composite move list
@@ -200,6 +202,10 @@ void launch_rm_to_cm(const TS *W, i64 ldw, TD *A, i64 lda, i64 m, i64 n, cudaStr
 // (columns [pc_lo, pc_lo + left_n) and [right_lo, right_lo + nother - left_n),
 // absolute) and to the panel row map (map[map_off + position]); nother = 0 and
 // map = null switch it off.
+// Other panel columns (panel width minus the leaf's) that the in-leaf row moves
+// reach; wider panels apply each leaf's interchanges with separate row moves.
+constexpr int LEAF_MAX_OTHER = 256;
+
 struct LeafPanel {
     int nother = 0, left_n = 0, pc_lo = 0, right_lo = 0, leaf_c0 = 0, map_off = 0;
     int *map = nullptr;
