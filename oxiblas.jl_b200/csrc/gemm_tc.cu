@@ -376,15 +376,52 @@ void launch_gemm_tc(int fmt /*0 fp16, 1 bf16*/, float *C, i64 ldc, const void *A
         OXI_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     }
     const i64 tiles = ((N + BN - 1) / BN) * ((M + BM - 1) / BM);
-    dim3 grid((unsigned)std::min<i64>(tiles, max_ctas > 0 ? std::min(max_ctas, sms) : sms));
-    ProfScope ps(KC_GEMM_TC, s, 2.0 * M * N * K, 8.0 * M * N + 2.0 * (M + N) * K);
-    if (fmt == 1) {
-        set_max_dyn_smem((const void *)k_gemm_tc<1>, SMEM_BYTES);
-        k_gemm_tc<1><<<grid, NTHREADS, SMEM_BYTES, s>>>(tmA, tmB, tmC, (int)M, (int)N, (int)K, scale, d_scale);
+    const void *kern = fmt == 1 ? (const void *)k_gemm_tc<1> : (const void *)k_gemm_tc<0>;
+    set_max_dyn_smem(kern, SMEM_BYTES);
+    cudaLaunchConfig_t cfg = {};
+    cfg.blockDim = dim3(NTHREADS);
+    cfg.dynamicSmemBytes = SMEM_BYTES;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    if (max_ctas == GEMM_CTAS_SPARE_GPC) {
+        // Persistent CTAs in clusters of GEMM_GPC_CLUSTER: each cluster fills the
+        // SMs of one GPC, and one cluster fewer than fit leaves a whole GPC to a
+        // concurrent leaf LU (a cluster of up to 16 CTAs on one GPC).  The kernel
+        // itself uses no cluster feature.
+        static int ncl[2] = {-1, -1};
+        int &nc = ncl[fmt == 1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = GEMM_GPC_CLUSTER;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        if (nc < 0) {
+            OXI_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+            cfg.gridDim = dim3(GEMM_GPC_CLUSTER);
+            int v = 0;
+            if (cudaOccupancyMaxActiveClusters(&v, kern, &cfg) != cudaSuccess) {
+                cudaGetLastError();
+                v = 0;
+            }
+            nc = v;
+        }
+        if (nc >= 2) {
+            const i64 want = (tiles + GEMM_GPC_CLUSTER - 1) / GEMM_GPC_CLUSTER * GEMM_GPC_CLUSTER;
+            cfg.gridDim = dim3((unsigned)std::min<i64>(want, (i64)(nc - 1) * GEMM_GPC_CLUSTER));
+        } else {  // no whole GPC to spare: plain launch leaving some SMs
+            cfg.attrs = nullptr;
+            cfg.numAttrs = 0;
+            cfg.gridDim = dim3((unsigned)std::min<i64>(tiles, std::max(1, sms - 24)));
+        }
     } else {
-        set_max_dyn_smem((const void *)k_gemm_tc<0>, SMEM_BYTES);
-        k_gemm_tc<0><<<grid, NTHREADS, SMEM_BYTES, s>>>(tmA, tmB, tmC, (int)M, (int)N, (int)K, scale, d_scale);
+        cfg.gridDim = dim3((unsigned)std::min<i64>(tiles, max_ctas > 0 ? std::min(max_ctas, sms) : sms));
     }
+    ProfScope ps(KC_GEMM_TC, s, 2.0 * M * N * K, 8.0 * M * N + 2.0 * (M + N) * K);
+    if (fmt == 1)
+        OXI_CUDA(cudaLaunchKernelEx(&cfg, k_gemm_tc<1>, tmA, tmB, tmC, (int)M, (int)N, (int)K, scale, d_scale));
+    else
+        OXI_CUDA(cudaLaunchKernelEx(&cfg, k_gemm_tc<0>, tmA, tmB, tmC, (int)M, (int)N, (int)K, scale, d_scale));
     OXI_LAUNCH_CHECK();
 }
 

@@ -235,7 +235,7 @@ void getrf_rowmajor(oxi_handle_s *h, T *W, i64 ld, i64 m, i64 n, int64_t *d_ipiv
             // SMs left free for the next panel's cluster
             h->stream = h->la_stream;
             h->tc_slot = 1;
-            h->gemm_ctas = std::max(1, h->sm_count - 24);
+            h->gemm_ctas = GEMM_CTAS_SPARE_GPC;
             launch_rowmoves_big<T>(W, ld, f, list, listcnt, maxcnt, 0, f, h->stream);
             launch_rowmoves_big<T>(W, ld, f, list, listcnt, maxcnt, l2, R.ncols_moved, h->stream);
             trsm_lower_unit<T>(h, L11, ld, W + f * ld + l2, ld, l - f, n - l2);

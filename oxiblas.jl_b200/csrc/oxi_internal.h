@@ -115,7 +115,8 @@ struct oxi_handle_s {
     oxi::DeviceBuffer tc_ws;     // 16-bit GEMM operands
     oxi::DeviceBuffer tc_ws2;    // the same for a second, concurrent trailing update
     int tc_slot = 0;             // which of the two operand buffers (and scale slots) to use
-    int gemm_ctas = 0;           // > 0: cap on the persistent tensor-core GEMM's CTAs
+    int gemm_ctas = 0;           // > 0: cap on the persistent tensor-core GEMM's CTAs;
+                                 // GEMM_CTAS_SPARE_GPC: leave one GPC free
     cudaStream_t la_stream = nullptr;        // lookahead: the trailing update's stream
     cudaStream_t la_main = nullptr;          // lookahead: the panels' stream (highest priority)
     cudaEvent_t la_in = nullptr, la_out = nullptr;  // caller's stream -> la_main -> caller's stream
@@ -205,6 +206,11 @@ void launch_rm_to_cm(const TS *W, i64 ldw, TD *A, i64 lda, i64 m, i64 n, cudaStr
 // Other panel columns (panel width minus the leaf's) that the in-leaf row moves
 // reach; wider panels apply each leaf's interchanges with separate row moves.
 constexpr int LEAF_MAX_OTHER = 256;
+
+// gemm_ctas value asking the persistent tensor-core GEMM to leave one whole GPC
+// free (clusters of GEMM_GPC_CLUSTER CTAs, one per GPC, one cluster fewer than fit)
+constexpr int GEMM_CTAS_SPARE_GPC = -1;
+constexpr int GEMM_GPC_CLUSTER = 16;
 
 struct LeafPanel {
     int nother = 0, left_n = 0, pc_lo = 0, right_lo = 0, leaf_c0 = 0, map_off = 0;
