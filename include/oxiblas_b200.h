@@ -274,6 +274,10 @@ enum oxi_kernel_class {
     OXI_K_GEMM_TC, OXI_K_CONVERT, OXI_K_TRSV, OXI_K_RESIDUAL, OXI_K_OTHER, OXI_K_COUNT
 };
 int oxi_profile_enable(oxi_handle_t h, int on);  /* also clears the records */
+/* The profiled launches in issue order, 4 doubles each: kernel class, stream
+ * index (order of first use), start and end in ms from the first launch's start.
+ * *count = the number of records (at most max written). */
+int oxi_profile_timeline(oxi_handle_t h, int64_t max, double *out, int64_t *count);
 int oxi_profile_read(oxi_handle_t h, int kind, int64_t *launches, double *total_ms,
                      double *flops, double *bytes);
 int oxi_launch_count(oxi_handle_t h, int64_t *count);

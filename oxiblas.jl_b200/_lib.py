@@ -74,6 +74,7 @@ _SIGS = {
     "oxi_sgemm_update_lowp": ([_vp, ctypes.c_int, _i64, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64],
                               ctypes.c_int),
     "oxi_profile_enable": ([_vp, ctypes.c_int], ctypes.c_int),
+    "oxi_profile_timeline": ([_vp, _i64, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_i64)], ctypes.c_int),
     "oxi_profile_read": ([_vp, ctypes.c_int, ctypes.POINTER(_i64), ctypes.POINTER(ctypes.c_double),
                           ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
     "oxi_launch_count": ([_vp, ctypes.POINTER(_i64)], ctypes.c_int),
@@ -163,6 +164,15 @@ class Handle:
             if c.value:
                 out[name] = (int(c.value), ms.value, fl.value, by.value)
         return out
+
+    def profile_timeline(self, max_records: int = 1 << 16):
+        """[(class, stream index, start ms, end ms)] of the profiled launches."""
+        buf = (ctypes.c_double * (4 * max_records))()
+        cnt = _i64(0)
+        self.check(self.lib.oxi_profile_timeline(self.ptr, max_records, buf, ctypes.byref(cnt)))
+        n = min(int(cnt.value), max_records)
+        return [(self.KERNEL_CLASSES[int(buf[4 * i])], int(buf[4 * i + 1]), buf[4 * i + 2], buf[4 * i + 3])
+                for i in range(n)]
 
     def launches(self) -> int:
         v = _i64(0)

@@ -4,6 +4,7 @@
 #include <mutex>
 #include <set>
 #include <tuple>
+#include <vector>
 #include "oxi_internal.h"
 
 namespace oxi {
@@ -257,6 +258,32 @@ int oxi_profile_read(oxi_handle_t h, int kind, int64_t *launches, double *total_
     if (total_ms) *total_ms = ms;
     if (flops) *flops = fl;
     if (bytes) *bytes = by;
+    return OXI_OK;
+}
+
+int oxi_profile_timeline(oxi_handle_t h, int64_t max, double *out, int64_t *count) {
+    if (!h || !count || (max > 0 && !out)) return OXI_EINVAL;
+    cudaSetDevice(h->device);
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) return OXI_ECUDA;
+    std::vector<cudaStream_t> seen;
+    int64_t k = 0;
+    const auto &recs = h->prof.recs;
+    for (size_t i = 0; i < recs.size(); ++i) {
+        if (k >= max) { ++k; continue; }
+        float t0 = 0, t1 = 0;
+        if (cudaEventElapsedTime(&t0, recs[0].a, recs[i].a) != cudaSuccess ||
+            cudaEventElapsedTime(&t1, recs[0].a, recs[i].b) != cudaSuccess)
+            return OXI_ECUDA;
+        size_t sid = 0;
+        while (sid < seen.size() && seen[sid] != recs[i].s) ++sid;
+        if (sid == seen.size()) seen.push_back(recs[i].s);
+        out[4 * k] = recs[i].kind;
+        out[4 * k + 1] = (double)sid;
+        out[4 * k + 2] = t0;
+        out[4 * k + 3] = t1;
+        ++k;
+    }
+    *count = k;
     return OXI_OK;
 }
 

@@ -383,11 +383,11 @@ void launch_gemm_tc(int fmt /*0 fp16, 1 bf16*/, float *C, i64 ldc, const void *A
     cfg.dynamicSmemBytes = SMEM_BYTES;
     cfg.stream = s;
     cudaLaunchAttribute at[1];
-    if (max_ctas == GEMM_CTAS_SPARE_GPC) {
-        // Persistent CTAs in clusters of GEMM_GPC_CLUSTER: each cluster fills the
-        // SMs of one GPC, and one cluster fewer than fit leaves a whole GPC to a
-        // concurrent leaf LU (a cluster of up to 16 CTAs on one GPC).  The kernel
-        // itself uses no cluster feature.
+    if (max_ctas < 0) {
+        // Persistent CTAs in at most -max_ctas clusters of GEMM_GPC_CLUSTER: each
+        // cluster fills the SMs of one GPC, and at least one cluster fewer than
+        // fit leaves a whole GPC to a concurrent leaf LU (a cluster of up to 16
+        // CTAs on one GPC).  The kernel itself uses no cluster feature.
         static int ncl[2] = {-1, -1};
         int &nc = ncl[fmt == 1];
         at[0].id = cudaLaunchAttributeClusterDimension;
@@ -408,7 +408,8 @@ void launch_gemm_tc(int fmt /*0 fp16, 1 bf16*/, float *C, i64 ldc, const void *A
         }
         if (nc >= 2) {
             const i64 want = (tiles + GEMM_GPC_CLUSTER - 1) / GEMM_GPC_CLUSTER * GEMM_GPC_CLUSTER;
-            cfg.gridDim = dim3((unsigned)std::min<i64>(want, (i64)(nc - 1) * GEMM_GPC_CLUSTER));
+            const int use = std::min(nc - 1, -max_ctas);
+            cfg.gridDim = dim3((unsigned)std::min<i64>(want, (i64)use * GEMM_GPC_CLUSTER));
         } else {  // no whole GPC to spare: plain launch leaving some SMs
             cfg.attrs = nullptr;
             cfg.numAttrs = 0;

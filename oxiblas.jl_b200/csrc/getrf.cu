@@ -9,6 +9,7 @@
 // which leaves each column with exactly the interchange sequence the reference
 // applies to it through its left/right laswp calls.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include "oxi_internal.h"
 
@@ -73,8 +74,67 @@ struct LuRun {
     // panel-level composition (null: each leaf moves every column itself)
     int *map = nullptr, *list = nullptr, *listcnt = nullptr;
     int *list2 = nullptr, *listcnt2 = nullptr;  // lookahead: the odd panels' move list
+    float *ubuf = nullptr;  // U12 of the FP32 right-looking panel steps (32 x LEAF_MAX_OTHER)
     i64 pf = 0, pl = 0;  // current panel columns [pf, pl)
 };
+
+// The leaf's row interchanges reach the rest of the current panel [pf, pl)
+// inside the leaf kernel (composed panels).
+template <typename T>
+static LeafPanel leaf_panel(const LuRun<T> &R, i64 c0, i64 w) {
+    LeafPanel pn;
+    pn.left_n = (int)(c0 - R.pf);
+    pn.nother = (int)((c0 - R.pf) + (R.pl - c0 - w));
+    pn.pc_lo = (int)R.pf;
+    pn.right_lo = (int)(c0 + w);
+    pn.leaf_c0 = (int)c0;
+    pn.map = R.map;
+    pn.map_off = (int)(c0 - R.pf);
+    return pn;
+}
+
+// FP32 panel of the mixed solve, right-looking over its leaves: each leaf is
+// followed by one fused launch (U12 solve + rank-w update of the panel's
+// columns to its right), so every in-panel update has K = leaf width, and the
+// TRSM never waits on a separate launch.  The factorization is the same LU
+// with partial pivoting; only the order of the in-panel updates differs from
+// the recursive split.
+template <typename T>
+static void panel_rl(LuRun<T> &R, i64 c0, i64 nc) {
+    oxi_handle_s *h = R.h;
+    const i64 cend = c0 + nc;
+    LeafPanel pend;  // the previous step's U12, still in R.ubuf
+    for (i64 c = c0; c < cend;) {
+        const i64 mrows = R.m - c;
+        if (mrows <= 0) break;
+        const int lw = leaf_width_for<T>(mrows);
+        if (lw == 0) throw CudaError{cudaErrorInvalidValue, "panel taller than the leaf capacity"};
+        const i64 w = std::min<i64>(lw, cend - c);
+        OXI_CUDA(cudaMemsetAsync(R.nmoves, 0, sizeof(int), h->stream));
+        LeafPanel pn = leaf_panel(R, c, w);
+        pn.u_src = pend.u_src;
+        pn.u_dst = pend.u_dst;
+        pn.u_rows = pend.u_rows;
+        pn.u_cols = pend.u_cols;
+        pend = LeafPanel();
+        launch_leaf<T>(R.W + c * R.ld + c, R.ld, mrows, (int)w, c, R.ipiv, R.info, R.moves, R.nmoves, lw,
+                       h->stream, pn);
+        if constexpr (sizeof(T) == 4) {
+            if (c + w < cend) {
+                const i64 N = cend - c - w;
+                launch_panel_rl(R.W + c * R.ld + c, R.ld, (int)w, mrows - w, N, R.ubuf, h->stream);
+                pend.u_src = R.ubuf;
+                pend.u_dst = R.W + c * R.ld + c + w;
+                pend.u_rows = (int)w;
+                pend.u_cols = (int)N;
+            }
+        }
+        c += w;
+    }
+    if (pend.u_rows > 0)  // no leaf follows (rows exhausted): copy U12 into place
+        OXI_CUDA(cudaMemcpy2DAsync(pend.u_dst, sizeof(T) * R.ld, pend.u_src, sizeof(T) * pend.u_cols,
+                                   sizeof(T) * pend.u_cols, pend.u_rows, cudaMemcpyDeviceToDevice, h->stream));
+}
 
 // Recursive panel on columns [c0, c0+nc), rows [c0, m).
 template <typename T>
@@ -84,6 +144,12 @@ static void panel_rec(LuRun<T> &R, i64 c0, i64 nc) {
     if (mrows <= 0 || nc <= 0) return;
     // FP32 inside the mixed solve: tournament-pivoting leaves (32 columns at any height)
     const bool ts = (sizeof(T) == 4) && h->tslu && tslu_applicable(mrows);
+    if constexpr (sizeof(T) == 4) {
+        if (!ts && R.map && h->trailing != TRAIL_NATIVE && h->opt.gemm == 0) {
+            panel_rl(R, c0, nc);
+            return;
+        }
+    }
     const int leafw = ts ? 32 : leaf_width_for<T>(mrows);
     if (leafw == 0) throw CudaError{cudaErrorInvalidValue, "panel taller than the leaf capacity"};
     if (nc <= leafw) {
@@ -100,15 +166,7 @@ static void panel_rec(LuRun<T> &R, i64 c0, i64 nc) {
                            leafw, h->stream, pn);
         };
         if (R.map) {  // inside the panel by the leaf itself, outside it once per panel
-            LeafPanel pn;
-            pn.left_n = (int)(c0 - R.pf);
-            pn.nother = (int)((c0 - R.pf) + (R.pl - c0 - nc));
-            pn.pc_lo = (int)R.pf;
-            pn.right_lo = (int)(c0 + nc);
-            pn.leaf_c0 = (int)c0;
-            pn.map = R.map;
-            pn.map_off = (int)(c0 - R.pf);
-            leaf(pn);
+            leaf(leaf_panel(R, c0, nc));
         } else {
             leaf(LeafPanel());
             launch_rowmoves<T>(R.W, R.ld, c0, R.moves, R.nmoves, 0, R.ncols_moved, c0, c0 + nc,
@@ -137,7 +195,9 @@ void getrf_rowmajor(oxi_handle_s *h, T *W, i64 ld, i64 m, i64 n, int64_t *d_ipiv
     // of panels up to LEAF_MAX_OTHER columns wider than a leaf
     const bool compose = nb > 32 && n > nb && nb <= LEAF_MAX_OTHER;
     if (compose) {
-        char *ws = (char *)h->rowmap_ws.get(sizeof(int) * (size_t)(m + 8 * nb + 128));
+        const size_t map_bytes = (sizeof(int) * (size_t)(m + 8 * nb + 128) + 255) & ~size_t(255);
+        char *ws = (char *)h->rowmap_ws.get(map_bytes + sizeof(float) * 32 * LEAF_MAX_OTHER);
+        R.ubuf = (float *)(ws + map_bytes);
         R.map = (int *)ws;
         R.list = R.map + m;
         R.listcnt = R.list + 4 * nb;
@@ -235,7 +295,16 @@ void getrf_rowmajor(oxi_handle_s *h, T *W, i64 ld, i64 m, i64 n, int64_t *d_ipiv
             // SMs left free for the next panel's cluster
             h->stream = h->la_stream;
             h->tc_slot = 1;
-            h->gemm_ctas = GEMM_CTAS_SPARE_GPC;
+            // As many GPCs as keep this update about as long as a panel (about
+            // 0.6 ms measured at n = 16384; ~17 ns per tile per K column on one
+            // SM), the rest left to the next panel: early updates take all but
+            // one GPC, late ones one or two.
+            {
+                const double tiles = (double)((m - l + 127) / 128) * (double)((n - l2 + 255) / 256);
+                const double kq = (h->trailing == TRAIL_FP16X3 || h->trailing == TRAIL_BF16X3) ? 3.0 : 1.0;
+                const double us = tiles * kq * (double)(l - f) * 0.017 / GEMM_GPC_CLUSTER;
+                h->gemm_ctas = -std::max(2, (int)std::ceil(us / 600.0));
+            }
             launch_rowmoves_big<T>(W, ld, f, list, listcnt, maxcnt, 0, f, h->stream);
             launch_rowmoves_big<T>(W, ld, f, list, listcnt, maxcnt, l2, R.ncols_moved, h->stream);
             trsm_lower_unit<T>(h, L11, ld, W + f * ld + l2, ld, l - f, n - l2);

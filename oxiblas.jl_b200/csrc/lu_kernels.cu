@@ -215,6 +215,13 @@ k_leaf_lu(T *__restrict__ P, i64 ld, int m, int wact, i64 gofs, int64_t *__restr
     else __syncthreads();
     bool dead = false;  // an exchange that timed out: stop waiting (g_leaf_err reports it)
 
+    // a block the previous launch left in a buffer (see LeafPanel): rows above the leaf
+    if (pn.u_rows > 0) {
+        const T *us = (const T *)pn.u_src;
+        T *ud = (T *)pn.u_dst;
+        for (int e = g; e < pn.u_rows * pn.u_cols; e += G) ud[(i64)(e / pn.u_cols) * ld + e % pn.u_cols] = us[e];
+    }
+
     // ---- load: rows of W elements, 16-byte vectors when the row is whole and aligned ----
     T r[R][W];
     int id[R];
@@ -1080,6 +1087,93 @@ void launch_gemm_simt(T *C, i64 ldc, const T *A, i64 lda, const T *B, i64 ldb, i
     OXI_LAUNCH_CHECK();
 }
 template void launch_gemm_simt<float>(float *, i64, const float *, i64, const float *, i64, i64, i64, i64, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Right-looking step inside an FP32 panel, after a KW-wide leaf:
+//   U12 <- L11^-1 A12     (L11 the leaf's KW x KW unit lower block, A12 the
+//                          panel's N columns right of the leaf in those rows)
+//   A22 <- A22 - L21 U12  (L21 the leaf's M rows below L11)
+// in ONE launch.  Every CTA solves the 64-column slice of U12 it needs (a
+// KW-step substitution, one thread per column, L11 from shared memory), the
+// CTAs of the first row tile write it to ubuf (the next leaf, or a copy,
+// moves it into place once no CTA reads A12 any more), and each CTA then
+// updates its 128 x 64 tile of A22 (K = KW).
+// ---------------------------------------------------------------------------
+template <int KW>
+__global__ void __launch_bounds__(256, 2) k_panel_rl(float *__restrict__ P, i64 ld, int M, int N,
+                                                  float *__restrict__ ubuf) {
+    constexpr int BM = 128, BN = 64;
+    __shared__ float Ls[KW][KW + 1];
+    __shared__ __align__(16) float Us[KW][BN + 4];
+    __shared__ __align__(16) float As[KW][BM + 4];  // the L21 tile, transposed
+    const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
+    const int n0 = blockIdx.x * BN, m0 = blockIdx.y * BM;
+    for (int e = t; e < KW * KW; e += 256) Ls[e / KW][e % KW] = P[(i64)(e / KW) * ld + e % KW];
+    for (int e = t; e < KW * BN; e += 256) {
+        const int i = e / BN, j = e % BN;
+        Us[i][j] = (n0 + j < N) ? P[(i64)i * ld + KW + n0 + j] : 0.f;
+    }
+    for (int e = t; e < BM * KW; e += 256) {
+        const int r = e / KW, k = e % KW;
+        As[k][r] = (m0 + r < M) ? P[(i64)(KW + m0 + r) * ld + k] : 0.f;
+    }
+    __syncthreads();
+    if (t < BN) {
+        float x[KW];
+#pragma unroll
+        for (int i = 0; i < KW; ++i) x[i] = Us[i][t];
+#pragma unroll
+        for (int p = 0; p < KW; ++p)
+#pragma unroll
+            for (int i = p + 1; i < KW; ++i) x[i] = fmaf(-Ls[i][p], x[p], x[i]);
+#pragma unroll
+        for (int i = 0; i < KW; ++i) Us[i][t] = x[i];
+        if (blockIdx.y == 0 && n0 + t < N) {  // not into A12: other CTAs may still read it
+#pragma unroll
+            for (int i = 0; i < KW; ++i) ubuf[(i64)i * N + n0 + t] = x[i];
+        }
+    }
+    __syncthreads();
+    float c[8][4];
+#pragma unroll
+    for (int x = 0; x < 8; ++x)
+#pragma unroll
+        for (int y = 0; y < 4; ++y) {
+            const int r = m0 + ty + 16 * x, col = n0 + tx + 16 * y;
+            c[x][y] = (r < M && col < N) ? P[(i64)(KW + r) * ld + KW + col] : 0.f;
+        }
+#pragma unroll 8
+    for (int k = 0; k < KW; ++k) {
+        float a[8], b[4];
+#pragma unroll
+        for (int x = 0; x < 8; ++x) a[x] = As[k][ty + 16 * x];
+#pragma unroll
+        for (int y = 0; y < 4; ++y) b[y] = Us[k][tx + 16 * y];
+#pragma unroll
+        for (int x = 0; x < 8; ++x)
+#pragma unroll
+            for (int y = 0; y < 4; ++y) c[x][y] = fmaf(-a[x], b[y], c[x][y]);
+    }
+#pragma unroll
+    for (int x = 0; x < 8; ++x)
+#pragma unroll
+        for (int y = 0; y < 4; ++y) {
+            const int r = m0 + ty + 16 * x, col = n0 + tx + 16 * y;
+            if (r < M && col < N) P[(i64)(KW + r) * ld + KW + col] = c[x][y];
+        }
+}
+
+void launch_panel_rl(float *P, i64 ld, int kw, i64 M, i64 N, float *ubuf, cudaStream_t s) {
+    if (N <= 0) return;
+    dim3 grid((unsigned)((N + 63) / 64), (unsigned)std::max<i64>(1, (M + 127) / 128));
+    ProfScope ps(KC_GEMM_REF, s, 2.0 * (double)std::max<i64>(M, 0) * N * kw + (double)kw * kw * N,
+                 4.0 * (2.0 * std::max<i64>(M, 0) * N + (double)(M + kw) * kw + 2.0 * kw * N));
+    if (kw == 32) k_panel_rl<32><<<grid, 256, 0, s>>>(P, ld, (int)M, (int)N, ubuf);
+    else if (kw == 16) k_panel_rl<16><<<grid, 256, 0, s>>>(P, ld, (int)M, (int)N, ubuf);
+    else if (kw == 8) k_panel_rl<8><<<grid, 256, 0, s>>>(P, ld, (int)M, (int)N, ubuf);
+    else throw CudaError{cudaErrorInvalidValue, "right-looking panel step: leaf width 8, 16 or 32"};
+    OXI_LAUNCH_CHECK();
+}
 
 template void launch_gemm_ref<double>(double *, i64, const double *, i64, const double *, i64, i64, i64, i64, cudaStream_t);
 template void launch_gemm_ref<float>(float *, i64, const float *, i64, const float *, i64, i64, i64, i64, cudaStream_t);

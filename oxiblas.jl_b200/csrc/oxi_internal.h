@@ -116,12 +116,13 @@ struct oxi_handle_s {
     oxi::DeviceBuffer tc_ws2;    // the same for a second, concurrent trailing update
     int tc_slot = 0;             // which of the two operand buffers (and scale slots) to use
     int gemm_ctas = 0;           // > 0: cap on the persistent tensor-core GEMM's CTAs;
-                                 // GEMM_CTAS_SPARE_GPC: leave one GPC free
+                                 // -k: at most k GPC-filling clusters, one GPC spared
     cudaStream_t la_stream = nullptr;        // lookahead: the trailing update's stream
     cudaStream_t la_main = nullptr;          // lookahead: the panels' stream (highest priority)
     cudaEvent_t la_in = nullptr, la_out = nullptr;  // caller's stream -> la_main -> caller's stream
     cudaEvent_t la_fork = nullptr, la_join = nullptr;
-    oxi::DeviceBuffer xtag_ws;   // tagged solution words of the FP32 triangular solves
+    oxi::DeviceBuffer xtag_ws;   // tagged solution words of the triangular solves
+    oxi::DeviceBuffer trsv_ws;   // per-block solve operators of getrs (inverse + two coupling blocks)
     oxi::DeviceBuffer rowmap_ws; // per-panel row map and composite move list
     oxi::DeviceBuffer tslu_ws;   // tournament-pivoting tree of the FP32 leaves
     int tslu = 0;                // 1 inside the mixed solve's FP32 factor: tournament leaves
@@ -207,19 +208,28 @@ void launch_rm_to_cm(const TS *W, i64 ldw, TD *A, i64 lda, i64 m, i64 n, cudaStr
 // reach; wider panels apply each leaf's interchanges with separate row moves.
 constexpr int LEAF_MAX_OTHER = 256;
 
-// gemm_ctas value asking the persistent tensor-core GEMM to leave one whole GPC
-// free (clusters of GEMM_GPC_CLUSTER CTAs, one per GPC, one cluster fewer than fit)
-constexpr int GEMM_CTAS_SPARE_GPC = -1;
+// gemm_ctas = -k asks the persistent tensor-core GEMM for at most k clusters of
+// GEMM_GPC_CLUSTER CTAs (one GPC each), always leaving at least one GPC free
 constexpr int GEMM_GPC_CLUSTER = 16;
 
 struct LeafPanel {
     int nother = 0, left_n = 0, pc_lo = 0, right_lo = 0, leaf_c0 = 0, map_off = 0;
     int *map = nullptr;
+    // a pending block copy the leaf performs first: u_rows x u_cols elements,
+    // row-major at u_src (leading dimension u_cols) to u_dst (the leaf's ld)
+    const void *u_src = nullptr;
+    void *u_dst = nullptr;
+    int u_rows = 0, u_cols = 0;
 };
 
 // Tournament-pivoting leaf (FP32, mixed solve only): same contract as
 // launch_leaf (pivots, info, moves, in-panel moves through pn).
 bool tslu_applicable(i64 m);
+// FP32 right-looking panel step after a kw-wide leaf at P (the leaf's diagonal
+// corner): U12 <- L11^-1 A12 and A22 -= L21 U12 for the panel's N columns right
+// of the leaf and the M rows below it.  U12 goes to ubuf (kw x N, row-major):
+// the launch's CTAs all read A12, so it is copied into place afterwards.
+void launch_panel_rl(float *P, i64 ld, int kw, i64 M, i64 N, float *ubuf, cudaStream_t s);
 void launch_tslu_leaf(oxi_handle_s *h, float *P, i64 ld, i64 m, int w, i64 gofs, int64_t *ipiv, int64_t *info,
                       int *moves, int *nmoves, cudaStream_t s, LeafPanel pn);
 

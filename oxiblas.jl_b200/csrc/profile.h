@@ -20,6 +20,7 @@ struct Profiler {
         int kind;
         cudaEvent_t a, b;
         double flops, bytes;
+        cudaStream_t s;
     };
     std::vector<Rec> recs;
     std::vector<cudaEvent_t> pool;
@@ -55,7 +56,7 @@ struct ProfScope {
     size_t idx = 0;
     ProfScope(int kind, cudaStream_t st, double flops, double bytes) : p(t_prof), s(st) {
         if (!p || !p->enabled) { p = nullptr; return; }
-        Profiler::Rec r{kind, p->take(), p->take(), flops, bytes};
+        Profiler::Rec r{kind, p->take(), p->take(), flops, bytes, st};
         cudaEventRecord(r.a, s);
         idx = p->recs.size();
         p->recs.push_back(r);

@@ -304,37 +304,6 @@ k_trsv2(const T *__restrict__ A, i64 lda, const T *__restrict__ Dinv, T *__restr
     }
 }
 
-// Inverses of the SB x SB diagonal blocks of the effective triangle M (unit or
-// not), row-major per block: one CTA per block, thread j solves M x = e_j.
-template <typename T, bool LOWER, bool UNIT, bool ROWACC>
-__global__ void __launch_bounds__(SB) k_tri_inv_blocks(const T *__restrict__ A, i64 lda, int n,
-                                                       T *__restrict__ Dinv) {
-    extern __shared__ __align__(16) unsigned char inv_smem[];
-    T(*sM)[SB + 1] = reinterpret_cast<T(*)[SB + 1]>(inv_smem);
-    T(*sX)[SB + 1] = reinterpret_cast<T(*)[SB + 1]>(inv_smem + sizeof(T) * SB * (SB + 1));
-    const int b = blockIdx.x, r0 = b * SB, rows = min(SB, n - r0);
-    const int j = threadIdx.x;
-    for (int r = 0; r < SB; ++r) {
-        T v = T(0);
-        if (r < rows && j < rows) v = ROWACC ? A[(i64)(r0 + r) * lda + r0 + j] : A[(i64)(r0 + r) + (i64)(r0 + j) * lda];
-        if (r >= rows || j >= rows) v = (r == j) ? T(1) : T(0);  // pad with the identity
-        sM[r][j] = v;
-    }
-    __syncthreads();
-    for (int st = 0; st < SB; ++st) {
-        const int i = LOWER ? st : SB - 1 - st;
-        T s = (i == j) ? T(1) : T(0);
-        if (LOWER) {
-            for (int p = 0; p < i; ++p) s = fma(-sM[i][p], sX[p][j], s);
-        } else {
-            for (int p = i + 1; p < SB; ++p) s = fma(-sM[i][p], sX[p][j], s);
-        }
-        sX[i][j] = UNIT ? s : s / sM[i][i];
-    }
-    __syncthreads();
-    for (int r = 0; r < SB; ++r) Dinv[(i64)b * SB * SB + (i64)r * SB + j] = sX[r][j];
-}
-
 template <typename T>
 __global__ void k_gather_rows(const T *__restrict__ B, i64 ldb, const int64_t *__restrict__ perm,
                               T *__restrict__ X, i64 ldx, int n, int nrhs, int scatter) {
@@ -345,14 +314,381 @@ __global__ void k_gather_rows(const T *__restrict__ B, i64 ldb, const int64_t *_
     else X[perm[i] + (i64)k * ldx] = B[i + (i64)k * ldb];
 }
 
+// ---------------------------------------------------------------------------
+// Block-operator triangular solve.  For block b of the effective triangle M in
+// solve order, with p1 and p2 the blocks solved one and two steps before it,
+//   x_b = Dinv_b (r_b - sum_{older c} M(b,c) x_c) - Q1_b x_p1 - Q2_b x_p2,
+//   Dinv_b = M(b,b)^-1,  Q1_b = Dinv_b M(b,p1),  Q2_b = Dinv_b M(b,p2),
+// the three 64 x 64 operators precomputed per factor (k_trsv_prep).  Everything
+// but the last term is formed while the previous block is still being solved,
+// so the dependency chain from block to block is one warp-local 64 x 64
+// matrix-vector product: each warp owns 8 rows, four lanes per row, and reads
+// x_p1 straight from the tagged words, with no CTA barrier on the chain.
+// Solved values travel as tagged 64-bit words (value bits | epoch << 32; FP64
+// as two such halves), so a consumer spins on the data itself.
+// ---------------------------------------------------------------------------
+template <typename T> struct TagWords { static constexpr int n = (int)sizeof(T) / 4; };
+
+__device__ __forceinline__ void tag_put(unsigned long long *w, float v, uint32_t epoch) {
+    *(volatile unsigned long long *)w = ((unsigned long long)epoch << 32) | __float_as_uint(v);
+}
+__device__ __forceinline__ void tag_put(unsigned long long *w, double v, uint32_t epoch) {
+    const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+    const unsigned long long e = (unsigned long long)epoch << 32;
+    *(volatile unsigned long long *)w = e | (b & 0xffffffffull);
+    *(volatile unsigned long long *)(w + 1) = e | (b >> 32);
+}
+template <typename T>
+__device__ __forceinline__ T tag_get(const unsigned long long *w, uint32_t epoch, int *err);
+template <>
+__device__ __forceinline__ float tag_get<float>(const unsigned long long *w, uint32_t epoch, int *err) {
+    return tagged_get(w, epoch, err);
+}
+template <>
+__device__ __forceinline__ double tag_get<double>(const unsigned long long *w, uint32_t epoch, int *err) {
+    unsigned long long lo = ld_volatile_u64(w), hi = ld_volatile_u64(w + 1);
+    if ((uint32_t)(lo >> 32) != epoch || (uint32_t)(hi >> 32) != epoch) {
+        const uint64_t t0 = global_ns();
+        uint32_t it = 0;
+        for (;;) {
+            lo = ld_volatile_u64(w);
+            hi = ld_volatile_u64(w + 1);
+            if ((uint32_t)(lo >> 32) == epoch && (uint32_t)(hi >> 32) == epoch) break;
+            if ((++it & 255) == 0 && global_ns() - t0 > kWaitLimitNs) {
+                atomicExch(err, 3);
+                break;
+            }
+        }
+    }
+    return __longlong_as_double((long long)((hi << 32) | (lo & 0xffffffffull)));
+}
+
+constexpr int TRSV_OPS = 3 * SB * SB;  // operator elements per block: Dinv, Q1, Q2
+
+__device__ __forceinline__ float tag_decode(const unsigned long long (&w)[1]) { return __uint_as_float((uint32_t)w[0]); }
+__device__ __forceinline__ double tag_decode(const unsigned long long (&w)[2]) {
+    return __longlong_as_double((long long)((w[1] << 32) | (w[0] & 0xffffffffull)));
+}
+
+// One warp stages the solution of a 64-row block (rows row0.., `cols` of them,
+// NR right-hand sides) from the tagged words into xs[64][NR]: every word's load
+// is in flight at once, and only words of an older epoch are polled again.
+template <typename T, int NR>
+__device__ __forceinline__ void stage_block(T (*xs)[NR], const unsigned long long *__restrict__ xtag, int row0,
+                                            int cols, uint32_t epoch, int *err, int lane) {
+    constexpr int TW = TagWords<T>::n;
+    constexpr int PL = SB * NR / 32;
+    unsigned long long w[PL][TW];
+#pragma unroll
+    for (int v = 0; v < PL; ++v) {
+        const int e = lane + 32 * v, jj = e % SB, k = e / SB;
+        const unsigned long long *p = xtag + ((i64)(row0 + jj) * NR + k) * TW;
+#pragma unroll
+        for (int h = 0; h < TW; ++h) w[v][h] = (jj < cols) ? ld_volatile_u64(p + h) : ((unsigned long long)epoch << 32);
+    }
+#pragma unroll
+    for (int v = 0; v < PL; ++v) {
+        const int e = lane + 32 * v, jj = e % SB, k = e / SB;
+        const unsigned long long *p = xtag + ((i64)(row0 + jj) * NR + k) * TW;
+        bool ready = true;
+#pragma unroll
+        for (int h = 0; h < TW; ++h) ready = ready && (uint32_t)(w[v][h] >> 32) == epoch;
+        if (!ready) {
+            const uint64_t t0 = global_ns();
+            uint32_t it = 0;
+            for (;;) {
+                ready = true;
+#pragma unroll
+                for (int h = 0; h < TW; ++h) {
+                    w[v][h] = ld_volatile_u64(p + h);
+                    ready = ready && (uint32_t)(w[v][h] >> 32) == epoch;
+                }
+                if (ready) break;
+                if ((++it & 255) == 0 && global_ns() - t0 > kWaitLimitNs) {
+                    atomicExch(err, 3);
+                    break;
+                }
+            }
+        }
+        xs[jj][k] = (jj < cols) ? (T)tag_decode(w[v]) : T(0);
+    }
+}
+
+// One CTA per block: the inverse of the diagonal block by substitution (64
+// threads, one column each), then the two coupling operators as 64 x 64 x 64
+// products.  Rows and columns past n are padded with the identity (Dinv) and
+// zeros (Q1, Q2).
+template <typename T, bool LOWER, bool UNIT, bool ROWACC>
+__global__ void __launch_bounds__(SOLVE_NT) k_trsv_prep(const T *__restrict__ A, i64 lda, int n,
+                                                       T *__restrict__ P) {
+    extern __shared__ __align__(16) unsigned char prep_smem[];
+    T(*sM)[SB + 1] = reinterpret_cast<T(*)[SB + 1]>(prep_smem);
+    T(*sX)[SB + 1] = reinterpret_cast<T(*)[SB + 1]>(prep_smem + sizeof(T) * SB * (SB + 1));
+    const int nb = (n + SB - 1) / SB;
+    const int bi = blockIdx.x;
+    const int b = LOWER ? bi : nb - 1 - bi;
+    const int r0 = b * SB, rows = min(SB, n - r0);
+    const int t = threadIdx.x;
+    auto Mv = [&](int r, int j) -> T { return ROWACC ? A[(i64)r * lda + j] : A[(i64)r + (i64)j * lda]; };
+    for (int e = t; e < SB * SB; e += SOLVE_NT) {
+        int r, j;
+        if (ROWACC) { r = e / SB; j = e % SB; } else { r = e % SB; j = e / SB; }
+        T v = (r == j) ? T(1) : T(0);
+        if (r < rows && j < rows && !(UNIT && r == j)) v = Mv(r0 + r, r0 + j);
+        sM[r][j] = v;
+    }
+    __syncthreads();
+    if (t < SB) {
+        const int j = t;
+        for (int st = 0; st < SB; ++st) {
+            const int i = LOWER ? st : SB - 1 - st;
+            T s = (i == j) ? T(1) : T(0);
+            if (LOWER) {
+                for (int p = 0; p < i; ++p) s = fma(-sM[i][p], sX[p][j], s);
+            } else {
+                for (int p = i + 1; p < SB; ++p) s = fma(-sM[i][p], sX[p][j], s);
+            }
+            sX[i][j] = UNIT ? s : s / sM[i][i];
+        }
+    }
+    __syncthreads();
+    T *Pb = P + (i64)bi * TRSV_OPS;
+    for (int e = t; e < SB * SB; e += SOLVE_NT) Pb[e] = sX[e / SB][e % SB];
+    for (int q = 1; q <= 2; ++q) {
+        if (bi - q < 0) break;
+        const int pb = LOWER ? b - q : b + q;
+        const int c0 = pb * SB, cols = min(SB, n - c0);
+        __syncthreads();
+        for (int e = t; e < SB * SB; e += SOLVE_NT) {
+            int r, j;
+            if (ROWACC) { r = e / SB; j = e % SB; } else { r = e % SB; j = e / SB; }
+            sM[r][j] = (r < rows && j < cols) ? Mv(r0 + r, c0 + j) : T(0);
+        }
+        __syncthreads();
+        const int r = t >> 2, j0 = (t & 3) * 16;
+        T o[16];
+#pragma unroll
+        for (int u = 0; u < 16; ++u) o[u] = T(0);
+        for (int p = 0; p < SB; ++p) {
+            const T xv = sX[r][p];
+#pragma unroll
+            for (int u = 0; u < 16; ++u) o[u] = fma(xv, sM[p][j0 + u], o[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < 16; ++u) Pb[q * SB * SB + r * SB + j0 + u] = o[u];
+    }
+}
+
+template <typename T, int NR>
+struct Trsv3Smem {
+    T xs[TRSV_WARPS][SB][NR];  // per-warp staging of solved blocks
+    T acc[TRSV_WARPS][SB][NR];
+    T y[SB][NR];
+    T z[SB][NR];
+    T part[SOLVE_NT / SB][SB][NR];
+    T op[3][SB][SB + 1];       // Dinv, Q1, Q2 of this block
+};
+
+template <typename T, bool LOWER, bool ROWACC, int NR>
+__global__ void __launch_bounds__(SOLVE_NT)
+k_trsv3(const T *__restrict__ A, i64 lda, const T *__restrict__ P, T *__restrict__ X, i64 ldx, int n,
+        int *__restrict__ ticket, int *__restrict__ err, unsigned long long *__restrict__ xtag, uint32_t epoch) {
+    constexpr int TW = TagWords<T>::n;
+    extern __shared__ __align__(16) unsigned char trsv3_smem[];
+    Trsv3Smem<T, NR> &S = *reinterpret_cast<Trsv3Smem<T, NR> *>(trsv3_smem);
+    __shared__ int s_blk;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int nb = (n + SB - 1) / SB;
+    if (t == 0) s_blk = atomicAdd(ticket, 1);
+    __syncthreads();
+    const int bi = s_blk;
+    if (bi >= nb) return;
+    const int b = LOWER ? bi : nb - 1 - bi;
+    const int r0 = b * SB;
+    const int rows = min(SB, n - r0);
+    auto xw = [&](int row, int k) { return xtag + ((i64)row * NR + k) * TW; };
+
+    // ---- this block's operators (no dependency on other blocks) ----
+    const T *Pb = P + (i64)bi * TRSV_OPS;
+    const int nops = bi >= 2 ? 3 : bi + 1;
+    for (int e = t; e < nops * SB * SB; e += SOLVE_NT) {
+        const int o = e / (SB * SB), rr = (e / SB) % SB, jj = e % SB;
+        S.op[o][rr][jj] = Pb[e];
+    }
+
+    // ---- products with the blocks solved three or more steps before ----
+    // Blocks in solve order; within each, warp w takes tile columns [8w, 8w+8)
+    // and each lane two rows.  The next block's tile and solution words are
+    // loaded before the current block's products, so the loads' latency is
+    // hidden and the loop runs at issue rate behind the chain.
+    {
+        const int jw = warp * 8;
+        const bool vec8 = ROWACC && ((lda * (i64)sizeof(T)) % 16 == 0) && ((((uintptr_t)A) & 15) == 0);
+        auto load_tile = [&](int step, T (&a)[2][8]) {
+            const int c = LOWER ? step : nb - 1 - step;
+            const int c0 = c * SB;
+            const int cols = min(SB, n - c0);
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int rr = lane + 32 * q;
+                if (ROWACC) {
+                    const T *arow = A + (i64)(r0 + rr) * lda + c0 + jw;
+                    if (rr < rows && vec8 && jw + 8 <= cols) {
+#pragma unroll
+                        for (int u = 0; u < 8; u += 16 / (int)sizeof(T)) *(int4 *)&a[q][u] = *(const int4 *)(arow + u);
+                    } else {
+#pragma unroll
+                        for (int u = 0; u < 8; ++u) a[q][u] = (rr < rows && jw + u < cols) ? arow[u] : T(0);
+                    }
+                } else {
+                    const T *acol = A + (i64)(r0 + rr) + (i64)(c0 + jw) * lda;
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) a[q][u] = (rr < rows && jw + u < cols) ? acol[(i64)u * lda] : T(0);
+                }
+            }
+        };
+        // solution words of the warp's 8 columns: lane e < 8 NR holds (column e % 8, rhs e / 8)
+        constexpr int XPL = (8 * NR + 31) / 32;  // words per lane
+        auto xidx = [&](int step, int v, int &row, int &k, bool &ok) {
+            const int c = LOWER ? step : nb - 1 - step;
+            const int e = lane + 32 * v;
+            row = c * SB + jw + (e & 7);
+            k = e >> 3;
+            ok = (e < 8 * NR) && (row < n);
+        };
+        T acc[2][NR];
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+#pragma unroll
+            for (int k = 0; k < NR; ++k) acc[q][k] = T(0);
+        const int nsteps = bi - 2;
+        T an[2][8];
+        T xn[XPL];
+        if (nsteps > 0) {
+            load_tile(0, an);
+#pragma unroll
+            for (int v = 0; v < XPL; ++v) {
+                int row, k; bool ok;
+                xidx(0, v, row, k, ok);
+                xn[v] = ok ? tag_get<T>(xw(row, k), epoch, err) : T(0);
+            }
+        }
+        for (int step = 0; step < nsteps; ++step) {
+            T a[2][8];
+#pragma unroll
+            for (int q = 0; q < 2; ++q)
+#pragma unroll
+                for (int u = 0; u < 8; ++u) a[q][u] = an[q][u];
+            T *xsw = &S.xs[warp][0][0];  // [rhs k][column u] at k * 8 + u
+#pragma unroll
+            for (int v = 0; v < XPL; ++v)
+                if (lane + 32 * v < 8 * NR) xsw[lane + 32 * v] = xn[v];
+            if (step + 1 < nsteps) {
+                load_tile(step + 1, an);
+#pragma unroll
+                for (int v = 0; v < XPL; ++v) {
+                    int row, k; bool ok;
+                    xidx(step + 1, v, row, k, ok);
+                    xn[v] = ok ? tag_get<T>(xw(row, k), epoch, err) : T(0);
+                }
+            }
+            __syncwarp();
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+#pragma unroll
+                for (int k = 0; k < NR; ++k) {
+                    const T xv = xsw[k * 8 + u];
+#pragma unroll
+                    for (int q = 0; q < 2; ++q) acc[q][k] = fma(a[q][u], xv, acc[q][k]);
+                }
+            __syncwarp();
+        }
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+#pragma unroll
+            for (int k = 0; k < NR; ++k) S.acc[warp][lane + 32 * q][k] = acc[q][k];
+    }
+    __syncthreads();
+    for (int e = t; e < SB * NR; e += SOLVE_NT) {
+        const int r = e % SB, k = e / SB;
+        T v = T(0);
+#pragma unroll
+        for (int w = 0; w < TRSV_WARPS; ++w) v += S.acc[w][r][k];
+        S.y[r][k] = (r < rows) ? (X[(i64)(r0 + r) + (i64)k * ldx] - v) : T(0);
+    }
+    __syncthreads();
+
+    // ---- the chain's operands: 8 rows per warp, 4 lanes per row (16 columns each) ----
+    const int r = warp * 8 + (lane >> 2), sg = lane & 3;
+    T s[NR];
+#pragma unroll
+    for (int k = 0; k < NR; ++k) s[k] = T(0);
+    auto couple = [&](int q) {  // s += Q_q x_(block solved q steps before)
+        const int pb = LOWER ? b - q : b + q;
+        const int c0 = pb * SB;
+        stage_block<T, NR>(S.xs[warp], xtag, c0, min(SB, n - c0), epoch, err, lane);
+        __syncwarp();
+#pragma unroll
+        for (int jj = 0; jj < 16; ++jj) {
+            const T a = S.op[q][r][sg * 16 + jj];
+#pragma unroll
+            for (int k = 0; k < NR; ++k) s[k] = fma(a, S.xs[warp][sg * 16 + jj][k], s[k]);
+        }
+        __syncwarp();
+    };
+    if (bi >= 2) couple(2);  // solved two steps ago: off the chain
+
+    // ---- z = Dinv y, over SEG column segments ----
+    constexpr int SEG = SOLVE_NT / SB, SEGW = SB / SEG;
+    {
+        const int pr = t % SB, ps = t / SB;
+        T pv[NR];
+#pragma unroll
+        for (int k = 0; k < NR; ++k) pv[k] = T(0);
+#pragma unroll
+        for (int jj = 0; jj < SEGW; ++jj) {
+            const T a = S.op[0][pr][ps * SEGW + jj];
+#pragma unroll
+            for (int k = 0; k < NR; ++k) pv[k] = fma(a, S.y[ps * SEGW + jj][k], pv[k]);
+        }
+#pragma unroll
+        for (int k = 0; k < NR; ++k) S.part[ps][pr][k] = pv[k];
+    }
+    __syncthreads();
+    for (int e = t; e < SB * NR; e += SOLVE_NT) {
+        const int rr = e % SB, k = e / SB;
+        T v = T(0);
+#pragma unroll
+        for (int q = 0; q < SEG; ++q) v += S.part[q][rr][k];
+        S.z[rr][k] = v;
+    }
+    __syncthreads();
+
+    // ---- the chain: x_b = z - Q2 x_p2 - Q1 x_p1, warp-local ----
+    if (bi >= 1) couple(1);
+#pragma unroll
+    for (int k = 0; k < NR; ++k) {
+        s[k] += __shfl_xor_sync(0xffffffffu, s[k], 1);
+        s[k] += __shfl_xor_sync(0xffffffffu, s[k], 2);
+    }
+    if (r < rows) {
+#pragma unroll
+        for (int k = 0; k < NR; ++k) {
+            if ((k & 3) != sg) continue;
+            const T x = S.z[r][k] - s[k];
+            X[(i64)(r0 + r) + (i64)k * ldx] = x;
+            tag_put(xw(r0 + r, k), x, epoch);
+        }
+    }
+}
+
 // UPPER_A / TRANS describe the stored factor as in LAPACK (column-major A,
 // op(A) = A or A^T); ROWACC access of the same memory is the transposed view.
-static std::atomic<uint32_t> g_trsv_epoch{0};  // tags of the FP32 exchange words
+static std::atomic<uint32_t> g_trsv_epoch{0};  // tags of the exchange words, one per launch
 
 template <typename T, bool UPPER_A, bool UNIT, bool TRANS>
 static void trsv_launch(const T *A, i64 lda, T *X, i64 ldx, int n, int nrhs, int *ctl, int *err,
-                        cudaStream_t s, const T *Dinv = nullptr,
-                        unsigned long long *xtag = nullptr) {
+                        cudaStream_t s) {
     constexpr bool LOWER = (UPPER_A == TRANS);
     const int nb = (n + SB - 1) / SB;
     ProfScope ps(KC_TRSV, s, (double)n * n * nrhs, (double)n * n * sizeof(T) / 2);
@@ -364,38 +700,12 @@ static void trsv_launch(const T *A, i64 lda, T *X, i64 ldx, int n, int nrhs, int
 #define OXI_TRSV_GO(NRV)                                                                              \
     do {                                                                                             \
         const int smem = (int)sizeof(TrsvSmem<T, NRV>);                                             \
-        const uint32_t ep = ++g_trsv_epoch;                                                          \
-        if (Dinv) {                                                                                  \
-            if constexpr (sizeof(T) == 4) {                                                          \
-                if (xtag) {                                                                          \
-                    auto kern = k_trsv2<T, LOWER, UNIT, TRANS, NRV, true, true>;                     \
-                    OXI_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)); \
-                    kern<<<nb, SOLVE_NT, smem, s>>>(A, lda, Dinv, Xk, ldx, n, ticket, flags, err, xtag, ep); \
-                    k0 += NRV;                                                                       \
-                    break;                                                                           \
-                }                                                                                    \
-            }                                                                                        \
-            auto kern = k_trsv2<T, LOWER, UNIT, TRANS, NRV, true>;                                   \
-            OXI_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)); \
-            kern<<<nb, SOLVE_NT, smem, s>>>(A, lda, Dinv, Xk, ldx, n, ticket, flags, err, nullptr, 0u); \
-        } else {                                                                                     \
-            auto kern = k_trsv2<T, LOWER, UNIT, TRANS, NRV, false>;                                  \
-            OXI_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)); \
-            kern<<<nb, SOLVE_NT, smem, s>>>(A, lda, Dinv, Xk, ldx, n, ticket, flags, err, nullptr, 0u); \
-        }                                                                                            \
+        auto kern = k_trsv2<T, LOWER, UNIT, TRANS, NRV, false>;                                      \
+        OXI_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));     \
+        kern<<<nb, SOLVE_NT, smem, s>>>(A, lda, nullptr, Xk, ldx, n, ticket, flags, err, nullptr, 0u); \
         k0 += NRV;                                                                                   \
     } while (0)
-        // several right-hand sides per launch read the factor once for all of them
-        // (FP32 up to 16 columns, FP64 up to 8: the staging fits shared memory)
-        bool wide = false;
-        if constexpr (sizeof(T) == 4) {
-            if (left >= 16) {
-                OXI_TRSV_GO(16);
-                wide = true;
-            }
-        }
-        if (wide) {
-        } else if (left >= 8) OXI_TRSV_GO(8);
+        if (left >= 8) OXI_TRSV_GO(8);
         else if (left >= 4) OXI_TRSV_GO(4);
         else if (left >= 2) OXI_TRSV_GO(2);
         else OXI_TRSV_GO(1);
@@ -405,14 +715,62 @@ static void trsv_launch(const T *A, i64 lda, T *X, i64 ldx, int n, int nrhs, int
 }
 
 template <typename T, bool UPPER_A, bool UNIT, bool TRANS>
-static void tri_inv_launch(const T *A, i64 lda, int n, T *Dinv, cudaStream_t s) {
+static void trsv_prep_launch(const T *A, i64 lda, int n, T *P, cudaStream_t s) {
     constexpr bool LOWER = (UPPER_A == TRANS);
     const int nb = (n + SB - 1) / SB;
     const int smem = 2 * (int)sizeof(T) * SB * (SB + 1);
-    OXI_CUDA(cudaFuncSetAttribute(k_tri_inv_blocks<T, LOWER, UNIT, TRANS>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    k_tri_inv_blocks<T, LOWER, UNIT, TRANS><<<nb, SB, smem, s>>>(A, lda, n, Dinv);
+    set_max_dyn_smem((const void *)k_trsv_prep<T, LOWER, UNIT, TRANS>, smem);
+    ProfScope ps(KC_TRSV, s, 2.0 * SB * SB * (double)n * 3, 3.0 * (double)n * SB * sizeof(T));
+    k_trsv_prep<T, LOWER, UNIT, TRANS><<<nb, SOLVE_NT, smem, s>>>(A, lda, n, P);
     OXI_LAUNCH_CHECK();
+}
+
+template <typename T, bool UPPER_A, bool TRANS>
+static void trsv3_launch(const T *A, i64 lda, T *X, i64 ldx, int n, int nrhs, int *ctl, int *err,
+                         cudaStream_t s, const T *P, unsigned long long *xtag) {
+    constexpr bool LOWER = (UPPER_A == TRANS);
+    const int nb = (n + SB - 1) / SB;
+    ProfScope ps(KC_TRSV, s, (double)n * n * nrhs, (double)n * n * sizeof(T) / 2);
+    for (int k0 = 0; k0 < nrhs;) {
+        const int left = nrhs - k0;
+        OXI_CUDA(cudaMemsetAsync(ctl, 0, sizeof(int), s));
+        T *Xk = X + (i64)k0 * ldx;
+#define OXI_TRSV3_GO(NRV)                                                                            \
+    do {                                                                                             \
+        const int smem = (int)sizeof(Trsv3Smem<T, NRV>);                                            \
+        const uint32_t ep = ++g_trsv_epoch;                                                          \
+        auto kern = k_trsv3<T, LOWER, TRANS, NRV>;                                                   \
+        set_max_dyn_smem((const void *)kern, smem);                                                  \
+        kern<<<nb, SOLVE_NT, smem, s>>>(A, lda, P, Xk, ldx, n, ctl, err, xtag, ep);                 \
+        k0 += NRV;                                                                                   \
+    } while (0)
+        bool wide = false;
+        if constexpr (sizeof(T) == 4) {
+            if (left >= 16) {
+                OXI_TRSV3_GO(16);
+                wide = true;
+            }
+        }
+        if (wide) {
+        } else if (left >= 8) OXI_TRSV3_GO(8);
+        else if (left >= 4) OXI_TRSV3_GO(4);
+        else if (left >= 2) OXI_TRSV3_GO(2);
+        else OXI_TRSV3_GO(1);
+#undef OXI_TRSV3_GO
+        OXI_LAUNCH_CHECK();
+    }
+}
+
+// Tagged solution words for the triangular solves: n rows x 16 words (FP32 up
+// to 16 right-hand sides, FP64 up to 8 at two words each).  A fresh or grown
+// buffer is zeroed: epoch 0 never matches a launch.
+static unsigned long long *xtag_words(oxi_handle_s *h, i64 n) {
+    const size_t need = sizeof(unsigned long long) * (size_t)n * 16;
+    if (h->xtag_ws.bytes < need) {
+        void *p = h->xtag_ws.get(need);
+        OXI_CUDA(cudaMemsetAsync(p, 0, h->xtag_ws.bytes, h->stream));
+    }
+    return (unsigned long long *)h->xtag_ws.get(need);
 }
 
 // Solve with device-resident permutation `perm` (0-based, A[perm,:] = L U).
@@ -426,18 +784,26 @@ void getrs_perm(oxi_handle_s *h, char trans, i64 n, i64 nrhs, const T *LU, i64 l
     int *ctl = (int *)(ws + ((sizeof(T) * (size_t)n * nrhs + 255) & ~size_t(255)));
     const i64 tot = n * nrhs;
     const int nt = 256;
+    // the two triangles' block operators (inverse and coupling blocks), then the solves
+    T *P1 = (T *)h->trsv_ws.get(2 * sizeof(T) * (size_t)nb * TRSV_OPS);
+    T *P2 = P1 + (size_t)nb * TRSV_OPS;
+    unsigned long long *xtag = xtag_words(h, n);
     if (trans == 'N') {
         k_gather_rows<T><<<(unsigned)((tot + nt - 1) / nt), nt, 0, s>>>(B, ldb, d_perm, X, n, (int)n, (int)nrhs, 0);
         OXI_LAUNCH_CHECK();
-        trsv_launch<T, false, true, false>(LU, lda, X, n, (int)n, (int)nrhs, ctl, d_err, s);
-        trsv_launch<T, true, false, false>(LU, lda, X, n, (int)n, (int)nrhs, ctl, d_err, s);
+        trsv_prep_launch<T, false, true, false>(LU, lda, (int)n, P1, s);
+        trsv_prep_launch<T, true, false, false>(LU, lda, (int)n, P2, s);
+        trsv3_launch<T, false, false>(LU, lda, X, n, (int)n, (int)nrhs, ctl, d_err, s, P1, xtag);
+        trsv3_launch<T, true, false>(LU, lda, X, n, (int)n, (int)nrhs, ctl, d_err, s, P2, xtag);
         OXI_CUDA(cudaMemcpy2DAsync(B, ldb * sizeof(T), X, n * sizeof(T), n * sizeof(T), nrhs,
                                    cudaMemcpyDeviceToDevice, s));
     } else {
         OXI_CUDA(cudaMemcpy2DAsync(X, n * sizeof(T), B, ldb * sizeof(T), n * sizeof(T), nrhs,
                                    cudaMemcpyDeviceToDevice, s));
-        trsv_launch<T, true, false, true>(LU, lda, X, n, (int)n, (int)nrhs, ctl, d_err, s);
-        trsv_launch<T, false, true, true>(LU, lda, X, n, (int)n, (int)nrhs, ctl, d_err, s);
+        trsv_prep_launch<T, true, false, true>(LU, lda, (int)n, P1, s);
+        trsv_prep_launch<T, false, true, true>(LU, lda, (int)n, P2, s);
+        trsv3_launch<T, true, true>(LU, lda, X, n, (int)n, (int)nrhs, ctl, d_err, s, P1, xtag);
+        trsv3_launch<T, false, true>(LU, lda, X, n, (int)n, (int)nrhs, ctl, d_err, s, P2, xtag);
         k_gather_rows<T><<<(unsigned)((tot + nt - 1) / nt), nt, 0, s>>>(X, n, d_perm, B, ldb, (int)n, (int)nrhs, 1);
         OXI_LAUNCH_CHECK();
     }
@@ -455,29 +821,26 @@ void lu_solve_rowmajor(oxi_handle_s *h, const T *W, i64 ld, i64 n, T *X, i64 ldx
     const i64 nb = (n + SB - 1) / SB;
     if (nb + 1 > kTrsvCtlInts) throw CudaError{cudaErrorInvalidValue, "system too large for the solve control block"};
     int *ctl = (int *)((char *)h->scratch.get(kScratchBytes) + kScratchTrsvOff);
-    unsigned long long *xtag = nullptr;
-    if (sizeof(T) == 4 && DinvL && DinvU) {
-        const size_t need = sizeof(unsigned long long) * (size_t)n * 16;  // NR <= 16 words per row
-        if (h->xtag_ws.bytes < need) {  // fresh words: epoch 0 never matches a launch
-            xtag = (unsigned long long *)h->xtag_ws.get(need);
-            OXI_CUDA(cudaMemsetAsync(xtag, 0, h->xtag_ws.bytes, h->stream));
-        }
-        xtag = (unsigned long long *)h->xtag_ws.get(need);
+    if (DinvL && DinvU) {  // block operators from lu_block_inverses_rowmajor
+        unsigned long long *xtag = xtag_words(h, n);
+        trsv3_launch<T, true, true>(W, ld, X, ldx, (int)n, (int)nrhs, ctl, d_err, h->stream, DinvL, xtag);
+        trsv3_launch<T, false, true>(W, ld, X, ldx, (int)n, (int)nrhs, ctl, d_err, h->stream, DinvU, xtag);
+        return;
     }
-    trsv_launch<T, true, true, true>(W, ld, X, ldx, (int)n, (int)nrhs, ctl, d_err, h->stream, DinvL, xtag);
-    trsv_launch<T, false, false, true>(W, ld, X, ldx, (int)n, (int)nrhs, ctl, d_err, h->stream, DinvU, xtag);
+    trsv_launch<T, true, true, true>(W, ld, X, ldx, (int)n, (int)nrhs, ctl, d_err, h->stream);
+    trsv_launch<T, false, false, true>(W, ld, X, ldx, (int)n, (int)nrhs, ctl, d_err, h->stream);
 }
 template void lu_solve_rowmajor<float>(oxi_handle_s *, const float *, i64, i64, float *, i64, i64, int *, const float *, const float *);
 template void lu_solve_rowmajor<double>(oxi_handle_s *, const double *, i64, i64, double *, i64, i64, int *, const double *, const double *);
 
 template <typename T>
 void lu_block_inverses_rowmajor(oxi_handle_s *h, const T *W, i64 ld, i64 n, T *DinvL, T *DinvU) {
-    tri_inv_launch<T, true, true, true>(W, ld, (int)n, DinvL, h->stream);
-    tri_inv_launch<T, false, false, true>(W, ld, (int)n, DinvU, h->stream);
+    trsv_prep_launch<T, true, true, true>(W, ld, (int)n, DinvL, h->stream);
+    trsv_prep_launch<T, false, false, true>(W, ld, (int)n, DinvU, h->stream);
 }
 template void lu_block_inverses_rowmajor<float>(oxi_handle_s *, const float *, i64, i64, float *, float *);
 template void lu_block_inverses_rowmajor<double>(oxi_handle_s *, const double *, i64, i64, double *, double *);
-i64 lu_block_inverse_elems(i64 n) { return ((n + SB - 1) / SB) * (i64)SB * SB; }
+i64 lu_block_inverse_elems(i64 n) { return ((n + SB - 1) / SB) * (i64)TRSV_OPS; }
 
 // LUFactor.p from the interchange sequence (src/lapack/factorizations.jl:72-75).
 void perm_from_ipiv(const int64_t *ipiv, i64 q, i64 m, int64_t *perm) {
