@@ -831,27 +831,32 @@ void launch_trsm_leaf(const T *L, i64 ldl, T *B, i64 ldb, int t, i64 N, cudaStre
 // substitution (lane = row, one warp per 4 columns).  One launch replaces the
 // recursive halving's leaves and GEMMs.
 // ---------------------------------------------------------------------------
-constexpr int TF_TB = 32, TF_CW = 32, TF_TMAX = 256;
+constexpr int TF_TB = 32, TF_TMAX = 256;
 
 // Right-looking: for each 32-row block J, solve its 32 x 32 diagonal block by
-// warp-shuffle substitution (lane = row, one warp per 4 columns), then update all
-// rows below with that block's solution in one pass (L column block staged in
-// shared memory, 7 x 4 outputs per thread).
-template <typename T>
+// warp-shuffle substitution (lane = row, one warp per CW/8 columns), then update
+// all rows below with that block's solution in one pass (L column block staged in
+// shared memory, four columns per thread).  CW = 32 columns per CTA for wide
+// right-hand sides, 8 for narrow ones (a panel's U12): four times the CTAs, a
+// quarter of the dependent chain per CTA.
+template <typename T, int CW>
 __global__ void __launch_bounds__(256) k_trsm_fused(const T *__restrict__ L, i64 ldl, T *__restrict__ B,
                                                     i64 ldb, int t, i64 N) {
+    constexpr int NG = CW / 4, RG = 256 / NG;                 // column groups of 4, row groups
+    constexpr int QMAX = (TF_TMAX - TF_TB + RG - 1) / RG;     // rows per thread below a block
+    constexpr int CPW = CW / 8;                               // chain columns per warp
     extern __shared__ __align__(16) unsigned char tf_smem[];
-    T(*X)[TF_CW + 1] = reinterpret_cast<T(*)[TF_CW + 1]>(tf_smem);
-    T(*Lc)[TF_TB + 1] = reinterpret_cast<T(*)[TF_TB + 1]>(tf_smem + sizeof(T) * TF_TMAX * (TF_CW + 1));
+    T(*X)[CW + 1] = reinterpret_cast<T(*)[CW + 1]>(tf_smem);
+    T(*Lc)[TF_TB + 1] = reinterpret_cast<T(*)[TF_TB + 1]>(tf_smem + sizeof(T) * TF_TMAX * (CW + 1));
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const i64 c0 = (i64)blockIdx.x * TF_CW;
-    const int cols = (int)((N - c0) < TF_CW ? (N - c0) : TF_CW);
-    for (int e = tid; e < t * TF_CW; e += 256) {
-        const int i = e / TF_CW, c = e % TF_CW;
+    const i64 c0 = (i64)blockIdx.x * CW;
+    const int cols = (int)((N - c0) < CW ? (N - c0) : CW);
+    for (int e = tid; e < t * CW; e += 256) {
+        const int i = e / CW, c = e % CW;
         X[i][c] = (c < cols) ? B[(i64)i * ldb + c0 + c] : T(0);
     }
     const int nblk = (t + TF_TB - 1) / TF_TB;
-    const int cq = (tid & 7) * 4, rq = tid >> 3;  // update mapping: rows rq + 32 q, columns cq..cq+3
+    const int cq = (tid % NG) * 4, rq = tid / NG;  // update mapping: rows rq + RG q, columns cq..cq+3
     for (int J = 0; J < nblk; ++J) {
         const int j0 = J * TF_TB, jrows = min(TF_TB, t - j0);
         const int rb = j0 + jrows, nrem = t - rb;  // rows below the block
@@ -862,8 +867,8 @@ __global__ void __launch_bounds__(256) k_trsm_fused(const T *__restrict__ L, i64
         }
         __syncthreads();
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int c = warp * 4 + q;
+        for (int q = 0; q < CPW; ++q) {
+            const int c = warp * CPW + q;
             T x = (lane < jrows) ? X[j0 + lane][c] : T(0);
             for (int p = 0; p < jrows - 1; ++p) {
                 const T xp = __shfl_sync(0xffffffffu, x, p);
@@ -873,17 +878,17 @@ __global__ void __launch_bounds__(256) k_trsm_fused(const T *__restrict__ L, i64
         }
         __syncthreads();
         if (nrem > 0) {
-            T acc[7][4];
+            T acc[QMAX][4];
 #pragma unroll
-            for (int q = 0; q < 7; ++q)
+            for (int q = 0; q < QMAX; ++q)
 #pragma unroll
                 for (int u = 0; u < 4; ++u) acc[q][u] = T(0);
 #pragma unroll 4
             for (int p = 0; p < jrows; ++p) {
                 const T x0 = X[j0 + p][cq], x1 = X[j0 + p][cq + 1], x2 = X[j0 + p][cq + 2], x3 = X[j0 + p][cq + 3];
 #pragma unroll
-                for (int q = 0; q < 7; ++q) {
-                    const int r = rq + 32 * q;
+                for (int q = 0; q < QMAX; ++q) {
+                    const int r = rq + RG * q;
                     if (r < nrem) {
                         const T l = Lc[TF_TB + r][p];
                         acc[q][0] = fma(l, x0, acc[q][0]);
@@ -894,8 +899,8 @@ __global__ void __launch_bounds__(256) k_trsm_fused(const T *__restrict__ L, i64
                 }
             }
 #pragma unroll
-            for (int q = 0; q < 7; ++q) {
-                const int r = rq + 32 * q;
+            for (int q = 0; q < QMAX; ++q) {
+                const int r = rq + RG * q;
                 if (r < nrem) {
 #pragma unroll
                     for (int u = 0; u < 4; ++u) X[rb + r][cq + u] -= acc[q][u];
@@ -904,8 +909,8 @@ __global__ void __launch_bounds__(256) k_trsm_fused(const T *__restrict__ L, i64
         }
         __syncthreads();
     }
-    for (int e = tid; e < t * TF_CW; e += 256) {
-        const int i = e / TF_CW, c = e % TF_CW;
+    for (int e = tid; e < t * CW; e += 256) {
+        const int i = e / CW, c = e % CW;
         if (c < cols) B[(i64)i * ldb + c0 + c] = X[i][c];
     }
 }
@@ -913,10 +918,18 @@ __global__ void __launch_bounds__(256) k_trsm_fused(const T *__restrict__ L, i64
 template <typename T>
 void launch_trsm_fused(const T *L, i64 ldl, T *B, i64 ldb, int t, i64 N, cudaStream_t s) {
     if (t <= 1 || N <= 0) return;
-    const size_t smem = sizeof(T) * ((size_t)TF_TMAX * (TF_CW + 1) + (size_t)TF_TMAX * (TF_TB + 1));
-    set_max_dyn_smem((const void *)k_trsm_fused<T>, (int)smem);
     ProfScope ps(KC_TRSM_LEAF, s, (double)t * t * N, 2.0 * (double)t * N * sizeof(T));
-    k_trsm_fused<T><<<(unsigned)((N + TF_CW - 1) / TF_CW), 256, smem, s>>>(L, ldl, B, ldb, t, N);
+    if (N <= 2048) {
+        constexpr int CW = 8;
+        const size_t smem = sizeof(T) * ((size_t)TF_TMAX * (CW + 1) + (size_t)TF_TMAX * (TF_TB + 1));
+        set_max_dyn_smem((const void *)k_trsm_fused<T, CW>, (int)smem);
+        k_trsm_fused<T, CW><<<(unsigned)((N + CW - 1) / CW), 256, smem, s>>>(L, ldl, B, ldb, t, N);
+    } else {
+        constexpr int CW = 32;
+        const size_t smem = sizeof(T) * ((size_t)TF_TMAX * (CW + 1) + (size_t)TF_TMAX * (TF_TB + 1));
+        set_max_dyn_smem((const void *)k_trsm_fused<T, CW>, (int)smem);
+        k_trsm_fused<T, CW><<<(unsigned)((N + CW - 1) / CW), 256, smem, s>>>(L, ldl, B, ldb, t, N);
+    }
     OXI_LAUNCH_CHECK();
 }
 template void launch_trsm_fused<double>(const double *, i64, double *, i64, int, i64, cudaStream_t);
