@@ -316,14 +316,16 @@ __global__ void k_gather_rows(const T *__restrict__ B, i64 ldb, const int64_t *_
 
 // ---------------------------------------------------------------------------
 // Block-operator triangular solve.  For block b of the effective triangle M in
-// solve order, with p1 and p2 the blocks solved one and two steps before it,
-//   x_b = Dinv_b (r_b - sum_{older c} M(b,c) x_c) - Q1_b x_p1 - Q2_b x_p2,
-//   Dinv_b = M(b,b)^-1,  Q1_b = Dinv_b M(b,p1),  Q2_b = Dinv_b M(b,p2),
-// the three 64 x 64 operators precomputed per factor (k_trsv_prep).  Everything
-// but the last term is formed while the previous block is still being solved,
-// so the dependency chain from block to block is one warp-local 64 x 64
-// matrix-vector product: each warp owns 8 rows, four lanes per row, and reads
-// x_p1 straight from the tagged words, with no CTA barrier on the chain.
+// solve order, with p1, p2, p3 the blocks solved one, two and three steps
+// before it,
+//   x_b = Dinv_b (r_b - sum_{older c} M(b,c) x_c) - sum_q Q_q,b x_pq,
+//   Dinv_b = M(b,b)^-1,  Q_q,b = Dinv_b M(b,p_q)  (q = 1..TRSV_WIN),
+// the operators precomputed per factor (k_trsv_prep).  The older products and
+// Dinv run while the previous blocks are still being solved (they need no
+// block solved less than TRSV_WIN + 1 steps before), so the dependency chain
+// from block to block is one warp-local 64 x 64 matrix-vector product: each
+// warp owns 8 rows, four lanes per row, and reads x_p1 straight from the
+// tagged words, with no CTA barrier on the chain.
 // Solved values travel as tagged 64-bit words (value bits | epoch << 32; FP64
 // as two such halves), so a consumer spins on the data itself.
 // ---------------------------------------------------------------------------
@@ -363,7 +365,8 @@ __device__ __forceinline__ double tag_get<double>(const unsigned long long *w, u
     return __longlong_as_double((long long)((hi << 32) | (lo & 0xffffffffull)));
 }
 
-constexpr int TRSV_OPS = 3 * SB * SB;  // operator elements per block: Dinv, Q1, Q2
+constexpr int TRSV_WIN = 3;                       // blocks coupled on the chain
+constexpr int TRSV_OPS = (1 + TRSV_WIN) * SB * SB;  // operator elements per block: Dinv, Q1..Q3
 
 __device__ __forceinline__ float tag_decode(const unsigned long long (&w)[1]) { return __uint_as_float((uint32_t)w[0]); }
 __device__ __forceinline__ double tag_decode(const unsigned long long (&w)[2]) {
@@ -415,9 +418,9 @@ __device__ __forceinline__ void stage_block(T (*xs)[NR], const unsigned long lon
 }
 
 // One CTA per block: the inverse of the diagonal block by substitution (64
-// threads, one column each), then the two coupling operators as 64 x 64 x 64
+// threads, one column each), then the coupling operators as 64 x 64 x 64
 // products.  Rows and columns past n are padded with the identity (Dinv) and
-// zeros (Q1, Q2).
+// zeros (Q).
 template <typename T, bool LOWER, bool UNIT, bool ROWACC>
 __global__ void __launch_bounds__(SOLVE_NT) k_trsv_prep(const T *__restrict__ A, i64 lda, int n,
                                                        T *__restrict__ P) {
@@ -454,7 +457,7 @@ __global__ void __launch_bounds__(SOLVE_NT) k_trsv_prep(const T *__restrict__ A,
     __syncthreads();
     T *Pb = P + (i64)bi * TRSV_OPS;
     for (int e = t; e < SB * SB; e += SOLVE_NT) Pb[e] = sX[e / SB][e % SB];
-    for (int q = 1; q <= 2; ++q) {
+    for (int q = 1; q <= TRSV_WIN; ++q) {
         if (bi - q < 0) break;
         const int pb = LOWER ? b - q : b + q;
         const int c0 = pb * SB, cols = min(SB, n - c0);
@@ -486,7 +489,7 @@ struct Trsv3Smem {
     T y[SB][NR];
     T z[SB][NR];
     T part[SOLVE_NT / SB][SB][NR];
-    T op[3][SB][SB + 1];       // Dinv, Q1, Q2 of this block
+    T op[1 + TRSV_WIN][SB][SB + 1];  // Dinv, Q1..Q3 of this block
 };
 
 template <typename T, bool LOWER, bool ROWACC, int NR>
@@ -510,13 +513,19 @@ k_trsv3(const T *__restrict__ A, i64 lda, const T *__restrict__ P, T *__restrict
 
     // ---- this block's operators (no dependency on other blocks) ----
     const T *Pb = P + (i64)bi * TRSV_OPS;
-    const int nops = bi >= 2 ? 3 : bi + 1;
+    const int nops = min(bi, TRSV_WIN) + 1;
     for (int e = t; e < nops * SB * SB; e += SOLVE_NT) {
         const int o = e / (SB * SB), rr = (e / SB) % SB, jj = e % SB;
         S.op[o][rr][jj] = Pb[e];
     }
 
-    // ---- products with the blocks solved three or more steps before ----
+    // right-hand side of this block, read before anything waits
+    for (int e = t; e < SB * NR; e += SOLVE_NT) {
+        const int r = e % SB, k = e / SB;
+        S.y[r][k] = (r < rows) ? X[(i64)(r0 + r) + (i64)k * ldx] : T(0);
+    }
+
+    // ---- products with the blocks solved TRSV_WIN + 1 or more steps before ----
     // Blocks in solve order; within each, warp w takes tile columns [8w, 8w+8)
     // and each lane two rows.  The next block's tile and solution words are
     // loaded before the current block's products, so the loads' latency is
@@ -561,7 +570,7 @@ k_trsv3(const T *__restrict__ A, i64 lda, const T *__restrict__ P, T *__restrict
         for (int q = 0; q < 2; ++q)
 #pragma unroll
             for (int k = 0; k < NR; ++k) acc[q][k] = T(0);
-        const int nsteps = bi - 2;
+        const int nsteps = bi - TRSV_WIN;
         T an[2][8];
         T xn[XPL];
         if (nsteps > 0) {
@@ -614,7 +623,7 @@ k_trsv3(const T *__restrict__ A, i64 lda, const T *__restrict__ P, T *__restrict
         T v = T(0);
 #pragma unroll
         for (int w = 0; w < TRSV_WARPS; ++w) v += S.acc[w][r][k];
-        S.y[r][k] = (r < rows) ? (X[(i64)(r0 + r) + (i64)k * ldx] - v) : T(0);
+        S.y[r][k] -= v;
     }
     __syncthreads();
 
@@ -636,8 +645,6 @@ k_trsv3(const T *__restrict__ A, i64 lda, const T *__restrict__ P, T *__restrict
         }
         __syncwarp();
     };
-    if (bi >= 2) couple(2);  // solved two steps ago: off the chain
-
     // ---- z = Dinv y, over SEG column segments ----
     constexpr int SEG = SOLVE_NT / SB, SEGW = SB / SEG;
     {
@@ -664,8 +671,10 @@ k_trsv3(const T *__restrict__ A, i64 lda, const T *__restrict__ P, T *__restrict
     }
     __syncthreads();
 
-    // ---- the chain: x_b = z - Q2 x_p2 - Q1 x_p1, warp-local ----
-    if (bi >= 1) couple(1);
+    // ---- the chain: x_b = z - sum_q Q_q x_pq, warp-local; only x_p1 is fresh ----
+#pragma unroll
+    for (int q = TRSV_WIN; q >= 1; --q)
+        if (bi >= q) couple(q);
 #pragma unroll
     for (int k = 0; k < NR; ++k) {
         s[k] += __shfl_xor_sync(0xffffffffu, s[k], 1);
