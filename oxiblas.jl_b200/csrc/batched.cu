@@ -812,6 +812,7 @@ static void run_batched(oxi_handle_s *h, const BatchDesc &d, int smem, int grid)
     const bool same = gc.seen > 0 && gc.key == key;
     if (usable && same && gc.exec) {
         OXI_CUDA(cudaGraphLaunch(gc.exec, h->stream));
+        if (t_prof) t_prof->launches += gc.nlaunch;  // the replay's kernels count as launched
         return;
     }
     if (usable && same) {
@@ -819,6 +820,7 @@ static void run_batched(oxi_handle_s *h, const BatchDesc &d, int smem, int grid)
         OXI_CUDA(cudaStreamIsCapturing(h->stream, &st));
         if (st == cudaStreamCaptureStatusNone) {
             OXI_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+            const uint64_t before = t_prof ? t_prof->launches : 0;
             try {
                 launch_batched(h, d, smem, grid);
             } catch (...) {
@@ -828,6 +830,7 @@ static void run_batched(oxi_handle_s *h, const BatchDesc &d, int smem, int grid)
                 throw;
             }
             OXI_CUDA(cudaStreamEndCapture(h->stream, &gc.graph));
+            gc.nlaunch = (t_prof ? t_prof->launches : 0) - before;
             OXI_CUDA(cudaGraphInstantiate(&gc.exec, gc.graph, 0));
             gc.seen = 2;
             OXI_CUDA(cudaGraphLaunch(gc.exec, h->stream));

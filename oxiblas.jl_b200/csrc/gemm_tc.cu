@@ -476,6 +476,20 @@ __global__ void k_fp16_scales(const unsigned int *__restrict__ umax_bits, float 
     sc[1] = ldexpf(1.f, -(su + 14));                       // epilogue: 2^-14 * 2^-su
 }
 
+// The lookahead's second trailing update (operand slot 1) multiplies the same
+// L21 as the first (slot 0), converted just before on the first stream, which
+// the second stream waits for; slot 0 is not rewritten until the second update
+// has finished.  Reuse that conversion.
+static const void *reuse_a16(const oxi_handle_s *h, const float *A, i64 lda, i64 M, i64 K) {
+    const auto &r = h->tc_last_a;
+    if (h->tc_slot != 1 || r.src != A || r.lda != lda || r.M != M || r.K != K || r.kind != h->trailing) return nullptr;
+    return r.a16;
+}
+static void note_a16(oxi_handle_s *h, const float *A, i64 lda, i64 M, i64 K, const void *a16) {
+    if (h->tc_slot != 0) return;
+    h->tc_last_a = {A, lda, M, K, h->trailing, a16};
+}
+
 void gemm_trailing_f32(oxi_handle_s *h, float *C, i64 ldc, const float *A, i64 lda, const float *B,
                        i64 ldb, i64 M, i64 N, i64 K) {
     if (M <= 0 || N <= 0 || K <= 0) return;
@@ -507,7 +521,9 @@ void gemm_trailing_f32(oxi_handle_s *h, float *C, i64 ldc, const float *A, i64 l
             k_fp16_scales<<<1, 1, 0, s>>>(umax, scal);
             OXI_LAUNCH_CHECK();
         }
-        {
+        if (const void *prev = reuse_a16(h, A, lda, M, K)) {
+            A16 = const_cast<void *>(prev);
+        } else {
             ProfScope ps(KC_CONVERT, s, 0.0, 10.0 * (double)M * K);
             dim3 g((unsigned)std::min<i64>((K + 255) / 256, 64), (unsigned)M);
             if (f16)
@@ -517,6 +533,7 @@ void gemm_trailing_f32(oxi_handle_s *h, float *C, i64 ldc, const float *A, i64 l
                 k_cvt_rows_split3<__nv_bfloat16><<<g, 256, 0, s>>>(A, lda, (__nv_bfloat16 *)A16, ldk3, (int)M,
                                                                    (int)K, 1.f, nullptr);
             OXI_LAUNCH_CHECK();
+            note_a16(h, A, lda, M, K, A16);
         }
         {
             ProfScope ps(KC_CONVERT, s, 0.0, 10.0 * (double)N * K);
@@ -542,8 +559,13 @@ void gemm_trailing_f32(oxi_handle_s *h, float *C, i64 ldc, const float *A, i64 l
     B16 = (void *)(((uintptr_t)B16 + 255) & ~uintptr_t(255));
     float *scal = (float *)((char *)h->scratch.get(kScratchBytes) + kScratchScalOff + 1536 + 256 * h->tc_slot);
     cudaStream_t s = h->stream;
+    const void *prev = reuse_a16(h, A, lda, M, K);
+    if (prev) A16 = const_cast<void *>(prev);
     if (fmt == 1) {
-        launch_cvt_rows16(1, A, lda, A16, ldk, M, K, 1.f, nullptr, s);
+        if (!prev) {
+            launch_cvt_rows16(1, A, lda, A16, ldk, M, K, 1.f, nullptr, s);
+            note_a16(h, A, lda, M, K, A16);
+        }
         launch_cvt_transpose16(1, B, ldb, B16, ldk, K, N, 1.f, nullptr, s);
         launch_gemm_tc(1, C, ldc, A16, ldk, B16, ldk, M, N, K, 1.f, nullptr, s, h->gemm_ctas);
     } else {
@@ -554,7 +576,10 @@ void gemm_trailing_f32(oxi_handle_s *h, float *C, i64 ldc, const float *A, i64 l
         OXI_LAUNCH_CHECK();
         k_fp16_scales<<<1, 1, 0, s>>>(umax, scal);
         OXI_LAUNCH_CHECK();
-        launch_cvt_rows16(0, A, lda, A16, ldk, M, K, 16384.f, nullptr, s);
+        if (!prev) {
+            launch_cvt_rows16(0, A, lda, A16, ldk, M, K, 16384.f, nullptr, s);
+            note_a16(h, A, lda, M, K, A16);
+        }
         launch_cvt_transpose16(0, B, ldb, B16, ldk, K, N, 1.f, scal, s);
         launch_gemm_tc(0, C, ldc, A16, ldk, B16, ldk, M, N, K, 1.f, scal + 1, s, h->gemm_ctas);
     }

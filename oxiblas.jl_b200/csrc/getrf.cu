@@ -371,6 +371,7 @@ void getrf_rowmajor_cached(oxi_handle_s *h, T *W, i64 ld, i64 m, i64 n, int64_t 
     const bool same = gc.seen > 0 && std::memcmp(gc.key, key, sizeof(key)) == 0;
     if (usable && same && gc.valid) {
         OXI_CUDA(cudaGraphLaunch(gc.exec, h->stream));
+        if (t_prof) t_prof->launches += gc.nlaunch;  // the replay's kernels count as launched
         return;
     }
     if (usable && same && gc.seen >= 1) {
@@ -380,6 +381,7 @@ void getrf_rowmajor_cached(oxi_handle_s *h, T *W, i64 ld, i64 m, i64 n, int64_t 
         OXI_CUDA(cudaStreamIsCapturing(h->stream, &st));
         if (st == cudaStreamCaptureStatusNone && h->stream != nullptr) {
             OXI_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+            const uint64_t before = t_prof ? t_prof->launches : 0;
             try {
                 getrf_rowmajor<T>(h, W, ld, m, n, d_ipiv, d_info, d_moves, d_nmoves);
             } catch (...) {
@@ -389,6 +391,7 @@ void getrf_rowmajor_cached(oxi_handle_s *h, T *W, i64 ld, i64 m, i64 n, int64_t 
                 throw;
             }
             OXI_CUDA(cudaStreamEndCapture(h->stream, &gc.graph));
+            gc.nlaunch = (t_prof ? t_prof->launches : 0) - before;
             OXI_CUDA(cudaGraphInstantiate(&gc.exec, gc.graph, cudaGraphInstantiateFlagUseNodePriority));
             std::memcpy(gc.key, key, sizeof(key));
             gc.valid = true;

@@ -115,6 +115,14 @@ struct oxi_handle_s {
     oxi::DeviceBuffer tc_ws;     // 16-bit GEMM operands
     oxi::DeviceBuffer tc_ws2;    // the same for a second, concurrent trailing update
     int tc_slot = 0;             // which of the two operand buffers (and scale slots) to use
+    // the last A operand converted into tc_ws: the lookahead's second trailing
+    // update has the same L21 and reuses it instead of converting it again
+    struct TcA16 {
+        const float *src = nullptr;
+        int64_t lda = 0, M = 0, K = 0;
+        int kind = -1;
+        const void *a16 = nullptr;
+    } tc_last_a;
     int gemm_ctas = 0;           // > 0: cap on the persistent tensor-core GEMM's CTAs;
                                  // -k: at most k GPC-filling clusters, one GPC spared
     cudaStream_t la_stream = nullptr;        // lookahead: the trailing update's stream
@@ -135,6 +143,7 @@ struct oxi_handle_s {
     struct GraphCache {
         bool valid = false;
         int seen = 0;
+        uint64_t nlaunch = 0;  // kernel launches one replay performs (launch counter)
         uint64_t key[12] = {};
         cudaGraphExec_t exec = nullptr;
         cudaGraph_t graph = nullptr;
@@ -158,6 +167,7 @@ struct oxi_handle_s {
     struct BatchGraph {
         std::vector<uint64_t> key;
         int seen = 0;
+        uint64_t nlaunch = 0;  // kernel launches one replay performs (launch counter)
         cudaGraphExec_t exec = nullptr;
         cudaGraph_t graph = nullptr;
         void reset() {

@@ -375,44 +375,68 @@ __device__ __forceinline__ double tag_decode(const unsigned long long (&w)[2]) {
 
 // One warp stages the solution of a 64-row block (rows row0.., `cols` of them,
 // NR right-hand sides) from the tagged words into xs[64][NR]: every word's load
-// is in flight at once, and only words of an older epoch are polled again.
+// is in flight at once, and the words still of an older epoch are polled again
+// together, one round trip per pass however many there are.
 template <typename T, int NR>
 __device__ __forceinline__ void stage_block(T (*xs)[NR], const unsigned long long *__restrict__ xtag, int row0,
                                             int cols, uint32_t epoch, int *err, int lane) {
     constexpr int TW = TagWords<T>::n;
     constexpr int PL = SB * NR / 32;
     unsigned long long w[PL][TW];
+    bool rdy[PL];
+    auto word = [&](int v) {
+        const int e = lane + 32 * v, jj = e % SB, k = e / SB;
+        return xtag + ((i64)(row0 + jj) * NR + k) * TW;
+    };
 #pragma unroll
     for (int v = 0; v < PL; ++v) {
-        const int e = lane + 32 * v, jj = e % SB, k = e / SB;
-        const unsigned long long *p = xtag + ((i64)(row0 + jj) * NR + k) * TW;
+        const int jj = (lane + 32 * v) % SB;
+        rdy[v] = jj >= cols;
 #pragma unroll
-        for (int h = 0; h < TW; ++h) w[v][h] = (jj < cols) ? ld_volatile_u64(p + h) : ((unsigned long long)epoch << 32);
+        for (int h = 0; h < TW; ++h) w[v][h] = rdy[v] ? 0ull : ld_volatile_u64(word(v) + h);
+    }
+    bool all = true;
+#pragma unroll
+    for (int v = 0; v < PL; ++v) {
+        if (!rdy[v]) {
+            bool ok = true;
+#pragma unroll
+            for (int h = 0; h < TW; ++h) ok = ok && (uint32_t)(w[v][h] >> 32) == epoch;
+            rdy[v] = ok;
+        }
+        all = all && rdy[v];
+    }
+    if (!all) {
+        const uint64_t t0 = global_ns();
+        uint32_t it = 0;
+        for (;;) {
+#pragma unroll
+            for (int v = 0; v < PL; ++v)
+                if (!rdy[v]) {
+#pragma unroll
+                    for (int h = 0; h < TW; ++h) w[v][h] = ld_volatile_u64(word(v) + h);
+                }
+            all = true;
+#pragma unroll
+            for (int v = 0; v < PL; ++v) {
+                if (!rdy[v]) {
+                    bool ok = true;
+#pragma unroll
+                    for (int h = 0; h < TW; ++h) ok = ok && (uint32_t)(w[v][h] >> 32) == epoch;
+                    rdy[v] = ok;
+                }
+                all = all && rdy[v];
+            }
+            if (all) break;
+            if ((++it & 63) == 0 && global_ns() - t0 > kWaitLimitNs) {
+                atomicExch(err, 3);
+                break;
+            }
+        }
     }
 #pragma unroll
     for (int v = 0; v < PL; ++v) {
         const int e = lane + 32 * v, jj = e % SB, k = e / SB;
-        const unsigned long long *p = xtag + ((i64)(row0 + jj) * NR + k) * TW;
-        bool ready = true;
-#pragma unroll
-        for (int h = 0; h < TW; ++h) ready = ready && (uint32_t)(w[v][h] >> 32) == epoch;
-        if (!ready) {
-            const uint64_t t0 = global_ns();
-            uint32_t it = 0;
-            for (;;) {
-                ready = true;
-#pragma unroll
-                for (int h = 0; h < TW; ++h) {
-                    w[v][h] = ld_volatile_u64(p + h);
-                    ready = ready && (uint32_t)(w[v][h] >> 32) == epoch;
-                }
-                if (ready) break;
-                if ((++it & 255) == 0 && global_ns() - t0 > kWaitLimitNs) {
-                    atomicExch(err, 3);
-                    break;
-                }
-            }
-        }
         xs[jj][k] = (jj < cols) ? (T)tag_decode(w[v]) : T(0);
     }
 }
@@ -571,16 +595,24 @@ k_trsv3(const T *__restrict__ A, i64 lda, const T *__restrict__ P, T *__restrict
 #pragma unroll
             for (int k = 0; k < NR; ++k) acc[q][k] = T(0);
         const int nsteps = bi - TRSV_WIN;
+        // the next step's tile and raw solution words are loaded one step ahead
+        // (all in flight at once); a word of an older epoch is polled again only
+        // when its step comes
         T an[2][8];
-        T xn[XPL];
-        if (nsteps > 0) {
-            load_tile(0, an);
+        unsigned long long xr[XPL][TW];
+        auto issue_x = [&](int step) {
 #pragma unroll
             for (int v = 0; v < XPL; ++v) {
                 int row, k; bool ok;
-                xidx(0, v, row, k, ok);
-                xn[v] = ok ? tag_get<T>(xw(row, k), epoch, err) : T(0);
+                xidx(step, v, row, k, ok);
+#pragma unroll
+                for (int hw = 0; hw < TW; ++hw)
+                    xr[v][hw] = ok ? ld_volatile_u64(xw(row, k) + hw) : ((unsigned long long)epoch << 32);
             }
+        };
+        if (nsteps > 0) {
+            load_tile(0, an);
+            issue_x(0);
         }
         for (int step = 0; step < nsteps; ++step) {
             T a[2][8];
@@ -590,16 +622,34 @@ k_trsv3(const T *__restrict__ A, i64 lda, const T *__restrict__ P, T *__restrict
                 for (int u = 0; u < 8; ++u) a[q][u] = an[q][u];
             T *xsw = &S.xs[warp][0][0];  // [rhs k][column u] at k * 8 + u
 #pragma unroll
-            for (int v = 0; v < XPL; ++v)
-                if (lane + 32 * v < 8 * NR) xsw[lane + 32 * v] = xn[v];
+            for (int v = 0; v < XPL; ++v) {
+                int row, k; bool ok;
+                xidx(step, v, row, k, ok);
+                bool ready = true;
+#pragma unroll
+                for (int hw = 0; hw < TW; ++hw) ready = ready && (uint32_t)(xr[v][hw] >> 32) == epoch;
+                if (!ready) {
+                    const uint64_t t0 = global_ns();
+                    uint32_t it = 0;
+                    for (;;) {
+                        ready = true;
+#pragma unroll
+                        for (int hw = 0; hw < TW; ++hw) {
+                            xr[v][hw] = ld_volatile_u64(xw(row, k) + hw);
+                            ready = ready && (uint32_t)(xr[v][hw] >> 32) == epoch;
+                        }
+                        if (ready) break;
+                        if ((++it & 255) == 0 && global_ns() - t0 > kWaitLimitNs) {
+                            atomicExch(err, 3);
+                            break;
+                        }
+                    }
+                }
+                if (lane + 32 * v < 8 * NR) xsw[lane + 32 * v] = ok ? (T)tag_decode(xr[v]) : T(0);
+            }
             if (step + 1 < nsteps) {
                 load_tile(step + 1, an);
-#pragma unroll
-                for (int v = 0; v < XPL; ++v) {
-                    int row, k; bool ok;
-                    xidx(step + 1, v, row, k, ok);
-                    xn[v] = ok ? tag_get<T>(xw(row, k), epoch, err) : T(0);
-                }
+                issue_x(step + 1);
             }
             __syncwarp();
 #pragma unroll
