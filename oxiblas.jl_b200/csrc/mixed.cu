@@ -125,7 +125,9 @@ __global__ void k_check_finite(const double *__restrict__ B, i64 ldb, int n, int
 // FP64 residual R = B - A X (or product Y = A X) with the componentwise error
 // ---------------------------------------------------------------------------
 // Each thread owns two adjacent rows (one 16-byte load per column when the
-// column base is 16-byte aligned); columns split into RS chunks.
+// column base is 16-byte aligned); columns split into RS chunks.  NR is the
+// accumulator count (a single right-hand side keeps fewer registers, so more
+// warps hide the loads' latency); partial sums are laid out NRMAX apart.
 template <int NR>
 __global__ void k_resid_part(const double *__restrict__ A, i64 lda, int n, const double *__restrict__ X,
                              i64 ldx, int nr, double *__restrict__ pax, double *__restrict__ pden) {
@@ -164,8 +166,8 @@ __global__ void k_resid_part(const double *__restrict__ A, i64 lda, int n, const
 #pragma unroll
         for (int k = 0; k < NR; ++k)
             if (k < nr) {
-                pax[((i64)s * NR + k) * n + i + h] = ax[h][k];
-                if (pden) pden[((i64)s * NR + k) * n + i + h] = den[h][k];
+                pax[((i64)s * NRMAX + k) * n + i + h] = ax[h][k];
+                if (pden) pden[((i64)s * NRMAX + k) * n + i + h] = den[h][k];
             }
     }
 }
@@ -378,7 +380,10 @@ static void residual(MixedRun &M, const double *Xin, double *Rout, std::vector<d
     for (int k0 = 0; k0 < nrhs; k0 += NRMAX) {
         const int nr = std::min(NRMAX, nrhs - k0);
         dim3 g1(blocks_for((n + 1) / 2, 128), RS);
-        k_resid_part<NRMAX><<<g1, 128, 0, s>>>(M.A, M.lda, n, Xin + (i64)k0 * M.ldx, M.ldx, nr, M.pax, M.pden);
+        if (nr == 1)
+            k_resid_part<1><<<g1, 128, 0, s>>>(M.A, M.lda, n, Xin + (i64)k0 * M.ldx, M.ldx, nr, M.pax, M.pden);
+        else
+            k_resid_part<NRMAX><<<g1, 128, 0, s>>>(M.A, M.lda, n, Xin + (i64)k0 * M.ldx, M.ldx, nr, M.pax, M.pden);
         OXI_LAUNCH_CHECK();
         dim3 g2(blocks_for(n), nr);
         k_resid_final<<<g2, 256, 0, s>>>(M.B + (i64)k0 * M.ldb, M.ldb, Rout + (i64)k0 * M.n, M.n,
@@ -407,7 +412,7 @@ static void matvec(MixedRun &M, const double *x, double *y) {
     cudaStream_t s = M.s;
     const int n = (int)M.n;
     dim3 g1(blocks_for((n + 1) / 2, 128), RS);
-    k_resid_part<NRMAX><<<g1, 128, 0, s>>>(M.A, M.lda, n, x, n, 1, M.pax, nullptr);
+    k_resid_part<1><<<g1, 128, 0, s>>>(M.A, M.lda, n, x, n, 1, M.pax, nullptr);
     OXI_LAUNCH_CHECK();
     k_resid_final<<<dim3(blocks_for(n), 1), 256, 0, s>>>(nullptr, 0, y, n, nullptr, 0, n, 1, 0, M.pax,
                                                          nullptr, 1, nullptr);
