@@ -35,9 +35,9 @@ __device__ __forceinline__ void st_release(int *p, int v) {
 // A CTA owns a row block (ticket order); its 8 warps take the solved column
 // blocks round-robin, each lane accumulating two rows, so the off-diagonal
 // products of one block run with 8-way memory parallelism and no cross-lane
-// reductions.  The diagonal block is solved by substitution, or -- when Dinv
-// holds the inverses of the diagonal blocks (computed once per factorization)
-// -- by a 64 x 64 matrix-vector product, which shortens the dependency chain.
+// reductions.  The diagonal block is solved by substitution.  The handle's
+// solves use the block-operator kernel below (k_trsv3); this one needs no
+// workspace beyond its flags and serves the no-allocation entry point.
 constexpr int TRSV_WARPS = SOLVE_NT / 32;
 
 template <typename T, int NR>
@@ -48,7 +48,7 @@ struct TrsvSmem {
     T x0[SB][NR];                // the critical block's solution
     T part[SOLVE_NT / SB][SB][NR];
     T tile[SB][SB + 1];          // the critical off-diagonal tile, prefetched
-    T diag[SB][SB + 1];          // diagonal block (substitution) or its inverse
+    T diag[SB][SB + 1];          // the diagonal block
 };
 
 __device__ __forceinline__ unsigned long long ld_volatile_u64(const unsigned long long *p) {
@@ -73,15 +73,12 @@ __device__ __forceinline__ float tagged_get(const unsigned long long *p, uint32_
     return __uint_as_float((uint32_t)w);
 }
 
-// TAGGED (FP32 only): solved values are also published as 64-bit words
-// (value bits | epoch << 32) in xtag; a consumer spins on the words themselves,
-// so no flag, no fence and no second round trip sit on the dependency chain.
-template <typename T, bool LOWER, bool UNIT, bool ROWACC, int NR, bool INV, bool TAGGED = false>
+// A solved block is published through its flag (release after the rows are
+// stored; consumers acquire it before reading the rows).
+template <typename T, bool LOWER, bool UNIT, bool ROWACC, int NR>
 __global__ void __launch_bounds__(SOLVE_NT)
-k_trsv2(const T *__restrict__ A, i64 lda, const T *__restrict__ Dinv, T *__restrict__ X, i64 ldx, int n,
-        int *__restrict__ ticket, int *__restrict__ flags, int *__restrict__ err,
-        unsigned long long *__restrict__ xtag = nullptr, uint32_t epoch = 0) {
-    static_assert(!TAGGED || sizeof(T) == 4, "tagged exchange packs FP32 values");
+k_trsv2(const T *__restrict__ A, i64 lda, T *__restrict__ X, i64 ldx, int n, int *__restrict__ ticket,
+        int *__restrict__ flags, int *__restrict__ err) {
     extern __shared__ __align__(16) unsigned char trsv_smem[];
     TrsvSmem<T, NR> &S = *reinterpret_cast<TrsvSmem<T, NR> *>(trsv_smem);
     __shared__ int s_blk;
@@ -106,8 +103,7 @@ k_trsv2(const T *__restrict__ A, i64 lda, const T *__restrict__ Dinv, T *__restr
         // threads run along the contiguous index of the stored factor
         int r, j;
         if (ROWACC) { r = e / SB; j = e % SB; } else { r = e % SB; j = e / SB; }
-        if (INV) S.diag[r][j] = Dinv[(i64)b * SB * SB + (i64)r * SB + j];
-        else S.diag[r][j] = (r < rows && j < rows) ? Mv(r0 + r, r0 + j) : T(0);
+        S.diag[r][j] = (r < rows && j < rows) ? Mv(r0 + r, r0 + j) : T(0);
         if (has_crit) S.tile[r][j] = (r < rows && j < ccols) ? Mv(r0 + r, cc0 + j) : T(0);
     }
 
@@ -124,27 +120,20 @@ k_trsv2(const T *__restrict__ A, i64 lda, const T *__restrict__ Dinv, T *__restr
         const int c = LOWER ? step : nb - 1 - step;
         const int c0 = c * SB;
         const int cols = min(SB, n - c0);
-        if constexpr (TAGGED) {
-            for (int e = lane; e < SB * NR; e += 32) {
-                const int jj = e % SB, k = e / SB;
-                S.x[warp][jj][k] = (jj < cols) ? (T)tagged_get(&xtag[(i64)(c0 + jj) * NR + k], epoch, err) : T(0);
-            }
-        } else {
-            if (lane == 0 && ld_acquire(&flags[c]) == 0) {
-                const uint64_t t0 = global_ns();
-                uint32_t it = 0;
-                while (ld_acquire(&flags[c]) == 0) {
-                    if ((++it & 255) == 0 && global_ns() - t0 > kWaitLimitNs) {
-                        atomicExch(err, 3);
-                        break;
-                    }
+        if (lane == 0 && ld_acquire(&flags[c]) == 0) {
+            const uint64_t t0 = global_ns();
+            uint32_t it = 0;
+            while (ld_acquire(&flags[c]) == 0) {
+                if ((++it & 255) == 0 && global_ns() - t0 > kWaitLimitNs) {
+                    atomicExch(err, 3);
+                    break;
                 }
             }
-            __syncwarp();
-            for (int e = lane; e < SB * NR; e += 32) {
-                const int jj = e % SB, k = e / SB;
-                S.x[warp][jj][k] = (jj < cols) ? __ldcg(&X[(i64)(c0 + jj) + (i64)k * ldx]) : T(0);
-            }
+        }
+        __syncwarp();
+        for (int e = lane; e < SB * NR; e += 32) {
+            const int jj = e % SB, k = e / SB;
+            S.x[warp][jj][k] = (jj < cols) ? __ldcg(&X[(i64)(c0 + jj) + (i64)k * ldx]) : T(0);
         }
         __syncwarp();
 #pragma unroll
@@ -197,27 +186,20 @@ k_trsv2(const T *__restrict__ A, i64 lda, const T *__restrict__ Dinv, T *__restr
     constexpr int SEG = SOLVE_NT / SB, SEGW = SB / SEG;
     const int pr = t % SB, ps = t / SB;
     if (has_crit) {
-        if constexpr (TAGGED) {
-            for (int e = t; e < SB * NR; e += SOLVE_NT) {
-                const int jj = e % SB, k = e / SB;
-                S.x0[jj][k] = (jj < ccols) ? (T)tagged_get(&xtag[(i64)(cc0 + jj) * NR + k], epoch, err) : T(0);
-            }
-        } else {
-            if (t == 0 && ld_acquire(&flags[cc]) == 0) {
-                const uint64_t t0 = global_ns();
-                uint32_t it = 0;
-                while (ld_acquire(&flags[cc]) == 0) {
-                    if ((++it & 255) == 0 && global_ns() - t0 > kWaitLimitNs) {
-                        atomicExch(err, 3);
-                        break;
-                    }
+        if (t == 0 && ld_acquire(&flags[cc]) == 0) {
+            const uint64_t t0 = global_ns();
+            uint32_t it = 0;
+            while (ld_acquire(&flags[cc]) == 0) {
+                if ((++it & 255) == 0 && global_ns() - t0 > kWaitLimitNs) {
+                    atomicExch(err, 3);
+                    break;
                 }
             }
-            __syncthreads();
-            for (int e = t; e < SB * NR; e += SOLVE_NT) {
-                const int jj = e % SB, k = e / SB;
-                S.x0[jj][k] = (jj < ccols) ? __ldcg(&X[(i64)(cc0 + jj) + (i64)k * ldx]) : T(0);
-            }
+        }
+        __syncthreads();
+        for (int e = t; e < SB * NR; e += SOLVE_NT) {
+            const int jj = e % SB, k = e / SB;
+            S.x0[jj][k] = (jj < ccols) ? __ldcg(&X[(i64)(cc0 + jj) + (i64)k * ldx]) : T(0);
         }
         __syncthreads();
         T pv[NR];
@@ -242,66 +224,33 @@ k_trsv2(const T *__restrict__ A, i64 lda, const T *__restrict__ Dinv, T *__restr
     }
     __syncthreads();
 
-    if (INV) {
-        // x_b = Dinv_b y, split over SEG column segments
-        T pv[NR];
+    // substitution on the diagonal block: warp k takes right-hand side k
+    for (int k = warp; k < NR; k += TRSV_WARPS) {
+        T y[2];
 #pragma unroll
-        for (int k = 0; k < NR; ++k) pv[k] = T(0);
-#pragma unroll
-        for (int jj = 0; jj < SEGW; ++jj) {
-            const T a = S.diag[pr][ps * SEGW + jj];
-#pragma unroll
-            for (int k = 0; k < NR; ++k) pv[k] = fma(a, S.y[ps * SEGW + jj][k], pv[k]);
-        }
-#pragma unroll
-        for (int k = 0; k < NR; ++k) S.part[ps][pr][k] = pv[k];
-        __syncthreads();
-        for (int e = t; e < SB * NR; e += SOLVE_NT) {
-            const int r = e % SB, k = e / SB;
-            if (r >= rows) continue;
-            T v = T(0);
-#pragma unroll
-            for (int q = 0; q < SEG; ++q) v += S.part[q][r][k];
-            X[(i64)(r0 + r) + (i64)k * ldx] = v;
-            if constexpr (TAGGED)
-                xtag[(i64)(r0 + r) * NR + k] = ((unsigned long long)epoch << 32) | __float_as_uint((float)v);
-        }
-    } else {
-        // substitution on the diagonal block: warp k takes right-hand side k
-        for (int k = warp; k < NR; k += TRSV_WARPS) {
-            T y[2];
-#pragma unroll
-            for (int q = 0; q < 2; ++q) y[q] = S.y[lane + 32 * q][k];
-            for (int st = 0; st < rows; ++st) {
-                const int p = LOWER ? st : rows - 1 - st;
-                const int hp = p >> 5, lp = p & 31;
-                const T yp = __shfl_sync(0xffffffffu, hp ? y[1] : y[0], lp);
-                const T xp = UNIT ? yp : yp / S.diag[p][p];
-                if (lane == lp) { if (hp) y[1] = xp; else y[0] = xp; }
-#pragma unroll
-                for (int q = 0; q < 2; ++q) {
-                    const int r = lane + 32 * q;
-                    const bool below = LOWER ? (r > p) : (r < p);
-                    if (below && r < rows) y[q] = fma(-S.diag[r][p], xp, y[q]);
-                }
-            }
+        for (int q = 0; q < 2; ++q) y[q] = S.y[lane + 32 * q][k];
+        for (int st = 0; st < rows; ++st) {
+            const int p = LOWER ? st : rows - 1 - st;
+            const int hp = p >> 5, lp = p & 31;
+            const T yp = __shfl_sync(0xffffffffu, hp ? y[1] : y[0], lp);
+            const T xp = UNIT ? yp : yp / S.diag[p][p];
+            if (lane == lp) { if (hp) y[1] = xp; else y[0] = xp; }
 #pragma unroll
             for (int q = 0; q < 2; ++q) {
                 const int r = lane + 32 * q;
-                if (r < rows) {
-                    X[(i64)(r0 + r) + (i64)k * ldx] = y[q];
-                    if constexpr (TAGGED)
-                        xtag[(i64)(r0 + r) * NR + k] =
-                            ((unsigned long long)epoch << 32) | __float_as_uint((float)y[q]);
-                }
+                const bool below = LOWER ? (r > p) : (r < p);
+                if (below && r < rows) y[q] = fma(-S.diag[r][p], xp, y[q]);
             }
         }
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int r = lane + 32 * q;
+            if (r < rows) X[(i64)(r0 + r) + (i64)k * ldx] = y[q];
+        }
     }
-    if constexpr (!TAGGED) {
-        __threadfence();
-        __syncthreads();
-        if (t == 0) st_release(&flags[b], 1);
-    }
+    __threadfence();
+    __syncthreads();
+    if (t == 0) st_release(&flags[b], 1);
 }
 
 template <typename T>
@@ -759,9 +708,9 @@ static void trsv_launch(const T *A, i64 lda, T *X, i64 ldx, int n, int nrhs, int
 #define OXI_TRSV_GO(NRV)                                                                              \
     do {                                                                                             \
         const int smem = (int)sizeof(TrsvSmem<T, NRV>);                                             \
-        auto kern = k_trsv2<T, LOWER, UNIT, TRANS, NRV, false>;                                      \
+        auto kern = k_trsv2<T, LOWER, UNIT, TRANS, NRV>;                                             \
         OXI_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));     \
-        kern<<<nb, SOLVE_NT, smem, s>>>(A, lda, nullptr, Xk, ldx, n, ticket, flags, err, nullptr, 0u); \
+        kern<<<nb, SOLVE_NT, smem, s>>>(A, lda, Xk, ldx, n, ticket, flags, err);                      \
         k0 += NRV;                                                                                   \
     } while (0)
         if (left >= 8) OXI_TRSV_GO(8);
@@ -871,9 +820,10 @@ template void getrs_perm<double>(oxi_handle_s *, char, i64, i64, const double *,
 template void getrs_perm<float>(oxi_handle_s *, char, i64, i64, const float *, i64, const int64_t *, float *, i64, int *);
 
 // Row-major factors W are the column-major matrix W^T: L (lower) is then an
-// upper-stored triangle read transposed, U likewise.  Dinv (optional): the
-// inverses of the 64 x 64 diagonal blocks of L and of U, from
-// lu_block_inverses_rowmajor.
+// upper-stored triangle read transposed, U likewise.  DinvL / DinvU (optional):
+// the per-block operators of L and of U (diagonal-block inverse and coupling
+// blocks) from lu_block_inverses_rowmajor; without them the substitution
+// kernel runs.
 template <typename T>
 void lu_solve_rowmajor(oxi_handle_s *h, const T *W, i64 ld, i64 n, T *X, i64 ldx, i64 nrhs,
                        int *d_err, const T *DinvL, const T *DinvU) {
@@ -1006,9 +956,10 @@ __global__ void __launch_bounds__(1024) k_perm_from_ipiv_na(const int64_t *__res
 template <bool UPPER_A, bool UNIT, bool TRANS>
 static void na_load_trsv(cudaFuncAttributes *fa) {
     constexpr bool LOWER = (UPPER_A == TRANS);
-    OXI_CUDA(cudaFuncGetAttributes(fa, k_trsv2<double, LOWER, UNIT, TRANS, 1, false>));
-    OXI_CUDA(cudaFuncGetAttributes(fa, k_trsv2<double, LOWER, UNIT, TRANS, 2, false>));
-    OXI_CUDA(cudaFuncGetAttributes(fa, k_trsv2<double, LOWER, UNIT, TRANS, 4, false>));
+    OXI_CUDA(cudaFuncGetAttributes(fa, k_trsv2<double, LOWER, UNIT, TRANS, 1>));
+    OXI_CUDA(cudaFuncGetAttributes(fa, k_trsv2<double, LOWER, UNIT, TRANS, 2>));
+    OXI_CUDA(cudaFuncGetAttributes(fa, k_trsv2<double, LOWER, UNIT, TRANS, 4>));
+    OXI_CUDA(cudaFuncGetAttributes(fa, k_trsv2<double, LOWER, UNIT, TRANS, 8>));
 }
 
 // Once per device, with that device current: the array's address, and the

@@ -214,3 +214,29 @@ def test_lookahead_gives_identical_factors(pkg, oracle, dtype):
         if dtype == np.float64:
             _, ipo, _ = oracle.getrf(A, blocksize=bs)
             assert np.array_equal(_np(F1.ipiv), ipo)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_many_rhs_solves_every_chunk_width(pkg, dtype):
+    """ldiv! with 23 right-hand sides runs the block-operator triangular solve
+    in chunks of 16 (FP32), 8, 4, 2 and 1 columns; n = 777 gives a partial last
+    64-row block and more blocks than the three the chain couples.  Each column
+    must equal the one-column solve of the same factor (relative 1e-13 FP64,
+    1e-5 FP32: the per-column arithmetic does not depend on the chunk width),
+    and the whole solve must have a normwise backward error <= 30 n eps, for N
+    and T."""
+    rng = np.random.default_rng(77)
+    n, k = 777, 23
+    A = (rng.standard_normal((n, n)) + 4 * np.eye(n)).astype(dtype)
+    B = rng.standard_normal((n, k)).astype(dtype)
+    F = pkg.lu(torch.from_numpy(A))
+    same = 1e-13 if dtype == np.float64 else 1e-5
+    eps = np.finfo(dtype).eps
+    A64, B64 = A.astype(np.float64), B.astype(np.float64)
+    for Fv, M in ((F, A64), (F.T, A64.T)):
+        X = _np(pkg.ldiv(Fv, torch.from_numpy(B))).astype(np.float64)
+        for j in (0, 7, 15, 16, 22):
+            xj = _np(pkg.ldiv(Fv, torch.from_numpy(np.ascontiguousarray(B[:, j])))).astype(np.float64)
+            assert np.abs(X[:, j] - xj).max() <= same * np.abs(xj).max(), (dtype, j)
+        bw = np.linalg.norm(M @ X - B64) / (np.linalg.norm(M) * np.linalg.norm(X))
+        assert bw <= 30 * n * eps, (dtype, bw)
