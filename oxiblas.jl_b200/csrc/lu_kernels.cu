@@ -87,14 +87,16 @@ template void launch_rm_to_cm<float, double>(const float *, i64, double *, i64, 
 //   a_ic = muladd(-l_ij, a_jc, a_ic) for c > j.
 // Per column each CTA reduces its candidate in registers/shared memory and
 // PUSHES it (|value|, position, the whole candidate row) into every CTA's
-// shared memory with st.async, each store completing its bytes on the
-// receiver's mbarrier; a CTA waits on its own barrier until all candidates
-// have landed and picks the same winner as every other CTA.  The CTA that owns
-// position j also pushes row j, so the two swapped rows never need a second
-// exchange.  Slots are double-buffered by column parity, which is what makes
-// one exchange per column sufficient.  Each row carries the index of the
-// row it started as; at the end a position whose row changed emits a (dst, src)
-// move, the net permutation applied to the other columns by k_rowmoves.
+// shared memory with st.async, one 16-byte store per thread, each completing
+// its bytes on the receiver's mbarrier; a CTA waits on its own barrier until
+// all candidates have landed and picks the same winner as every other CTA.
+// The CTA that owns position j also pushes row j, so the two swapped rows
+// never need a second exchange.  Slots are double-buffered by column parity,
+// which is what makes one exchange per column sufficient.  Each row carries
+// the index of the row it started as; at the end a position whose row changed
+// emits a (dst, src) move.  The net permutation reaches the other columns by
+// k_rowmoves, or, inside a composed panel, through the leaf itself after a
+// cluster barrier (one warp per moved row).
 // ---------------------------------------------------------------------------
 // ---------------------------------------------------------------------------
 // Warp arg-max for the pivot search with redux.sync: |v| >= 0 orders like its
