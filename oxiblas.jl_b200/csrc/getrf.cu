@@ -104,14 +104,15 @@ static void panel_rl(LuRun<T> &R, i64 c0, i64 nc) {
     oxi_handle_s *h = R.h;
     const i64 cend = c0 + nc;
     LeafPanel pend;  // the previous step's U12, still in R.ubuf
+    OXI_CUDA(cudaMemsetAsync(R.nmoves, 0, sizeof(int), h->stream));  // each leaf zeroes it again at its end
     for (i64 c = c0; c < cend;) {
         const i64 mrows = R.m - c;
         if (mrows <= 0) break;
         const int lw = leaf_width_for<T>(mrows);
         if (lw == 0) throw CudaError{cudaErrorInvalidValue, "panel taller than the leaf capacity"};
         const i64 w = std::min<i64>(lw, cend - c);
-        OXI_CUDA(cudaMemsetAsync(R.nmoves, 0, sizeof(int), h->stream));
         LeafPanel pn = leaf_panel(R, c, w);
+        pn.reset_nmoves = 1;
         pn.u_src = pend.u_src;
         pn.u_dst = pend.u_dst;
         pn.u_rows = pend.u_rows;

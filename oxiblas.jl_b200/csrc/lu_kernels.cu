@@ -507,6 +507,11 @@ k_leaf_lu(T *__restrict__ P, i64 ld, int m, int wact, i64 gofs, int64_t *__restr
     }
     // keep every CTA's shared memory alive until all remote pushes have landed
     if (CS > 1) cl.sync();
+    // the move counter back to zero for the next leaf, once every CTA has read it
+    if (pn.reset_nmoves) {
+        if (CS == 1) __syncthreads();
+        if (cr == 0 && t == 0) *nmoves = 0;
+    }
 }
 
 int *leaf_wait_err_addr() {

@@ -230,6 +230,8 @@ struct LeafPanel {
     const void *u_src = nullptr;
     void *u_dst = nullptr;
     int u_rows = 0, u_cols = 0;
+    // set the move counter back to zero at the end (saves the next leaf's memset)
+    int reset_nmoves = 0;
 };
 
 // Tournament-pivoting leaf (FP32, mixed solve only): same contract as
