@@ -104,7 +104,11 @@ static void panel_rl(LuRun<T> &R, i64 c0, i64 nc) {
     oxi_handle_s *h = R.h;
     const i64 cend = c0 + nc;
     LeafPanel pend;  // the previous step's U12, still in R.ubuf
-    OXI_CUDA(cudaMemsetAsync(R.nmoves, 0, sizeof(int), h->stream));  // each leaf zeroes it again at its end
+    // The move counter is zero at a panel's first column (k_rowmap_init), and
+    // each of these leaves zeroes it again at its end; a right half reached
+    // inside a recursive panel (tournament leaves on its left) starts from a
+    // counter those leaves left set.
+    if (c0 != R.pf) OXI_CUDA(cudaMemsetAsync(R.nmoves, 0, sizeof(int), h->stream));
     for (i64 c = c0; c < cend;) {
         const i64 mrows = R.m - c;
         if (mrows <= 0) break;
@@ -263,9 +267,8 @@ void getrf_rowmajor(oxi_handle_s *h, T *W, i64 ld, i64 m, i64 n, int64_t *d_ipiv
             if (compose) {
                 R.pf = f;
                 R.pl = l;
-                launch_rowmap_init(R.map, m - f, sA);
+                launch_rowmap_init(R.map, m - f, R.nmoves, listcnt, sA);
                 panel_rec(R, f, l - f);
-                OXI_CUDA(cudaMemsetAsync(listcnt, 0, sizeof(int), sA));
                 launch_rowmap_extract(R.map, m - f, list, listcnt, sA);
                 if (b_pending) {  // the previous trailing update reads L21 and writes the columns moved now
                     OXI_CUDA(cudaStreamWaitEvent(sA, h->la_join, 0));

@@ -637,9 +637,15 @@ template void launch_rowmoves<float>(float *, i64, i64, const int *, const int *
 // leaf's moves compose into it, and at the end of the panel the positions with
 // map[p] != p form one move list for all the columns outside the panel.
 // ---------------------------------------------------------------------------
-__global__ void k_rowmap_init(int *__restrict__ map, int len) {
+// identity row map of a panel; also zeroes the panel's move counter and its
+// move-list count (no separate memsets on the panel's critical path)
+__global__ void k_rowmap_init(int *__restrict__ map, int len, int *__restrict__ zero0, int *__restrict__ zero1) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p < len) map[p] = p;
+    if (p == 0) {
+        if (zero0) *zero0 = 0;
+        if (zero1) *zero1 = 0;
+    }
 }
 __global__ void k_rowmap_apply(int *__restrict__ map, int offset, const int *__restrict__ moves,
                                const int *__restrict__ nmoves) {
@@ -710,9 +716,9 @@ __global__ void __launch_bounds__(256) k_rowmoves_big(T *__restrict__ W, i64 ld,
     }
 }
 
-void launch_rowmap_init(int *map, i64 len, cudaStream_t s) {
+void launch_rowmap_init(int *map, i64 len, int *zero0, int *zero1, cudaStream_t s) {
     if (len <= 0) return;
-    k_rowmap_init<<<(unsigned)((len + 255) / 256), 256, 0, s>>>(map, (int)len);
+    k_rowmap_init<<<(unsigned)((len + 255) / 256), 256, 0, s>>>(map, (int)len, zero0, zero1);
     OXI_LAUNCH_CHECK();
 }
 void launch_rowmap_apply(int *map, i64 offset, const int *moves, const int *nmoves, cudaStream_t s) {

@@ -258,7 +258,7 @@ void launch_rowmoves(T *W, i64 ld, i64 r0, const int *moves, const int *nmoves, 
                      i64 c_hi, i64 skip_lo, i64 skip_hi, cudaStream_t s);
 
 // Per-panel composition of the leaves' row permutations (see lu_kernels.cu).
-void launch_rowmap_init(int *map, i64 len, cudaStream_t s);
+void launch_rowmap_init(int *map, i64 len, int *zero0, int *zero1, cudaStream_t s);
 void launch_rowmap_apply(int *map, i64 offset, const int *moves, const int *nmoves, cudaStream_t s);
 void launch_rowmap_extract(const int *map, i64 len, int *list, int *cnt, cudaStream_t s);
 template <typename T>
