@@ -693,6 +693,13 @@ k_trsv3(const T *__restrict__ A, i64 lda, const T *__restrict__ P, T *__restrict
 // UPPER_A / TRANS describe the stored factor as in LAPACK (column-major A,
 // op(A) = A or A^T); ROWACC access of the same memory is the transposed view.
 static std::atomic<uint32_t> g_trsv_epoch{0};  // tags of the exchange words, one per launch
+// The next launch's tag; 0 is skipped on wrap-around, since zeroed (fresh)
+// words carry it.
+static uint32_t next_trsv_epoch() {
+    uint32_t e = ++g_trsv_epoch;
+    if (e == 0) e = ++g_trsv_epoch;
+    return e;
+}
 
 template <typename T, bool UPPER_A, bool UNIT, bool TRANS>
 static void trsv_launch(const T *A, i64 lda, T *X, i64 ldx, int n, int nrhs, int *ctl, int *err,
@@ -746,7 +753,7 @@ static void trsv3_launch(const T *A, i64 lda, T *X, i64 ldx, int n, int nrhs, in
 #define OXI_TRSV3_GO(NRV)                                                                            \
     do {                                                                                             \
         const int smem = (int)sizeof(Trsv3Smem<T, NRV>);                                            \
-        const uint32_t ep = ++g_trsv_epoch;                                                          \
+        const uint32_t ep = next_trsv_epoch();                                                       \
         auto kern = k_trsv3<T, LOWER, TRANS, NRV>;                                                   \
         set_max_dyn_smem((const void *)kern, smem);                                                  \
         kern<<<nb, SOLVE_NT, smem, s>>>(A, lda, P, Xk, ldx, n, ctl, err, xtag, ep);                 \
