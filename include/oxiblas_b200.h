@@ -68,10 +68,21 @@ enum oxi_option {
     OXI_OPT_GMRES_RESTART = 7,   /* GMRES-IR restart length (30)                    */
     OXI_OPT_GRAPHS = 8,          /* 1 (default): a factorization repeated with the same
                                     shape and workspace replays as a CUDA graph      */
-    OXI_OPT_TOURNAMENT = 9       /* 1: the mixed solve's FP32 factor picks each 32-column
+    OXI_OPT_TOURNAMENT = 9,      /* 1: the mixed solve's FP32 factor picks each 32-column
                                     leaf's pivots by tournament (TSLU); 0 (default):
                                     partial pivoting, the reference's rule (faster on
                                     B200, see oxiblas.jl_b200/csrc/tslu.cu)           */
+    OXI_OPT_WAIT_LIMIT_US = 10,  /* limit of every bounded device wait of this handle's
+                                    calls, in microseconds (default 2000000 = 2 s).  The
+                                    first wait that runs out sets the call's sticky abort
+                                    word: every later wait and kernel of the call returns
+                                    at once and the call returns OXI_ETIMEOUT.        */
+    OXI_OPT_TEST_MISSING_PRODUCER = 11 /* test hook: k > 0 makes the next factorization on
+                                    this handle wait, before its k-th leaf, for a flag
+                                    that no kernel sets (a consumer whose producer was
+                                    never launched).  One-shot; the call runs without
+                                    its CUDA graph and returns OXI_ETIMEOUT after one
+                                    wait limit.  No counterpart in the reference.     */
 };
 int oxi_set_option(oxi_handle_t h, int option, int64_t value);
 int oxi_get_option(oxi_handle_t h, int option, int64_t *value);

@@ -58,6 +58,12 @@ def lib():
         L.orc_mixed_solve.restype = ctypes.c_int
         L.orc_lu_adjoint.argtypes = [_i64, _dp, _i64, _ip, _dp, _dp, _dp, _dp, _i64]
         L.orc_lu_adjoint.restype = ctypes.c_int
+        for P, fp in (("d", _dp), ("s", _fp)):
+            f = getattr(L, f"orc_{P}gemm_update")
+            f.argtypes = [_i64, _i64, _i64, fp, _i64, fp, _i64, fp, _i64]
+            f.restype = None
+        L.orc_set_gemm_tiled.argtypes = [ctypes.c_int]
+        L.orc_set_gemm_tiled.restype = None
         L.orc_num_threads.restype = ctypes.c_int
         L.orc_set_num_threads.argtypes = [ctypes.c_int]
         _lib = L
@@ -74,6 +80,12 @@ def num_threads() -> int:
 
 def set_num_threads(t: int) -> None:
     lib().orc_set_num_threads(int(t))
+
+
+def set_gemm_tiled(on: bool) -> None:
+    """Register-tiled (default) or plain scalar trailing-update GEMM; both
+    produce the same bits, element by element."""
+    lib().orc_set_gemm_tiled(1 if on else 0)
 
 
 class SingularError(Exception):
@@ -105,6 +117,21 @@ def getrf(A, blocksize: int = 128, check: bool = True, dtype=np.float64, steps: 
     if rc != 0:
         raise ValueError(f"oracle getrf failed ({rc})")
     return A, ipiv[:q].copy(), int(info[0])
+
+
+def gemm_update(C, A, B):
+    """gemm!(C, A, B, -1, 1): returns C - A @ B in the reference's order
+    (one fma chain per element along k from zero, then C - s)."""
+    dtype = np.asarray(C).dtype
+    t = ctypes.c_double if dtype == np.float64 else ctypes.c_float
+    C = np.array(C, dtype=dtype, order="F", copy=True)
+    A = np.asfortranarray(A, dtype=dtype)
+    B = np.asfortranarray(B, dtype=dtype)
+    m, n = C.shape
+    k = A.shape[1]
+    f = getattr(lib(), "orc_dgemm_update" if dtype == np.float64 else "orc_sgemm_update")
+    f(m, n, k, _ptr(C, t), max(m, 1), _ptr(A, t), max(m, 1), _ptr(B, t), max(k, 1))
+    return C
 
 
 def perm_from_ipiv(ipiv, m):

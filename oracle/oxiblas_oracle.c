@@ -27,8 +27,127 @@
 #ifdef _OPENMP
 #include <omp.h>
 #endif
+#include <immintrin.h>
 
 typedef int64_t i64;
+
+/* 1 (default): the trailing-update GEMM runs register-tiled; 0: the plain
+ * scalar loops.  Both give the same bits (see _gemm_tiled); the switch exists
+ * so that the tests can check that. */
+static int orc_gemm_tiled = 1;
+void orc_set_gemm_tiled(int on) { orc_gemm_tiled = on != 0; }
+
+/* ------------------------------------------------------------------------ */
+/* Trailing-update kernel C <- C - A*B, register-tiled.                      */
+/* ------------------------------------------------------------------------ */
+/* Element by element this is the arithmetic of src/blas/gemm.jl:286-298
+ * (_reference!): s = fma chain over p = 0..k-1 in order, from zero, then
+ * C - s.  It is also the order of the reference's packed SIMD path for every
+ * GEMM of the factorization (gemm.jl:414 _packed_region! -> simd.jl:151
+ * _simd_micro!): the micro-kernel keeps one accumulator per element of its
+ * register tile, fma-chained along p from zero over a kc-block, and stores
+ * fma(beta = 1, C, alpha * acc) = C - acc; getrf's updates have k <= nb = 128,
+ * below kc = 448 (Float64) / 896 (Float32), so there is one block.  The tiles
+ * here (8 x 6 doubles, 16 x 6 floats: two AVX2 vectors by six broadcast
+ * columns, as the reference's W = 4/8, R = 2, N = 6 tile) only make it fast:
+ * the per-element operations and their order are those of the scalar form.
+ * Rows are blocked by MC for the L2 cache; OpenMP splits row blocks x
+ * 48-column chunks (the reference's worker grid, gemm.jl:561). */
+#define ORC_MC 256
+#define ORC_NCH 48
+
+static void d_tile_8x6(i64 k, const double *A, i64 lda, const double *B, i64 ldb, double *C, i64 ldc) {
+    __m256d c00 = _mm256_setzero_pd(), c01 = c00, c02 = c00, c03 = c00, c04 = c00, c05 = c00;
+    __m256d c10 = c00, c11 = c00, c12 = c00, c13 = c00, c14 = c00, c15 = c00;
+    const double *b0 = B, *b1 = B + ldb, *b2 = B + 2 * ldb, *b3 = B + 3 * ldb, *b4 = B + 4 * ldb,
+                 *b5 = B + 5 * ldb;
+    for (i64 p = 0; p < k; ++p) {
+        const __m256d a0 = _mm256_loadu_pd(A + p * lda), a1 = _mm256_loadu_pd(A + p * lda + 4);
+        __m256d b = _mm256_broadcast_sd(b0 + p);
+        c00 = _mm256_fmadd_pd(a0, b, c00); c10 = _mm256_fmadd_pd(a1, b, c10);
+        b = _mm256_broadcast_sd(b1 + p);
+        c01 = _mm256_fmadd_pd(a0, b, c01); c11 = _mm256_fmadd_pd(a1, b, c11);
+        b = _mm256_broadcast_sd(b2 + p);
+        c02 = _mm256_fmadd_pd(a0, b, c02); c12 = _mm256_fmadd_pd(a1, b, c12);
+        b = _mm256_broadcast_sd(b3 + p);
+        c03 = _mm256_fmadd_pd(a0, b, c03); c13 = _mm256_fmadd_pd(a1, b, c13);
+        b = _mm256_broadcast_sd(b4 + p);
+        c04 = _mm256_fmadd_pd(a0, b, c04); c14 = _mm256_fmadd_pd(a1, b, c14);
+        b = _mm256_broadcast_sd(b5 + p);
+        c05 = _mm256_fmadd_pd(a0, b, c05); c15 = _mm256_fmadd_pd(a1, b, c15);
+    }
+#define ORC_D_ST(j, lo, hi)                                                                   \
+    _mm256_storeu_pd(C + (j) * ldc, _mm256_sub_pd(_mm256_loadu_pd(C + (j) * ldc), lo));       \
+    _mm256_storeu_pd(C + (j) * ldc + 4, _mm256_sub_pd(_mm256_loadu_pd(C + (j) * ldc + 4), hi));
+    ORC_D_ST(0, c00, c10) ORC_D_ST(1, c01, c11) ORC_D_ST(2, c02, c12)
+    ORC_D_ST(3, c03, c13) ORC_D_ST(4, c04, c14) ORC_D_ST(5, c05, c15)
+#undef ORC_D_ST
+}
+
+static void s_tile_16x6(i64 k, const float *A, i64 lda, const float *B, i64 ldb, float *C, i64 ldc) {
+    __m256 c00 = _mm256_setzero_ps(), c01 = c00, c02 = c00, c03 = c00, c04 = c00, c05 = c00;
+    __m256 c10 = c00, c11 = c00, c12 = c00, c13 = c00, c14 = c00, c15 = c00;
+    const float *b0 = B, *b1 = B + ldb, *b2 = B + 2 * ldb, *b3 = B + 3 * ldb, *b4 = B + 4 * ldb,
+                *b5 = B + 5 * ldb;
+    for (i64 p = 0; p < k; ++p) {
+        const __m256 a0 = _mm256_loadu_ps(A + p * lda), a1 = _mm256_loadu_ps(A + p * lda + 8);
+        __m256 b = _mm256_broadcast_ss(b0 + p);
+        c00 = _mm256_fmadd_ps(a0, b, c00); c10 = _mm256_fmadd_ps(a1, b, c10);
+        b = _mm256_broadcast_ss(b1 + p);
+        c01 = _mm256_fmadd_ps(a0, b, c01); c11 = _mm256_fmadd_ps(a1, b, c11);
+        b = _mm256_broadcast_ss(b2 + p);
+        c02 = _mm256_fmadd_ps(a0, b, c02); c12 = _mm256_fmadd_ps(a1, b, c12);
+        b = _mm256_broadcast_ss(b3 + p);
+        c03 = _mm256_fmadd_ps(a0, b, c03); c13 = _mm256_fmadd_ps(a1, b, c13);
+        b = _mm256_broadcast_ss(b4 + p);
+        c04 = _mm256_fmadd_ps(a0, b, c04); c14 = _mm256_fmadd_ps(a1, b, c14);
+        b = _mm256_broadcast_ss(b5 + p);
+        c05 = _mm256_fmadd_ps(a0, b, c05); c15 = _mm256_fmadd_ps(a1, b, c15);
+    }
+#define ORC_S_ST(j, lo, hi)                                                                   \
+    _mm256_storeu_ps(C + (j) * ldc, _mm256_sub_ps(_mm256_loadu_ps(C + (j) * ldc), lo));       \
+    _mm256_storeu_ps(C + (j) * ldc + 8, _mm256_sub_ps(_mm256_loadu_ps(C + (j) * ldc + 8), hi));
+    ORC_S_ST(0, c00, c10) ORC_S_ST(1, c01, c11) ORC_S_ST(2, c02, c12)
+    ORC_S_ST(3, c03, c13) ORC_S_ST(4, c04, c14) ORC_S_ST(5, c05, c15)
+#undef ORC_S_ST
+}
+
+#define DEFINE_GEMM_TILED(T, P, FMA, MR, TILE)                                           \
+static void P##_gemm_elem(i64 k, const T *A, i64 lda, const T *B, T *c) {                \
+    T s = 0;                                                                             \
+    for (i64 p = 0; p < k; ++p) s = FMA(A[p * lda], B[p], s);                            \
+    *c = *c - s;                                                                         \
+}                                                                                        \
+static void P##_gemm_tiled(i64 m, i64 n, i64 k, const T *A, i64 lda, const T *B,       \
+                           i64 ldb, T *C, i64 ldc) {                                     \
+    const i64 mt = m / MR * MR, nib = (mt + ORC_MC - 1) / ORC_MC;                        \
+    const i64 njb = (n + ORC_NCH - 1) / ORC_NCH;                                         \
+    const int par = (double)m * n * k > 2e6;                                             \
+    _Pragma("omp parallel if(par)")                                                      \
+    {                                                                                    \
+        _Pragma("omp for collapse(2) schedule(dynamic)")                                 \
+        for (i64 ib = 0; ib < nib; ++ib)                                                 \
+            for (i64 jb = 0; jb < njb; ++jb) {                                           \
+                const i64 i0 = ib * ORC_MC, i1 = i0 + ORC_MC < mt ? i0 + ORC_MC : mt;    \
+                const i64 j0 = jb * ORC_NCH, j1 = j0 + ORC_NCH < n ? j0 + ORC_NCH : n;   \
+                i64 j = j0;                                                              \
+                for (; j + 6 <= j1; j += 6)                                              \
+                    for (i64 i = i0; i < i1; i += MR)                                    \
+                        TILE(k, A + i, lda, B + j * ldb, ldb, C + i + j * ldc, ldc);     \
+                for (; j < j1; ++j)                                                      \
+                    for (i64 i = i0; i < i1; ++i)                                        \
+                        P##_gemm_elem(k, A + i, lda, B + j * ldb, C + i + j * ldc);      \
+            }                                                                            \
+        if (mt < m) {                                                                    \
+            _Pragma("omp for schedule(static)")                                          \
+            for (i64 j = 0; j < n; ++j)                                                  \
+                for (i64 i = mt; i < m; ++i)                                             \
+                    P##_gemm_elem(k, A + i, lda, B + j * ldb, C + i + j * ldc);          \
+        }                                                                                \
+    }                                                                                    \
+}
+DEFINE_GEMM_TILED(double, d, fma, 8, d_tile_8x6)
+DEFINE_GEMM_TILED(float, s, fmaf, 16, s_tile_16x6)
 
 /* ------------------------------------------------------------------------ */
 /* Type-generic body: instantiated for double (d) and float (s).            */
@@ -42,6 +161,7 @@ typedef int64_t i64;
 static void P##_gemm_minus(i64 m, i64 n, i64 k, const T *A, i64 lda, const T *B,        \
                            i64 ldb, T *C, i64 ldc) {                                     \
     if (m <= 0 || n <= 0 || k <= 0) return;                                              \
+    if (orc_gemm_tiled) { P##_gemm_tiled(m, n, k, A, lda, B, ldb, C, ldc); return; }     \
     int par = (double)m * n * k > 2e6;                                                   \
     _Pragma("omp parallel if(par)")                                                      \
     {                                                                                    \
@@ -124,6 +244,7 @@ static void P##_trsm(i64 nt, i64 nrhs, const T *A, i64 lda, T *B, i64 ldb, int u
  * piv holds 1-based row indices relative to row 0 of A plus `off` (global -> local). */\
 static void P##_swap(T *A, i64 lda, const i64 *piv, i64 off, i64 j1, i64 j2, i64 c0,    \
                      i64 c1) {                                                           \
+    _Pragma("omp parallel for schedule(static) if((c1 - c0) * (j2 - j1 + 1) > 65536)")   \
     for (i64 col = c0; col < c1; ++col) {                                                \
         T *a = A + col * lda;                                                            \
         for (i64 j = j1; j <= j2; ++j) {                                                 \
@@ -165,6 +286,7 @@ static int P##_panel(T *Pm, i64 ldp, i64 mp, i64 np, i64 *piv, i64 off, i64 *inf
                 continue;                                                                \
             }                                                                            \
             for (i64 i = j + 1; i < mp; ++i) Pm[i + j * ldp] /= d;                       \
+            _Pragma("omp parallel for schedule(static) if((mp - j) * (np - j) > 262144)")  \
             for (i64 col = j + 1; col < np; ++col) {                                     \
                 T u = Pm[j + col * ldp];                                                 \
                 T *pc = Pm + col * ldp; const T *pj = Pm + j * ldp;                      \
@@ -256,6 +378,16 @@ int orc_##P##getrs(char trans, i64 n, i64 nrhs, const T *LU, i64 lda, const i64 
 
 DEFINE_LU(double, d, fma, fabs)
 DEFINE_LU(float, s, fmaf, fabsf)
+
+/* gemm!(C, A, B, -1, 1) alone (the trailing update), column-major. */
+void orc_dgemm_update(i64 m, i64 n, i64 k, double *C, i64 ldc, const double *A, i64 lda,
+                      const double *B, i64 ldb) {
+    d_gemm_minus(m, n, k, A, lda, B, ldb, C, ldc);
+}
+void orc_sgemm_update(i64 m, i64 n, i64 k, float *C, i64 ldc, const float *A, i64 lda,
+                      const float *B, i64 ldb) {
+    s_gemm_minus(m, n, k, A, lda, B, ldb, C, ldc);
+}
 
 /* ------------------------------------------------------------------------ */
 /* Mixed precision pieces (FP64 only)                                        */

@@ -20,6 +20,7 @@ OXI_ESCRATCH = 9
 OPT_BLOCKSIZE, OPT_GEMM, OPT_TRSM_LEAF, OPT_LOOKAHEAD = 1, 2, 3, 4
 OPT_MIXED_BLOCKSIZE, OPT_STOP_NORMWISE, OPT_GMRES_RESTART = 5, 6, 7
 OPT_GRAPHS, OPT_TOURNAMENT = 8, 9
+OPT_WAIT_LIMIT_US, OPT_TEST_MISSING_PRODUCER = 10, 11
 
 
 class SingularException(Exception):

@@ -6,28 +6,62 @@
 #include <tuple>
 #include <vector>
 #include "oxi_internal.h"
+#include "tma_util.cuh"
 
 namespace oxi {
 thread_local Profiler *t_prof = nullptr;
 
-void queue_wait_errors(oxi_handle_s *h, int *hdst) {
-    int *a[3] = {leaf_wait_err_addr(), dmma_wait_err_addr(), tc_wait_err_addr()};
-    for (int i = 0; i < 3; ++i)
-        OXI_CUDA(cudaMemcpyAsync(hdst + i, a[i], sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+thread_local int *t_abort = nullptr;
+
+int *abort_word(oxi_handle_s *h) {
+    return (int *)((char *)h->scratch.get(kScratchBytes) + kScratchErrOff);
 }
 
-int check_wait_errors(oxi_handle_s *h, const int *hsrc) {
-    int *a[3] = {leaf_wait_err_addr(), dmma_wait_err_addr(), tc_wait_err_addr()};
-    bool any = false;
-    for (int i = 0; i < 3; ++i)
-        if (hsrc[i]) {
-            any = true;
-            OXI_CUDA(cudaMemsetAsync(a[i], 0, sizeof(int), h->stream));
-        }
-    if (!any) return OXI_OK;
-    OXI_CUDA(cudaStreamSynchronize(h->stream));
-    h->last_error = "a bounded device wait timed out (leaf exchange / GEMM pipeline); results are void";
+AbortScope::AbortScope(oxi_handle_s *h) : saved(t_abort), word(abort_word(h)) {
+    if (h->wait_limit_dev != h->wait_limit_ns) {
+        // first call of the handle, or the option changed: a blocking copy
+        const uint64_t v = (uint64_t)h->wait_limit_ns;
+        OXI_CUDA(cudaStreamSynchronize(h->stream));
+        OXI_CUDA(cudaMemcpy(word + 2, &v, sizeof(v), cudaMemcpyHostToDevice));
+        h->wait_limit_dev = h->wait_limit_ns;
+    }
+    OXI_CUDA(cudaMemsetAsync(word, 0, 2 * sizeof(int), h->stream));
+    t_abort = word;  // only once nothing above can throw
+}
+
+void queue_abort_read(oxi_handle_s *h, int *hdst) {
+    OXI_CUDA(cudaMemcpyAsync(hdst, abort_word(h), sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+}
+
+int check_abort(oxi_handle_s *h, const int *hsrc) {
+    if (*hsrc == 0) return OXI_OK;
+    static const char *what[] = {"", "leaf pivot exchange", "FP64 tensor-core GEMM pipeline",
+                                 "triangular-solve chain", "low-precision conversion",
+                                 "tensor-core GEMM pipeline", "missing producer (test hook)"};
+    const int c = *hsrc;
+    h->last_error = std::string("a bounded device wait timed out (") +
+                    ((c > 0 && c < 7) ? what[c] : "unknown") + "); the call's results are void";
     return OXI_ETIMEOUT;
+}
+
+// One thread polls a flag nobody writes, with the call's bounded wait.
+__global__ void k_await_missing_producer(const int *__restrict__ flag, int *__restrict__ ab) {
+    if (aborted(ab)) return;
+    const uint64_t t0 = global_ns();
+    uint32_t it = 0;
+    while (*(const volatile int *)flag == 0)
+        if (spin_give_up<64>(it, t0, ab, 6)) return;
+}
+
+void launch_await_missing_producer(oxi_handle_s *h, cudaStream_t s) {
+    const int *flag = (const int *)((char *)h->scratch.get(kScratchBytes) + kScratchStallOff);
+    k_await_missing_producer<<<1, 1, 0, s>>>(flag, cur_abort());
+    OXI_LAUNCH_CHECK();
+}
+
+void maybe_stall_before_leaf(oxi_handle_s *h, cudaStream_t s) {
+    if (h->stall_at <= 0) return;
+    if (--h->stall_at == 0) launch_await_missing_producer(h, s);
 }
 
 void set_max_dyn_smem(const void *func, int bytes) {
@@ -157,6 +191,15 @@ int oxi_set_option(oxi_handle_t h, int option, int64_t value) {
         case OXI_OPT_TOURNAMENT:
             h->opt.tournament = value ? 1 : 0;
             return OXI_OK;
+        case OXI_OPT_WAIT_LIMIT_US:
+            if (value < 1000 || value > 60000000) return OXI_EINVAL;  // 1 ms .. 60 s
+            h->wait_limit_ns = value * 1000;
+            return OXI_OK;
+        case OXI_OPT_TEST_MISSING_PRODUCER:
+            if (value < 0) return OXI_EINVAL;
+            h->stall_at = value;
+            if (value) h->gcache.reset();
+            return OXI_OK;
         default: return OXI_EINVAL;
     }
 }
@@ -173,6 +216,10 @@ int oxi_get_option(oxi_handle_t h, int option, int64_t *value) {
         case OXI_OPT_GMRES_RESTART: *value = h->opt.gmres_restart; return OXI_OK;
         case OXI_OPT_GRAPHS: *value = h->opt.graphs; return OXI_OK;
         case OXI_OPT_TOURNAMENT: *value = h->opt.tournament; return OXI_OK;
+        case OXI_OPT_WAIT_LIMIT_US:
+            *value = (h->wait_limit_ns ? h->wait_limit_ns : (int64_t)oxi::kWaitLimitNs) / 1000;
+            return OXI_OK;
+        case OXI_OPT_TEST_MISSING_PRODUCER: *value = h->stall_at; return OXI_OK;
         default: return OXI_EINVAL;
     }
 }
@@ -187,11 +234,12 @@ int oxi_dgemm_update(oxi_handle_t h, int64_t m, int64_t n, int64_t k, double *dC
     try {
         oxi::ProfGuard pg(&h->prof);
         OXI_CUDA(cudaSetDevice(h->device));
+        oxi::AbortScope ab(h);
         oxi::gemm_minus<double>(h, dC, ldc, dB, ldb, dA, lda, n, m, k);
         int *he = (int *)h->host_ws.get(64);
-        oxi::queue_wait_errors(h, he);
+        oxi::queue_abort_read(h, he);
         OXI_CUDA(cudaStreamSynchronize(h->stream));
-        return oxi::check_wait_errors(h, he);
+        return oxi::check_abort(h, he);
     } catch (const oxi::CudaError &e) {
         h->last_error = std::string(e.what) + ": " + cudaGetErrorString(e.code);
         return OXI_ECUDA;
@@ -210,6 +258,7 @@ int oxi_sgemm_update_lowp(oxi_handle_t h, int prec, int64_t m, int64_t n, int64_
     try {
         oxi::ProfGuard pg(&h->prof);
         OXI_CUDA(cudaSetDevice(h->device));
+        oxi::AbortScope ab(h);
         h->trailing = prec;  // OXI_PREC_{FP32,BF16,FP16,BF16X3,FP16X3} == TRAIL_{NATIVE,...,FP16X3}
         if (prec == OXI_PREC_FP32)
             oxi::gemm_minus<float>(h, dC, ldc, dB, ldb, dA, lda, n, m, k);
@@ -217,9 +266,9 @@ int oxi_sgemm_update_lowp(oxi_handle_t h, int prec, int64_t m, int64_t n, int64_
             oxi::gemm_trailing_f32(h, dC, ldc, dB, ldb, dA, lda, n, m, k);
         h->trailing = saved;
         int *he = (int *)h->host_ws.get(64);
-        oxi::queue_wait_errors(h, he);
+        oxi::queue_abort_read(h, he);
         OXI_CUDA(cudaStreamSynchronize(h->stream));
-        return oxi::check_wait_errors(h, he);
+        return oxi::check_abort(h, he);
     } catch (const oxi::CudaError &e) {
         h->trailing = saved;
         h->last_error = std::string(e.what) + ": " + cudaGetErrorString(e.code);

@@ -50,17 +50,9 @@ constexpr int NTHREADS = (NCONSUMER_WARPS + 1) * 32;
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
 }  // namespace
 
-__device__ int g_gemm_dmma_err;
-
-int *dmma_wait_err_addr() {
-    void *p = nullptr;
-    OXI_CUDA(cudaGetSymbolAddress(&p, g_gemm_dmma_err));
-    return (int *)p;
-}
-
 __global__ void __launch_bounds__(NTHREADS, 2)
 k_gemm_dmma(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-            double *__restrict__ C, i64 ldc, int M, int N, int K) {
+            double *__restrict__ C, i64 ldc, int M, int N, int K, int *__restrict__ ab) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~uintptr_t(1023));
     uint64_t *full = (uint64_t *)(smem + STAGES * STAGE_BYTES);
@@ -70,14 +62,17 @@ k_gemm_dmma(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUt
     const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
     const int KT = (K + BK - 1) / BK;
 
+    __shared__ int s_skip;
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], NCONSUMER_WARPS);
         }
+        s_skip = aborted(ab) ? 1 : 0;  // one reading for the whole CTA
         fence_barrier_init();
     }
     __syncthreads();
+    if (s_skip) return;  // the call was aborted by an earlier wait
 
     if (warp == NCONSUMER_WARPS) {
         // ---------------- producer ----------------
@@ -87,7 +82,7 @@ k_gemm_dmma(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUt
             for (int kt = 0; kt < KT; ++kt) {
                 const int s = kt % STAGES;
                 if (kt >= STAGES) {
-                    if (!mbar_wait(&empty[s], ((kt / STAGES) + 1) & 1, &g_gemm_dmma_err, 1)) break;
+                    if (!mbar_wait(&empty[s], ((kt / STAGES) + 1) & 1, ab, 2)) break;
                 }
                 uint8_t *sa = smem + s * STAGE_BYTES;
                 uint8_t *sb = sa + A_STAGE_BYTES;
@@ -114,7 +109,7 @@ k_gemm_dmma(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUt
 
     for (int kt = 0; kt < KT; ++kt) {
         const int s = kt % STAGES;
-        if (!mbar_wait(&full[s], (kt / STAGES) & 1, &g_gemm_dmma_err, 2)) return;
+        if (!mbar_wait(&full[s], (kt / STAGES) & 1, ab, 2)) return;
         const uint8_t *sa = smem + s * STAGE_BYTES;
         const uint8_t *sb = sa + A_STAGE_BYTES;
 #pragma unroll
@@ -203,7 +198,7 @@ void launch_gemm_dmma(double *C, i64 ldc, const double *A, i64 lda, const double
     set_max_dyn_smem((const void *)k_gemm_dmma, SMEM_BYTES);
     dim3 grid((unsigned)((N + BN - 1) / BN), (unsigned)((M + BM - 1) / BM));
     ProfScope ps(KC_GEMM_DMMA, s, 2.0 * M * N * K, 8.0 * (2.0 * M * N + M * K + K * N));
-    k_gemm_dmma<<<grid, NTHREADS, SMEM_BYTES, s>>>(tmA, tmB, C, ldc, (int)M, (int)N, (int)K);
+    k_gemm_dmma<<<grid, NTHREADS, SMEM_BYTES, s>>>(tmA, tmB, C, ldc, (int)M, (int)N, (int)K, cur_abort());
     OXI_LAUNCH_CHECK();
 }
 

@@ -27,14 +27,6 @@ constexpr int TMEM_COLS = 256;  // per accumulator buffer (two buffers)
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + C_BYTES + 1024 + 256;
 }  // namespace tc
 
-__device__ int g_gemm_tc_err;
-
-int *tc_wait_err_addr() {
-    void *p = nullptr;
-    OXI_CUDA(cudaGetSymbolAddress(&p, g_gemm_tc_err));
-    return (int *)p;
-}
-
 // UMMA shared-memory descriptor, K-major operand in the 128-byte swizzle
 // layout TMA writes (rows of 128 bytes, 8-row groups 1024 bytes apart).
 __device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t smem_addr) {
@@ -67,18 +59,23 @@ __device__ __forceinline__ void tma_store_2d(const CUtensorMap *tm, const void *
         : "memory");
 }
 
-// Bounded wait that also gives up when another role of the CTA has aborted.
-__device__ __forceinline__ bool mbar_wait_ab(uint64_t *bar, uint32_t parity, int code,
-                                             volatile int *abort_flag) {
+// Bounded wait that also gives up when another role of the CTA, or another
+// wait of the same call (the call's abort word ab), has given up.
+__device__ __forceinline__ bool mbar_wait_ab(uint64_t *bar, uint32_t parity, volatile int *abort_flag,
+                                             int *ab) {
     if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = global_ns();
+    const uint64_t lim = wait_limit_ns(ab);
     for (;;) {
         for (int it = 0; it < 256; ++it)
             if (mbar_try_wait(bar, parity)) return true;
-        if (*abort_flag) return false;
-        if (global_ns() - t0 > kWaitLimitNs) break;
+        if (*abort_flag || aborted(ab)) {
+            *abort_flag = 1;
+            return false;
+        }
+        if (global_ns() - t0 > lim) break;
     }
-    atomicExch(&g_gemm_tc_err, code);
+    raise_abort(ab, 5);
     *abort_flag = 1;
     return false;
 }
@@ -95,7 +92,7 @@ template <int AB_FORMAT>
 __global__ void __launch_bounds__(256, 1)
 k_gemm_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
           const __grid_constant__ CUtensorMap tmC, int M, int N, int K, float scale,
-          const float *__restrict__ d_scale) {
+          const float *__restrict__ d_scale, int *__restrict__ ab) {
     using namespace tc;
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~uintptr_t(1023));
@@ -125,7 +122,7 @@ k_gemm_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
         }
         mbar_init(cfull, 1);
         mbar_init(cempty, 1);
-        *abort_flag = 0;
+        *abort_flag = aborted(ab) ? 1 : 0;  // an aborted call: every role skips its loop
         fence_barrier_init();
     }
     if (warp == 1) {
@@ -147,7 +144,7 @@ k_gemm_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
             const int m0 = (tile / tilesN) * BM, n0 = (tile % tilesN) * BN;
             for (int kt = 0; kt < KT; ++kt, ++kb) {
                 const int s = kb % STAGES;
-                if (kb >= STAGES && !mbar_wait_ab(&empty[s], ((kb / STAGES) + 1) & 1, 1, abort_flag)) break;
+                if (kb >= STAGES && !mbar_wait_ab(&empty[s], ((kb / STAGES) + 1) & 1, abort_flag, ab)) break;
                 uint8_t *sa = smem + s * STAGE_BYTES;
                 mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
                 tma_load_2d(sa, &tmA, &full[s], kt * BK, m0);
@@ -159,12 +156,12 @@ k_gemm_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
         int kb = 0, li = 0;
         for (int tile = blockIdx.x; tile < ntiles && !*abort_flag; tile += gridDim.x, ++li) {
             const int b = li & 1;
-            if (li >= 2 && !mbar_wait_ab(&tempty[b], ((li >> 1) + 1) & 1, 2, abort_flag)) break;
+            if (li >= 2 && !mbar_wait_ab(&tempty[b], ((li >> 1) + 1) & 1, abort_flag, ab)) break;
             tc_fence_after();
             const uint32_t dacc = tmem + (uint32_t)(b * TMEM_COLS);
             for (int kt = 0; kt < KT; ++kt, ++kb) {
                 const int s = kb % STAGES;
-                if (!mbar_wait_ab(&full[s], (kb / STAGES) & 1, 3, abort_flag)) break;
+                if (!mbar_wait_ab(&full[s], (kb / STAGES) & 1, abort_flag, ab)) break;
                 tc_fence_after();
                 const uint32_t sa = smem_u32(smem + s * STAGE_BYTES);
                 const uint64_t da = umma_desc_sw128(sa), db = umma_desc_sw128(sa + A_BYTES);
@@ -192,7 +189,7 @@ k_gemm_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
         int li = 0;
         for (int tile = blockIdx.x; tile < ntiles && !*abort_flag; tile += gridDim.x, ++li) {
             const int m0 = (tile / tilesN) * BM, n0 = (tile % tilesN) * BN;
-            if (li >= 1 && !mbar_wait_ab(cempty, (li - 1) & 1, 4, abort_flag)) break;
+            if (li >= 1 && !mbar_wait_ab(cempty, (li - 1) & 1, abort_flag, ab)) break;
             mbar_arrive_expect_tx(cfull, C_BYTES);
 #pragma unroll
             for (int bx = 0; bx < NCBOX; ++bx)
@@ -206,8 +203,8 @@ k_gemm_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
         for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++li) {
             const int m0 = (tile / tilesN) * BM, n0 = (tile % tilesN) * BN;
             const int b = li & 1;
-            const bool ok = mbar_wait_ab(&tfull[b], (li >> 1) & 1, 5, abort_flag) &&
-                            mbar_wait_ab(cfull, li & 1, 6, abort_flag);
+            const bool ok = mbar_wait_ab(&tfull[b], (li >> 1) & 1, abort_flag, ab) &&
+                            mbar_wait_ab(cfull, li & 1, abort_flag, ab);
             // uniform decision across the epilogue warpgroup (it meets at a named barrier)
             uint32_t all_ok;
             asm volatile(
@@ -420,9 +417,9 @@ void launch_gemm_tc(int fmt /*0 fp16, 1 bf16*/, float *C, i64 ldc, const void *A
     }
     ProfScope ps(KC_GEMM_TC, s, 2.0 * M * N * K, 8.0 * M * N + 2.0 * (M + N) * K);
     if (fmt == 1)
-        OXI_CUDA(cudaLaunchKernelEx(&cfg, k_gemm_tc<1>, tmA, tmB, tmC, (int)M, (int)N, (int)K, scale, d_scale));
+        OXI_CUDA(cudaLaunchKernelEx(&cfg, k_gemm_tc<1>, tmA, tmB, tmC, (int)M, (int)N, (int)K, scale, d_scale, cur_abort()));
     else
-        OXI_CUDA(cudaLaunchKernelEx(&cfg, k_gemm_tc<0>, tmA, tmB, tmC, (int)M, (int)N, (int)K, scale, d_scale));
+        OXI_CUDA(cudaLaunchKernelEx(&cfg, k_gemm_tc<0>, tmA, tmB, tmC, (int)M, (int)N, (int)K, scale, d_scale, cur_abort()));
     OXI_LAUNCH_CHECK();
 }
 

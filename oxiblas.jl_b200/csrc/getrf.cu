@@ -122,6 +122,7 @@ static void panel_rl(LuRun<T> &R, i64 c0, i64 nc) {
         pn.u_rows = pend.u_rows;
         pn.u_cols = pend.u_cols;
         pend = LeafPanel();
+        maybe_stall_before_leaf(h, h->stream);
         launch_leaf<T>(R.W + c * R.ld + c, R.ld, mrows, (int)w, c, R.ipiv, R.info, R.moves, R.nmoves, lw,
                        h->stream, pn);
         if constexpr (sizeof(T) == 4) {
@@ -160,6 +161,7 @@ static void panel_rec(LuRun<T> &R, i64 c0, i64 nc) {
     if (nc <= leafw) {
         OXI_CUDA(cudaMemsetAsync(R.nmoves, 0, sizeof(int), h->stream));
         auto leaf = [&](LeafPanel pn) {
+            maybe_stall_before_leaf(h, h->stream);
             if constexpr (sizeof(T) == 4) {
                 if (ts) {
                     launch_tslu_leaf(h, R.W + c0 * R.ld + c0, R.ld, mrows, (int)nc, c0, R.ipiv, R.info, R.moves,
@@ -341,7 +343,7 @@ void getrf_rowmajor_cached(oxi_handle_s *h, T *W, i64 ld, i64 m, i64 n, int64_t 
                            int64_t *d_info, int *d_moves, int *d_nmoves) {
     // The legacy default stream cannot be captured: run on the handle's own
     // stream, ordered after and before the caller's work through events.
-    if (h->stream == nullptr && h->opt.graphs && !h->prof.enabled) {
+    if (h->stream == nullptr && h->opt.graphs && !h->prof.enabled && h->stall_at == 0) {
         if (!h->aux_stream) {
             OXI_CUDA(cudaStreamCreateWithFlags(&h->aux_stream, cudaStreamNonBlocking));
             OXI_CUDA(cudaEventCreateWithFlags(&h->aux_fork, cudaEventDisableTiming));
@@ -371,7 +373,7 @@ void getrf_rowmajor_cached(oxi_handle_s *h, T *W, i64 ld, i64 m, i64 n, int64_t 
                               (uint64_t)(uintptr_t)h->stream,
                               (uint64_t)(uintptr_t)h->rowmap_ws.ptr ^ (uint64_t)(uintptr_t)h->tc_ws.ptr ^
                                   ((uint64_t)(uintptr_t)h->tslu_ws.ptr << 1)};
-    const bool usable = h->opt.graphs && !h->prof.enabled;
+    const bool usable = h->opt.graphs && !h->prof.enabled && h->stall_at == 0;
     const bool same = gc.seen > 0 && std::memcmp(gc.key, key, sizeof(key)) == 0;
     if (usable && same && gc.valid) {
         OXI_CUDA(cudaGraphLaunch(gc.exec, h->stream));
@@ -428,6 +430,7 @@ static int getrf_entry(oxi_handle_s *h, i64 m, i64 n, T *dA, i64 lda, int64_t *d
     try {
         ProfGuard pg(&h->prof);
         OXI_CUDA(cudaSetDevice(h->device));
+        AbortScope ab(h);
         const i64 ld = round_up(n, 32);
         T *W = (T *)h->work.get((size_t)m * ld * sizeof(T));
         char *sc = (char *)h->scratch.get(kScratchBytes);
@@ -440,13 +443,15 @@ static int getrf_entry(oxi_handle_s *h, i64 m, i64 n, T *dA, i64 lda, int64_t *d
         launch_rm_to_cm<T, T>(W, ld, dA, lda, m, n, h->stream);
         int64_t *hi = (int64_t *)h->host_ws.get(64);
         OXI_CUDA(cudaMemcpyAsync(hi, d_info, sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
-        queue_wait_errors(h, (int *)(hi + 2));
+        queue_abort_read(h, (int *)(hi + 2));
         OXI_CUDA(cudaStreamSynchronize(h->stream));
+        h->stall_at = 0;  // the test hook is one-shot
         *h_info = hi[0];
-        const int we = check_wait_errors(h, (const int *)(hi + 2));
+        const int we = check_abort(h, (const int *)(hi + 2));
         if (we != OXI_OK) return we;
         return hi[0] > 0 ? OXI_ESINGULAR : OXI_OK;
     } catch (const CudaError &e) {
+        h->stall_at = 0;
         h->last_error = std::string(e.what) + ": " + cudaGetErrorString(e.code);
         return OXI_ECUDA;
     }

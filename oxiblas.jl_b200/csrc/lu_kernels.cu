@@ -170,7 +170,6 @@ __device__ __forceinline__ void load_row(T (&v)[W], const T *src) {
 constexpr int LEAF_NT = 512;
 constexpr int LEAF_MAX_CS = 16;
 
-__device__ int g_leaf_err;  // a leaf exchange wait that timed out (read by the host after a call)
 
 template <typename T, int W, int R, int NT>
 __global__ void __launch_bounds__(NT, 1)
@@ -206,8 +205,10 @@ k_leaf_lu(T *__restrict__ P, i64 ld, int m, int wact, i64 gofs, int64_t *__restr
     __shared__ int s_jid;
     __shared__ int s_piv[W];   // pivots and info stay on chip until the end: no global
     __shared__ int s_info;     // store ahead of the per-column exchange
+    __shared__ int s_skip;     // the call was aborted before this launch
     if (t == 0) {
         s_info = 0;
+        s_skip = aborted(pn.abort) ? 1 : 0;
         mbar_init(&s_xbar[0], 1);
         mbar_init(&s_xbar[1], 1);
         fence_barrier_init();
@@ -215,7 +216,17 @@ k_leaf_lu(T *__restrict__ P, i64 ld, int m, int wact, i64 gofs, int64_t *__restr
     // every CTA's exchange barriers exist before any CTA pushes into them
     if (CS > 1) cl.sync();
     else __syncthreads();
-    bool dead = false;  // an exchange that timed out: stop waiting (g_leaf_err reports it)
+    // CTA 0's reading of the abort word decides for the whole cluster (the
+    // word may change between the CTAs' own readings)
+    const int skip = (CS > 1) ? *cl.map_shared_rank(&s_skip, 0) : s_skip;
+    if (skip) {
+        if (CS > 1) cl.sync();  // CTA 0's shared memory stays alive until every CTA read it
+        return;
+    }
+    // An exchange wait that gave up (timeout or the call aborted elsewhere):
+    // the CTA leaves the column loop together (at its next barrier), stores
+    // nothing and emits no moves, but still meets every cluster barrier.
+    bool dead = false;
 
     // a block the previous launch left in a buffer (see LeafPanel): rows above the leaf
     if (pn.u_rows > 0) {
@@ -311,7 +322,7 @@ k_leaf_lu(T *__restrict__ P, i64 ld, int m, int wact, i64 gofs, int64_t *__restr
         // its own barrier: no cluster-wide barrier per column.  A slot is
         // rewritten two columns later, after its receiver has pushed the column in
         // between, i.e. after it finished reading the slot.
-        if (CS > 1) {
+        if (CS > 1 && !dead) {
             constexpr int PER = 1 + W * (int)sizeof(T) / 16;  // stores per row: meta + 16-byte chunks
             const int npush = CS * PER;                          // this CTA's candidate, to every CTA
             if (t == 0) mbar_arrive_expect_tx(&s_xbar[par], (uint32_t)((CS + 1) * 16 * PER));
@@ -344,7 +355,7 @@ k_leaf_lu(T *__restrict__ P, i64 ld, int m, int wact, i64 gofs, int64_t *__restr
                 }
                 st_async_v4(raddr, v, cluster_map_u32(&s_xbar[par], dst));
             }
-            if (!dead && !mbar_wait(&s_xbar[par], (uint32_t)((j >> 1) & 1), &g_leaf_err, 1)) dead = true;
+            if (!mbar_wait(&s_xbar[par], (uint32_t)((j >> 1) & 1), pn.abort, 1)) dead = true;
         }
         // (e) winner, identical in every CTA: lanes 0..CS-1 hold one candidate each;
         // the winning row sits in the slot of the CTA that owns its position
@@ -416,9 +427,9 @@ k_leaf_lu(T *__restrict__ P, i64 ld, int m, int wact, i64 gofs, int64_t *__restr
         }
     }
     // pivots and info, written once
-    __syncthreads();
-    if (cr == 0 && t < q) ipiv[gofs + t] = gofs + s_piv[t] + 1;
-    if (cr == 0 && t == 0 && s_info != 0 && *info == 0) *info = gofs + s_info;
+    dead = __syncthreads_or(dead);
+    if (!dead && cr == 0 && t < q) ipiv[gofs + t] = gofs + s_piv[t] + 1;
+    if (!dead && cr == 0 && t == 0 && s_info != 0 && *info == 0) *info = gofs + s_info;
     // undo the rotation left by q < W steps (slot s holds column (s + q) mod W)
     const int rot = q % W;
 
@@ -426,7 +437,7 @@ k_leaf_lu(T *__restrict__ P, i64 ld, int m, int wact, i64 gofs, int64_t *__restr
 #pragma unroll
     for (int k = 0; k < R; ++k) {
         const int i = k * G + g;
-        if (i < m) {
+        if (i < m && !dead) {
             T *dst = P + (i64)i * ld;
             if (vec_ok && rot == 0) {
 #pragma unroll
@@ -485,7 +496,7 @@ k_leaf_lu(T *__restrict__ P, i64 ld, int m, int wact, i64 gofs, int64_t *__restr
 #pragma unroll
         for (int k = 0; k < R; ++k) {
             const int i = k * G + g;
-            mapv[k] = (pn.map && i < m && id[k] != i) ? pn.map[pn.map_off + id[k]] : 0;
+            mapv[k] = (!dead && pn.map && i < m && id[k] != i) ? pn.map[pn.map_off + id[k]] : 0;
         }
         if (CS > 1) cl.sync(); else __syncthreads();
 #pragma unroll
@@ -502,7 +513,7 @@ k_leaf_lu(T *__restrict__ P, i64 ld, int m, int wact, i64 gofs, int64_t *__restr
 #pragma unroll
         for (int k = 0; k < R; ++k) {
             const int i = k * G + g;
-            if (pn.map && i < m && id[k] != i) pn.map[pn.map_off + i] = mapv[k];
+            if (!dead && pn.map && i < m && id[k] != i) pn.map[pn.map_off + i] = mapv[k];
         }
     }
     // keep every CTA's shared memory alive until all remote pushes have landed
@@ -514,11 +525,6 @@ k_leaf_lu(T *__restrict__ P, i64 ld, int m, int wact, i64 gofs, int64_t *__restr
     }
 }
 
-int *leaf_wait_err_addr() {
-    void *p = nullptr;
-    OXI_CUDA(cudaGetSymbolAddress(&p, g_leaf_err));
-    return (int *)p;
-}
 
 template <typename T> int leaf_width_for(i64 m);
 template <> int leaf_width_for<double>(i64 m) {
@@ -560,6 +566,7 @@ static void launch_leaf_wr(T *P, i64 ld, i64 m, int w, i64 gofs, int64_t *ipiv, 
     cfg.numAttrs = 1;
     if (pn.nother > LEAF_MAX_OTHER)
         throw CudaError{cudaErrorInvalidValue, "panel too wide for the in-leaf row moves"};
+    pn.abort = cur_abort();
     ProfScope ps(KC_LEAF, s, 0.0, 2.0 * (double)m * w * sizeof(T));
     OXI_CUDA(cudaLaunchKernelEx(&cfg, kern, P, ld, (int)m, w, gofs, ipiv, info, moves, nmoves, pn));
     count_launch();

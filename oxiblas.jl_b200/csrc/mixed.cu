@@ -595,7 +595,8 @@ static int dgesv_mixed(oxi_handle_s *h, int prec, int refine, i64 n, i64 nrhs, c
     char *hb = (char *)h->host_ws.get(sizeof(int64_t) * (n + 16) + sizeof(double) * 512);
     M.hpiv = (int64_t *)hb;
     M.hsc = (double *)(hb + sizeof(int64_t) * (n + 16));
-    OXI_CUDA(cudaMemsetAsync(M.err, 0, 64, s));
+    // M.err (the call's abort word, also set to 4 by an overflowing conversion)
+    // and the non-finite flag were cleared by the entry point's AbortScope
 
     // ---- 1-2. finiteness + equilibration ----
     {
@@ -778,13 +779,17 @@ extern "C" int oxi_dgesv_mixed(oxi_handle_t h, int prec, int refine, int64_t n, 
     try {
         oxi::ProfGuard pg(&h->prof);
         OXI_CUDA(cudaSetDevice(h->device));
+        oxi::AbortScope ab(h);
         const int st = oxi::dgesv_mixed(h, prec, refine, n, nrhs, dA, lda, dB, ldb, dX, ldx, maxiter, rtol, out);
+        h->stall_at = 0;  // the test hook is one-shot
+        if (st == OXI_EOVERFLOW) return st;  // the conversion's code in the abort word
         int *he = (int *)h->host_ws.get(64);
-        oxi::queue_wait_errors(h, he);
+        oxi::queue_abort_read(h, he);
         OXI_CUDA(cudaStreamSynchronize(h->stream));
-        const int we = oxi::check_wait_errors(h, he);
+        const int we = oxi::check_abort(h, he);
         return we != OXI_OK ? we : st;
     } catch (const oxi::CudaError &e) {
+        h->stall_at = 0;
         h->last_error = std::string(e.what) + ": " + cudaGetErrorString(e.code);
         return OXI_ECUDA;
     }

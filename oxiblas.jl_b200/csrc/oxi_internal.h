@@ -36,7 +36,8 @@ struct CudaError {
 // Fixed layout of the handle's small control block (allocated once at this size,
 // so pointers into it stay valid for the whole call).
 constexpr size_t kScratchBytes = 65536;
-constexpr size_t kScratchErrOff = 1024;     // int error words
+constexpr size_t kScratchErrOff = 1024;     // the abort block (16 bytes), then other int error words
+constexpr size_t kScratchStallOff = 1984;   // flag of the missing-producer test hook (never set)
 constexpr size_t kScratchScalOff = 2048;    // double scalars of the mixed path
 constexpr size_t kScratchTrsvOff = 8192;    // triangular-solve tickets and flags
 constexpr int kTrsvCtlInts = (int)((kScratchBytes - kScratchTrsvOff) / sizeof(int));
@@ -103,6 +104,9 @@ struct oxi_handle_s {
     int device = 0;
     cudaStream_t stream = nullptr;
     oxi::Options opt;
+    int64_t wait_limit_ns = 0;      // bounded-wait limit of this handle's calls (0: kWaitLimitNs)
+    int64_t wait_limit_dev = -1;    // the value last written into the abort block
+    int64_t stall_at = 0;           // OXI_OPT_TEST_MISSING_PRODUCER: > 0 arms the hook before that leaf
     std::string last_error;
     int sm_count = 148;
     // workspaces
@@ -183,16 +187,39 @@ struct oxi_handle_s {
 
 namespace oxi {
 
-// Device error words of the kernels with bounded waits (one per translation
-// unit).  A non-zero word means a wait timed out and that call's results are
-// void.  queue_wait_errors enqueues their copies into hdst[0..2] (pinned host
-// memory) on the handle's stream; after the stream is idle, check_wait_errors
-// returns OXI_ETIMEOUT if any was set (and clears the words), else OXI_OK.
-int *leaf_wait_err_addr();
-int *dmma_wait_err_addr();
-int *tc_wait_err_addr();
-void queue_wait_errors(oxi_handle_s *h, int *hdst);
-int check_wait_errors(oxi_handle_s *h, const int *hsrc);
+// The abort block of a handle: 16 bytes at kScratchErrOff of its scratch.
+// int 0 is the sticky abort code of the running call (0: healthy; set by the
+// first bounded wait that gives up, read by every later wait and kernel entry
+// of the call), int 1 the mixed path's non-finite flag, ints 2-3 the wait limit
+// in ns (0: kWaitLimitNs).  Each handle has its own block, so calls on
+// different handles never see each other's timeouts.
+//
+// AbortScope (entry points): makes the handle's abort word the one the
+// launchers of this host thread pass to their kernels (t_abort), clears the
+// word on the handle's stream, and writes the wait limit when it changed.
+// queue_abort_read enqueues the word's copy into *hdst (pinned) on the
+// handle's stream; after the stream is idle, check_abort returns OXI_ETIMEOUT
+// if it was set, else OXI_OK.
+extern thread_local int *t_abort;
+inline int *cur_abort() { return t_abort; }
+int *abort_word(oxi_handle_s *h);
+struct AbortScope {
+    int *saved;
+    int *word;
+    explicit AbortScope(oxi_handle_s *h);
+    ~AbortScope() { t_abort = saved; }
+};
+void queue_abort_read(oxi_handle_s *h, int *hdst);
+int check_abort(oxi_handle_s *h, const int *hsrc);
+
+// Test hook of the bounded waits (OXI_OPT_TEST_MISSING_PRODUCER): a one-thread
+// kernel waits for a handle-owned flag that no kernel sets -- the wait of a
+// consumer whose producer was never launched -- and so makes the call's
+// abort word trip after the wait limit.
+void launch_await_missing_producer(oxi_handle_s *h, cudaStream_t s);
+// Called before every leaf launch of a factorization: launches the test hook
+// before the armed leaf (h->stall_at counts leaves down to it).
+void maybe_stall_before_leaf(oxi_handle_s *h, cudaStream_t s);
 
 // Raise a kernel's dynamic shared-memory limit to `bytes`, once per device
 // (the attribute belongs to the device's context).  A kernel keeps ONE limit,
@@ -232,6 +259,8 @@ struct LeafPanel {
     int u_rows = 0, u_cols = 0;
     // set the move counter back to zero at the end (saves the next leaf's memset)
     int reset_nmoves = 0;
+    // the call's abort word (set by launch_leaf)
+    int *abort = nullptr;
 };
 
 // Tournament-pivoting leaf (FP32, mixed solve only): same contract as

@@ -64,10 +64,7 @@ __device__ __forceinline__ float tagged_get(const unsigned long long *p, uint32_
         const uint64_t t0 = global_ns();
         uint32_t it = 0;
         while ((uint32_t)((w = ld_volatile_u64(p)) >> 32) != epoch) {
-            if ((++it & 255) == 0 && global_ns() - t0 > kWaitLimitNs) {
-                atomicExch(err, 3);
-                break;
-            }
+            if (spin_give_up<256>(it, t0, err, 3)) break;
         }
     }
     return __uint_as_float((uint32_t)w);
@@ -84,7 +81,7 @@ k_trsv2(const T *__restrict__ A, i64 lda, T *__restrict__ X, i64 ldx, int n, int
     __shared__ int s_blk;
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const int nb = (n + SB - 1) / SB;
-    if (t == 0) s_blk = atomicAdd(ticket, 1);
+    if (t == 0) s_blk = aborted(err) ? nb : atomicAdd(ticket, 1);  // an aborted call: no block
     __syncthreads();
     const int bi = s_blk;
     if (bi >= nb) return;
@@ -124,10 +121,7 @@ k_trsv2(const T *__restrict__ A, i64 lda, T *__restrict__ X, i64 ldx, int n, int
             const uint64_t t0 = global_ns();
             uint32_t it = 0;
             while (ld_acquire(&flags[c]) == 0) {
-                if ((++it & 255) == 0 && global_ns() - t0 > kWaitLimitNs) {
-                    atomicExch(err, 3);
-                    break;
-                }
+                if (spin_give_up<256>(it, t0, err, 3)) break;
             }
         }
         __syncwarp();
@@ -190,10 +184,7 @@ k_trsv2(const T *__restrict__ A, i64 lda, T *__restrict__ X, i64 ldx, int n, int
             const uint64_t t0 = global_ns();
             uint32_t it = 0;
             while (ld_acquire(&flags[cc]) == 0) {
-                if ((++it & 255) == 0 && global_ns() - t0 > kWaitLimitNs) {
-                    atomicExch(err, 3);
-                    break;
-                }
+                if (spin_give_up<256>(it, t0, err, 3)) break;
             }
         }
         __syncthreads();
@@ -305,10 +296,7 @@ __device__ __forceinline__ double tag_get<double>(const unsigned long long *w, u
             lo = ld_volatile_u64(w);
             hi = ld_volatile_u64(w + 1);
             if ((uint32_t)(lo >> 32) == epoch && (uint32_t)(hi >> 32) == epoch) break;
-            if ((++it & 255) == 0 && global_ns() - t0 > kWaitLimitNs) {
-                atomicExch(err, 3);
-                break;
-            }
+            if (spin_give_up<256>(it, t0, err, 3)) break;
         }
     }
     return __longlong_as_double((long long)((hi << 32) | (lo & 0xffffffffull)));
@@ -377,10 +365,7 @@ __device__ __forceinline__ void stage_block(T (*xs)[NR], const unsigned long lon
                 all = all && rdy[v];
             }
             if (all) break;
-            if ((++it & 63) == 0 && global_ns() - t0 > kWaitLimitNs) {
-                atomicExch(err, 3);
-                break;
-            }
+            if (spin_give_up<64>(it, t0, err, 3)) break;
         }
     }
 #pragma unroll
@@ -475,7 +460,7 @@ k_trsv3(const T *__restrict__ A, i64 lda, const T *__restrict__ P, T *__restrict
     __shared__ int s_blk;
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const int nb = (n + SB - 1) / SB;
-    if (t == 0) s_blk = atomicAdd(ticket, 1);
+    if (t == 0) s_blk = aborted(err) ? nb : atomicAdd(ticket, 1);  // an aborted call: no block
     __syncthreads();
     const int bi = s_blk;
     if (bi >= nb) return;
@@ -588,10 +573,7 @@ k_trsv3(const T *__restrict__ A, i64 lda, const T *__restrict__ P, T *__restrict
                             ready = ready && (uint32_t)(xr[v][hw] >> 32) == epoch;
                         }
                         if (ready) break;
-                        if ((++it & 255) == 0 && global_ns() - t0 > kWaitLimitNs) {
-                            atomicExch(err, 3);
-                            break;
-                        }
+                        if (spin_give_up<256>(it, t0, err, 3)) break;
                     }
                 }
                 if (lane + 32 * v < 8 * NR) xsw[lane + 32 * v] = ok ? (T)tag_decode(xr[v]) : T(0);
@@ -889,18 +871,16 @@ static int getrs_entry(oxi_handle_s *h, char trans, i64 n, i64 nrhs, const T *dL
         for (i64 j = 0; j < n; ++j)
             if (ip[j] < 1 || ip[j] > n) return OXI_EINVAL;
         perm_from_ipiv(ip.data(), n, n, perm.data());
-        char *sc = (char *)h->scratch.get(kScratchBytes);
-        int *d_err = (int *)(sc + kScratchErrOff);
+        AbortScope ab(h);
         int64_t *dperm = (int64_t *)h->perm_ws.get(sizeof(int64_t) * n);
         int64_t *hperm = (int64_t *)h->host_ws.get(sizeof(int64_t) * (n + 8));
         std::copy(perm.begin(), perm.end(), hperm);
         OXI_CUDA(cudaMemcpyAsync(dperm, hperm, sizeof(int64_t) * n, cudaMemcpyHostToDevice, h->stream));
-        OXI_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), h->stream));
-        getrs_perm<T>(h, trans, n, nrhs, dLU, lda, dperm, dB, ldb, d_err);
+        getrs_perm<T>(h, trans, n, nrhs, dLU, lda, dperm, dB, ldb, ab.word);
         int *herr = (int *)(hperm + n);
-        OXI_CUDA(cudaMemcpyAsync(herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+        queue_abort_read(h, herr);
         OXI_CUDA(cudaStreamSynchronize(h->stream));
-        return *herr ? OXI_ETIMEOUT : OXI_OK;
+        return check_abort(h, herr);
     } catch (const CudaError &e) {
         h->last_error = std::string(e.what) + ": " + cudaGetErrorString(e.code);
         return OXI_ECUDA;
@@ -909,8 +889,10 @@ static int getrs_entry(oxi_handle_s *h, char trans, i64 n, i64 nrhs, const T *dL
 
 // ---------------------------------------------------------------------------
 // No-allocation FP64 getrs.  Its scratch is one file-scope device array:
-//   [0, 4)        timeout word of the triangular solves (cleared every call)
+//   [0, 4)        abort word of the triangular solves (cleared every call)
 //   [4, 8)        invalid-pivot flag (cleared every call)
+//   [8, 16)       wait limit of the solves' bounded waits: never written, so
+//                 zero (the default, 2 s) from the module's load
 //   [256, 4356)   tickets + per-block flags of k_trsv2 (cleared per launch)
 //   [8 KiB, +8n)  0-based permutation, int64 (written whole every call)
 //   [1 MiB, 8 MiB) the solve vector X, n x nrhs (written before it is read)

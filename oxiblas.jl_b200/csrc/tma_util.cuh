@@ -10,13 +10,44 @@
 namespace oxi {
 
 // Waits on the GPU are bounded in time: a waiter that has seen no progress for
-// kWaitLimitNs records an error code and gives up instead of hanging the device.
+// the call's wait limit (kWaitLimitNs unless the handle sets another) records an
+// error code in the call's abort word and gives up instead of hanging the device.
 constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s; legitimate waits are microseconds
 
 __device__ __forceinline__ uint64_t global_ns() {
     uint64_t t;
     asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
     return t;
+}
+
+// The abort block of a call (handle-owned, see AbortBlock in oxi_internal.h):
+// int 0 is the sticky abort code, ints 2-3 the wait limit in ns (0: default).
+// Once any wait of the call gives up, every later wait and every kernel entry
+// of the same call sees the code and returns at once, so one broken wait costs
+// one wait limit, not one per launch.
+__device__ __forceinline__ bool aborted(const int *ab) {
+    return ab != nullptr && *(const volatile int *)ab != 0;
+}
+__device__ __forceinline__ uint64_t wait_limit_ns(const int *ab) {
+    if (!ab) return kWaitLimitNs;
+    const uint64_t v = *(const volatile unsigned long long *)(ab + 2);
+    return v ? v : kWaitLimitNs;
+}
+__device__ __forceinline__ void raise_abort(int *ab, int code) {
+    if (ab) atomicCAS(ab, 0, code);
+}
+// Bookkeeping of a polling loop: call once per poll; true when the loop must
+// stop (this wait ran past the limit, recorded as `code`, or the call was
+// aborted elsewhere).  The clock and the abort word are read every `every` polls.
+template <uint32_t every = 256>
+__device__ __forceinline__ bool spin_give_up(uint32_t &it, uint64_t t0, int *ab, int code) {
+    if ((++it & (every - 1)) != 0) return false;
+    if (aborted(ab)) return true;
+    if (global_ns() - t0 > wait_limit_ns(ab)) {
+        raise_abort(ab, code);
+        return true;
+    }
+    return false;
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -50,16 +81,18 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// Bounded wait; returns false (and sets *err) on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err, int code) {
+// Bounded wait; returns false when it ran past the call's limit (recording
+// `code` in the abort word ab) or when the call has been aborted.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *ab, int code) {
     if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = global_ns();
     for (;;) {
         for (int it = 0; it < 256; ++it)
             if (mbar_try_wait(bar, parity)) return true;
-        if (global_ns() - t0 > kWaitLimitNs) break;
+        if (aborted(ab)) return false;
+        if (global_ns() - t0 > wait_limit_ns(ab)) break;
     }
-    if (err) atomicExch(err, code);
+    raise_abort(ab, code);
     return false;
 }
 

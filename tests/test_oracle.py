@@ -87,3 +87,29 @@ def test_oracle_adjoint_matches_finite_differences(oracle):
         f = lambda M: 0.5 * np.sum(np.linalg.solve(M, b) ** 2)
         fd = (f(A + h * dA) - f(A - h * dA)) / (2 * h)
         assert abs(fd - np.sum(Abar * dA)) <= 1e-6 * max(1, abs(fd))
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_oracle_tiled_gemm_is_bit_identical(oracle, dtype):
+    """The register-tiled trailing update (the fast path used at benchmark
+    sizes) performs, element by element, the scalar form's operations in the
+    scalar form's order: factors and pivots are the same bits."""
+    rng = np.random.default_rng(21)
+    try:
+        for (m, n, bs) in [(1000, 1000, 128), (1537, 1211, 128), (777, 1500, 64), (3000, 300, 128)]:
+            A = rng.standard_normal((m, n)).astype(dtype)
+            oracle.set_gemm_tiled(True)
+            F1, i1, _ = oracle.getrf(A, blocksize=bs, dtype=dtype, check=False)
+            oracle.set_gemm_tiled(False)
+            F2, i2, _ = oracle.getrf(A, blocksize=bs, dtype=dtype, check=False)
+            assert np.array_equal(i1, i2) and np.array_equal(F1, F2), (m, n, bs)
+            C = rng.standard_normal((301, 203)).astype(dtype)
+            Am = rng.standard_normal((301, 77)).astype(dtype)
+            Bm = rng.standard_normal((77, 203)).astype(dtype)
+            oracle.set_gemm_tiled(True)
+            G1 = oracle.gemm_update(C, Am, Bm)
+            oracle.set_gemm_tiled(False)
+            G2 = oracle.gemm_update(C, Am, Bm)
+            assert np.array_equal(G1, G2)
+    finally:
+        oracle.set_gemm_tiled(True)
