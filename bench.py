@@ -166,85 +166,90 @@ def max_over_ranks(ws, v):
 
 
 # ---------------------------------------------------------------------------
-# CPU oracle legs (baseline only; bounded samples extrapolated by flop count)
+# CPU legs: the reference's own algorithm, restated by the oracle (Julia, the
+# reference's language, is not installed), timed on the host cores
 # ---------------------------------------------------------------------------
 def lu_flops(n):
     return 2.0 / 3.0 * n ** 3
 
 
-def prefix_flops(n, nb, steps):
-    f = 0.0
-    for s in range(steps):
-        k = s * nb
-        m = n - k
-        # panel (m x nb), U block row TRSM, trailing update
-        f += m * nb * nb + nb * nb * (n - k - nb) + 2.0 * (m - nb) * (n - k - nb) * nb
-    return f
+def load_synthetic():
+    """The seeded input generator alone (torch only): the reference arm builds
+    the GPU arm's system without importing the engine package."""
+    import importlib.util
+    path = os.path.join(ROOT, "oxiblas.jl_b200", "synthetic.py")
+    spec = importlib.util.spec_from_file_location("oxiblas_synthetic", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
 
 
-def cpu_mixed_estimate(A_np_colmajor_f32, n, panels=3):
-    """FP32 LU prefix (first `panels` panels of 128 columns) on the host cores,
-    extrapolated to the full factorization by flop count, plus one measured
-    FP64 refinement iteration (FP64 residual + FP32 correction solve) times the
-    iterations the reference's mixed_solve needs at this conditioning (3)."""
+def host_system(n, kappa, seed, nrhs, row_scale):
+    """The GPU arm's seeded system (same generator, same seed) as host arrays:
+    A column-major (Fortran order), B (n x nrhs)."""
     import numpy as np
-    import __graft_entry__ as E
-    orc = E.load_oracle()
-    W = A_np_colmajor_f32
-    t0 = time.perf_counter()
-    orc.getrf(W, blocksize=128, check=False, dtype=np.float32, steps=panels)
-    t_prefix = time.perf_counter() - t0
-    frac = prefix_flops(n, 128, panels) / lu_flops(n)
-    t_lu = t_prefix / frac
-    return t_lu, t_prefix, frac, orc.num_threads()
+    import torch
+    syn = load_synthetic()
+    dev = torch.device("cuda", torch.cuda.current_device()) if torch.cuda.is_available() else "cpu"
+    A = syn.kappa_matrix(n, kappa, seed=seed, device=dev, row_scale_decades=row_scale)
+    g = torch.Generator(device=dev).manual_seed(seed + 1)
+    b = torch.randn(n, nrhs, dtype=torch.float64, device=dev, generator=g)
+    An = np.asfortranarray(A.cpu().numpy())
+    bn = b.cpu().numpy()
+    del A, b
+    if torch.cuda.is_available():
+        torch.cuda.empty_cache()
+    return An, (bn[:, 0].copy() if nrhs == 1 else np.asfortranarray(bn))
 
 
-def cpu_refine_iteration(A64, x, b, LU32, ipiv):
-    import numpy as np
-    import __graft_entry__ as E
-    orc = E.load_oracle()
+def cpu_mixed_solve(orc, A, b, tol):
+    """One full mixed_solve on the host cores: radix equilibration, FP32 LU
+    (nb = 128, recursive panel, the reference's pivot rule and packed-GEMM
+    order), FP64 residuals and corrections until the normwise backward error
+    is <= tol (the GPU arm's stop test).  Returns (seconds, result dict)."""
     t0 = time.perf_counter()
-    R, _ = orc.refinement_residual(A64, x, b)
-    orc.getrs(LU32, ipiv, R.astype(np.float32))
-    return time.perf_counter() - t0
+    r = orc.mixed_solve_ex(A, b, maxiter=30, rtol=tol, normwise=True)
+    return time.perf_counter() - t0, r
 
 
 def reference_arm(args, ws, rank):
-    """The reference's own CPU implementation of the path, restated by the
-    oracle (Julia is not installed): mixed_solve = FP32 LU + FP64 refinement,
-    on all host cores, each step a bounded prefix sample extrapolated to the
-    full n=16384 solve."""
+    """The reference's own CPU implementation of the path (mixed_solve, FP32 LU
+    + FP64 refinement, src/lapack/extended_lapack.jl:175-226), restated by the
+    oracle, on all host cores, on the GPU arm's system: every timed step is one
+    full solve to the same stop test.  The warm-up steps solve a small system
+    (threads and code warm; a full-size warm-up would add minutes)."""
     if rank != 0:
         return
     import numpy as np
     import __graft_entry__ as E
     orc = E.load_oracle()
     n = args.n
-    rng = np.random.default_rng(20261104)
-    A = np.asfortranarray(rng.standard_normal((n, n)).astype(np.float32))
-    times = []
-    for it in range(args.warmup + args.steps):
-        W = A.copy(order="F")
-        t_lu, t_prefix, frac, cores = cpu_mixed_estimate(W, n, panels=2)
-        if it >= args.warmup:
-            times.append(t_lu)
-    # one refinement iteration at full size on a small factor stand-in: the
-    # O(n^2) residual dominates it; the correction solve uses an identity factor
-    x = np.zeros(n)
-    b = rng.standard_normal(n)
-    A64 = np.asfortranarray(A.astype(np.float64))
-    t0 = time.perf_counter()
-    orc.refinement_residual(A64, x, b)
-    t_iter = time.perf_counter() - t0
-    ms = (statistics.median(times) + 3 * t_iter) * 1e3
+    A, b = host_system(n, args.kappa, 20261104, 1, args.row_scale)
+    rng = np.random.default_rng(7)
+    Aw = np.asfortranarray(rng.standard_normal((1024, 1024)) + 1024 * np.eye(1024))
+    bw = rng.standard_normal(1024)
+    for _ in range(args.warmup):
+        cpu_mixed_solve(orc, Aw, bw, args.tol)
+    times, res = [], None
+    for _ in range(args.steps):
+        dt, res = cpu_mixed_solve(orc, A, b, args.tol)
+        times.append(dt)
+    ms = statistics.mean(times) * 1e3
     cores = orc.num_threads()
-    sample = (f"FP32 blocked LU (nb=128) of the first 2 panels of a 16384^2 matrix, extrapolated by "
-              f"flop fraction {frac:.4f}, + 3 x one full-size FP64 residual ({t_iter*1e3:.0f} ms)")
+    sample = (f"full run: every step one complete mixed_solve of the GPU arm's n={n} system "
+              f"(seed 20261104): radix equilibration, FP32 blocked LU (nb=128), FP64 refinement to "
+              f"normwise backward error <= {args.tol:g} ({res['iterations']} iterations, final "
+              f"{res['backward_error_normwise']:.2e}); warm-up steps on a 1024^2 system")
     line = {"metric": METRIC, "value": round(ms, 3), "unit": "ms", "impl": "reference",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(ms, 3), "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "n": n, "nrhs": 1},
+            "config": {"workload": WORKLOAD, "n": n, "nrhs": 1, "kappa": args.kappa,
+                       "stop": f"normwise<={args.tol}"},
+            "refinement": {"iterations": res["iterations"],
+                           "backward_error_normwise": res["backward_error_normwise"],
+                           "backward_error": res["backward_error"], "converged": res["converged"]},
+            "ms_per_step_each": [round(t * 1e3, 1) for t in times],
             "cpu_baseline": {"value": round(ms, 3), "unit": "ms", "cores": cores, "kind": "port",
                              "sample": sample},
             "e2e": {"value": round(ms, 3), "unit": "ms", "h2d_bytes_per_step": 0,
@@ -425,24 +430,19 @@ def ours(args, ws, rank, local, metric=METRIC, workload=WORKLOAD):
     assert r["converged"]
     del A_host
 
-    # ---- CPU baseline (rank 0, N=1) ----
+    # ---- CPU baseline (rank 0, N=1): one full solve of this system ----
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu and metric == METRIC:
-        A32 = np.asfortranarray(Acm.t().float().cpu().numpy())
-        t_lu, t_prefix, frac, cores = cpu_mixed_estimate(A32, n, panels=3)
-        del A32
+        orc = E.load_oracle()
         A64 = np.asfortranarray(Acm.t().cpu().numpy())
-        x0 = Xcm[0].cpu().numpy()  # first right-hand side
-        t0 = time.perf_counter()
-        import __graft_entry__ as E2
-        E2.load_oracle().refinement_residual(A64, x0, b[:, 0].cpu().numpy())
-        t_res = time.perf_counter() - t0
+        b64 = b[:, 0].cpu().numpy()
+        t_cpu, rc = cpu_mixed_solve(orc, A64, b64, args.tol)
         del A64
-        cpu_ms = (t_lu + 3 * t_res) * 1e3
-        cpu = {"value": round(cpu_ms, 1), "unit": "ms", "cores": cores, "kind": "port",
-               "sample": (f"oracle FP32 blocked LU (nb=128), first 3 panels of this 16384^2 matrix "
-                          f"({t_prefix:.2f} s, flop fraction {frac:.4f}) extrapolated, + 3 x one "
-                          f"full-size FP64 residual ({t_res*1e3:.0f} ms): the reference's mixed_solve")}
+        cpu = {"value": round(t_cpu * 1e3, 1), "unit": "ms", "cores": orc.num_threads(), "kind": "port",
+               "sample": (f"full run: one complete mixed_solve of this n={n} system on the host cores "
+                          f"(oracle restatement: radix equilibration, FP32 blocked LU nb=128, FP64 "
+                          f"refinement to normwise <= {args.tol:g}: {rc['iterations']} iterations, "
+                          f"final {rc['backward_error_normwise']:.2e})")}
 
     line = {
         "metric": metric, "value": round(ms_mixed, 3), "unit": "ms", "n_gpus": ws,

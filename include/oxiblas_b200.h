@@ -232,6 +232,15 @@ int oxi_dgesv_mixed(oxi_handle_t h, int prec, int refine, int64_t n, int64_t nrh
                     const double *dA, int64_t lda, const double *dB, int64_t ldb, double *dX,
                     int64_t ldx, int maxiter, double rtol, oxi_refine_report *out);
 
+/* Radix equilibration, the first step of the mixed solve, as its own call:
+ * equilibrate(A; radix=true) (src/lapack/dense_utilities.jl:191-213).  For the
+ * m x n column-major A: d_rows[i] = 2^round(log2 max_j |A[i,j]|) (1 for a zero
+ * row), then d_cols[j] = the same of column j of the row-scaled matrix, both
+ * clamped to Float64's exponent range; dE (nullable, leading dimension lde)
+ * receives A ./ d_rows ./ d_cols^T.  OXI_ENONFINITE for non-finite input. */
+int oxi_dequilibrate(oxi_handle_t h, int64_t m, int64_t n, const double *dA, int64_t lda,
+                     double *d_rows, double *d_cols, double *dE, int64_t lde);
+
 /* ---------------------------------------------------------------------------
  * Batched LU of many independent small matrices of uneven orders (1..256), in
  * one persistent launch that takes matrices from a size-bucketed work queue

@@ -56,6 +56,10 @@ def lib():
         L.orc_mixed_solve.argtypes = [_i64, _i64, _dp, _i64, _dp, _i64, _dp, _i64, _i64,
                                       ctypes.c_double, _ip, _dp, ctypes.POINTER(ctypes.c_int)]
         L.orc_mixed_solve.restype = ctypes.c_int
+        L.orc_mixed_solve_ex.argtypes = [_i64, _i64, _dp, _i64, _dp, _i64, _dp, _i64, _i64,
+                                         ctypes.c_double, ctypes.c_int, _ip, _dp, _dp,
+                                         ctypes.POINTER(ctypes.c_int)]
+        L.orc_mixed_solve_ex.restype = ctypes.c_int
         L.orc_lu_adjoint.argtypes = [_i64, _dp, _i64, _ip, _dp, _dp, _dp, _dp, _i64]
         L.orc_lu_adjoint.restype = ctypes.c_int
         for P, fp in (("d", _dp), ("s", _fp)):
@@ -216,6 +220,31 @@ def mixed_solve(A, b, maxiter: int = 10, rtol: float = 1e-13):
     e = float(err[0])
     return dict(x=X[:, 0] if vec else X, converged=e <= rtol, iterations=int(it[0]),
                 backward_error=e, fallback=bool(fb.value))
+
+
+def mixed_solve_ex(A, b, maxiter: int = 10, rtol: float = 1e-13, normwise: bool = False):
+    """mixed_solve with the stop test on the componentwise (reference) or the
+    normwise backward error; both final errors are returned."""
+    A = np.asfortranarray(A, dtype=np.float64)
+    n = A.shape[0]
+    vec = np.ndim(b) == 1
+    B = np.asfortranarray(np.reshape(b, (n, -1)), dtype=np.float64)
+    nrhs = B.shape[1]
+    X = np.zeros((n, nrhs), order="F")
+    it = np.zeros(1, dtype=np.int64)
+    cw = np.zeros(1)
+    nw = np.zeros(1)
+    fb = ctypes.c_int(0)
+    rc = lib().orc_mixed_solve_ex(n, nrhs, _ptr(A), max(n, 1), _ptr(B), max(n, 1), _ptr(X), max(n, 1),
+                                  maxiter, rtol, 1 if normwise else 0, _ptr(it, ctypes.c_int64), _ptr(cw),
+                                  _ptr(nw), ctypes.byref(fb))
+    if rc == 1:
+        raise SingularError(0)
+    if rc != 0:
+        raise OverflowError("mixed solve conversion overflow")
+    e = float(nw[0] if normwise else cw[0])
+    return dict(x=X[:, 0] if vec else X, converged=e <= rtol, iterations=int(it[0]),
+                backward_error=float(cw[0]), backward_error_normwise=float(nw[0]), fallback=bool(fb.value))
 
 
 def lu_adjoint(LU, ipiv, x, xbar):

@@ -10,7 +10,7 @@ from ._lib import (ArgumentError, DimensionMismatch, ExtensionMissing, Handle, S
                    exported_symbols, load)
 from .lu import (LU, colmajor_copy, det, gemm_update, ldiv, ldiv_, ldiv_into, logabsdet, lu, lu_,
                  options)
-from .mixed import gemm_update_lowp, mixed_solve, mixed_solve_device
+from .mixed import equilibrate, gemm_update_lowp, mixed_solve, mixed_solve_device
 from .adjoint import lu_adjoint, solve
 from .batched import BatchedLU, autotune as batched_autotune, set_tuning as batched_set_tuning, \
     tuning as batched_tuning
@@ -20,5 +20,6 @@ __all__ = [
     "LU", "lu", "lu_", "ldiv", "ldiv_", "ldiv_into", "det", "logabsdet", "gemm_update", "options",
     "colmajor_copy", "SingularException", "DimensionMismatch", "ArgumentError", "ExtensionMissing",
     "Handle", "load", "exported_symbols", "mixed_solve", "mixed_solve_device", "gemm_update_lowp",
+    "equilibrate",
     "lu_adjoint", "solve", "BatchedLU", "batched_autotune", "batched_tuning", "batched_set_tuning",
 ]

@@ -80,6 +80,7 @@ _SIGS = {
                           ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
     "oxi_launch_count": ([_vp, ctypes.POINTER(_i64)], ctypes.c_int),
     "oxi_launch_count_reset": ([_vp], ctypes.c_int),
+    "oxi_dequilibrate": ([_vp, _i64, _i64, _vp, _i64, _vp, _vp, _vp, _i64], ctypes.c_int),
     "oxi_dgesv_mixed": ([_vp, ctypes.c_int, ctypes.c_int, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64,
                          ctypes.c_int, ctypes.c_double, _vp], ctypes.c_int),
 }

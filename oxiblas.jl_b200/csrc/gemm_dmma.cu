@@ -82,7 +82,7 @@ k_gemm_dmma(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUt
             for (int kt = 0; kt < KT; ++kt) {
                 const int s = kt % STAGES;
                 if (kt >= STAGES) {
-                    if (!mbar_wait(&empty[s], ((kt / STAGES) + 1) & 1, ab, 2)) break;
+                    if (!mbar_wait<false>(&empty[s], ((kt / STAGES) + 1) & 1, ab, 2)) break;
                 }
                 uint8_t *sa = smem + s * STAGE_BYTES;
                 uint8_t *sb = sa + A_STAGE_BYTES;
@@ -109,7 +109,7 @@ k_gemm_dmma(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUt
 
     for (int kt = 0; kt < KT; ++kt) {
         const int s = kt % STAGES;
-        if (!mbar_wait(&full[s], (kt / STAGES) & 1, ab, 2)) return;
+        if (!mbar_wait<false>(&full[s], (kt / STAGES) & 1, ab, 2)) return;
         const uint8_t *sa = smem + s * STAGE_BYTES;
         const uint8_t *sb = sa + A_STAGE_BYTES;
 #pragma unroll

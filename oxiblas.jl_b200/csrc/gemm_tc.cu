@@ -59,8 +59,10 @@ __device__ __forceinline__ void tma_store_2d(const CUtensorMap *tm, const void *
         : "memory");
 }
 
-// Bounded wait that also gives up when another role of the CTA, or another
-// wait of the same call (the call's abort word ab), has given up.
+// Bounded wait that also gives up when another role of the CTA has given up.
+// A wait that runs past the call's limit records it in the call's abort word
+// ab.  The word itself is read at entry only: with TMA loads and MMAs of its
+// own in flight, the CTA must not leave because some other kernel failed.
 __device__ __forceinline__ bool mbar_wait_ab(uint64_t *bar, uint32_t parity, volatile int *abort_flag,
                                              int *ab) {
     if (mbar_try_wait(bar, parity)) return true;
@@ -69,10 +71,7 @@ __device__ __forceinline__ bool mbar_wait_ab(uint64_t *bar, uint32_t parity, vol
     for (;;) {
         for (int it = 0; it < 256; ++it)
             if (mbar_try_wait(bar, parity)) return true;
-        if (*abort_flag || aborted(ab)) {
-            *abort_flag = 1;
-            return false;
-        }
+        if (*abort_flag) return false;
         if (global_ns() - t0 > lim) break;
     }
     raise_abort(ab, 5);

@@ -42,12 +42,14 @@ __device__ __forceinline__ void atomic_max_nonneg(double *addr, double v) {
 // ---------------------------------------------------------------------------
 // Equilibration
 // ---------------------------------------------------------------------------
-__global__ void k_row_stats_part(const double *__restrict__ A, i64 lda, int n, int chunk,
+// Row statistics of the m x n column-major A over column chunk blockIdx.y:
+// max |a| and sum |a| per row, and a flag for non-finite entries.
+__global__ void k_row_stats_part(const double *__restrict__ A, i64 lda, int m, int n, int chunk,
                                  double *__restrict__ pmax, double *__restrict__ psum,
                                  int *__restrict__ nonfinite) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int s = blockIdx.y;
-    if (i >= n) return;
+    if (i >= m) return;
     const int j0 = s * chunk, j1 = min(n, j0 + chunk);
     double mx = 0.0, sm = 0.0;
     bool bad = false;
@@ -59,8 +61,8 @@ __global__ void k_row_stats_part(const double *__restrict__ A, i64 lda, int n, i
         mx = fmax(mx, v);
         sm += v;
     }
-    pmax[(i64)s * n + i] = mx;
-    psum[(i64)s * n + i] = sm;
+    pmax[(i64)s * m + i] = mx;
+    psum[(i64)s * m + i] = sm;
     if (bad) atomicExch(nonfinite, 1);
 }
 
@@ -78,11 +80,11 @@ __global__ void k_row_stats_final(const double *__restrict__ pmax, const double 
     atomic_max_nonneg(anorm, sm);
 }
 
-__global__ void k_col_scale(const double *__restrict__ A, i64 lda, int n,
+__global__ void k_col_scale(const double *__restrict__ A, i64 lda, int m,
                             const double *__restrict__ rows, double *__restrict__ cols) {
     const int j = blockIdx.x;
     double mx = 0.0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) mx = fmax(mx, fabs(A[i + (i64)j * lda]) / rows[i]);
+    for (int i = threadIdx.x; i < m; i += blockDim.x) mx = fmax(mx, fabs(A[i + (i64)j * lda]) / rows[i]);
     __shared__ double red[32];
     for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
@@ -112,6 +114,16 @@ __global__ void k_equilibrated_rm(const double *__restrict__ A, i64 lda, T *__re
         const int i = i0 + r, j = j0 + tx;
         if (i < n && j < n) W[(i64)i * ldw + j] = tile[tx][r];
     }
+}
+
+// E = A ./ rows ./ cols (column-major m x n): the matrix of equilibrate(A).
+__global__ void k_equilibrated_cm(const double *__restrict__ A, i64 lda, double *__restrict__ E, i64 lde,
+                                  int m, int n, const double *__restrict__ rows,
+                                  const double *__restrict__ cols) {
+    const i64 idx = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (i64)m * n) return;
+    const int i = (int)(idx % m), j = (int)(idx / m);
+    E[i + (i64)j * lde] = (A[i + (i64)j * lda] / rows[i]) / cols[j];
 }
 
 __global__ void k_check_finite(const double *__restrict__ B, i64 ldb, int n, int nrhs, int *flag) {
@@ -602,7 +614,7 @@ static int dgesv_mixed(oxi_handle_s *h, int prec, int refine, i64 n, i64 nrhs, c
     {
         const int chunk = (int)((n + RS - 1) / RS);
         dim3 g(blocks_for(n, 128), RS);
-        k_row_stats_part<<<g, 128, 0, s>>>(dA, lda, (int)n, chunk, M.pmax, M.psum, nonfinite);
+        k_row_stats_part<<<g, 128, 0, s>>>(dA, lda, (int)n, (int)n, chunk, M.pmax, M.psum, nonfinite);
         OXI_LAUNCH_CHECK();
         k_check_finite<<<blocks_for(n * nrhs), 256, 0, s>>>(dB, ldb, (int)n, (int)nrhs, nonfinite);
         OXI_LAUNCH_CHECK();
@@ -790,6 +802,59 @@ extern "C" int oxi_dgesv_mixed(oxi_handle_t h, int prec, int refine, int64_t n, 
         return we != OXI_OK ? we : st;
     } catch (const oxi::CudaError &e) {
         h->stall_at = 0;
+        h->last_error = std::string(e.what) + ": " + cudaGetErrorString(e.code);
+        return OXI_ECUDA;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// equilibrate(A; radix=true) alone (src/lapack/dense_utilities.jl:191-213): the
+// row scales (powers of two nearest each row's max |a|), then the column scales
+// of the row-scaled matrix, and optionally the equilibrated matrix itself.
+extern "C" int oxi_dequilibrate(oxi_handle_t h, int64_t m, int64_t n, const double *dA, int64_t lda,
+                                double *d_rows, double *d_cols, double *dE, int64_t lde) {
+    using namespace oxi;
+    if (!h || m < 0 || n < 0 || lda < std::max<int64_t>(1, m)) return OXI_EINVAL;
+    if (dE && lde < std::max<int64_t>(1, m)) return OXI_EINVAL;
+    if (m >= (1ll << 31) || n >= (1ll << 31)) return OXI_EINVAL;
+    if (m == 0 && n == 0) return OXI_OK;
+    if ((m > 0 && !d_rows) || (n > 0 && !d_cols) || (m > 0 && n > 0 && !dA)) return OXI_EINVAL;
+    try {
+        ProfGuard pg(&h->prof);
+        OXI_CUDA(cudaSetDevice(h->device));
+        AbortScope ab(h);
+        cudaStream_t s = h->stream;
+        int *nonfinite = ab.word + 1;  // cleared by the scope
+        if (m == 0) {  // no rows: every column scale is one
+            std::vector<double> one((size_t)n, 1.0);
+            OXI_CUDA(cudaMemcpyAsync(d_cols, one.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s));
+            OXI_CUDA(cudaStreamSynchronize(s));
+            return OXI_OK;
+        }
+        const int parts = (int)std::min<int64_t>(RS, std::max<int64_t>(1, n));
+        const int chunk = (int)((std::max<int64_t>(n, 1) + parts - 1) / parts);
+        double *ws = (double *)h->mixed_ws.get(sizeof(double) * (2 * (size_t)parts * m + 8));
+        double *pmax = ws, *psum = ws + (size_t)parts * m, *anorm = psum + (size_t)parts * m;
+        OXI_CUDA(cudaMemsetAsync(anorm, 0, sizeof(double), s));
+        dim3 g(blocks_for(m, 128), parts);
+        k_row_stats_part<<<g, 128, 0, s>>>(dA, lda, (int)m, (int)n, chunk, pmax, psum, nonfinite);
+        OXI_LAUNCH_CHECK();
+        k_row_stats_final<<<blocks_for(m), 256, 0, s>>>(pmax, psum, (int)m, parts, d_rows, anorm);
+        OXI_LAUNCH_CHECK();
+        if (n > 0) {
+            k_col_scale<<<(unsigned)n, 256, 0, s>>>(dA, lda, (int)m, d_rows, d_cols);
+            OXI_LAUNCH_CHECK();
+            if (dE) {
+                k_equilibrated_cm<<<blocks_for(m * n), 256, 0, s>>>(dA, lda, dE, lde, (int)m, (int)n, d_rows,
+                                                                     d_cols);
+                OXI_LAUNCH_CHECK();
+            }
+        }
+        int *hflag = (int *)h->host_ws.get(64);
+        OXI_CUDA(cudaMemcpyAsync(hflag, nonfinite, sizeof(int), cudaMemcpyDeviceToHost, s));
+        OXI_CUDA(cudaStreamSynchronize(s));
+        return hflag[0] ? OXI_ENONFINITE : OXI_OK;
+    } catch (const CudaError &e) {
         h->last_error = std::string(e.what) + ": " + cudaGetErrorString(e.code);
         return OXI_ECUDA;
     }

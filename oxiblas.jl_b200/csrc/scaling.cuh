@@ -7,14 +7,12 @@
 namespace oxi {
 
 // 2^round(log2 v) clamped to Float64's exponent range (equilibrate's radix
-// scale).  log2 v = e + log2 f with v = f 2^e, f in [0.5, 1): it rounds to e
-// exactly when f >= 2^-1/2 (an irrational bound, so no ties arise).
+// scale): log2 rounded to the nearest integer, ties to even (Julia's round),
+// the same formula as the reference's ldexp(1, clamp(round(Int, log2(v)), ...)).
 __device__ __forceinline__ double radix_scale(double v) {
-    int e;
-    const double f = frexp(v, &e);
-    int r = (f >= 0.70710678118654757) ? e : e - 1;
-    r = max(-1022, min(1023, r));
-    return ldexp(1.0, r);
+    double e = rint(log2(v));
+    e = fmin(1023.0, fmax(-1022.0, e));
+    return ldexp(1.0, (int)e);
 }
 
 // power of two 2^exponent(m) (Julia's exponent: floor(log2 m)), 0 for m == 0

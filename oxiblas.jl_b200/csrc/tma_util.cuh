@@ -82,14 +82,19 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
     return ok != 0;
 }
 // Bounded wait; returns false when it ran past the call's limit (recording
-// `code` in the abort word ab) or when the call has been aborted.
+// `code` in the abort word ab) or, with POLL_ABORT, when the call has been
+// aborted elsewhere.  Kernels with asynchronous copies or tensor-core work in
+// flight (TMA loads, tcgen05.mma) wait with POLL_ABORT = false: leaving early
+// because of another kernel's failure would let the CTA exit with its own
+// transfers still landing; they read the abort word at entry only.
+template <bool POLL_ABORT = true>
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *ab, int code) {
     if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = global_ns();
     for (;;) {
         for (int it = 0; it < 256; ++it)
             if (mbar_try_wait(bar, parity)) return true;
-        if (aborted(ab)) return false;
+        if (POLL_ABORT && aborted(ab)) return false;
         if (global_ns() - t0 > wait_limit_ns(ab)) break;
     }
     raise_abort(ab, code);

@@ -121,6 +121,30 @@ def mixed_solve(A, b, *, maxiter: int = 10, rtol: float = 1e-13, precision: str 
                 factor_ms=sum(r.factor_ms for r in reps), refine_ms=sum(r.refine_ms for r in reps))
 
 
+def equilibrate(A, radix: bool = True):
+    """equilibrate(A; radix=true) (src/lapack/dense_utilities.jl:191-213) on the
+    GPU: returns dict(matrix, row_scale, column_scale) with
+    matrix = A ./ row_scale ./ column_scale', the scales powers of two."""
+    if not radix:
+        raise ArgumentError("only the radix (power-of-two) equilibration runs on the GPU engine")
+    At = _as_tensor(A)
+    if At.ndim != 2:
+        raise DimensionMismatch("a matrix is required")
+    m, n = At.shape
+    Acm = colmajor_copy(At, torch.float64)  # (n, m) storage = column-major A
+    Ecm = torch.empty_like(Acm)
+    rows = torch.ones(m, dtype=torch.float64, device=Acm.device)
+    cols = torch.ones(n, dtype=torch.float64, device=Acm.device)
+    h = Handle.get()
+    st = h.lib.oxi_dequilibrate(h.ptr, m, n, ctypes.c_void_p(Acm.data_ptr()), max(1, m),
+                                ctypes.c_void_p(rows.data_ptr()), ctypes.c_void_p(cols.data_ptr()),
+                                ctypes.c_void_p(Ecm.data_ptr()), max(1, m))
+    if st == OXI_ENONFINITE:
+        raise ArgumentError("finite input required")
+    h.check(st)
+    return dict(matrix=Ecm.t(), row_scale=rows, column_scale=cols)
+
+
 def gemm_update_lowp(C: torch.Tensor, A: torch.Tensor, B: torch.Tensor, precision="bf16"):
     """C <- C - A @ B with A, B rounded to 16 bits and FP32 accumulation: the
     mixed path's trailing-update kernel (tcgen05) on float32 CUDA tensors."""
