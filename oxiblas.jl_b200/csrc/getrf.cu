@@ -17,13 +17,16 @@ namespace oxi {
 
 static inline i64 round_up(i64 x, i64 a) { return (x + a - 1) / a * a; }
 
-// Split point of a recursion node.  Reference order keeps the reference's exact
-// halving (n / 2, src/lapack/factorizations.jl:141 and src/blas/level3.jl:340);
-// the tensor-core engine keeps column offsets on 8-element multiples so every
+// Split point of a recursion node.  FP64 and the reference summation order keep
+// the reference's exact halving (n / 2, src/lapack/factorizations.jl:141 and
+// src/blas/level3.jl:340): an odd column offset only sends the FP64 GEMM to its
+// non-TMA kernel, which has the same arithmetic.  The FP32 tensor-core engine
+// keeps column offsets on 8-element multiples so that every 16-bit operand's
 // TMA tile base stays 16-byte aligned.
+template <typename T>
 static inline i64 split_point(const oxi_handle_s *h, i64 n) {
     i64 half = n / 2;
-    if (h->opt.gemm == 1) return half;
+    if (h->opt.gemm == 1 || sizeof(T) == 8) return half;
     i64 a = half & ~i64(7);
     return a >= 8 ? a : half;
 }
@@ -48,15 +51,23 @@ template <typename T>
 void trsm_lower_unit(oxi_handle_s *h, const T *L, i64 ldl, T *B, i64 ldb, i64 t, i64 N) {
     if (t <= 1 || N <= 0) return;
     if (h->opt.gemm == 0 && t <= 256) {  // tensor-core engine: one fused launch
-        launch_trsm_fused<T>(L, ldl, B, ldb, (int)t, N, h->stream);
-        return;
+        if constexpr (sizeof(T) == 8) {
+            // FP64 (the drop-in path): the reference's recursion, bit for bit
+            if (trsm_refo_applicable((int)t)) {
+                launch_trsm_refo(L, ldl, B, ldb, (int)t, N, h->stream);
+                return;
+            }
+        } else {
+            launch_trsm_fused<T>(L, ldl, B, ldb, (int)t, N, h->stream);
+            return;
+        }
     }
     const i64 leaf = std::min<i64>(std::max<i64>(h->opt.trsm_leaf, 1), 32);
     if (t <= leaf) {
         launch_trsm_leaf<T>(L, ldl, B, ldb, (int)t, N, h->stream, h->opt.gemm == 1);
         return;
     }
-    const i64 t1 = split_point(h, t);
+    const i64 t1 = split_point<T>(h, t);
     trsm_lower_unit<T>(h, L, ldl, B, ldb, t1, N);
     gemm_minus<T>(h, B + t1 * ldb, ldb, L + t1 * ldl, ldl, B, ldb, t - t1, N, t1);
     trsm_lower_unit<T>(h, L + t1 * ldl + t1, ldl, B + t1 * ldb, ldb, t - t1, N);
@@ -142,6 +153,37 @@ static void panel_rl(LuRun<T> &R, i64 c0, i64 nc) {
                                    sizeof(T) * pend.u_cols, pend.u_rows, cudaMemcpyDeviceToDevice, h->stream));
 }
 
+// The reference's leaf of up to 32 columns (src/lapack/factorizations.jl:117-139)
+// on a panel taller than a 32-column leaf kernel holds (FP64, more than 8192
+// rows): leaves of w columns in turn, each followed by the substitution solve
+// of its rows for the columns to its right and the sequential rank-w update of
+// the rows below.  Every element then receives the 32-column leaf's rank-1
+// steps in the same order, so the bits are the same.
+template <typename T>
+static void panel_leaf32(LuRun<T> &R, i64 c0, i64 nc, int w) {
+    oxi_handle_s *h = R.h;
+    for (i64 c = c0; c < c0 + nc; c += w) {
+        const i64 wc = std::min<i64>(w, c0 + nc - c);
+        const i64 mrows = R.m - c;
+        if (mrows <= 0) break;
+        OXI_CUDA(cudaMemsetAsync(R.nmoves, 0, sizeof(int), h->stream));
+        maybe_stall_before_leaf(h, h->stream);
+        launch_leaf<T>(R.W + c * R.ld + c, R.ld, mrows, (int)wc, c, R.ipiv, R.info, R.moves, R.nmoves, w,
+                       h->stream, leaf_panel(R, c, wc));
+        const i64 right = c0 + nc - (c + wc);
+        if (right <= 0) continue;
+        if constexpr (sizeof(T) == 8) {
+            T *Lk = R.W + c * R.ld + c;
+            // rows [c, c+wc) of the columns to the right: substitution with the
+            // leaf's unit lower block (a one-block fused solve is substitution)
+            launch_trsm_fused<T>(Lk, R.ld, Lk + wc, R.ld, (int)wc, right, h->stream);
+            if (mrows > wc)
+                launch_rankk_seq(Lk + wc * R.ld + wc, R.ld, Lk + wc * R.ld, R.ld, Lk + wc, R.ld, mrows - wc, right,
+                                 wc, h->stream);
+        }
+    }
+}
+
 // Recursive panel on columns [c0, c0+nc), rows [c0, m).
 template <typename T>
 static void panel_rec(LuRun<T> &R, i64 c0, i64 nc) {
@@ -158,6 +200,12 @@ static void panel_rec(LuRun<T> &R, i64 c0, i64 nc) {
     }
     const int leafw = ts ? 32 : leaf_width_for<T>(mrows);
     if (leafw == 0) throw CudaError{cudaErrorInvalidValue, "panel taller than the leaf capacity"};
+    if constexpr (sizeof(T) == 8) {
+        if (nc > leafw && nc <= 32 && R.map && h->opt.gemm == 0) {
+            panel_leaf32(R, c0, nc, leafw);
+            return;
+        }
+    }
     if (nc <= leafw) {
         OXI_CUDA(cudaMemsetAsync(R.nmoves, 0, sizeof(int), h->stream));
         auto leaf = [&](LeafPanel pn) {
@@ -181,7 +229,7 @@ static void panel_rec(LuRun<T> &R, i64 c0, i64 nc) {
         }
         return;
     }
-    const i64 hh = split_point(h, nc);
+    const i64 hh = split_point<T>(h, nc);
     panel_rec(R, c0, hh);
     T *L11 = R.W + c0 * R.ld + c0;
     trsm_lower_unit<T>(h, L11, R.ld, L11 + hh, R.ld, hh, nc - hh);

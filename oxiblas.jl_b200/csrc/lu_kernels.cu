@@ -952,6 +952,137 @@ void launch_trsm_fused(const T *L, i64 ldl, T *B, i64 ldb, int t, i64 N, cudaStr
     }
     OXI_LAUNCH_CHECK();
 }
+// ---------------------------------------------------------------------------
+// Reference-order TRSM (FP64, t <= 128): B (t x N) <- L^-1 B for a unit lower
+// L, performing element by element the operations of the reference's
+// recursive solve (src/blas/level3.jl:338-355, _trsm_blocks_left!): halve the
+// triangle (h = t / 2), solve the top half, update the bottom half with one
+// fma chain from zero per element followed by a subtraction (the GEMM of
+// src/blas/gemm.jl:286-298 / simd.jl:151 for k <= kc), solve the bottom half;
+// leaves of <= 8 rows by substitution, s = b; s = fma(-L[i,p], x[p], s) for
+// p < i (_trsm_leaf_generic!, level3.jl:309-321).  The host flattens the
+// recursion into a list of leaf and update steps in the recursion's order; one
+// CTA takes CW columns and runs the list with L and its columns in shared
+// memory, so one launch gives the recursive solve's bits.
+// ---------------------------------------------------------------------------
+struct TrsmSteps {
+    int count;
+    int4 step[64];  // {kind (0 leaf, 1 update), a, b, c}: leaf rows [a, b); update rows [b, c) from [a, b)
+};
+
+static void trsm_steps_rec(int a, int b, TrsmSteps &st) {
+    if (b - a <= 8) {
+        st.step[st.count++] = make_int4(0, a, b, 0);
+        return;
+    }
+    const int h = (b - a) / 2;
+    trsm_steps_rec(a, a + h, st);
+    st.step[st.count++] = make_int4(1, a, a + h, b);
+    trsm_steps_rec(a + h, b, st);
+}
+
+constexpr int TR_TMAX = 128;
+
+template <int CW>
+__global__ void __launch_bounds__(256) k_trsm_refo(const double *__restrict__ L, i64 ldl, double *__restrict__ B,
+                                                   i64 ldb, int t, i64 N, const __grid_constant__ TrsmSteps st) {
+    extern __shared__ __align__(16) double tr_smem[];
+    const int lp = t + 1;  // padded L row
+    double *Ls = tr_smem;
+    double *X = tr_smem + (size_t)t * lp;  // t x (CW + 1)
+    constexpr int XP = CW + 1;
+    const int tid = threadIdx.x;
+    const i64 c0 = (i64)blockIdx.x * CW;
+    const int cols = (int)((N - c0) < CW ? (N - c0) : CW);
+    for (int e = tid; e < t * t; e += 256) {
+        const int r = e / t, pcol = e - r * t;
+        Ls[r * lp + pcol] = (pcol < r) ? L[(i64)r * ldl + pcol] : 0.0;
+    }
+    for (int e = tid; e < t * CW; e += 256) {
+        const int i = e / CW, c = e - i * CW;
+        X[i * XP + c] = (c < cols) ? B[(i64)i * ldb + c0 + c] : 0.0;
+    }
+    __syncthreads();
+    for (int k = 0; k < st.count; ++k) {
+        const int4 o = st.step[k];
+        if (o.x == 0) {
+            if (tid < CW) {
+                for (int i = o.y; i < o.z; ++i) {
+                    double sv = X[i * XP + tid];
+                    for (int pp = o.y; pp < i; ++pp) sv = fma(-Ls[i * lp + pp], X[pp * XP + tid], sv);
+                    X[i * XP + tid] = sv;
+                }
+            }
+        } else {
+            const int nr = o.w - o.z;
+            for (int e = tid; e < nr * CW; e += 256) {
+                const int r = o.z + e / CW, c = e % CW;
+                double acc = 0.0;
+                for (int pp = o.y; pp < o.z; ++pp) acc = fma(Ls[r * lp + pp], X[pp * XP + c], acc);
+                X[r * XP + c] -= acc;
+            }
+        }
+        __syncthreads();
+    }
+    for (int e = tid; e < t * CW; e += 256) {
+        const int i = e / CW, c = e - i * CW;
+        if (c < cols) B[(i64)i * ldb + c0 + c] = X[i * XP + c];
+    }
+}
+
+bool trsm_refo_applicable(int t) { return t >= 2 && t <= TR_TMAX; }
+
+void launch_trsm_refo(const double *L, i64 ldl, double *B, i64 ldb, int t, i64 N, cudaStream_t s) {
+    if (t <= 1 || N <= 0) return;
+    if (t > TR_TMAX) throw CudaError{cudaErrorInvalidValue, "reference-order TRSM: triangle too large"};
+    TrsmSteps st{};
+    trsm_steps_rec(0, t, st);
+    ProfScope ps(KC_TRSM_LEAF, s, (double)t * t * N, 2.0 * (double)t * N * 8);
+    if (N <= 2048) {
+        constexpr int CW = 8;
+        const size_t smem = sizeof(double) * ((size_t)t * (t + 1) + (size_t)t * (CW + 1));
+        set_max_dyn_smem((const void *)k_trsm_refo<CW>,
+                         (int)(sizeof(double) * ((size_t)TR_TMAX * (TR_TMAX + 1) + (size_t)TR_TMAX * (CW + 1))));
+        k_trsm_refo<CW><<<(unsigned)((N + CW - 1) / CW), 256, smem, s>>>(L, ldl, B, ldb, t, N, st);
+    } else {
+        constexpr int CW = 32;
+        const size_t smem = sizeof(double) * ((size_t)t * (t + 1) + (size_t)t * (CW + 1));
+        set_max_dyn_smem((const void *)k_trsm_refo<CW>,
+                         (int)(sizeof(double) * ((size_t)TR_TMAX * (TR_TMAX + 1) + (size_t)TR_TMAX * (CW + 1))));
+        k_trsm_refo<CW><<<(unsigned)((N + CW - 1) / CW), 256, smem, s>>>(L, ldl, B, ldb, t, N, st);
+    }
+    OXI_LAUNCH_CHECK();
+}
+
+// ---------------------------------------------------------------------------
+// Rank-k update in the order of a panel leaf's rank-1 steps (FP64): for every
+// element of C (M x N, row-major), s = C; s = fma(-A[r,k], B[k,c], s) for
+// k = 0..K-1.  Inside the reference's 32-column leaf (src/lapack/
+// factorizations.jl:117-139) the columns right of step k receive exactly this
+// sequence, so a leaf narrower than 32 columns followed by this update (and a
+// substitution solve of its rows) reproduces the 32-column leaf's bits.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_rankk_seq(double *__restrict__ C, i64 ldc, const double *__restrict__ A,
+                                                   i64 lda, const double *__restrict__ B, i64 ldb, int M, int N,
+                                                   int K) {
+    const i64 idx = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (i64)M * N) return;
+    const int r = (int)(idx / N), c = (int)(idx - (i64)r * N);
+    const double *a = A + (i64)r * lda;
+    double sv = C[(i64)r * ldc + c];
+    for (int k = 0; k < K; ++k) sv = fma(-a[k], B[(i64)k * ldb + c], sv);
+    C[(i64)r * ldc + c] = sv;
+}
+
+void launch_rankk_seq(double *C, i64 ldc, const double *A, i64 lda, const double *B, i64 ldb, i64 M, i64 N,
+                      i64 K, cudaStream_t s) {
+    if (M <= 0 || N <= 0 || K <= 0) return;
+    ProfScope ps(KC_GEMM_REF, s, 2.0 * M * N * K, 8.0 * (2.0 * M * N + M * K + K * N));
+    const i64 tot = M * N;
+    k_rankk_seq<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(C, ldc, A, lda, B, ldb, (int)M, (int)N, (int)K);
+    OXI_LAUNCH_CHECK();
+}
+
 template void launch_trsm_fused<double>(const double *, i64, double *, i64, int, i64, cudaStream_t);
 template void launch_trsm_fused<float>(const float *, i64, float *, i64, int, i64, cudaStream_t);
 

@@ -301,6 +301,14 @@ void launch_trsm_leaf(const T *L, i64 ldl, T *B, i64 ldb, int t, i64 N, cudaStre
 // Fused blocked TRSM, unit lower L with t <= 256 (one launch).
 template <typename T>
 void launch_trsm_fused(const T *L, i64 ldl, T *B, i64 ldb, int t, i64 N, cudaStream_t s);
+// Reference-order TRSM for FP64 (t <= 128): the recursive solve's operations,
+// element by element, in one launch (see lu_kernels.cu).
+bool trsm_refo_applicable(int t);
+void launch_trsm_refo(const double *L, i64 ldl, double *B, i64 ldb, int t, i64 N, cudaStream_t s);
+// C (M x N) <- C - A (M x K) B (K x N), row-major, as K sequential fma steps per
+// element starting from C (the order of a panel leaf's rank-1 updates).
+void launch_rankk_seq(double *C, i64 ldc, const double *A, i64 lda, const double *B, i64 ldb, i64 M, i64 N,
+                      i64 K, cudaStream_t s);
 // FP32 register-blocked CUDA-core GEMM (any summation order).
 template <typename T>
 void launch_gemm_simt(T *C, i64 ldc, const T *A, i64 lda, const T *B, i64 ldb, i64 M, i64 N, i64 K,

@@ -15,6 +15,10 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200, sm_100a)")
 
 
+def entry_oracle():
+    return entry.load_oracle()
+
+
 @pytest.fixture(scope="session")
 def oracle():
     return entry.load_oracle()
