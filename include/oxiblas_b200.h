@@ -155,6 +155,23 @@ int oxi_dlu_adjoint(oxi_handle_t h, int64_t n, int64_t nrhs, const double *dLU, 
                     int64_t ldxbar, double *dBbar, int64_t ldbbar, double *dAbar,
                     int64_t ldabar);
 
+/* Batched form for many independent small factorizations (orders 0..256,
+ * 0..8 right-hand sides each; the factors and pivots of
+ * oxi_dgetrf_batched_uneven / oxi_dgesv_batched_uneven with prec FP64), one
+ * launch: per problem i, Bbar_i = A_i^-T Xbar_i and Abar_i = -Bbar_i X_i^T.  All
+ * arrays are DEVICE arrays of `count` entries (d_nrhs nullable: one right-hand
+ * side each); Bbar_i may be Xbar_i itself.  d_info[i]: 0, -1 for bad arguments
+ * of that problem, or the first zero diagonal of its U.  Returns OXI_EINVAL /
+ * OXI_ESINGULAR when any problem had that outcome.  The reference has no
+ * batched factorization; its batching precedent is gemm_batched!
+ * (src/blas/batched.jl:4-49), and per problem this is oxi_dlu_adjoint. */
+int oxi_dlu_adjoint_batched_uneven(oxi_handle_t h, int64_t count, const int32_t *d_n,
+                                   const int32_t *d_nrhs, double *const *d_LU, const int64_t *d_ldlu,
+                                   int64_t *const *d_ipiv, double *const *d_X, const int64_t *d_ldx,
+                                   double *const *d_Xbar, const int64_t *d_ldxbar,
+                                   double *const *d_Bbar, const int64_t *d_ldbbar,
+                                   double *const *d_Abar, const int64_t *d_ldabar, int32_t *d_info);
+
 /* ---------------------------------------------------------------------------
  * Trailing-update GEMM as a standalone kernel: C <- C - A*B (column-major),
  * the gemm!(C, A, B, -1, 1) call of src/lapack/factorizations.jl:69
@@ -231,6 +248,55 @@ int oxi_sgemm_update_lowp(oxi_handle_t h, int prec, int64_t m, int64_t n, int64_
 int oxi_dgesv_mixed(oxi_handle_t h, int prec, int refine, int64_t n, int64_t nrhs,
                     const double *dA, int64_t lda, const double *dB, int64_t ldb, double *dX,
                     int64_t ldx, int maxiter, double rtol, oxi_refine_report *out);
+
+/* ---------------------------------------------------------------------------
+ * Expert solves and the condition estimate (FP64).
+ * ------------------------------------------------------------------------- */
+typedef struct oxi_solve_report {
+    int64_t iterations;             /* refinement steps taken (reference `iterations`) */
+    double backward_error;          /* componentwise, max_i |r_i| / (|A||x| + |b|)_i */
+    double residual_norm;           /* ||B - A X||_F of the final iterate */
+    double rcond_estimate;          /* refine_solve: min(1, 1 / (||A||_1 est(||A^-1||_1))) */
+    double forward_error_estimate;  /* refine_solve: delta / (1 - delta), delta =
+                                       est(||A^-1||_1) ||R||_1 / ||X||_1 (Inf if delta >= 1) */
+    double inverse_norm_estimate;   /* refine_solve: est(||A^-1||_1) */
+    int64_t info;                   /* expert_solve: first zero row or zero pivot (1-based) */
+    int32_t converged;
+    int32_t reserved;
+} oxi_solve_report;
+
+/* expert_solve(A, b; maxiter=8, rtol=8eps, equilibrate=true)
+ * (src/lapack/advanced_factorizations.jl:591-645): rows scaled by their max
+ * |a| (a zero row: OXI_ESINGULAR, info = its 1-based index), then columns by
+ * theirs, FP64 partial-pivoted LU of the scaled matrix, scaled solves and
+ * componentwise iterative refinement to rtol.  A (n x n), B and X (n x nrhs,
+ * nrhs <= 16) column-major.  Optional outputs (NULL to skip): the row and
+ * column scales (n each) and the factorization of the scaled matrix (dF, n x n,
+ * leading dimension ldf; d_ipiv, n) -- the reference's `factor` field.
+ * OXI_OK when converged, OXI_ENOTCONVERGED at maxiter (report filled). */
+int oxi_dexpert_solve(oxi_handle_t h, int64_t n, int64_t nrhs, const double *dA, int64_t lda,
+                      const double *dB, int64_t ldb, double *dX, int64_t ldx, int maxiter, double rtol,
+                      int equilibrate, double *d_row_scale, double *d_col_scale, double *dF,
+                      int64_t ldf, int64_t *d_ipiv, oxi_solve_report *out);
+/* refine_solve(A, F, b; maxiter=8, rtol=8eps) (src/lapack/expert_refinement.jl:89-104):
+ * X = F \ B, then FP64 residuals and corrections with the factors of oxi_dgetrf
+ * (dLU, d_ipiv) until the componentwise backward error is <= rtol; the report
+ * adds the reference's rcond and forward-error estimates. */
+int oxi_drefine_solve(oxi_handle_t h, int64_t n, int64_t nrhs, const double *dA, int64_t lda,
+                      const double *dLU, int64_t ldlu, const int64_t *d_ipiv, const double *dB,
+                      int64_t ldb, double *dX, int64_t ldx, int maxiter, double rtol,
+                      oxi_solve_report *out);
+/* inverse_norm_estimate(F, T, n; maxiter=8) (src/lapack/expert_refinement.jl:45-60):
+ * Hager-Higham estimate of ||A^-1||_1 from solves with the factors of oxi_dgetrf
+ * and with their transpose.  An estimate, not a certified bound. */
+int oxi_dinverse_norm_estimate(oxi_handle_t h, int64_t n, const double *dLU, int64_t lda,
+                               const int64_t *d_ipiv, int maxiter, double *h_estimate);
+/* inv(F) (src/api/linalg_api.jl:1143-1144; OxiBLAS.inv of a dense matrix,
+ * native_inverse, src/lapack/dense_utilities.jl:14-32, factors first): the
+ * n x n inverse from the factors of oxi_dgetrf, as the solve with the
+ * identity, into dAinv (column-major, leading dimension ldainv). */
+int oxi_dgetri(oxi_handle_t h, int64_t n, const double *dLU, int64_t lda, const int64_t *d_ipiv,
+               double *dAinv, int64_t ldainv);
 
 /* Radix equilibration, the first step of the mixed solve, as its own call:
  * equilibrate(A; radix=true) (src/lapack/dense_utilities.jl:191-213).  For the

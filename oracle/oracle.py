@@ -60,6 +60,16 @@ def lib():
                                          ctypes.c_double, ctypes.c_int, _ip, _dp, _dp,
                                          ctypes.POINTER(ctypes.c_int)]
         L.orc_mixed_solve_ex.restype = ctypes.c_int
+        L.orc_inverse_norm_estimate.argtypes = [_i64, _dp, _i64, _ip, _i64]
+        L.orc_inverse_norm_estimate.restype = ctypes.c_double
+        L.orc_refine_solve.argtypes = [_i64, _i64, _dp, _i64, _dp, _i64, _ip, _dp, _i64, _dp, _i64, _i64,
+                                       ctypes.c_double, _dp]
+        L.orc_refine_solve.restype = ctypes.c_int
+        L.orc_expert_solve.argtypes = [_i64, _i64, _dp, _i64, _dp, _i64, _dp, _i64, _i64, ctypes.c_double,
+                                       ctypes.c_int, _dp, _dp, _dp, _ip, _ip, _dp]
+        L.orc_expert_solve.restype = ctypes.c_int
+        L.orc_inverse.argtypes = [_i64, _dp, _i64, _ip, _dp, _i64]
+        L.orc_inverse.restype = ctypes.c_int
         L.orc_lu_adjoint.argtypes = [_i64, _dp, _i64, _ip, _dp, _dp, _dp, _dp, _i64]
         L.orc_lu_adjoint.restype = ctypes.c_int
         for P, fp in (("d", _dp), ("s", _fp)):
@@ -261,3 +271,62 @@ def lu_adjoint(LU, ipiv, x, xbar):
     if rc != 0:
         raise ValueError("oracle adjoint failed")
     return bbar, Abar
+
+
+def inverse_norm_estimate(LU, ipiv, maxiter: int = 8) -> float:
+    """inverse_norm_estimate(F, T, n; maxiter): Hager-Higham ||A^-1||_1 estimate."""
+    LU = np.asfortranarray(LU, dtype=np.float64)
+    n = LU.shape[0]
+    ipiv = np.ascontiguousarray(ipiv, dtype=np.int64)
+    return lib().orc_inverse_norm_estimate(n, _ptr(LU), max(n, 1), _ptr(ipiv, ctypes.c_int64), maxiter)
+
+
+def refine_solve(A, LU, ipiv, b, maxiter: int = 8, rtol: float = 8 * np.finfo(float).eps):
+    """refine_solve(A, F, b; maxiter, rtol) -> the reference's NamedTuple as a dict."""
+    A = np.asfortranarray(A, dtype=np.float64)
+    LU = np.asfortranarray(LU, dtype=np.float64)
+    n = A.shape[0]
+    vec = np.ndim(b) == 1
+    B = np.asfortranarray(np.reshape(b, (n, -1)), dtype=np.float64)
+    nrhs = B.shape[1]
+    X = np.zeros((n, nrhs), order="F")
+    out = np.zeros(6)
+    ipiv = np.ascontiguousarray(ipiv, dtype=np.int64)
+    lib().orc_refine_solve(n, nrhs, _ptr(A), max(n, 1), _ptr(LU), max(n, 1), _ptr(ipiv, ctypes.c_int64), _ptr(B),
+                           max(n, 1), _ptr(X), max(n, 1), maxiter, rtol, _ptr(out))
+    return dict(x=X[:, 0] if vec else X, converged=bool(out[0] <= rtol), iterations=int(out[5]),
+                backward_error=float(out[0]), residual_norm=float(out[1]), rcond_estimate=float(out[2]),
+                forward_error_estimate=float(out[3]), inverse_norm=float(out[4]))
+
+
+def expert_solve(A, b, maxiter: int = 8, rtol: float = 8 * np.finfo(float).eps, equilibrate: bool = True):
+    """expert_solve(A, b; maxiter, rtol, equilibrate) -> dict (x, converged,
+    iterations, backward_error, row_scale, column_scale, factors, ipiv)."""
+    A = np.asfortranarray(A, dtype=np.float64)
+    n = A.shape[0]
+    vec = np.ndim(b) == 1
+    B = np.asfortranarray(np.reshape(b, (n, -1)), dtype=np.float64)
+    nrhs = B.shape[1]
+    X = np.zeros((n, nrhs), order="F")
+    rows, cols = np.ones(n), np.ones(n)
+    F = np.zeros((n, n), order="F")
+    ipiv = np.zeros(max(n, 1), dtype=np.int64)
+    info = np.zeros(1, dtype=np.int64)
+    out = np.zeros(2)
+    rc = lib().orc_expert_solve(n, nrhs, _ptr(A), max(n, 1), _ptr(B), max(n, 1), _ptr(X), max(n, 1), maxiter,
+                                rtol, 1 if equilibrate else 0, _ptr(rows), _ptr(cols), _ptr(F),
+                                _ptr(ipiv, ctypes.c_int64), _ptr(info, ctypes.c_int64), _ptr(out))
+    if rc == 1:
+        raise SingularError(int(info[0]))
+    return dict(x=X[:, 0] if vec else X, converged=bool(out[0] <= rtol), iterations=int(out[1]),
+                backward_error=float(out[0]), row_scale=rows, column_scale=cols, factors=F, ipiv=ipiv[:n].copy())
+
+
+def inverse(LU, ipiv):
+    """inv(F) for LU factors: the solve with the identity."""
+    LU = np.asfortranarray(LU, dtype=np.float64)
+    n = LU.shape[0]
+    X = np.zeros((n, n), order="F")
+    ipiv = np.ascontiguousarray(ipiv, dtype=np.int64)
+    lib().orc_inverse(n, _ptr(LU), max(n, 1), _ptr(ipiv, ctypes.c_int64), _ptr(X), max(n, 1))
+    return X

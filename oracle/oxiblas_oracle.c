@@ -682,3 +682,183 @@ void orc_set_num_threads(int t) {
     (void)t;
 #endif
 }
+
+/* ------------------------------------------------------------------------ */
+/* Expert solves and the condition estimate (FP64)                           */
+/* ------------------------------------------------------------------------ */
+
+/* inverse_norm_estimate(F, T, n; maxiter): src/lapack/expert_refinement.jl:45-60.
+ * Hager-Higham estimate of ||A^-1||_1 from solves with the factors and with
+ * their transpose (_adjoint_solve -> solve_transposed for an LU, :2-23).
+ * Sums run in index order (the reference's sum(abs, y) is a pairwise
+ * reduction; the estimate agrees to rounding). */
+double orc_inverse_norm_estimate(i64 n, const double *LU, i64 lda, const i64 *ipiv, i64 maxiter) {
+    if (n <= 0) return 0.0;
+    double *x = (double *)malloc(sizeof(double) * (size_t)n);
+    double *y = (double *)malloc(sizeof(double) * (size_t)n);
+    double *z = (double *)malloc(sizeof(double) * (size_t)n);
+    for (i64 i = 0; i < n; ++i) x[i] = 1.0 / (double)n;
+    double est = 0.0;
+    i64 prev = -1;
+    for (i64 it = 0; it < maxiter; ++it) {
+        memcpy(y, x, sizeof(double) * (size_t)n);
+        orc_dgetrs('N', n, 1, LU, lda, ipiv, y, n);
+        double next = 0.0;
+        for (i64 i = 0; i < n; ++i) next += fabs(y[i]);
+        if (next > est) est = next;
+        for (i64 i = 0; i < n; ++i) z[i] = (y[i] == 0.0) ? 1.0 : y[i] / fabs(y[i]);
+        orc_dgetrs('T', n, 1, LU, lda, ipiv, z, n);
+        i64 idx = 0;
+        for (i64 i = 1; i < n; ++i)
+            if (fabs(z[i]) > fabs(z[idx])) idx = i;  /* argmax: the first maximum */
+        double dot = 0.0;
+        for (i64 i = 0; i < n; ++i) dot += z[i] * x[i];
+        if (fabs(z[idx]) <= dot) break;
+        if (idx == prev) break;
+        for (i64 i = 0; i < n; ++i) x[i] = 0.0;
+        x[idx] = 1.0;
+        prev = idx;
+    }
+    const double den = (double)(n > 1 ? n - 1 : 1);
+    for (i64 i = 0; i < n; ++i) x[i] = ((i % 2 == 0) ? 1.0 : -1.0) * (1.0 + (double)i / den);
+    orc_dgetrs('N', n, 1, LU, lda, ipiv, x, n);
+    double alt = 0.0;
+    for (i64 i = 0; i < n; ++i) alt += fabs(x[i]);
+    alt = 2.0 * alt / (3.0 * (double)n);
+    free(x); free(y); free(z);
+    return est > alt ? est : alt;
+}
+
+static double one_norm(i64 m, i64 n, const double *A, i64 lda) {
+    double best = 0.0;
+    for (i64 j = 0; j < n; ++j) {
+        double s = 0.0;
+        for (i64 i = 0; i < m; ++i) s += fabs(A[i + j * lda]);
+        if (s > best) best = s;
+    }
+    return best;
+}
+
+/* refine_solve(A, F, b; maxiter, rtol): src/lapack/expert_refinement.jl:89-104.
+ * out[0..5] = backward_error, residual_norm, rcond_estimate,
+ * forward_error_estimate, inverse_norm, iterations. */
+int orc_refine_solve(i64 n, i64 nrhs, const double *A, i64 lda, const double *LU, i64 ldlu, const i64 *ipiv,
+                     const double *B, i64 ldb, double *X, i64 ldx, i64 maxiter, double rtol, double *out) {
+    double *R = (double *)malloc(sizeof(double) * (size_t)n * nrhs);
+    for (i64 j = 0; j < nrhs; ++j)
+        for (i64 i = 0; i < n; ++i) X[i + j * ldx] = B[i + j * ldb];
+    orc_dgetrs('N', n, nrhs, LU, ldlu, ipiv, X, ldx);
+    double err = INFINITY;
+    i64 it = 0;
+    for (i64 iter = 0; iter <= maxiter; ++iter) {
+        err = orc_refinement_residual(n, nrhs, A, lda, X, ldx, B, ldb, R, n);
+        it = iter;
+        if (err <= rtol || iter == maxiter) break;
+        orc_dgetrs('N', n, nrhs, LU, ldlu, ipiv, R, n);  /* correction = solve(F, residual) */
+        for (i64 j = 0; j < nrhs; ++j)
+            for (i64 i = 0; i < n; ++i) X[i + j * ldx] += R[i + j * n];
+        /* the next residual overwrites R */
+    }
+    const double inv_norm = orc_inverse_norm_estimate(n, LU, ldlu, ipiv, 8);
+    const double anorm = one_norm(n, n, A, lda);
+    const double cond = anorm * inv_norm;
+    const double rcond = (cond == 0.0) ? 1.0 : fmin(1.0, 1.0 / cond);
+    double r2 = 0.0;
+    for (i64 e = 0; e < n * nrhs; ++e) r2 += R[e] * R[e];
+    const double rnorm = sqrt(r2);
+    const double xnorm = one_norm(n, nrhs, X, ldx);
+    const double delta = (xnorm == 0.0) ? (rnorm == 0.0 ? 0.0 : INFINITY)
+                                        : inv_norm * one_norm(n, nrhs, R, n) / xnorm;
+    out[0] = err;
+    out[1] = rnorm;
+    out[2] = rcond;
+    out[3] = delta < 1.0 ? delta / (1.0 - delta) : INFINITY;
+    out[4] = inv_norm;
+    out[5] = (double)it;
+    free(R);
+    return 0;
+}
+
+/* expert_solve(A, b; maxiter, rtol, equilibrate): src/lapack/advanced_factorizations.jl:
+ * 591-645.  Row scales (max |a| of each row; a zero row is singular), then
+ * column scales of the row-scaled matrix, partial-pivoted LU of the scaled
+ * matrix, scaled solves and componentwise refinement in the working type.
+ * F (n x n, leading dimension n) and ipiv receive the factorization.
+ * out[0..1] = backward_error, iterations.  Returns 0, or 1 with *info set
+ * (a zero row, or a zero pivot). */
+int orc_expert_solve(i64 n, i64 nrhs, const double *A, i64 lda, const double *B, i64 ldb, double *X, i64 ldx,
+                     i64 maxiter, double rtol, int equilibrate, double *rows, double *cols, double *F,
+                     i64 *ipiv, i64 *info, double *out) {
+    *info = 0;
+    for (i64 j = 0; j < n; ++j)
+        for (i64 i = 0; i < n; ++i) F[i + j * n] = A[i + j * lda];
+    for (i64 i = 0; i < n; ++i) rows[i] = cols[i] = 1.0;
+    if (equilibrate) {
+        for (i64 i = 0; i < n; ++i) {
+            double v = 0.0;
+            for (i64 j = 0; j < n; ++j) v = fmax(v, fabs(F[i + j * n]));
+            if (v == 0.0) { *info = i + 1; return 1; }
+            rows[i] = v;
+            for (i64 j = 0; j < n; ++j) F[i + j * n] /= v;
+        }
+        for (i64 j = 0; j < n; ++j) {
+            double v = 0.0;
+            for (i64 i = 0; i < n; ++i) v = fmax(v, fabs(F[i + j * n]));
+            cols[j] = (v == 0.0) ? 1.0 : v;
+            for (i64 i = 0; i < n; ++i) F[i + j * n] /= cols[j];
+        }
+    }
+    if (orc_dgetrf(n, n, F, n, 128, 1, ipiv, info) != 0) return 1;
+    double *R = (double *)malloc(sizeof(double) * (size_t)n * nrhs);
+    for (i64 j = 0; j < nrhs; ++j)
+        for (i64 i = 0; i < n; ++i) X[i + j * ldx] = B[i + j * ldb] / rows[i];
+    orc_dgetrs('N', n, nrhs, F, n, ipiv, X, ldx);
+    for (i64 j = 0; j < nrhs; ++j)
+        for (i64 i = 0; i < n; ++i) X[i + j * ldx] /= cols[i];
+    double err = INFINITY;
+    i64 it = 0;
+    for (i64 iter = 0; iter <= maxiter; ++iter) {
+        err = 0.0;
+        for (i64 j = 0; j < nrhs; ++j) {
+            double local = 0.0;
+#pragma omp parallel for reduction(max : local) schedule(static) if (n >= 512)
+            for (i64 i = 0; i < n; ++i) {
+                double s = 0.0, den = fabs(B[i + j * ldb]);
+                for (i64 k = 0; k < n; ++k) {
+                    s += A[i + k * lda] * X[k + j * ldx];
+                    den += fabs(A[i + k * lda]) * fabs(X[k + j * ldx]);
+                }
+                const double r = B[i + j * ldb] - s;
+                R[i + j * n] = r;
+                double e;
+                if (!isfinite(den)) e = INFINITY;
+                else if (den == 0.0) e = (r == 0.0) ? 0.0 : INFINITY;
+                else e = fabs(r) / den;
+                if (e > local || isnan(e)) local = e;
+            }
+            if (local > err || isnan(local)) err = local;
+        }
+        it = iter;
+        if (err <= rtol) break;
+        if (iter == maxiter) break;
+        for (i64 j = 0; j < nrhs; ++j)
+            for (i64 i = 0; i < n; ++i) R[i + j * n] /= rows[i];
+        orc_dgetrs('N', n, nrhs, F, n, ipiv, R, n);
+        for (i64 j = 0; j < nrhs; ++j)
+            for (i64 i = 0; i < n; ++i) X[i + j * ldx] += R[i + j * n] / cols[i];
+    }
+    out[0] = err;
+    out[1] = (double)it;
+    free(R);
+    return 0;
+}
+
+/* native_inverse(A) (src/lapack/dense_utilities.jl:14-32) for the engine's
+ * factors: inv(A) = U^-1 L^-1 P.  Restated as the solve with the identity
+ * (the columns of the inverse are A^-1 e_j), which is what LinearAlgebra's
+ * inv(F) does for an OxiBLAS factorization (src/api/linalg_api.jl:1143-1144). */
+int orc_inverse(i64 n, const double *LU, i64 lda, const i64 *ipiv, double *X, i64 ldx) {
+    for (i64 j = 0; j < n; ++j)
+        for (i64 i = 0; i < n; ++i) X[i + j * ldx] = (i == j) ? 1.0 : 0.0;
+    return orc_dgetrs('N', n, n, LU, lda, ipiv, X, ldx);
+}

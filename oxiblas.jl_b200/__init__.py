@@ -12,6 +12,7 @@ from .lu import (LU, colmajor_copy, det, gemm_update, ldiv, ldiv_, ldiv_into, lo
                  options)
 from .mixed import equilibrate, gemm_update_lowp, mixed_solve, mixed_solve_device
 from .adjoint import lu_adjoint, solve
+from .expert import expert_solve, factorize, inv, inverse_norm_estimate, refine_solve
 from .batched import BatchedLU, autotune as batched_autotune, set_tuning as batched_set_tuning, \
     tuning as batched_tuning
 from . import synthetic
@@ -20,6 +21,6 @@ __all__ = [
     "LU", "lu", "lu_", "ldiv", "ldiv_", "ldiv_into", "det", "logabsdet", "gemm_update", "options",
     "colmajor_copy", "SingularException", "DimensionMismatch", "ArgumentError", "ExtensionMissing",
     "Handle", "load", "exported_symbols", "mixed_solve", "mixed_solve_device", "gemm_update_lowp",
-    "equilibrate",
+    "equilibrate", "expert_solve", "refine_solve", "inverse_norm_estimate", "inv", "factorize",
     "lu_adjoint", "solve", "BatchedLU", "batched_autotune", "batched_tuning", "batched_set_tuning",
 ]

@@ -63,6 +63,7 @@ _SIGS = {
     "oxi_dgetrs_noalloc": ([_vp, ctypes.c_char, _i64, _i64, _vp, _i64, _vp, _vp, _i64], ctypes.c_int),
     "oxi_dlu_adjoint": ([_vp, _i64, _i64, _vp, _i64, _vp, _vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64],
                         ctypes.c_int),
+    "oxi_dlu_adjoint_batched_uneven": ([_vp, _i64] + [_vp] * 14, ctypes.c_int),
     "oxi_dgetrf_batched_uneven": ([_vp, _i64, _vp, _vp, _vp, _vp, _vp], ctypes.c_int),
     "oxi_dgesv_batched_uneven": ([_vp, ctypes.c_int, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                   _vp, _vp, ctypes.c_int, ctypes.c_double], ctypes.c_int),
@@ -80,6 +81,13 @@ _SIGS = {
                           ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
     "oxi_launch_count": ([_vp, ctypes.POINTER(_i64)], ctypes.c_int),
     "oxi_launch_count_reset": ([_vp], ctypes.c_int),
+    "oxi_dexpert_solve": ([_vp, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64, ctypes.c_int, ctypes.c_double,
+                           ctypes.c_int, _vp, _vp, _vp, _i64, _vp, _vp], ctypes.c_int),
+    "oxi_drefine_solve": ([_vp, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _vp, _i64, _vp, _i64, ctypes.c_int,
+                           ctypes.c_double, _vp], ctypes.c_int),
+    "oxi_dinverse_norm_estimate": ([_vp, _i64, _vp, _i64, _vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)],
+                                   ctypes.c_int),
+    "oxi_dgetri": ([_vp, _i64, _vp, _i64, _vp, _vp, _i64], ctypes.c_int),
     "oxi_dequilibrate": ([_vp, _i64, _i64, _vp, _i64, _vp, _vp, _vp, _i64], ctypes.c_int),
     "oxi_dgesv_mixed": ([_vp, ctypes.c_int, ctypes.c_int, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64,
                          ctypes.c_int, ctypes.c_double, _vp], ctypes.c_int),

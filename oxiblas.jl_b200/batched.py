@@ -4,6 +4,7 @@
     P.load(As, Bs)                     copy the matrices / right-hand sides in
     info = P.getrf()                   every A_i -> its LU factors (in place)
     X, rep = P.gesv(prec="fp64"|"fp32", maxiter=10, rtol=1e-13)
+    P.adjoint(xbars)                   pullback of every X_i = A_i \\ B_i: Bbar(i), Abar(i)
     autotune(orders, prec, nrhs)       pick panel widths / shared-memory threshold
 
 Each problem is exactly lu(A_i) / ldiv!(F_i, B_i) of the reference
@@ -141,6 +142,62 @@ class BatchedLU:
 
     def solution(self, i, prec="fp64"):
         return self.B(i) if prec == "fp64" else self.X(i)
+
+    # ---- adjoint of X_i = A_i \ B_i with the stored FP64 factors ----
+    def _adjoint_pools(self):
+        if not hasattr(self, "poolXbar"):
+            self.poolXbar = torch.zeros_like(self.poolB)
+            self.poolBbar = torch.zeros_like(self.poolB)
+            self.poolAbar = torch.zeros_like(self.poolA)
+            base = lambda t, off: torch.from_numpy(
+                np.ascontiguousarray(t.data_ptr() + 8 * off[:-1], dtype=np.int64)).to(self.dev)
+            self.d_Xbar = base(self.poolXbar, self._offB)
+            self.d_Bbar = base(self.poolBbar, self._offB)
+            self.d_Abar = base(self.poolAbar, self._offA)
+            self.d_adj_info = torch.zeros(self.count, dtype=torch.int32, device=self.dev)
+
+    def Xbar(self, i):
+        self._adjoint_pools()
+        n, k = int(self.orders[i]), int(self.nrhs[i])
+        return self.poolXbar[self._offB[i]:self._offB[i] + n * k].view(k, n).t()
+
+    def Bbar(self, i):
+        self._adjoint_pools()
+        n, k = int(self.orders[i]), int(self.nrhs[i])
+        return self.poolBbar[self._offB[i]:self._offB[i] + n * k].view(k, n).t()
+
+    def Abar(self, i):
+        self._adjoint_pools()
+        n = int(self.orders[i])
+        return self.poolAbar[self._offA[i]:self._offA[i] + n * n].view(n, n).t()
+
+    def adjoint(self, xbars=None, solution="B", check=True):
+        """Pullback of every X_i = A_i \\ B_i (the rrule's bbar, Abar) with the
+        FP64 factors left in the A pool by getrf() / gesv("fp64").  xbars: the
+        upstream gradients (None: the Xbar pool as already filled); the
+        solutions X_i are the B pool after gesv("fp64") (solution="B") or the X
+        pool (solution="X").  Results: Bbar(i), Abar(i); returns the info vector."""
+        self._adjoint_pools()
+        if xbars is not None:
+            if len(xbars) != self.count:
+                raise DimensionMismatch("one upstream gradient per problem expected")
+            for i, xb in enumerate(xbars):
+                t = torch.as_tensor(xb, dtype=torch.float64).reshape(int(self.orders[i]), -1)
+                self.Xbar(i).copy_(t)
+        d_x = self.d_B if solution == "B" else self.d_X
+        h = Handle.get()
+        st = h.lib.oxi_dlu_adjoint_batched_uneven(h.ptr, self.count, _vp(self.d_n), _vp(self.d_nrhs),
+                                                  _vp(self.d_A), _vp(self.d_ld), _vp(self.d_P), _vp(d_x),
+                                                  _vp(self.d_ld), _vp(self.d_Xbar), _vp(self.d_ld),
+                                                  _vp(self.d_Bbar), _vp(self.d_ld), _vp(self.d_Abar),
+                                                  _vp(self.d_ld), _vp(self.d_adj_info))
+        info = self.d_adj_info.cpu().numpy()
+        if st == OXI_ESINGULAR:
+            if check:
+                raise SingularException(int(info[info > 0][0]))
+        else:
+            h.check(st)
+        return info
 
 
 def autotune(orders, prec="fp64", nrhs=4):

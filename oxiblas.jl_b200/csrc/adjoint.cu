@@ -152,3 +152,172 @@ extern "C" int oxi_dlu_adjoint(oxi_handle_t h, int64_t n, int64_t nrhs, const do
         return OXI_ECUDA;
     }
 }
+
+// ---------------------------------------------------------------------------
+// Batched adjoint: the same rule for many independent small factorizations
+// (the stored factors of oxi_dgetrf_batched_uneven / oxi_dgesv_batched_uneven),
+// one CTA per problem.  Per problem i (order n <= 256, k <= 8 right-hand sides):
+//   Bbar = A^-T Xbar  -- U^T W = Xbar (forward), L^T V = W (backward, unit
+//                        diagonal), Bbar = the interchanges undone in reverse
+//                        order (as ldiv!(transpose(F), B), src/api/linalg_api.jl:
+//                        176-184);
+//   Abar = -Bbar X^T  -- n x n, written once, coalesced down the columns.
+// Each right-hand side's two substitutions run on one warp: step i reads the
+// contiguous column i of the factors (coalesced), reduces it against the
+// solved entries across the warp, and the lane that owns row i finishes it.
+// ---------------------------------------------------------------------------
+namespace oxi {
+namespace {
+constexpr int BADJ_NT = 256, BADJ_NMAX = 256, BADJ_KMAX = 8;
+}
+
+struct BatchAdjDesc {
+    int count;
+    const int32_t *n, *nrhs;
+    double *const *LU;
+    const int64_t *ldlu;
+    int64_t *const *ipiv;
+    double *const *X;
+    const int64_t *ldx;
+    double *const *Xbar;
+    const int64_t *ldxbar;
+    double *const *Bbar;
+    const int64_t *ldbbar;
+    double *const *Abar;
+    const int64_t *ldabar;
+    int32_t *info;
+    int *status;  // [0] invalid problems, [1] singular ones
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    return v;
+}
+
+__global__ void __launch_bounds__(BADJ_NT) k_lu_adjoint_batched(const __grid_constant__ BatchAdjDesc d) {
+    __shared__ double s_w[BADJ_KMAX][BADJ_NMAX];  // Xbar -> W -> V -> Bbar, per right-hand side
+    __shared__ double s_x[BADJ_KMAX][BADJ_NMAX];  // X
+    __shared__ int s_bad;
+    const int pi = blockIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int n = d.n[pi], k = d.nrhs ? d.nrhs[pi] : 1;
+    const double *LU = d.LU[pi];
+    const i64 ld = d.ldlu[pi], ldx = d.ldx[pi], ldxb = d.ldxbar[pi], ldbb = d.ldbbar[pi], ldab = d.ldabar[pi];
+    const bool bad = n < 0 || n > BADJ_NMAX || k < 0 || k > BADJ_KMAX || (n > 0 && (!LU || !d.ipiv[pi] || !d.Abar[pi])) ||
+                     (n > 0 && k > 0 && (!d.X[pi] || !d.Xbar[pi] || !d.Bbar[pi])) || (n > 0 && (ld < n || ldab < n)) ||
+                     (n > 0 && k > 0 && (ldx < n || ldxb < n || ldbb < n));
+    if (bad) {
+        if (tid == 0) {
+            d.info[pi] = -1;
+            atomicAdd(&d.status[0], 1);
+        }
+        return;
+    }
+    if (tid == 0) s_bad = 0;
+    if (n == 0) {
+        if (tid == 0) d.info[pi] = 0;
+        return;
+    }
+    const double *Xb = d.Xbar[pi], *X = d.X[pi];
+    for (int e = tid; e < n * k; e += BADJ_NT) {
+        const int i = e % n, r = e / n;
+        s_w[r][i] = Xb[i + (i64)r * ldxb];
+        s_x[r][i] = X[i + (i64)r * ldx];
+    }
+    __syncthreads();
+    if (warp < k) {
+        double *w = s_w[warp];
+        // U^T W = Xbar: w_i = (xbar_i - sum_{p<i} U[p,i] w_p) / U[i,i]
+        for (int i = 0; i < n; ++i) {
+            const double *col = LU + (i64)i * ld;
+            double acc = 0.0;
+            for (int p = lane; p < i; p += 32) acc = fma(col[p], w[p], acc);
+            acc = warp_sum(acc);
+            if (lane == 0) {
+                const double u = col[i];
+                if (u == 0.0) s_bad = i + 1;
+                w[i] = (w[i] - acc) / u;
+            }
+            __syncwarp();
+        }
+        // L^T V = W (unit): v_i = w_i - sum_{p>i} L[p,i] v_p
+        for (int i = n - 1; i >= 0; --i) {
+            const double *col = LU + (i64)i * ld;
+            double acc = 0.0;
+            for (int p = i + 1 + lane; p < n; p += 32) acc = fma(col[p], w[p], acc);
+            acc = warp_sum(acc);
+            if (lane == 0) w[i] -= acc;
+            __syncwarp();
+        }
+        // the interchanges undone in reverse order
+        if (lane == 0) {
+            const int64_t *ip = d.ipiv[pi];
+            for (int j = n - 1; j >= 0; --j) {
+                const int q = (int)ip[j] - 1;
+                if (q != j && q >= 0 && q < n) {
+                    const double t = w[j];
+                    w[j] = w[q];
+                    w[q] = t;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    double *Bb = d.Bbar[pi];
+    for (int e = tid; e < n * k; e += BADJ_NT) {
+        const int i = e % n, r = e / n;
+        Bb[i + (i64)r * ldbb] = s_w[r][i];
+    }
+    double *Ab = d.Abar[pi];
+    for (int e = tid; e < n * n; e += BADJ_NT) {
+        const int i = e % n, j = e / n;
+        double v = 0.0;
+        for (int r = 0; r < k; ++r) v = fma(s_w[r][i], s_x[r][j], v);
+        Ab[i + (i64)j * ldab] = -v;
+    }
+    if (tid == 0) {
+        d.info[pi] = s_bad;
+        if (s_bad) atomicAdd(&d.status[1], 1);
+    }
+}
+
+}  // namespace oxi
+
+extern "C" int oxi_dlu_adjoint_batched_uneven(oxi_handle_t h, int64_t count, const int32_t *d_n,
+                                              const int32_t *d_nrhs, double *const *d_LU, const int64_t *d_ldlu,
+                                              int64_t *const *d_ipiv, double *const *d_X, const int64_t *d_ldx,
+                                              double *const *d_Xbar, const int64_t *d_ldxbar,
+                                              double *const *d_Bbar, const int64_t *d_ldbbar,
+                                              double *const *d_Abar, const int64_t *d_ldabar, int32_t *d_info) {
+    using namespace oxi;
+    if (!h || count < 0 || count >= (1ll << 31)) return OXI_EINVAL;
+    if (count == 0) return OXI_OK;
+    if (!d_n || !d_LU || !d_ldlu || !d_ipiv || !d_X || !d_ldx || !d_Xbar || !d_ldxbar || !d_Bbar || !d_ldbbar ||
+        !d_Abar || !d_ldabar || !d_info)
+        return OXI_EINVAL;
+    try {
+        ProfGuard pg(&h->prof);
+        OXI_CUDA(cudaSetDevice(h->device));
+        AbortScope ab(h);
+        int *status = (int *)((char *)h->scratch.get(kScratchBytes) + kScratchErrOff + 64);
+        OXI_CUDA(cudaMemsetAsync(status, 0, 2 * sizeof(int), h->stream));
+        BatchAdjDesc d{(int)count, d_n, d_nrhs, d_LU, d_ldlu, d_ipiv, d_X, d_ldx, d_Xbar, d_ldxbar,
+                       d_Bbar, d_ldbbar, d_Abar, d_ldabar, d_info, status};
+        {
+            ProfScope ps(KC_OTHER, h->stream, 0.0, 0.0);
+            k_lu_adjoint_batched<<<(unsigned)count, BADJ_NT, 0, h->stream>>>(d);
+            OXI_LAUNCH_CHECK();
+        }
+        int *hs = (int *)h->host_ws.get(64);
+        OXI_CUDA(cudaMemcpyAsync(hs, status, 2 * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+        queue_abort_read(h, hs + 4);
+        OXI_CUDA(cudaStreamSynchronize(h->stream));
+        const int we = check_abort(h, hs + 4);
+        if (we != OXI_OK) return we;
+        if (hs[0]) return OXI_EINVAL;
+        return hs[1] ? OXI_ESINGULAR : OXI_OK;
+    } catch (const CudaError &e) {
+        h->last_error = std::string(e.what) + ": " + cudaGetErrorString(e.code);
+        return OXI_ECUDA;
+    }
+}

@@ -66,9 +66,13 @@ __global__ void k_row_stats_part(const double *__restrict__ A, i64 lda, int m, i
     if (bad) atomicExch(nonfinite, 1);
 }
 
+// Row scales: radix = 1 (mixed_solve): the power of two nearest each row's
+// max |a|, 1 for a zero row; radix = 0 (expert_solve): the max itself, and a
+// zero row recorded in *zero_row (the smallest 1-based index; the reference
+// throws SingularException for it).
 __global__ void k_row_stats_final(const double *__restrict__ pmax, const double *__restrict__ psum,
                                   int n, int parts, double *__restrict__ rows,
-                                  double *__restrict__ anorm) {
+                                  double *__restrict__ anorm, int radix = 1, int *__restrict__ zero_row = nullptr) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double mx = 0.0, sm = 0.0;
@@ -76,12 +80,14 @@ __global__ void k_row_stats_final(const double *__restrict__ pmax, const double 
         mx = fmax(mx, pmax[(i64)s * n + i]);
         sm += psum[(i64)s * n + i];
     }
-    rows[i] = mx > 0.0 ? radix_scale(mx) : 1.0;
+    if (radix) rows[i] = mx > 0.0 ? radix_scale(mx) : 1.0;
+    else rows[i] = mx > 0.0 ? mx : 1.0;
+    if (!(mx > 0.0) && zero_row) atomicMin(zero_row, i + 1);
     atomic_max_nonneg(anorm, sm);
 }
 
 __global__ void k_col_scale(const double *__restrict__ A, i64 lda, int m,
-                            const double *__restrict__ rows, double *__restrict__ cols) {
+                            const double *__restrict__ rows, double *__restrict__ cols, int radix = 1) {
     const int j = blockIdx.x;
     double mx = 0.0;
     for (int i = threadIdx.x; i < m; i += blockDim.x) mx = fmax(mx, fabs(A[i + (i64)j * lda]) / rows[i]);
@@ -92,7 +98,7 @@ __global__ void k_col_scale(const double *__restrict__ A, i64 lda, int m,
     if (threadIdx.x < 32) {
         mx = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
         for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
-        if (threadIdx.x == 0) cols[j] = mx > 0.0 ? radix_scale(mx) : 1.0;
+        if (threadIdx.x == 0) cols[j] = mx > 0.0 ? (radix ? radix_scale(mx) : mx) : 1.0;
     }
 }
 
@@ -124,6 +130,17 @@ __global__ void k_equilibrated_cm(const double *__restrict__ A, i64 lda, double 
     if (idx >= (i64)m * n) return;
     const int i = (int)(idx % m), j = (int)(idx / m);
     E[i + (i64)j * lde] = (A[i + (i64)j * lda] / rows[i]) / cols[j];
+}
+
+// column j of the n x n identity (grid: row blocks x columns)
+__global__ void k_identity(double *__restrict__ X, i64 ldx, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+    if (i < n) X[i + (i64)j * ldx] = (i == j) ? 1.0 : 0.0;
+}
+
+__global__ void k_fill(double *__restrict__ v, int n, double x) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = x;
 }
 
 __global__ void k_check_finite(const double *__restrict__ B, i64 ldb, int n, int nrhs, int *flag) {
@@ -556,9 +573,26 @@ static int gmres_correction(MixedRun &M, const double *r, double *x, double tol,
     return iters;
 }
 
+// expert_solve's differences from mixed_solve (src/lapack/advanced_factorizations.jl:
+// 591-645): scales are the row and column maxima themselves (not powers of two),
+// a zero row is singular, the factor is FP64, the stop test componentwise, and
+// the scales and the factorization go back to the caller.
+struct ExpertOpts {
+    int equilibrate = 1;
+    double *rows_out = nullptr, *cols_out = nullptr;  // device, n each (nullable)
+    double *F_out = nullptr;                           // device, column-major n x n (nullable)
+    i64 ldf = 0;
+    int64_t *ipiv_out = nullptr;                       // device, n (nullable)
+    int64_t zero_row = 0;                              // out: first zero row (1-based), 0 if none
+};
+
 static int dgesv_mixed(oxi_handle_s *h, int prec, int refine, i64 n, i64 nrhs, const double *dA,
                        i64 lda, const double *dB, i64 ldb, double *dX, i64 ldx, int maxiter, double rtol,
-                       oxi_refine_report *out) {
+                       oxi_refine_report *out, ExpertOpts *xo = nullptr) {
+    if (xo) {
+        prec = OXI_PREC_FP64;
+        refine = OXI_REFINE_IR;
+    }
     cudaStream_t s = h->stream;
     MixedRun M;
     M.h = h; M.s = s; M.n = n; M.nrhs = nrhs; M.A = dA; M.lda = lda; M.B = dB; M.ldb = ldb;
@@ -619,16 +653,37 @@ static int dgesv_mixed(oxi_handle_s *h, int prec, int refine, i64 n, i64 nrhs, c
         k_check_finite<<<blocks_for(n * nrhs), 256, 0, s>>>(dB, ldb, (int)n, (int)nrhs, nonfinite);
         OXI_LAUNCH_CHECK();
         OXI_CUDA(cudaMemsetAsync(M.scal, 0, sizeof(double) * 128, s));
-        k_row_stats_final<<<blocks_for(n), 256, 0, s>>>(M.pmax, M.psum, (int)n, RS, M.rows, M.scal);
+        const int radix = xo ? 0 : 1;
+        int *zrow = (int *)(M.scal + 120);
+        if (xo) {
+            const int big = 0x7fffffff;
+            OXI_CUDA(cudaMemcpyAsync(zrow, &big, sizeof(int), cudaMemcpyHostToDevice, s));
+        }
+        k_row_stats_final<<<blocks_for(n), 256, 0, s>>>(M.pmax, M.psum, (int)n, RS, M.rows, M.scal, radix,
+                                                         xo ? zrow : nullptr);
         OXI_LAUNCH_CHECK();
-        k_col_scale<<<(unsigned)n, 256, 0, s>>>(dA, lda, (int)n, M.rows, M.cols);
+        k_col_scale<<<(unsigned)n, 256, 0, s>>>(dA, lda, (int)n, M.rows, M.cols, radix);
         OXI_LAUNCH_CHECK();
         int *hflag = (int *)(M.hsc + 300);
         OXI_CUDA(cudaMemcpyAsync(hflag, nonfinite, sizeof(int), cudaMemcpyDeviceToHost, s));
         OXI_CUDA(cudaMemcpyAsync(M.hsc + 301, M.scal, sizeof(double), cudaMemcpyDeviceToHost, s));
+        if (xo) OXI_CUDA(cudaMemcpyAsync(hflag + 1, zrow, sizeof(int), cudaMemcpyDeviceToHost, s));
         OXI_CUDA(cudaStreamSynchronize(s));
         if (hflag[0]) return OXI_ENONFINITE;
         M.anorm = M.hsc[301];
+        if (xo) {
+            if (xo->equilibrate && hflag[1] != 0x7fffffff) {  // a zero row: SingularException(i)
+                xo->zero_row = hflag[1];
+                if (out) out->info = hflag[1];
+                return OXI_ESINGULAR;
+            }
+            if (!xo->equilibrate) {  // unscaled: both scale vectors are ones
+                k_fill<<<blocks_for(n), 256, 0, s>>>(M.rows, (int)n, 1.0);
+                OXI_LAUNCH_CHECK();
+                k_fill<<<blocks_for(n), 256, 0, s>>>(M.cols, (int)n, 1.0);
+                OXI_LAUNCH_CHECK();
+            }
+        }
     }
 
     // ---- 3. low-precision factorization ----
@@ -696,6 +751,15 @@ static int dgesv_mixed(oxi_handle_s *h, int prec, int refine, i64 n, i64 nrhs, c
     }
     if (out) out->info = low_info;
     if (info != 0) return OXI_ESINGULAR;
+    if (xo) {  // the scales and the factorization of the scaled matrix
+        if (xo->rows_out)
+            OXI_CUDA(cudaMemcpyAsync(xo->rows_out, M.rows, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+        if (xo->cols_out)
+            OXI_CUDA(cudaMemcpyAsync(xo->cols_out, M.cols, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+        if (xo->ipiv_out)
+            OXI_CUDA(cudaMemcpyAsync(xo->ipiv_out, M.ipiv, sizeof(int64_t) * n, cudaMemcpyDeviceToDevice, s));
+        if (xo->F_out) launch_rm_to_cm<double, double>((const double *)M.W, ldw, xo->F_out, xo->ldf, n, n, s);
+    }
     OXI_CUDA(cudaEventRecord(e1, s));
 
     // ---- 4-5. first solve and refinement ----
@@ -721,7 +785,7 @@ static int dgesv_mixed(oxi_handle_s *h, int prec, int refine, i64 n, i64 nrhs, c
     i64 gm_total = 0;
     bool use_gmres = (refine == OXI_REFINE_GMRES);
     int refine_used = use_gmres ? OXI_REFINE_GMRES : OXI_REFINE_IR;
-    const bool stop_nw = h->opt.stop_normwise != 0;
+    const bool stop_nw = h->opt.stop_normwise != 0 && !xo;
     for (int iter = 0; iter <= maxiter; ++iter) {
         residual(M, dX, M.R, cw, nw, r2);
         double ecw = 0, enw = 0;
@@ -854,6 +918,353 @@ extern "C" int oxi_dequilibrate(oxi_handle_t h, int64_t m, int64_t n, const doub
         OXI_CUDA(cudaMemcpyAsync(hflag, nonfinite, sizeof(int), cudaMemcpyDeviceToHost, s));
         OXI_CUDA(cudaStreamSynchronize(s));
         return hflag[0] ? OXI_ENONFINITE : OXI_OK;
+    } catch (const CudaError &e) {
+        h->last_error = std::string(e.what) + ": " + cudaGetErrorString(e.code);
+        return OXI_ECUDA;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// expert_solve, refine_solve, inverse_norm_estimate and the inverse
+// ---------------------------------------------------------------------------
+namespace oxi {
+
+// One CTA: out[0] = sum |v|, out[1] = max |v|, out[2] = its first index,
+// out[3] = v . x (x nullable).
+__global__ void __launch_bounds__(1024) k_vec_stats(const double *__restrict__ v, const double *__restrict__ x,
+                                                    int n, double *__restrict__ out) {
+    __shared__ double s_sum[32], s_dot[32], s_max[32];
+    __shared__ int s_idx[32];
+    double sm = 0.0, dt = 0.0, mx = -1.0;
+    int ix = 0x7fffffff;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double a = fabs(v[i]);
+        sm += a;
+        if (x) dt += v[i] * x[i];
+        if (a > mx) { mx = a; ix = i; }  // i ascends per thread: the first maximum
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        sm += __shfl_xor_sync(0xffffffffu, sm, off);
+        dt += __shfl_xor_sync(0xffffffffu, dt, off);
+        const double om = __shfl_xor_sync(0xffffffffu, mx, off);
+        const int oi = __shfl_xor_sync(0xffffffffu, ix, off);
+        if (om > mx || (om == mx && oi < ix)) { mx = om; ix = oi; }
+    }
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) { s_sum[w] = sm; s_dot[w] = dt; s_max[w] = mx; s_idx[w] = ix; }
+    __syncthreads();
+    if (w == 0) {
+        const int nw = blockDim.x >> 5;
+        sm = lane < nw ? s_sum[lane] : 0.0;
+        dt = lane < nw ? s_dot[lane] : 0.0;
+        mx = lane < nw ? s_max[lane] : -1.0;
+        ix = lane < nw ? s_idx[lane] : 0x7fffffff;
+        for (int off = 16; off > 0; off >>= 1) {
+            sm += __shfl_xor_sync(0xffffffffu, sm, off);
+            dt += __shfl_xor_sync(0xffffffffu, dt, off);
+            const double om = __shfl_xor_sync(0xffffffffu, mx, off);
+            const int oi = __shfl_xor_sync(0xffffffffu, ix, off);
+            if (om > mx || (om == mx && oi < ix)) { mx = om; ix = oi; }
+        }
+        if (lane == 0) { out[0] = sm; out[1] = mx; out[2] = (double)ix; out[3] = dt; }
+    }
+}
+
+// z = sign(y) with sign(0) = 1 (value / abs(value), the reference's signs)
+__global__ void k_signs(const double *__restrict__ y, double *__restrict__ z, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) z[i] = (y[i] == 0.0) ? 1.0 : y[i] / fabs(y[i]);
+}
+// x = e_idx
+__global__ void k_unit(double *__restrict__ x, int n, int idx) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] = (i == idx) ? 1.0 : 0.0;
+}
+// x_i = (-1)^i (1 + i / max(1, n - 1)), 0-based i: the final probe vector
+__global__ void k_alt_probe(double *__restrict__ x, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] = ((i & 1) ? -1.0 : 1.0) * (1.0 + (double)i / (double)(n > 1 ? n - 1 : 1));
+}
+// max_j sum_i |A[i, j]| (column-major m x n), one CTA per column
+__global__ void __launch_bounds__(256) k_one_norm(const double *__restrict__ A, i64 lda, int m,
+                                                  double *__restrict__ out) {
+    const int j = blockIdx.x;
+    double sm = 0.0;
+    for (int i = threadIdx.x; i < m; i += blockDim.x) sm += fabs(A[i + (i64)j * lda]);
+    __shared__ double red[8];
+    for (int off = 16; off > 0; off >>= 1) sm += __shfl_xor_sync(0xffffffffu, sm, off);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = sm;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < 8; ++w) t += red[w];
+        atomic_max_nonneg(out, t);
+    }
+}
+
+// 0-based permutation of the factors' ipiv, uploaded into the handle's perm
+// workspace (validating every entry): OXI_OK or OXI_EINVAL.
+static int upload_perm(oxi_handle_s *h, i64 n, const int64_t *d_ipiv, int64_t **dperm_out) {
+    std::vector<int64_t> ip(n), perm(n);
+    OXI_CUDA(cudaMemcpyAsync(ip.data(), d_ipiv, sizeof(int64_t) * n, cudaMemcpyDeviceToHost, h->stream));
+    OXI_CUDA(cudaStreamSynchronize(h->stream));
+    for (i64 j = 0; j < n; ++j)
+        if (ip[j] < 1 || ip[j] > n) return OXI_EINVAL;
+    perm_from_ipiv(ip.data(), n, n, perm.data());
+    int64_t *dperm = (int64_t *)h->perm_ws.get(sizeof(int64_t) * n);
+    int64_t *hperm = (int64_t *)h->host_ws.get(sizeof(int64_t) * (n + 64));
+    std::copy(perm.begin(), perm.end(), hperm);
+    OXI_CUDA(cudaMemcpyAsync(dperm, hperm, sizeof(int64_t) * n, cudaMemcpyHostToDevice, h->stream));
+    OXI_CUDA(cudaStreamSynchronize(h->stream));
+    *dperm_out = dperm;
+    return OXI_OK;
+}
+
+// inverse_norm_estimate (src/lapack/expert_refinement.jl:45-60): Hager-Higham
+// with solves by the factors (trans 'N') and their transpose ('T'); the
+// decisions (stop tests, next unit vector) are taken on the host from one
+// reduction per solve.  ws: 3n + 8 doubles of device memory.
+static double inverse_norm_est(oxi_handle_s *h, i64 n, const double *LU, i64 lda, const int64_t *dperm,
+                               int maxiter, double *ws, int *ab) {
+    cudaStream_t s = h->stream;
+    double *x = ws, *y = ws + n, *z = ws + 2 * n, *st = ws + 3 * n;
+    double *hs = (double *)h->host_ws.get(sizeof(double) * 64) + 32;
+    const unsigned gb = blocks_for(n);
+    k_fill<<<gb, 256, 0, s>>>(x, (int)n, 1.0 / (double)n);
+    OXI_LAUNCH_CHECK();
+    double est = 0.0;
+    long prev = -1;
+    for (int it = 0; it < maxiter; ++it) {
+        OXI_CUDA(cudaMemcpyAsync(y, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+        getrs_perm<double>(h, 'N', n, 1, LU, lda, dperm, y, n, ab);
+        k_signs<<<gb, 256, 0, s>>>(y, z, (int)n);
+        OXI_LAUNCH_CHECK();
+        k_vec_stats<<<1, 1024, 0, s>>>(y, nullptr, (int)n, st);
+        OXI_LAUNCH_CHECK();
+        getrs_perm<double>(h, 'T', n, 1, LU, lda, dperm, z, n, ab);
+        k_vec_stats<<<1, 1024, 0, s>>>(z, x, (int)n, st + 4);
+        OXI_LAUNCH_CHECK();
+        OXI_CUDA(cudaMemcpyAsync(hs, st, sizeof(double) * 8, cudaMemcpyDeviceToHost, s));
+        OXI_CUDA(cudaStreamSynchronize(s));
+        est = std::max(est, hs[0]);
+        const long idx = (long)hs[6];
+        if (hs[5] <= hs[7]) break;  // |z[idx]| <= z . x
+        if (idx == prev) break;
+        k_unit<<<gb, 256, 0, s>>>(x, (int)n, (int)idx);
+        OXI_LAUNCH_CHECK();
+        prev = idx;
+    }
+    k_alt_probe<<<gb, 256, 0, s>>>(x, (int)n);
+    OXI_LAUNCH_CHECK();
+    getrs_perm<double>(h, 'N', n, 1, LU, lda, dperm, x, n, ab);
+    k_vec_stats<<<1, 1024, 0, s>>>(x, nullptr, (int)n, st);
+    OXI_LAUNCH_CHECK();
+    OXI_CUDA(cudaMemcpyAsync(hs, st, sizeof(double), cudaMemcpyDeviceToHost, s));
+    OXI_CUDA(cudaStreamSynchronize(s));
+    return std::max(est, 2.0 * hs[0] / (3.0 * (double)n));
+}
+
+}  // namespace oxi
+
+extern "C" int oxi_dinverse_norm_estimate(oxi_handle_t h, int64_t n, const double *dLU, int64_t lda,
+                                          const int64_t *d_ipiv, int maxiter, double *h_estimate) {
+    using namespace oxi;
+    if (!h || !h_estimate || n < 0 || maxiter < 1 || lda < std::max<int64_t>(1, n)) return OXI_EINVAL;
+    *h_estimate = 0.0;
+    if (n == 0) return OXI_OK;
+    if (!dLU || !d_ipiv || n >= (1ll << 31)) return OXI_EINVAL;
+    try {
+        ProfGuard pg(&h->prof);
+        OXI_CUDA(cudaSetDevice(h->device));
+        AbortScope ab(h);
+        int64_t *dperm = nullptr;
+        if (upload_perm(h, n, d_ipiv, &dperm) != OXI_OK) return OXI_EINVAL;
+        double *ws = (double *)h->mixed_ws.get(sizeof(double) * (3 * (size_t)n + 8));
+        const double est = inverse_norm_est(h, n, dLU, lda, dperm, maxiter, ws, ab.word);
+        int *he = (int *)h->host_ws.get(64);
+        queue_abort_read(h, he);
+        OXI_CUDA(cudaStreamSynchronize(h->stream));
+        const int st = check_abort(h, he);
+        if (st == OXI_OK) *h_estimate = est;
+        return st;
+    } catch (const CudaError &e) {
+        h->last_error = std::string(e.what) + ": " + cudaGetErrorString(e.code);
+        return OXI_ECUDA;
+    }
+}
+
+// refine_solve(A, F, b; maxiter, rtol) (src/lapack/expert_refinement.jl:89-104)
+// with the factors of oxi_dgetrf.
+extern "C" int oxi_drefine_solve(oxi_handle_t h, int64_t n, int64_t nrhs, const double *dA, int64_t lda,
+                                 const double *dLU, int64_t ldlu, const int64_t *d_ipiv, const double *dB,
+                                 int64_t ldb, double *dX, int64_t ldx, int maxiter, double rtol,
+                                 oxi_solve_report *out) {
+    using namespace oxi;
+    if (!h) return OXI_EINVAL;
+    if (out) *out = oxi_solve_report{};
+    const int64_t mn = std::max<int64_t>(1, n);
+    if (n < 0 || nrhs < 0 || maxiter < 0 || !(rtol >= 0) || lda < mn || ldlu < mn || ldb < mn || ldx < mn)
+        return OXI_EINVAL;
+    if (n == 0 || nrhs == 0) {
+        if (out) { out->converged = 1; out->rcond_estimate = 1.0; }
+        return OXI_OK;
+    }
+    if (!dA || !dLU || !d_ipiv || !dB || !dX || n >= (1ll << 31)) return OXI_EINVAL;
+    try {
+        ProfGuard pg(&h->prof);
+        OXI_CUDA(cudaSetDevice(h->device));
+        AbortScope ab(h);
+        cudaStream_t s = h->stream;
+        int64_t *dperm = nullptr;
+        if (upload_perm(h, n, d_ipiv, &dperm) != OXI_OK) return OXI_EINVAL;
+        // workspace: residual partials, R (n x nrhs), the estimator's vectors
+        size_t off = 0;
+        auto take = [&](size_t bytes) { size_t o = off; off += (bytes + 255) & ~size_t(255); return o; };
+        const size_t o_pax = take(8 * n * RS * NRMAX), o_pden = take(8 * n * RS * NRMAX),
+                     o_R = take(8 * n * nrhs), o_est = take(8 * (3 * n + 8)), o_nrm = take(8 * 8);
+        char *ws = (char *)h->mixed_ws.get(off);
+        MixedRun M;
+        M.h = h; M.s = s; M.n = n; M.nrhs = nrhs; M.A = dA; M.lda = lda; M.B = dB; M.ldb = ldb;
+        M.X = dX; M.ldx = ldx;
+        M.pax = (double *)(ws + o_pax); M.pden = (double *)(ws + o_pden);
+        M.R = (double *)(ws + o_R);
+        M.scal = (double *)((char *)h->scratch.get(kScratchBytes) + kScratchScalOff);
+        M.hsc = (double *)h->host_ws.get(sizeof(double) * 512);
+        M.anorm = 0.0;
+        double *nrm = (double *)(ws + o_nrm);
+        // X = solve(F, B)
+        OXI_CUDA(cudaMemcpy2DAsync(dX, ldx * 8, dB, ldb * 8, n * 8, nrhs, cudaMemcpyDeviceToDevice, s));
+        getrs_perm<double>(h, 'N', n, nrhs, dLU, ldlu, dperm, dX, ldx, ab.word);
+        std::vector<double> cw, nw;
+        double r2 = 0.0, err = INFINITY;
+        int it = 0;
+        for (int iter = 0; iter <= maxiter; ++iter) {
+            residual(M, dX, M.R, cw, nw, r2);
+            err = 0.0;
+            for (double e : cw) err = (e > err || std::isnan(e)) ? e : err;
+            it = iter;
+            if (err <= rtol || iter == maxiter) break;
+            // correction = solve(F, residual): in place in R, then X += R (R is
+            // recomputed at the next step)
+            getrs_perm<double>(h, 'N', n, nrhs, dLU, ldlu, dperm, M.R, n, ab.word);
+            for (i64 k = 0; k < nrhs; ++k) {
+                k_add_to<<<blocks_for(n), 256, 0, s>>>(dX + k * ldx, M.R + k * n, (int)n);
+                OXI_LAUNCH_CHECK();
+            }
+        }
+        // the final residual stays in R; the estimates of the reference's tuple
+        const double inv_norm = inverse_norm_est(h, n, dLU, ldlu, dperm, 8, (double *)(ws + o_est), ab.word);
+        OXI_CUDA(cudaMemsetAsync(nrm, 0, sizeof(double) * 3, s));
+        k_one_norm<<<(unsigned)n, 256, 0, s>>>(dA, lda, (int)n, nrm);
+        OXI_LAUNCH_CHECK();
+        k_one_norm<<<(unsigned)nrhs, 256, 0, s>>>(dX, ldx, (int)n, nrm + 1);
+        OXI_LAUNCH_CHECK();
+        k_one_norm<<<(unsigned)nrhs, 256, 0, s>>>(M.R, n, (int)n, nrm + 2);
+        OXI_LAUNCH_CHECK();
+        double *hn = M.hsc + 400;
+        OXI_CUDA(cudaMemcpyAsync(hn, nrm, sizeof(double) * 3, cudaMemcpyDeviceToHost, s));
+        int *he = (int *)(M.hsc + 408);
+        queue_abort_read(h, he);
+        OXI_CUDA(cudaStreamSynchronize(s));
+        const int st = check_abort(h, he);
+        if (st != OXI_OK) return st;
+        const double anorm = hn[0], xnorm = hn[1], rnorm1 = hn[2];
+        const double cond = anorm * inv_norm;
+        const double rnorm = std::sqrt(r2);
+        const double delta = xnorm == 0.0 ? (rnorm == 0.0 ? 0.0 : INFINITY) : inv_norm * rnorm1 / xnorm;
+        if (out) {
+            out->iterations = it;
+            out->backward_error = err;
+            out->residual_norm = rnorm;
+            out->rcond_estimate = cond == 0.0 ? 1.0 : std::min(1.0, 1.0 / cond);
+            out->forward_error_estimate = delta < 1.0 ? delta / (1.0 - delta) : INFINITY;
+            out->inverse_norm_estimate = inv_norm;
+            out->converged = err <= rtol ? 1 : 0;
+        }
+        return err <= rtol ? OXI_OK : OXI_ENOTCONVERGED;
+    } catch (const CudaError &e) {
+        h->last_error = std::string(e.what) + ": " + cudaGetErrorString(e.code);
+        return OXI_ECUDA;
+    }
+}
+
+// expert_solve(A, b; maxiter, rtol, equilibrate) (src/lapack/advanced_factorizations.jl:591-645).
+extern "C" int oxi_dexpert_solve(oxi_handle_t h, int64_t n, int64_t nrhs, const double *dA, int64_t lda,
+                                 const double *dB, int64_t ldb, double *dX, int64_t ldx, int maxiter, double rtol,
+                                 int equilibrate, double *d_row_scale, double *d_col_scale, double *dF,
+                                 int64_t ldf, int64_t *d_ipiv, oxi_solve_report *out) {
+    using namespace oxi;
+    if (!h) return OXI_EINVAL;
+    if (out) *out = oxi_solve_report{};
+    const int64_t mn = std::max<int64_t>(1, n);
+    if (n < 0 || nrhs < 0 || maxiter < 0 || !(rtol >= 0) || !std::isfinite(rtol) || lda < mn || ldb < mn ||
+        ldx < mn || (dF && ldf < mn))
+        return OXI_EINVAL;
+    if (n == 0 || nrhs == 0) {
+        if (out) out->converged = 1;
+        return OXI_OK;
+    }
+    if (!dA || !dB || !dX || nrhs > 16) return OXI_EINVAL;
+    if (leaf_width_for<double>(n) == 0 || n >= (1ll << 31)) return OXI_EINVAL;
+    try {
+        ProfGuard pg(&h->prof);
+        OXI_CUDA(cudaSetDevice(h->device));
+        AbortScope ab(h);
+        ExpertOpts xo;
+        xo.equilibrate = equilibrate != 0;
+        xo.rows_out = d_row_scale;
+        xo.cols_out = d_col_scale;
+        xo.F_out = dF;
+        xo.ldf = ldf;
+        xo.ipiv_out = d_ipiv;
+        oxi_refine_report rep{};
+        const int st = dgesv_mixed(h, OXI_PREC_FP64, OXI_REFINE_IR, n, nrhs, dA, lda, dB, ldb, dX, ldx, maxiter,
+                                   rtol, &rep, &xo);
+        h->stall_at = 0;
+        if (out) {
+            out->iterations = rep.iterations;
+            out->backward_error = rep.backward_error;
+            out->residual_norm = rep.residual_norm;
+            out->rcond_estimate = NAN;
+            out->forward_error_estimate = NAN;
+            out->inverse_norm_estimate = NAN;
+            out->info = rep.info;
+            out->converged = rep.converged;
+        }
+        if (st == OXI_EOVERFLOW || st == OXI_ESINGULAR || st == OXI_ENONFINITE) return st;
+        int *he = (int *)h->host_ws.get(64);
+        queue_abort_read(h, he);
+        OXI_CUDA(cudaStreamSynchronize(h->stream));
+        const int we = check_abort(h, he);
+        return we != OXI_OK ? we : st;
+    } catch (const CudaError &e) {
+        h->stall_at = 0;
+        h->last_error = std::string(e.what) + ": " + cudaGetErrorString(e.code);
+        return OXI_ECUDA;
+    }
+}
+
+// inv(F) for the factors of oxi_dgetrf: the solve with the identity, the
+// columns of A^-1 (LinearAlgebra's inv over ldiv!, src/api/linalg_api.jl:1143-1144).
+extern "C" int oxi_dgetri(oxi_handle_t h, int64_t n, const double *dLU, int64_t lda, const int64_t *d_ipiv,
+                          double *dAinv, int64_t ldainv) {
+    using namespace oxi;
+    if (!h || n < 0 || lda < std::max<int64_t>(1, n) || ldainv < std::max<int64_t>(1, n)) return OXI_EINVAL;
+    if (n == 0) return OXI_OK;
+    if (!dLU || !d_ipiv || !dAinv || n >= (1ll << 31)) return OXI_EINVAL;
+    try {
+        ProfGuard pg(&h->prof);
+        OXI_CUDA(cudaSetDevice(h->device));
+        AbortScope ab(h);
+        int64_t *dperm = nullptr;
+        if (upload_perm(h, n, d_ipiv, &dperm) != OXI_OK) return OXI_EINVAL;
+        k_identity<<<dim3((unsigned)((n + 255) / 256), (unsigned)n), 256, 0, h->stream>>>(dAinv, ldainv, (int)n);
+        OXI_LAUNCH_CHECK();
+        getrs_perm<double>(h, 'N', n, n, dLU, lda, dperm, dAinv, ldainv, ab.word);
+        int *he = (int *)h->host_ws.get(64);
+        queue_abort_read(h, he);
+        OXI_CUDA(cudaStreamSynchronize(h->stream));
+        return check_abort(h, he);
     } catch (const CudaError &e) {
         h->last_error = std::string(e.what) + ": " + cudaGetErrorString(e.code);
         return OXI_ECUDA;

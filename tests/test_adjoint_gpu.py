@@ -128,3 +128,82 @@ def test_adjoint_many_rhs_odd_ld_and_errors(pkg):
     assert st == 1
     with pytest.raises(pkg.DimensionMismatch):
         pkg.lu_adjoint(F, torch.zeros(n + 1), torch.zeros(n + 1))
+
+
+def _kappa_small(rng, n, kappa):
+    U, R = np.linalg.qr(rng.standard_normal((n, n)))
+    U *= np.sign(np.diag(R))
+    V, R = np.linalg.qr(rng.standard_normal((n, n)))
+    V *= np.sign(np.diag(R))
+    s = 10.0 ** (-np.log10(kappa) * rng.uniform(0, 1, n))
+    s[0], s[-1] = 1.0, 1.0 / kappa
+    return (U * s) @ V.T
+
+
+def test_batched_adjoint_1024_problems(pkg, oracle):
+    """The batched rrule: 1024 problems, n ~ U{32..128}, kappa ~ 1e3 (the
+    sigma-spectrum construction), loss 0.5||x||^2 per problem.  Each problem's
+    (bbar, Abar) against the oracle's pullback from the same factors, and a
+    sample against central finite differences (h = 1e-6)."""
+    rng = np.random.default_rng(2026)
+    orders = rng.integers(32, 129, 1024)
+    mats = [_kappa_small(rng, int(n), 1e3) for n in orders]
+    rhs = [rng.standard_normal(int(n)) for n in orders]
+    P = pkg.BatchedLU(orders, np.ones_like(orders))
+    P.load(mats, rhs)
+    rep = P.gesv("fp64")
+    assert np.all(rep["info"] == 0)
+    xs = [_np(P.B(i))[:, 0].copy() for i in range(len(orders))]
+    info = P.adjoint([x for x in xs])  # loss 0.5||x||^2: xbar = x
+    assert np.all(info == 0)
+    worst = 0.0
+    for i in range(len(orders)):
+        F, ip = _np(P.A(i)), _np(P.ipiv(i))
+        bo, Ao = oracle.lu_adjoint(F, ip, xs[i], xs[i])
+        bb, Ab = _np(P.Bbar(i))[:, 0], _np(P.Abar(i))
+        worst = max(worst, np.linalg.norm(bb - bo) / np.linalg.norm(bo),
+                    np.linalg.norm(Ab - Ao) / np.linalg.norm(Ao))
+    assert worst <= 1e-12, worst
+    h = 1e-6
+    for i in rng.choice(len(orders), 8, replace=False):
+        A, b = mats[i], rhs[i]
+        Ab = _np(P.Abar(i))
+        bb = _np(P.Bbar(i))[:, 0]
+        f = lambda M, v: 0.5 * np.sum(np.linalg.solve(M, v) ** 2)
+        for _ in range(4):
+            dA = rng.standard_normal(A.shape)
+            fd = (f(A + h * dA, b) - f(A - h * dA, b)) / (2 * h)
+            assert abs(fd - np.sum(Ab * dA)) <= 1e-6 * max(1.0, abs(fd)), (i, fd)
+            db = rng.standard_normal(b.shape)
+            fd = (f(A, b + h * db) - f(A, b - h * db)) / (2 * h)
+            assert abs(fd - bb @ db) <= 1e-6 * max(1.0, abs(fd)), (i, fd)
+
+
+def test_batched_adjoint_several_rhs_and_edges(pkg, oracle):
+    rng = np.random.default_rng(7)
+    orders = np.array([1, 5, 64, 200, 256, 0])
+    nrhs = np.array([1, 3, 8, 2, 4, 1])
+    mats = [rng.standard_normal((n, n)) + n * np.eye(n) for n in orders]
+    rhs = [rng.standard_normal((n, k)) for n, k in zip(orders, nrhs)]
+    P = pkg.BatchedLU(orders, nrhs)
+    P.load(mats, rhs)
+    P.gesv("fp64")
+    xbars = [rng.standard_normal((n, k)) for n, k in zip(orders, nrhs)]
+    info = P.adjoint(xbars)
+    assert np.all(info == 0)
+    for i, n in enumerate(orders):
+        if n == 0:
+            continue
+        X = _np(P.B(i))
+        Ainv_T = np.linalg.inv(mats[i]).T
+        bbar = Ainv_T @ xbars[i]
+        assert np.allclose(_np(P.Bbar(i)), bbar, rtol=1e-11, atol=1e-13)
+        assert np.allclose(_np(P.Abar(i)), -bbar @ X.T, rtol=1e-11, atol=1e-13)
+    # a singular factor: the zero diagonal is reported
+    S = rng.standard_normal((6, 6))
+    S[:, 2] = 0.0
+    Q = pkg.BatchedLU([6])
+    Q.load([S], [rng.standard_normal(6)])
+    Q.getrf()
+    with pytest.raises(pkg.SingularException):
+        Q.adjoint([np.ones(6)], solution="B")

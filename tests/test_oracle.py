@@ -113,3 +113,24 @@ def test_oracle_tiled_gemm_is_bit_identical(oracle, dtype):
             assert np.array_equal(G1, G2)
     finally:
         oracle.set_gemm_tiled(True)
+
+
+def test_oracle_expert_solves(oracle):
+    """The oracle's expert_solve / refine_solve / inverse_norm_estimate against
+    the reference's properties (test/lapack/expert_* style checks)."""
+    rng = np.random.default_rng(17)
+    n = 120
+    A = rng.standard_normal((n, n)) * (10.0 ** rng.uniform(-3, 3, (n, 1)))
+    b = rng.standard_normal(n)
+    r = oracle.expert_solve(A, b)
+    assert r["converged"] and r["backward_error"] <= 8 * np.finfo(float).eps
+    assert np.all(r["row_scale"] > 0) and np.all(r["column_scale"] > 0)
+    F, ip, _ = oracle.getrf(A)
+    est = oracle.inverse_norm_estimate(F, ip)
+    true = np.linalg.norm(np.linalg.inv(A), 1)
+    assert true / 3 <= est <= true * (1 + 1e-10)
+    rs = oracle.refine_solve(A, F, ip, b)
+    assert rs["converged"]
+    assert np.isclose(rs["rcond_estimate"], 1 / (np.linalg.norm(A, 1) * est), rtol=1e-12)
+    X = oracle.inverse(F, ip)
+    assert np.allclose(X @ A, np.eye(n), atol=1e-8)
