@@ -14,7 +14,9 @@ side), factor + refinement until the normwise backward error
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 N > 1 runs N independent replicas (one system per rank, different seeds); the
-LU of one matrix does not shard.  Rank 0 prints one JSON line.
+LU of one matrix does not shard.  The batched workload splits one global batch
+by size bucket over the ranks.  Without an external launcher (torchrun sets
+WORLD_SIZE), --gpus N starts the N ranks itself.  Rank 0 prints one JSON line.
 """
 from __future__ import annotations
 
@@ -503,10 +505,16 @@ def batched_workload(args, ws, rank, local):
     import __graft_entry__ as E
     pkg = E.load_package()
     dev = torch.device("cuda", local)
-    rng = np.random.default_rng(20261104 + rank)
-    count = args.count
-    orders = rng.integers(16, 257, size=count)
-    k = rng.integers(1, 9, size=count)
+    # one global batch (the same seed on every rank); with N ranks each takes
+    # its share of every size bucket (no collective until the timing's max)
+    rng = np.random.default_rng(20261104)
+    count_all = args.count
+    orders_all = rng.integers(16, 257, size=count_all)
+    k_all = rng.integers(1, 9, size=count_all)
+    from oxiblas_b200 import distributed as D
+    mine = D.partition_by_bucket(orders_all, ws)[rank]
+    orders, k = orders_all[mine], k_all[mine]
+    count = len(orders)
     P = pkg.BatchedLU(orders, k, device=dev)
     g = torch.Generator(device=dev).manual_seed(20261104 + rank)
     P.poolA.normal_(generator=g)
@@ -542,9 +550,9 @@ def batched_workload(args, ws, rank, local):
     t_plain = _timed_each(stream, lambda: P.gesv("fp64"), args.steps, pre=restore)
     ms_mixed = max_over_ranks(ws, statistics.median(t_mixed))
     ms_plain = max_over_ranks(ws, statistics.median(t_plain))
-    flops = float(np.sum(2.0 / 3.0 * orders.astype(float) ** 3 + 2.0 * orders.astype(float) ** 2 * k))
+    flops = float(np.sum(2.0 / 3.0 * orders_all.astype(float) ** 3 + 2.0 * orders_all.astype(float) ** 2 * k_all))
     # plain FP64: read A, write LU, read B, write X once (algorithmic bytes)
-    bytes_plain = float(np.sum(16.0 * orders.astype(float) ** 2 + 16.0 * orders * k))
+    bytes_plain = float(np.sum(16.0 * orders_all.astype(float) ** 2 + 16.0 * orders_all * k_all))
     # check a sample of the plain answers against the untouched copy
     restore()
     Bref = B0.clone()
@@ -561,11 +569,12 @@ def batched_workload(args, ws, rank, local):
     line = {
         "metric": "batched uneven LU+solve time: 4096 FP64 systems, n~U{16..256}, 1-8 RHS",
         "value": round(ms_mixed, 3), "unit": "ms", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": round(ms_mixed, 3), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "ms_per_step": round(ms_mixed, 3), "higher_is_better": False, "scaling": "strong", "vs_baseline": None,
         "dtype": "f32+f64", "data": "synthetic",
-        "config": {"workload": f"batched uneven LU, {count} problems, n~U{{16..256}}, N(0,1)+nI, "
-                               "nrhs~U{1..8}; one persistent graph-replayed launch",
-                   "l2": "pools (≈0.8 GB) larger than L2", "parallelism": f"replicas{ws}"},
+        "config": {"workload": f"batched uneven LU, {count_all} problems, n~U{{16..256}}, N(0,1)+nI, "
+                               "nrhs~U{1..8}; one persistent graph-replayed launch per GPU",
+                   "l2": "pools (≈0.8 GB) larger than L2",
+                   "parallelism": f"problems split by size bucket over {ws} GPU(s)"},
         "plain_fp64_ms": round(ms_plain, 3),
         "speedup_vs_plain_fp64": round(ms_plain / ms_mixed, 3),
         "tflops": {"mixed": round(flops / ms_mixed / 1e9, 3), "plain_fp64": round(flops / ms_plain / 1e9, 3)},
@@ -638,8 +647,26 @@ def adjoint_workload(args, ws, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def _spawned_rank(rank, world, port, argv):
+    """One rank of a self-launched multi-GPU run (no external launcher)."""
+    os.environ.update({"RANK": str(rank), "LOCAL_RANK": str(rank), "WORLD_SIZE": str(world),
+                       "MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port)})
+    sys.argv = argv
+    main()
+
+
 def main():
     args = parse()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # `bench.py --gpus N` on its own: start the N ranks here, one process per
+        # GPU (torchrun sets WORLD_SIZE and comes straight through)
+        import socket
+        import torch.multiprocessing as mp
+        with socket.socket() as sk:
+            sk.bind(("127.0.0.1", 0))
+            port = sk.getsockname()[1]
+        mp.spawn(_spawned_rank, args=(args.gpus, port, list(sys.argv)), nprocs=args.gpus, join=True)
+        return
     ws, rank, local = dist_setup(args)
     try:
         if args.impl == "reference":

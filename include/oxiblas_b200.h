@@ -126,9 +126,10 @@ int oxi_sgetrs(oxi_handle_t h, char trans, int64_t n, int64_t nrhs, const float 
  * Its scratch (permutation, solve vector, control words) is one file-scope
  * device array of OXI_NOALLOC_SCRATCH_BYTES per device.  Limits:
  * n <= OXI_NOALLOC_MAX_N and n * nrhs <= OXI_NOALLOC_MAX_ELEMS, else
- * OXI_ESCRATCH (nothing is launched).  The first call on a device resolves
- * the array's address and loads the kernels it uses; make that first call
- * before any stream capture.  Every call shares the array and leaves its
+ * OXI_ESCRATCH (nothing is launched).  The first call on a device (and the
+ * first after its context was re-created, e.g. by a device reset) resolves the
+ * array's address and loads the kernels it uses; make that first call before
+ * any stream capture.  Every call shares the array and leaves its
  * contents behind: calls that overlap on the GPU (two streams, two host
  * threads) race and must be serialised by the caller.  It calls no cudaMalloc,
  * cudaFree or allocating library routine.  The call synchronises `stream`.

@@ -100,6 +100,8 @@ class BatchedLU:
             self.A(i).copy_(t)
         if Bs is not None:
             for i, b in enumerate(Bs):
+                if int(self.orders[i]) == 0:
+                    continue
                 t = torch.as_tensor(b, dtype=torch.float64).reshape(int(self.orders[i]), -1)
                 if t.shape[1] != int(self.nrhs[i]):
                     raise DimensionMismatch(f"right-hand side {i} has {t.shape[1]} columns")
@@ -182,6 +184,8 @@ class BatchedLU:
             if len(xbars) != self.count:
                 raise DimensionMismatch("one upstream gradient per problem expected")
             for i, xb in enumerate(xbars):
+                if int(self.orders[i]) == 0:
+                    continue
                 t = torch.as_tensor(xb, dtype=torch.float64).reshape(int(self.orders[i]), -1)
                 self.Xbar(i).copy_(t)
         d_x = self.d_B if solution == "B" else self.d_X

@@ -54,7 +54,8 @@ __global__ void k_await_missing_producer(const int *__restrict__ flag, int *__re
 }
 
 void launch_await_missing_producer(oxi_handle_s *h, cudaStream_t s) {
-    const int *flag = (const int *)((char *)h->scratch.get(kScratchBytes) + kScratchStallOff);
+    int *flag = (int *)((char *)h->scratch.get(kScratchBytes) + kScratchStallOff);
+    OXI_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), s));  // the flag starts clear; nothing sets it
     k_await_missing_producer<<<1, 1, 0, s>>>(flag, cur_abort());
     OXI_LAUNCH_CHECK();
 }

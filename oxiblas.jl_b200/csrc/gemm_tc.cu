@@ -100,9 +100,9 @@ k_gemm_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
     uint64_t *empty = full + STAGES;
     uint64_t *tfull = empty + STAGES;  // [2]
     uint64_t *tempty = tfull + 2;      // [2]
-    uint64_t *cfull = tempty + 2;
-    uint64_t *cempty = cfull + 1;
-    uint32_t *tmem_slot = (uint32_t *)(cempty + 1);
+    uint64_t *cfull = tempty + 2;      // [NCBOX]: C box loaded
+    uint64_t *cempty = cfull + NCBOX;  // [NCBOX]: C box stored (read out of shared memory)
+    uint32_t *tmem_slot = (uint32_t *)(cempty + NCBOX);
     volatile int *abort_flag = (volatile int *)(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -119,8 +119,10 @@ k_gemm_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
             mbar_init(&tfull[b], 1);
             mbar_init(&tempty[b], 4);
         }
-        mbar_init(cfull, 1);
-        mbar_init(cempty, 1);
+        for (int c = 0; c < NCBOX; ++c) {
+            mbar_init(&cfull[c], 1);
+            mbar_init(&cempty[c], 1);
+        }
         *abort_flag = aborted(ab) ? 1 : 0;  // an aborted call: every role skips its loop
         fence_barrier_init();
     }
@@ -184,39 +186,53 @@ k_gemm_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
                 : "memory");
         }
     } else if (warp == 2 && lane == 0) {
+        // C producer: box by box, each as soon as the previous tile's store
+        // of that box has left shared memory
         prefetch_tmap(&tmC);
         int li = 0;
-        for (int tile = blockIdx.x; tile < ntiles && !*abort_flag; tile += gridDim.x, ++li) {
+        bool go = true;
+        for (int tile = blockIdx.x; go && tile < ntiles && !*abort_flag; tile += gridDim.x, ++li) {
             const int m0 = (tile / tilesN) * BM, n0 = (tile % tilesN) * BN;
-            if (li >= 1 && !mbar_wait_ab(cempty, (li - 1) & 1, abort_flag, ab)) break;
-            mbar_arrive_expect_tx(cfull, C_BYTES);
-#pragma unroll
-            for (int bx = 0; bx < NCBOX; ++bx)
-                tma_load_2d(sC + bx * CBOX_BYTES, &tmC, cfull, n0 + bx * CBOX_COLS, m0);
+            for (int bx = 0; bx < NCBOX; ++bx) {
+                if (li >= 1 && !mbar_wait_ab(&cempty[bx], (li - 1) & 1, abort_flag, ab)) {
+                    go = false;
+                    break;
+                }
+                mbar_arrive_expect_tx(&cfull[bx], CBOX_BYTES);
+                tma_load_2d(sC + bx * CBOX_BYTES, &tmC, &cfull[bx], n0 + bx * CBOX_COLS, m0);
+            }
         }
     } else if (warp >= 4) {
         const int ew = warp - 4;          // TMEM lane quadrant of this warp
         const int r = ew * 32 + lane;     // tile row owned by this thread
         const float sc = d_scale ? scale * (*d_scale) : scale;
+        // Box by box: wait for the box's C (and, for the first box, the
+        // accumulator), C - scale * D into shared memory, TMA store of the box;
+        // the store of box c is confirmed read before box c's slot is handed
+        // back to the producer, one box later.  Every wait's outcome is made
+        // uniform over the four warps before they meet at a named barrier.
         int li = 0;
-        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++li) {
+        bool go = true;
+        for (int tile = blockIdx.x; go && tile < ntiles; tile += gridDim.x, ++li) {
             const int m0 = (tile / tilesN) * BM, n0 = (tile % tilesN) * BN;
             const int b = li & 1;
-            const bool ok = mbar_wait_ab(&tfull[b], (li >> 1) & 1, abort_flag, ab) &&
-                            mbar_wait_ab(cfull, li & 1, abort_flag, ab);
-            // uniform decision across the epilogue warpgroup (it meets at a named barrier)
-            uint32_t all_ok;
-            asm volatile(
-                "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n"
-                " bar.red.and.pred q, 1, 128, p;\n selp.u32 %0, 1, 0, q;\n}\n"
-                : "=r"(all_ok)
-                : "r"((uint32_t)ok)
-                : "memory");
-            if (!all_ok) break;
-            tc_fence_after();
             const uint32_t base = tmem + (uint32_t)(b * TMEM_COLS) + ((uint32_t)(ew * 32) << 16);
 #pragma unroll 1
             for (int c = 0; c < NCBOX; ++c) {
+                const bool ok = (c > 0 || mbar_wait_ab(&tfull[b], (li >> 1) & 1, abort_flag, ab)) &&
+                                mbar_wait_ab(&cfull[c], li & 1, abort_flag, ab);
+                uint32_t all_ok;
+                asm volatile(
+                    "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n"
+                    " bar.red.and.pred q, 1, 128, p;\n selp.u32 %0, 1, 0, q;\n}\n"
+                    : "=r"(all_ok)
+                    : "r"((uint32_t)ok)
+                    : "memory");
+                if (!all_ok) {
+                    go = false;
+                    break;
+                }
+                if (c == 0) tc_fence_after();
                 uint32_t v[32];
                 asm volatile(
                     "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,"
@@ -229,6 +245,11 @@ k_gemm_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
                       "=r"(v[31])
                     : "r"(base + (uint32_t)(c * 32)));
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                if (c == NCBOX - 1) {  // the accumulator is drained: the MMA warp may reuse it
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&tempty[b]);
+                }
                 uint8_t *rowp = sC + c * CBOX_BYTES + r * 128;
 #pragma unroll
                 for (int q = 0; q < 8; ++q) {
@@ -240,20 +261,20 @@ k_gemm_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
                     x.w -= sc * __uint_as_float(v[4 * q + 3]);
                     *p4 = x;
                 }
-            }
-            // the accumulator buffer is drained: the MMA warp may reuse it
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&tempty[b]);
-            fence_proxy_async();  // shared-memory writes -> visible to the TMA (async proxy)
-            asm volatile("bar.sync 1, 128;" ::: "memory");
-            if (ew == 0 && lane == 0) {
-#pragma unroll
-                for (int bx = 0; bx < NCBOX; ++bx)
-                    tma_store_2d(&tmC, sC + bx * CBOX_BYTES, n0 + bx * CBOX_COLS, m0);
-                asm volatile("cp.async.bulk.commit_group;" ::: "memory");
-                asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
-                mbar_arrive(cempty);  // the C buffer may be refilled
+                fence_proxy_async();  // shared-memory writes -> visible to the TMA (async proxy)
+                asm volatile("bar.sync 1, 128;" ::: "memory");
+                if (ew == 0 && lane == 0) {
+                    tma_store_2d(&tmC, sC + c * CBOX_BYTES, n0 + c * CBOX_COLS, m0);
+                    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+                    if (c > 0) {
+                        asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+                        mbar_arrive(&cempty[c - 1]);  // box c-1's slot may be refilled
+                    }
+                    if (c == NCBOX - 1) {
+                        asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+                        mbar_arrive(&cempty[c]);
+                    }
+                }
             }
         }
         if (ew == 0 && lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");

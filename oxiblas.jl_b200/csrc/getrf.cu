@@ -168,8 +168,14 @@ static void panel_leaf32(LuRun<T> &R, i64 c0, i64 nc, int w) {
         if (mrows <= 0) break;
         OXI_CUDA(cudaMemsetAsync(R.nmoves, 0, sizeof(int), h->stream));
         maybe_stall_before_leaf(h, h->stream);
-        launch_leaf<T>(R.W + c * R.ld + c, R.ld, mrows, (int)wc, c, R.ipiv, R.info, R.moves, R.nmoves, w,
-                       h->stream, leaf_panel(R, c, wc));
+        if (R.map) {  // the leaf moves the panel's other columns itself
+            launch_leaf<T>(R.W + c * R.ld + c, R.ld, mrows, (int)wc, c, R.ipiv, R.info, R.moves, R.nmoves, w,
+                           h->stream, leaf_panel(R, c, wc));
+        } else {      // no composed panel: its interchanges on every other column after it
+            launch_leaf<T>(R.W + c * R.ld + c, R.ld, mrows, (int)wc, c, R.ipiv, R.info, R.moves, R.nmoves, w,
+                           h->stream, LeafPanel());
+            launch_rowmoves<T>(R.W, R.ld, c, R.moves, R.nmoves, 0, R.ncols_moved, c, c + wc, h->stream);
+        }
         const i64 right = c0 + nc - (c + wc);
         if (right <= 0) continue;
         if constexpr (sizeof(T) == 8) {
@@ -201,7 +207,7 @@ static void panel_rec(LuRun<T> &R, i64 c0, i64 nc) {
     const int leafw = ts ? 32 : leaf_width_for<T>(mrows);
     if (leafw == 0) throw CudaError{cudaErrorInvalidValue, "panel taller than the leaf capacity"};
     if constexpr (sizeof(T) == 8) {
-        if (nc > leafw && nc <= 32 && R.map && h->opt.gemm == 0) {
+        if (nc > leafw && nc <= 32 && h->opt.gemm == 0) {
             panel_leaf32(R, c0, nc, leafw);
             return;
         }

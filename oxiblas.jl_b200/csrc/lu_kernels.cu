@@ -962,8 +962,8 @@ void launch_trsm_fused(const T *L, i64 ldl, T *B, i64 ldb, int t, i64 N, cudaStr
 // leaves of <= 8 rows by substitution, s = b; s = fma(-L[i,p], x[p], s) for
 // p < i (_trsm_leaf_generic!, level3.jl:309-321).  The host flattens the
 // recursion into a list of leaf and update steps in the recursion's order; one
-// CTA takes CW columns and runs the list with L and its columns in shared
-// memory, so one launch gives the recursive solve's bits.
+// CTA takes CW columns and runs the list with its columns in shared memory, so
+// one launch gives the recursive solve's bits.
 // ---------------------------------------------------------------------------
 struct TrsmSteps {
     int count;
@@ -986,18 +986,15 @@ constexpr int TR_TMAX = 128;
 template <int CW>
 __global__ void __launch_bounds__(256) k_trsm_refo(const double *__restrict__ L, i64 ldl, double *__restrict__ B,
                                                    i64 ldb, int t, i64 N, const __grid_constant__ TrsmSteps st) {
+    // L is read through the L1 cache (threads of a warp that share a row read
+    // the same element: one broadcast load), the CTA's columns stay in shared
+    // memory: t x (CW + 1) doubles, several CTAs per SM.
     extern __shared__ __align__(16) double tr_smem[];
-    const int lp = t + 1;  // padded L row
-    double *Ls = tr_smem;
-    double *X = tr_smem + (size_t)t * lp;  // t x (CW + 1)
+    double *X = tr_smem;
     constexpr int XP = CW + 1;
     const int tid = threadIdx.x;
     const i64 c0 = (i64)blockIdx.x * CW;
     const int cols = (int)((N - c0) < CW ? (N - c0) : CW);
-    for (int e = tid; e < t * t; e += 256) {
-        const int r = e / t, pcol = e - r * t;
-        Ls[r * lp + pcol] = (pcol < r) ? L[(i64)r * ldl + pcol] : 0.0;
-    }
     for (int e = tid; e < t * CW; e += 256) {
         const int i = e / CW, c = e - i * CW;
         X[i * XP + c] = (c < cols) ? B[(i64)i * ldb + c0 + c] : 0.0;
@@ -1006,20 +1003,53 @@ __global__ void __launch_bounds__(256) k_trsm_refo(const double *__restrict__ L,
     for (int k = 0; k < st.count; ++k) {
         const int4 o = st.step[k];
         if (o.x == 0) {
+            // leaf of nl <= 8 rows: the column in registers, the triangle's
+            // loads all issued up front (fully unrolled, predicated)
             if (tid < CW) {
-                for (int i = o.y; i < o.z; ++i) {
-                    double sv = X[i * XP + tid];
-                    for (int pp = o.y; pp < i; ++pp) sv = fma(-Ls[i * lp + pp], X[pp * XP + tid], sv);
-                    X[i * XP + tid] = sv;
+                const int nl = o.z - o.y;
+                double xv[8], lv[8][8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    xv[u] = (u < nl) ? X[(o.y + u) * XP + tid] : 0.0;
+#pragma unroll
+                    for (int pp = 0; pp < u; ++pp)
+                        lv[u][pp] = (u < nl) ? __ldg(L + (i64)(o.y + u) * ldl + o.y + pp) : 0.0;
                 }
+#pragma unroll
+                for (int u = 1; u < 8; ++u)
+#pragma unroll
+                    for (int pp = 0; pp < u; ++pp) xv[u] = fma(-lv[u][pp], xv[pp], xv[u]);
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    if (u < nl) X[(o.y + u) * XP + tid] = xv[u];
             }
         } else {
-            const int nr = o.w - o.z;
-            for (int e = tid; e < nr * CW; e += 256) {
-                const int r = o.z + e / CW, c = e % CW;
-                double acc = 0.0;
-                for (int pp = o.y; pp < o.z; ++pp) acc = fma(Ls[r * lp + pp], X[pp * XP + c], acc);
-                X[r * XP + c] -= acc;
+            // rows [o.z, o.w) -= L[rows, o.y:o.z] X[o.y:o.z]: a thread takes four
+            // columns of up to two rows (register blocking; each element is
+            // still one fma chain in pp order, then the subtraction)
+            constexpr int NG = CW / 4, RGS = 256 / NG;
+            const int cq = (tid % NG) * 4, rg = tid / NG;
+            for (int r0 = o.z + rg; r0 < o.w; r0 += 2 * RGS) {
+                const int r1 = r0 + RGS;
+                const bool has1 = r1 < o.w;
+                const double *L0 = L + (i64)r0 * ldl, *L1 = L + (i64)(has1 ? r1 : r0) * ldl;
+                double a0[4] = {0.0, 0.0, 0.0, 0.0}, a1[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 8
+                for (int pp = o.y; pp < o.z; ++pp) {
+                    const double l0 = __ldg(L0 + pp), l1 = __ldg(L1 + pp);
+                    const double *xr = X + pp * XP + cq;
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        a0[u] = fma(l0, xr[u], a0[u]);
+                        a1[u] = fma(l1, xr[u], a1[u]);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) X[r0 * XP + cq + u] -= a0[u];
+                if (has1) {
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) X[r1 * XP + cq + u] -= a1[u];
+                }
             }
         }
         __syncthreads();
@@ -1040,15 +1070,11 @@ void launch_trsm_refo(const double *L, i64 ldl, double *B, i64 ldb, int t, i64 N
     ProfScope ps(KC_TRSM_LEAF, s, (double)t * t * N, 2.0 * (double)t * N * 8);
     if (N <= 2048) {
         constexpr int CW = 8;
-        const size_t smem = sizeof(double) * ((size_t)t * (t + 1) + (size_t)t * (CW + 1));
-        set_max_dyn_smem((const void *)k_trsm_refo<CW>,
-                         (int)(sizeof(double) * ((size_t)TR_TMAX * (TR_TMAX + 1) + (size_t)TR_TMAX * (CW + 1))));
+        const size_t smem = sizeof(double) * (size_t)t * (CW + 1);
         k_trsm_refo<CW><<<(unsigned)((N + CW - 1) / CW), 256, smem, s>>>(L, ldl, B, ldb, t, N, st);
     } else {
         constexpr int CW = 32;
-        const size_t smem = sizeof(double) * ((size_t)t * (t + 1) + (size_t)t * (CW + 1));
-        set_max_dyn_smem((const void *)k_trsm_refo<CW>,
-                         (int)(sizeof(double) * ((size_t)TR_TMAX * (TR_TMAX + 1) + (size_t)TR_TMAX * (CW + 1))));
+        const size_t smem = sizeof(double) * (size_t)t * (CW + 1);
         k_trsm_refo<CW><<<(unsigned)((N + CW - 1) / CW), 256, smem, s>>>(L, ldl, B, ldb, t, N, st);
     }
     OXI_LAUNCH_CHECK();

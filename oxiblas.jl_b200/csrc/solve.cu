@@ -951,16 +951,55 @@ static void na_load_trsv(cudaFuncAttributes *fa) {
     OXI_CUDA(cudaFuncGetAttributes(fa, k_trsv2<double, LOWER, UNIT, TRANS, 8>));
 }
 
-// Once per device, with that device current: the array's address, and the
-// kernels of this path loaded (so no later call loads a module).
+// Identity of the current context (cuCtxGetCurrent + cuCtxGetId through the
+// runtime's driver entry points): the array's address belongs to the context
+// that resolved it.
+static unsigned long long current_context_id() {
+    using GetCurrent = CUresult (*)(CUcontext *);
+    using GetId = CUresult (*)(CUcontext, unsigned long long *);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    if (!get_current || !get_id) {
+        void *p1 = nullptr, *p2 = nullptr;
+        cudaDriverEntryPointQueryResult q1, q2;
+        OXI_CUDA(cudaGetDriverEntryPoint("cuCtxGetCurrent", &p1, cudaEnableDefault, &q1));
+        OXI_CUDA(cudaGetDriverEntryPoint("cuCtxGetId", &p2, cudaEnableDefault, &q2));
+        if (!p1 || !p2 || q1 != cudaDriverEntryPointSuccess || q2 != cudaDriverEntryPointSuccess)
+            throw CudaError{cudaErrorNotSupported, "cuCtxGetCurrent / cuCtxGetId unavailable"};
+        get_current = (GetCurrent)p1;
+        get_id = (GetId)p2;
+    }
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&ctx) != CUDA_SUCCESS || !ctx) {
+        // this host thread has not used the runtime yet: a symbol query makes
+        // the device's primary context current (it allocates nothing)
+        void *sym = nullptr;
+        OXI_CUDA(cudaGetSymbolAddress(&sym, g_noalloc_scratch));
+        if (get_current(&ctx) != CUDA_SUCCESS || !ctx) throw CudaError{cudaErrorInvalidResourceHandle, "no current context"};
+    }
+    if (get_id(ctx, &id) != CUDA_SUCCESS) throw CudaError{cudaErrorInvalidResourceHandle, "cuCtxGetId"};
+    return id;
+}
+
+// Once per device and context, with that device current: the array's address,
+// and the kernels of this path loaded (so no later call loads a module).  A
+// device reset or a re-created primary context gives a new context id, and the
+// address is resolved again.
 static char *noalloc_scratch(int dev) {
-    static std::atomic<char *> ptrs[kNaMaxDevices];
+    struct Slot {
+        std::atomic<char *> ptr{nullptr};
+        std::atomic<unsigned long long> ctx{0};
+    };
+    static Slot slots[kNaMaxDevices];
     static std::mutex mu;
-    char *p = ptrs[dev].load(std::memory_order_acquire);
-    if (p) return p;
+    const unsigned long long ctx = current_context_id();
+    Slot &sl = slots[dev];
+    char *p = sl.ptr.load(std::memory_order_acquire);
+    if (p && sl.ctx.load(std::memory_order_acquire) == ctx) return p;
     std::lock_guard<std::mutex> lk(mu);
-    p = ptrs[dev].load(std::memory_order_acquire);
-    if (p) return p;
+    p = sl.ptr.load(std::memory_order_acquire);
+    if (p && sl.ctx.load(std::memory_order_acquire) == ctx) return p;
     void *sym = nullptr;
     OXI_CUDA(cudaGetSymbolAddress(&sym, g_noalloc_scratch));
     OXI_CUDA(cudaFuncSetAttribute(k_perm_from_ipiv_na, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -972,7 +1011,8 @@ static char *noalloc_scratch(int dev) {
     na_load_trsv<true, false, true>(&fa);
     na_load_trsv<false, true, true>(&fa);
     p = (char *)sym;
-    ptrs[dev].store(p, std::memory_order_release);
+    sl.ctx.store(ctx, std::memory_order_release);
+    sl.ptr.store(p, std::memory_order_release);
     return p;
 }
 

@@ -170,11 +170,13 @@ def test_batched_adjoint_1024_problems(pkg, oracle):
         Ab = _np(P.Abar(i))
         bb = _np(P.Bbar(i))[:, 0]
         f = lambda M, v: 0.5 * np.sum(np.linalg.solve(M, v) ** 2)
-        for _ in range(4):
+        for _ in range(4):  # unit directions (Frobenius / 2-norm), as the single-matrix test
             dA = rng.standard_normal(A.shape)
+            dA /= np.linalg.norm(dA)
             fd = (f(A + h * dA, b) - f(A - h * dA, b)) / (2 * h)
             assert abs(fd - np.sum(Ab * dA)) <= 1e-6 * max(1.0, abs(fd)), (i, fd)
             db = rng.standard_normal(b.shape)
+            db /= np.linalg.norm(db)
             fd = (f(A, b + h * db) - f(A, b - h * db)) / (2 * h)
             assert abs(fd - bb @ db) <= 1e-6 * max(1.0, abs(fd)), (i, fd)
 

@@ -61,10 +61,12 @@ def test_randn_pivots_and_factors(pkg, oracle, n, bs):
     assert np.array_equal(_np(F.ipiv), piv + 1)  # == LAPACK getrf
 
 
-def test_tall_panel_leaf_widths(pkg):
-    """m > 8192 rows switches the FP64 leaf to 16 columns (4 rows per thread)."""
+@pytest.mark.parametrize("m,n", [(9000, 300), (17000, 100), (17000, 200)])
+def test_tall_panel_leaf_widths(pkg, m, n):
+    """m > 8192 rows switches the FP64 leaf kernel to 16 columns, m > 16384 to
+    8: the 32-column leaf is emulated (in a composed panel, n > 128, and in a
+    single narrow panel)."""
     rng = np.random.default_rng(9)
-    m, n = 9000, 300
     A = rng.standard_normal((m, n))
     F = pkg.lu(A)
     _, piv = sl.lu_factor(A)

@@ -71,3 +71,85 @@ def test_noalloc_rejects_sizes_beyond_its_scratch(pkg):
     assert st == OXI_ESCRATCH
     assert b"scratch" in L.oxi_status_string(st)
     assert bool((B == 1).all())  # nothing launched
+
+
+def test_noalloc_many_rhs_matches_getrs(pkg):
+    """nrhs = 19: several launches of the solve kernels (8 + 8 + 2 + 1
+    columns) reuse the one scratch array within a call."""
+    h = pkg.Handle.get()
+    L = h.lib
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    rng = np.random.default_rng(13)
+    n, nrhs = 1500, 19
+    A = rng.standard_normal((n, n)) + 2 * np.eye(n)
+    B = rng.standard_normal((nrhs, n))
+    LU, ipiv = _factor(pkg, h, A)
+    for trans in (b"N", b"T"):
+        Bref = torch.from_numpy(B).cuda()
+        h.check(L.oxi_dgetrs(h.ptr, trans, n, nrhs, _vp(LU), n, _vp(ipiv), _vp(Bref), n))
+        Bna = torch.from_numpy(B).cuda()
+        assert L.oxi_dgetrs_noalloc(stream, trans, n, nrhs, _vp(LU), n, _vp(ipiv), _vp(Bna), n) == 0
+        Xref = Bref.cpu().numpy()
+        assert np.abs(Bna.cpu().numpy() - Xref).max() <= 1e-12 * max(1.0, np.abs(Xref).max())
+
+
+def test_noalloc_largest_order_on_a_permutation_factor(pkg):
+    """n = OXI_NOALLOC_MAX_N (65536), one right-hand side, on a cheap factor:
+    L = U = I with a random interchange sequence, so X is the permuted B.  This
+    exercises the shared-memory permutation kernel at its 16-bit-row limit."""
+    h = pkg.Handle.get()
+    L = h.lib
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    n = 65536
+    rng = np.random.default_rng(14)
+    LU = torch.eye(n, dtype=torch.float64, device="cuda")  # 34 GB: symmetric, so its memory is column-major I
+    ipiv_h = np.array([rng.integers(j + 1, n + 1) for j in range(n)], dtype=np.int64)
+    ipiv = torch.from_numpy(ipiv_h).cuda()
+    b = rng.standard_normal(n)
+    p = np.arange(n)
+    for j, pj in enumerate(ipiv_h - 1):
+        p[j], p[pj] = p[pj], p[j]
+    B = torch.from_numpy(b.copy()).cuda()
+    assert L.oxi_dgetrs_noalloc(stream, b"N", n, 1, _vp(LU), n, _vp(ipiv), _vp(B), n) == 0
+    assert np.array_equal(B.cpu().numpy(), b[p])  # L U x = P b with L = U = I
+    Bref = torch.from_numpy(b.copy()).cuda()
+    h.check(L.oxi_dgetrs(h.ptr, b"N", n, 1, _vp(LU), n, _vp(ipiv), _vp(Bref), n))
+    assert torch.equal(B, Bref)
+    del LU
+    torch.cuda.empty_cache()
+
+
+def test_noalloc_invalid_pivot_leaves_b_untouched(pkg):
+    h = pkg.Handle.get()
+    L = h.lib
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    rng = np.random.default_rng(15)
+    n = 200
+    LU, ipiv = _factor(pkg, h, rng.standard_normal((n, n)) + 2 * np.eye(n))
+    bad = ipiv.clone()
+    bad[57] = n + 3  # out of range
+    B = torch.from_numpy(rng.standard_normal((2, n))).cuda()
+    B0 = B.clone()
+    st = L.oxi_dgetrs_noalloc(stream, b"N", n, 2, _vp(LU), n, _vp(bad), _vp(B), n)
+    assert st == 1  # OXI_EINVAL
+    assert torch.equal(B, B0)
+
+
+def test_noalloc_call_allocates_no_device_memory(pkg):
+    """After a first (set-up) call, a call leaves the device's free memory
+    exactly as it was: no cudaMalloc, no allocating library routine."""
+    h = pkg.Handle.get()
+    L = h.lib
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    rng = np.random.default_rng(16)
+    n, nrhs = 900, 5
+    LU, ipiv = _factor(pkg, h, rng.standard_normal((n, n)) + 2 * np.eye(n))
+    B = torch.from_numpy(rng.standard_normal((nrhs, n))).cuda()
+    assert L.oxi_dgetrs_noalloc(stream, b"N", n, nrhs, _vp(LU), n, _vp(ipiv), _vp(B), n) == 0
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for trans in (b"N", b"T", b"N"):
+        assert L.oxi_dgetrs_noalloc(stream, trans, n, nrhs, _vp(LU), n, _vp(ipiv), _vp(B), n) == 0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
