@@ -33,7 +33,8 @@ enum oxi_status {
     OXI_ETIMEOUT = 6,    /* a bounded device-side wait expired                         */
     OXI_ENOMEM = 7,      /* workspace allocation failed                                */
     OXI_ENOTCONVERGED = 8, /* refinement stopped at maxiter (report still filled)     */
-    OXI_ESCRATCH = 9       /* size beyond the fixed scratch of oxi_dgetrs_noalloc       */
+    OXI_ESCRATCH = 9,      /* size beyond the fixed scratch of oxi_dgetrs_noalloc       */
+    OXI_ENOTPOSDEF = 10    /* PosDefException(info): *h_info holds the failing column     */
 };
 
 typedef struct oxi_handle_s *oxi_handle_t;
@@ -298,6 +299,32 @@ int oxi_dinverse_norm_estimate(oxi_handle_t h, int64_t n, const double *dLU, int
  * identity, into dAinv (column-major, leading dimension ldainv). */
 int oxi_dgetri(oxi_handle_t h, int64_t n, const double *dLU, int64_t lda, const int64_t *d_ipiv,
                double *dAinv, int64_t ldainv);
+
+/* ---------------------------------------------------------------------------
+ * Cholesky (FP64): the reference's other dense factorization on the same
+ * engine (src/lapack/factorizations.jl:205-305; OxiBLAS.cholesky / cholesky!,
+ * src/api/linalg_api.jl:221-290).
+ * oxi_dpotrf: the lower triangle of A (n x n, column-major) is overwritten by
+ * L with A = L L^T and the strict upper triangle set to zero; the upper
+ * triangle is not read.  A pivot that is not finite and positive stops it:
+ * *h_info = that column (1-based), OXI_ENOTPOSDEF, the upper triangle left as
+ * it was.  oxi_dpotrs: B (n x nrhs) <- A^-1 B with the factor of oxi_dpotrf. */
+int oxi_dpotrf(oxi_handle_t h, int64_t n, double *dA, int64_t lda, int64_t *h_info);
+int oxi_dpotrs(oxi_handle_t h, int64_t n, int64_t nrhs, const double *dL, int64_t ldl, double *dB,
+               int64_t ldb);
+
+/* ---------------------------------------------------------------------------
+ * Complex LU (ComplexF64, interleaved real/imaginary pairs, column-major,
+ * 16-byte aligned): _lu_factor! / _lu_panel! for Complex{Float64}
+ * (src/lapack/factorizations.jl:30-152; 16-column leaves, the pivot the
+ * largest abs2 with abs when that square is not finite, :92-113) and
+ * ldiv!(F, B) / ldiv!(transpose(F), B) / ldiv!(F', B)
+ * (src/api/linalg_api.jl:168-184).  Same contracts as oxi_dgetrf /
+ * oxi_dgetrs; trans 'N', 'T' or 'C'. */
+int oxi_zgetrf(oxi_handle_t h, int64_t m, int64_t n, void *dA, int64_t lda, int64_t *d_ipiv,
+               int64_t *h_info);
+int oxi_zgetrs(oxi_handle_t h, char trans, int64_t n, int64_t nrhs, const void *dLU, int64_t lda,
+               const int64_t *d_ipiv, void *dB, int64_t ldb);
 
 /* Radix equilibration, the first step of the mixed solve, as its own call:
  * equilibrate(A; radix=true) (src/lapack/dense_utilities.jl:191-213).  For the

@@ -70,6 +70,15 @@ def lib():
         L.orc_expert_solve.restype = ctypes.c_int
         L.orc_inverse.argtypes = [_i64, _dp, _i64, _ip, _dp, _i64]
         L.orc_inverse.restype = ctypes.c_int
+        L.orc_dpotrf.argtypes = [_i64, _dp, _i64]
+        L.orc_dpotrf.restype = _i64
+        L.orc_dpotrs.argtypes = [_i64, _i64, _dp, _i64, _dp, _i64]
+        L.orc_dpotrs.restype = None
+        _zp = ctypes.c_void_p
+        L.orc_zgetrf.argtypes = [_i64, _i64, _zp, _i64, _i64, ctypes.c_int, _ip, _ip]
+        L.orc_zgetrf.restype = ctypes.c_int
+        L.orc_zgetrs.argtypes = [ctypes.c_char, _i64, _i64, _zp, _i64, _ip, _zp, _i64]
+        L.orc_zgetrs.restype = ctypes.c_int
         L.orc_lu_adjoint.argtypes = [_i64, _dp, _i64, _ip, _dp, _dp, _dp, _dp, _i64]
         L.orc_lu_adjoint.restype = ctypes.c_int
         for P, fp in (("d", _dp), ("s", _fp)):
@@ -330,3 +339,44 @@ def inverse(LU, ipiv):
     ipiv = np.ascontiguousarray(ipiv, dtype=np.int64)
     lib().orc_inverse(n, _ptr(LU), max(n, 1), _ptr(ipiv, ctypes.c_int64), _ptr(X), max(n, 1))
     return X
+
+
+def potrf(A):
+    """cholesky_factor(A) -> (L, info): L lower (strict upper zeroed on success)."""
+    L = np.array(A, dtype=np.float64, order="F", copy=True)
+    n = L.shape[0]
+    info = lib().orc_dpotrf(n, _ptr(L), max(n, 1))
+    return L, int(info)
+
+
+def potrs(L, B):
+    """solve(F::CholeskyFactor, B)."""
+    L = np.asfortranarray(L, dtype=np.float64)
+    vec = np.ndim(B) == 1
+    X = np.array(np.reshape(B, (L.shape[0], -1)), dtype=np.float64, order="F", copy=True)
+    n, nrhs = X.shape
+    lib().orc_dpotrs(n, nrhs, _ptr(L), max(n, 1), _ptr(X), max(n, 1))
+    return X[:, 0].copy() if vec else X
+
+
+def zgetrf(A, blocksize: int = 128, check: bool = False):
+    """_lu_factor! for ComplexF64 -> (LU, ipiv (1-based), info)."""
+    LU = np.array(A, dtype=np.complex128, order="F", copy=True)
+    m, n = LU.shape
+    ipiv = np.zeros(max(min(m, n), 1), dtype=np.int64)
+    info = ctypes.c_int64(0)
+    lib().orc_zgetrf(m, n, ctypes.c_void_p(LU.ctypes.data), max(m, 1), blocksize, 1 if check else 0,
+                     _ptr(ipiv, ctypes.c_int64), ctypes.byref(info))
+    return LU, ipiv[:min(m, n)], int(info.value)
+
+
+def zgetrs(LU, ipiv, B, trans: str = "N"):
+    """ldiv!(F, B) ('N'), ldiv!(transpose(F), B) ('T'), ldiv!(F', B) ('C')."""
+    LU = np.asfortranarray(LU, dtype=np.complex128)
+    vec = np.ndim(B) == 1
+    X = np.array(np.reshape(B, (LU.shape[0], -1)), dtype=np.complex128, order="F", copy=True)
+    n, nrhs = X.shape
+    ipiv = np.ascontiguousarray(ipiv, dtype=np.int64)
+    lib().orc_zgetrs(trans.encode(), n, nrhs, ctypes.c_void_p(LU.ctypes.data), max(n, 1),
+                     _ptr(ipiv, ctypes.c_int64), ctypes.c_void_p(X.ctypes.data), max(n, 1))
+    return X[:, 0].copy() if vec else X

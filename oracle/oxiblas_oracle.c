@@ -862,3 +862,261 @@ int orc_inverse(i64 n, const double *LU, i64 lda, const i64 *ipiv, double *X, i6
         for (i64 i = 0; i < n; ++i) X[i + j * ldx] = (i == j) ? 1.0 : 0.0;
     return orc_dgetrs('N', n, n, LU, lda, ipiv, X, ldx);
 }
+
+/* ------------------------------------------------------------------------ */
+/* Cholesky (FP64)                                                           */
+/* ------------------------------------------------------------------------ */
+
+/* _cholesky_recursive!: src/lapack/factorizations.jl:263-291 (LAPACK potrf2).
+ * L (n x n, column-major, lower triangle) in place; leaves of <= `leaf`
+ * columns right-looking (d = sqrt(l_cc), column scaled, l_ij = fma(-l_ic, l_jc,
+ * l_ij) for j > c, i >= j); above, L21 = A21 L11^-T (right solve), A22 -=
+ * L21 L21^T on the lower triangle (one fma chain per element from zero, then
+ * the subtraction), then L22.  Returns 0 or the global 1-based column of the
+ * first pivot that is not finite and positive. */
+static i64 chol_rec(double *L, i64 ld, i64 n, i64 offset, i64 leaf) {
+    if (n <= leaf) {
+        for (i64 c = 0; c < n; ++c) {
+            double d = L[c + c * ld];
+            if (!(isfinite(d) && d > 0)) return offset + c + 1;
+            d = sqrt(d);
+            L[c + c * ld] = d;
+            for (i64 i = c + 1; i < n; ++i) L[i + c * ld] /= d;
+            for (i64 j = c + 1; j < n; ++j) {
+                const double cj = L[j + c * ld];
+                for (i64 i = j; i < n; ++i) L[i + j * ld] = fma(-L[i + c * ld], cj, L[i + j * ld]);
+            }
+        }
+        return 0;
+    }
+    const i64 h = n / 2;
+    i64 info = chol_rec(L, ld, h, offset, leaf);
+    if (info) return info;
+    /* L21 (n-h x h) <- L21 L11^-T: row r of L21 solves x L11^T = a, i.e.
+     * x_j = (a_j - sum_{p<j} x_p l_jp) / l_jj, j ascending */
+    double *L21 = L + h;
+#pragma omp parallel for schedule(static) if ((n - h) * h > 65536)
+    for (i64 r = 0; r < n - h; ++r) {
+        for (i64 j = 0; j < h; ++j) {
+            double s = L21[r + j * ld];
+            for (i64 p = 0; p < j; ++p) s = fma(-L21[r + p * ld], L[j + p * ld], s);
+            L21[r + j * ld] = s / L[j + j * ld];
+        }
+    }
+    /* A22 -= L21 L21^T, lower triangle */
+    double *A22 = L + h + h * ld;
+    const i64 m = n - h;
+#pragma omp parallel for schedule(dynamic, 8) if (m * m * h > 2000000)
+    for (i64 j = 0; j < m; ++j)
+        for (i64 i = j; i < m; ++i) {
+            double s = 0.0;
+            for (i64 p = 0; p < h; ++p) s = fma(L21[i + p * ld], L21[j + p * ld], s);
+            A22[i + j * ld] -= s;
+        }
+    return chol_rec(A22, ld, m, offset + h, leaf);
+}
+
+/* cholesky_factor(A): L from the lower triangle of A (leaf 64 for real types,
+ * :212-216), strict upper triangle zeroed when it succeeds.  Returns info. */
+i64 orc_dpotrf(i64 n, double *A, i64 lda) {
+    const i64 info = chol_rec(A, lda, n, 0, 64);
+    if (info == 0)
+        for (i64 j = 0; j < n; ++j)
+            for (i64 i = 0; i < j; ++i) A[i + j * lda] = 0.0;
+    return info;
+}
+
+/* solve(F::CholeskyFactor, b) (:293-305): L y = b, then L^T x = y. */
+void orc_dpotrs(i64 n, i64 nrhs, const double *L, i64 ldl, double *B, i64 ldb) {
+    for (i64 c = 0; c < nrhs; ++c) {
+        double *b = B + c * ldb;
+        for (i64 i = 0; i < n; ++i) {
+            double s = b[i];
+            for (i64 p = 0; p < i; ++p) s = fma(-L[i + p * ldl], b[p], s);
+            b[i] = s / L[i + i * ldl];
+        }
+        for (i64 i = n - 1; i >= 0; --i) {
+            double s = b[i];
+            for (i64 p = i + 1; p < n; ++p) s = fma(-L[p + i * ldl], b[p], s);
+            b[i] = s / L[i + i * ldl];
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Complex LU (ComplexF64)                                                   */
+/* ------------------------------------------------------------------------ */
+#include <complex.h>
+typedef double _Complex zc_t;
+
+/* muladd(a, b, c) on complex numbers: the product, then the sum */
+static inline zc_t zmuladd(zc_t a, zc_t b, zc_t c) {
+    const double ar = creal(a), ai = cimag(a), br = creal(b), bi = cimag(b);
+    return CMPLX(ar * br - ai * bi + creal(c), ar * bi + ai * br + cimag(c));
+}
+static inline double zabs2(zc_t a) { return creal(a) * creal(a) + cimag(a) * cimag(a); }
+/* a / b as Julia's complex division (Smith-style scaling is not restated: the
+ * test matrices keep |b| moderate) */
+static inline zc_t zdiv(zc_t a, zc_t b) { return a / b; }
+
+/* _lu_pivot, complex branch (src/lapack/factorizations.jl:92-107): abs2
+ * compared with strict '>', the first row wins a tie; if the largest square
+ * is not finite, the scan is redone with abs. */
+static i64 z_pivot(const zc_t *c, i64 mp, i64 j) {
+    i64 p = j;
+    double best = zabs2(c[j]);
+    for (i64 i = j + 1; i < mp; ++i) {
+        const double v = zabs2(c[i]);
+        if (v > best) { best = v; p = i; }
+    }
+    if (isfinite(best)) return p;
+    p = j;
+    best = cabs(c[j]);
+    for (i64 i = j + 1; i < mp; ++i) {
+        const double v = cabs(c[i]);
+        if (v > best) { best = v; p = i; }
+    }
+    return p;
+}
+
+static void z_swap(zc_t *A, i64 lda, const i64 *piv, i64 off, i64 j1, i64 j2, i64 c0, i64 c1) {
+    for (i64 col = c0; col < c1; ++col) {
+        zc_t *a = A + col * lda;
+        for (i64 j = j1; j <= j2; ++j) {
+            const i64 p = piv[off + j] - 1 - off;
+            if (p != j) { zc_t t = a[j]; a[j] = a[p]; a[p] = t; }
+        }
+    }
+}
+
+/* C - A B, one dot product per element in k order from zero, then the
+ * subtraction (the reference GEMM's form) */
+static void z_gemm_minus(i64 m, i64 n, i64 k, const zc_t *A, i64 lda, const zc_t *B, i64 ldb, zc_t *C,
+                         i64 ldc) {
+    if (m <= 0 || n <= 0 || k <= 0) return;
+#pragma omp parallel for schedule(static) if ((double)m * n * k > 2e6)
+    for (i64 j = 0; j < n; ++j)
+        for (i64 i = 0; i < m; ++i) {
+            zc_t s = 0;
+            for (i64 p = 0; p < k; ++p) s = zmuladd(A[i + p * lda], B[p + j * ldb], s);
+            C[i + j * ldc] -= s;
+        }
+}
+
+/* unit lower (upper = 0) or non-unit upper (upper = 1) left solve by rows,
+ * s = b; s = muladd(-A[i,p], b[p], s) (_trsm_leaf_generic!); conj applies the
+ * conjugate transpose of A (for the 'C' solves) */
+static void z_trsm(i64 nt, i64 nrhs, const zc_t *A, i64 lda, zc_t *B, i64 ldb, int upper, int unit,
+                   int transposed, int conjugate) {
+    for (i64 j = 0; j < nrhs; ++j) {
+        zc_t *b = B + j * ldb;
+        if (!upper) {
+            for (i64 i = 0; i < nt; ++i) {
+                zc_t s = b[i];
+                for (i64 p = 0; p < i; ++p) {
+                    zc_t a = transposed ? A[p + i * lda] : A[i + p * lda];
+                    if (conjugate) a = conj(a);
+                    s = zmuladd(-a, b[p], s);
+                }
+                if (!unit) { zc_t d = A[i + i * lda]; if (conjugate) d = conj(d); s = zdiv(s, d); }
+                b[i] = s;
+            }
+        } else {
+            for (i64 i = nt - 1; i >= 0; --i) {
+                zc_t s = b[i];
+                for (i64 p = i + 1; p < nt; ++p) {
+                    zc_t a = transposed ? A[p + i * lda] : A[i + p * lda];
+                    if (conjugate) a = conj(a);
+                    s = zmuladd(-a, b[p], s);
+                }
+                if (!unit) { zc_t d = A[i + i * lda]; if (conjugate) d = conj(d); s = zdiv(s, d); }
+                b[i] = s;
+            }
+        }
+    }
+}
+
+/* _lu_panel! with the complex leaf of 16 columns (:113) */
+static int z_panel(zc_t *Pm, i64 ldp, i64 mp, i64 np, i64 *piv, i64 off, i64 *info, int check) {
+    if (np <= 16) {
+        const i64 q = mp < np ? mp : np;
+        for (i64 j = 0; j < q; ++j) {
+            const i64 p = z_pivot(Pm + j * ldp, mp, j);
+            piv[off + j] = off + p + 1;
+            if (p != j)
+                for (i64 col = 0; col < np; ++col) {
+                    zc_t t = Pm[j + col * ldp]; Pm[j + col * ldp] = Pm[p + col * ldp]; Pm[p + col * ldp] = t;
+                }
+            const zc_t d = Pm[j + j * ldp];
+            if (d == 0) {
+                if (*info == 0) *info = off + j + 1;
+                if (check) return 1;
+                continue;
+            }
+            for (i64 i = j + 1; i < mp; ++i) Pm[i + j * ldp] = zdiv(Pm[i + j * ldp], d);
+            for (i64 col = j + 1; col < np; ++col) {
+                const zc_t u = Pm[j + col * ldp];
+                for (i64 i = j + 1; i < mp; ++i) Pm[i + col * ldp] = zmuladd(-Pm[i + j * ldp], u, Pm[i + col * ldp]);
+            }
+        }
+        return 0;
+    }
+    const i64 h = np / 2;
+    if (z_panel(Pm, ldp, mp, h, piv, off, info, check)) return 1;
+    z_swap(Pm, ldp, piv, off, 0, h - 1, h, np);
+    z_trsm(h, np - h, Pm, ldp, Pm + h * ldp, ldp, 0, 1, 0, 0);
+    if (mp > h) {
+        z_gemm_minus(mp - h, np - h, h, Pm + h, ldp, Pm + h * ldp, ldp, Pm + h + h * ldp, ldp);
+        if (z_panel(Pm + h + h * ldp, ldp, mp - h, np - h, piv, off + h, info, check)) return 1;
+        const i64 q = mp < np ? mp : np;
+        z_swap(Pm, ldp, piv, off, h, q - 1, 0, h);
+    }
+    return 0;
+}
+
+/* _lu_factor! for ComplexF64 (blocked right-looking, nb, sequential order) */
+int orc_zgetrf(i64 m, i64 n, zc_t *A, i64 lda, i64 nb, int check, i64 *ipiv, i64 *info) {
+    const i64 q = m < n ? m : n;
+    *info = 0;
+    if (nb <= 0) return 2;
+    for (i64 f = 0; f < q; f += nb) {
+        const i64 l = f + nb < q ? f + nb : q;
+        if (z_panel(A + f + f * lda, lda, m - f, l - f, ipiv, f, info, check)) return 1;
+        z_swap(A, lda, ipiv, 0, f, l - 1, 0, f);
+        z_swap(A, lda, ipiv, 0, f, l - 1, l, n);
+        if (l >= n) continue;
+        z_trsm(l - f, n - l, A + f + f * lda, lda, A + f + l * lda, lda, 0, 1, 0, 0);
+        if (l >= m) continue;
+        z_gemm_minus(m - l, n - l, l - f, A + l + f * lda, lda, A + f + l * lda, lda, A + l + l * lda, lda);
+    }
+    return 0;
+}
+
+/* ldiv!(F, B) ('N'), ldiv!(transpose(F), B) ('T'), ldiv!(F', B) ('C') */
+int orc_zgetrs(char trans, i64 n, i64 nrhs, const zc_t *LU, i64 lda, const i64 *ipiv, zc_t *B, i64 ldb) {
+    if (n == 0 || nrhs == 0) return 0;
+    if (trans == 'N') {
+        for (i64 c = 0; c < nrhs; ++c) {
+            zc_t *b = B + c * ldb;
+            for (i64 j = 0; j < n; ++j) {
+                const i64 p = ipiv[j] - 1;
+                if (p != j) { zc_t t = b[j]; b[j] = b[p]; b[p] = t; }
+            }
+        }
+        z_trsm(n, nrhs, LU, lda, B, ldb, 0, 1, 0, 0);
+        z_trsm(n, nrhs, LU, lda, B, ldb, 1, 0, 0, 0);
+        return 0;
+    }
+    const int cj = (trans == 'C');
+    /* U^T (or U^H) is lower and non-unit, L^T (L^H) upper and unit */
+    z_trsm(n, nrhs, LU, lda, B, ldb, 0, 0, 1, cj);
+    z_trsm(n, nrhs, LU, lda, B, ldb, 1, 1, 1, cj);
+    for (i64 c = 0; c < nrhs; ++c) {
+        zc_t *b = B + c * ldb;
+        for (i64 j = n - 1; j >= 0; --j) {
+            const i64 p = ipiv[j] - 1;
+            if (p != j) { zc_t t = b[j]; b[j] = b[p]; b[p] = t; }
+        }
+    }
+    return 0;
+}

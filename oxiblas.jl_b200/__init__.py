@@ -13,6 +13,7 @@ from .lu import (LU, colmajor_copy, det, gemm_update, ldiv, ldiv_, ldiv_into, lo
 from .mixed import equilibrate, gemm_update_lowp, mixed_solve, mixed_solve_device
 from .adjoint import lu_adjoint, solve
 from .expert import expert_solve, factorize, inv, inverse_norm_estimate, refine_solve
+from .cholesky import Cholesky, PosDefException, cholesky, cholesky_
 from .batched import BatchedLU, autotune as batched_autotune, set_tuning as batched_set_tuning, \
     tuning as batched_tuning
 from . import synthetic
@@ -22,5 +23,6 @@ __all__ = [
     "colmajor_copy", "SingularException", "DimensionMismatch", "ArgumentError", "ExtensionMissing",
     "Handle", "load", "exported_symbols", "mixed_solve", "mixed_solve_device", "gemm_update_lowp",
     "equilibrate", "expert_solve", "refine_solve", "inverse_norm_estimate", "inv", "factorize",
+    "Cholesky", "PosDefException", "cholesky", "cholesky_",
     "lu_adjoint", "solve", "BatchedLU", "batched_autotune", "batched_tuning", "batched_set_tuning",
 ]

@@ -17,6 +17,7 @@ LIB_PATH = os.path.join(HERE, "liboxiblas_b200.so")
 OXI_OK, OXI_EINVAL, OXI_ESINGULAR, OXI_ENONFINITE, OXI_EOVERFLOW = 0, 1, 2, 3, 4
 OXI_ECUDA, OXI_ETIMEOUT, OXI_ENOMEM, OXI_ENOTCONVERGED = 5, 6, 7, 8
 OXI_ESCRATCH = 9
+OXI_ENOTPOSDEF = 10
 OPT_BLOCKSIZE, OPT_GEMM, OPT_TRSM_LEAF, OPT_LOOKAHEAD = 1, 2, 3, 4
 OPT_MIXED_BLOCKSIZE, OPT_STOP_NORMWISE, OPT_GMRES_RESTART = 5, 6, 7
 OPT_GRAPHS, OPT_TOURNAMENT = 8, 9
@@ -88,6 +89,10 @@ _SIGS = {
     "oxi_dinverse_norm_estimate": ([_vp, _i64, _vp, _i64, _vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)],
                                    ctypes.c_int),
     "oxi_dgetri": ([_vp, _i64, _vp, _i64, _vp, _vp, _i64], ctypes.c_int),
+    "oxi_dpotrf": ([_vp, _i64, _vp, _i64, ctypes.POINTER(_i64)], ctypes.c_int),
+    "oxi_dpotrs": ([_vp, _i64, _i64, _vp, _i64, _vp, _i64], ctypes.c_int),
+    "oxi_zgetrf": ([_vp, _i64, _i64, _vp, _i64, _vp, ctypes.POINTER(_i64)], ctypes.c_int),
+    "oxi_zgetrs": ([_vp, ctypes.c_char, _i64, _i64, _vp, _i64, _vp, _vp, _i64], ctypes.c_int),
     "oxi_dequilibrate": ([_vp, _i64, _i64, _vp, _i64, _vp, _vp, _vp, _i64], ctypes.c_int),
     "oxi_dgesv_mixed": ([_vp, ctypes.c_int, ctypes.c_int, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64,
                          ctypes.c_int, ctypes.c_double, _vp], ctypes.c_int),

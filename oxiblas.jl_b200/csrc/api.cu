@@ -143,6 +143,7 @@ const char *oxi_status_string(int s) {
         case OXI_ETIMEOUT: return "device wait timed out";
         case OXI_ENOMEM: return "out of memory";
         case OXI_ENOTCONVERGED: return "refinement did not converge";
+        case OXI_ENOTPOSDEF: return "matrix is not positive definite";
         case OXI_ESCRATCH:
             return "size exceeds the fixed scratch of oxi_dgetrs_noalloc "
                    "(n <= 65536 and n * nrhs <= 917504)";

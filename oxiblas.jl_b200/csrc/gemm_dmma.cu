@@ -52,7 +52,7 @@ constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barrier
 
 __global__ void __launch_bounds__(NTHREADS, 2)
 k_gemm_dmma(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-            double *__restrict__ C, i64 ldc, int M, int N, int K, int *__restrict__ ab) {
+            double *__restrict__ C, i64 ldc, int M, int N, int K, int *__restrict__ ab, int upper_only) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~uintptr_t(1023));
     uint64_t *full = (uint64_t *)(smem + STAGES * STAGE_BYTES);
@@ -60,6 +60,9 @@ k_gemm_dmma(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUt
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    // upper_only (a symmetric rank-k update of the upper triangle): tiles that
+    // lie wholly below the diagonal are not computed
+    if (upper_only && m0 > n0 + BN - 1) return;
     const int KT = (K + BK - 1) / BK;
 
     __shared__ int s_skip;
@@ -147,8 +150,11 @@ k_gemm_dmma(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUt
     }
 
     // epilogue: C -= acc.  The eight C pairs of a row are loaded before any is
-    // used so their round trips overlap (16-byte accesses when aligned).
-    const bool vec2 = ((ldc & 1) == 0) && ((((uintptr_t)C) & 15) == 0);
+    // used so their round trips overlap (16-byte accesses when aligned).  A
+    // symmetric update's tile that crosses the diagonal writes only the
+    // elements on and above it (the other triangle stays as it was).
+    const bool vec2 = ((ldc & 1) == 0) && ((((uintptr_t)C) & 15) == 0) && !(upper_only && m0 + BM - 1 > n0);
+    const int cmin_row = upper_only ? 1 : 0;  // 1: column c is written only when c >= r
 #pragma unroll
     for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
@@ -162,8 +168,8 @@ k_gemm_dmma(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUt
                 const int c = n0 + wn * 32 + nt * 8 + 2 * tig;
                 if (c + 1 < N && vec2) cv[nt] = __ldcs((const double2 *)(crow + c));
                 else {
-                    cv[nt].x = (c < N) ? crow[c] : 0.0;
-                    cv[nt].y = (c + 1 < N) ? crow[c + 1] : 0.0;
+                    cv[nt].x = (c < N && (!cmin_row || c >= r)) ? crow[c] : 0.0;
+                    cv[nt].y = (c + 1 < N && (!cmin_row || c + 1 >= r)) ? crow[c + 1] : 0.0;
                 }
             }
 #pragma unroll
@@ -174,19 +180,21 @@ k_gemm_dmma(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUt
                 v.y = cv[nt].y - acc[mt][nt][2 * h + 1];
                 if (c + 1 < N && vec2) __stcs((double2 *)(crow + c), v);
                 else {
-                    if (c < N) crow[c] = v.x;
-                    if (c + 1 < N) crow[c + 1] = v.y;
+                    if (c < N && (!cmin_row || c >= r)) crow[c] = v.x;
+                    if (c + 1 < N && (!cmin_row || c + 1 >= r)) crow[c + 1] = v.y;
                 }
             }
         }
 }
 
 void launch_gemm_dmma(double *C, i64 ldc, const double *A, i64 lda, const double *B, i64 ldb, i64 M,
-                      i64 N, i64 K, cudaStream_t s) {
+                      i64 N, i64 K, cudaStream_t s, bool upper_only) {
     if (M <= 0 || N <= 0 || K <= 0) return;
     const bool aligned = ((uintptr_t)A % 16 == 0) && ((uintptr_t)B % 16 == 0) && (lda % 2 == 0) &&
                          (ldb % 2 == 0) && M < (1 << 30) && N < (1 << 30) && K < (1 << 30);
-    if (!aligned) {  // TMA needs 16-byte aligned bases and pitches
+    if (!aligned) {  // TMA needs 16-byte aligned bases and pitches (the whole block: same results)
+        if (upper_only)  // the plain kernel would write both triangles; callers align first
+            throw CudaError{cudaErrorInvalidValue, "symmetric update needs 16-byte aligned operands"};
         launch_gemm_ref<double>(C, ldc, A, lda, B, ldb, M, N, K, s);
         return;
     }
@@ -197,8 +205,9 @@ void launch_gemm_dmma(double *C, i64 ldc, const double *A, i64 lda, const double
                  CU_TENSOR_MAP_SWIZZLE_NONE);
     set_max_dyn_smem((const void *)k_gemm_dmma, SMEM_BYTES);
     dim3 grid((unsigned)((N + BN - 1) / BN), (unsigned)((M + BM - 1) / BM));
-    ProfScope ps(KC_GEMM_DMMA, s, 2.0 * M * N * K, 8.0 * (2.0 * M * N + M * K + K * N));
-    k_gemm_dmma<<<grid, NTHREADS, SMEM_BYTES, s>>>(tmA, tmB, C, ldc, (int)M, (int)N, (int)K, cur_abort());
+    ProfScope ps(KC_GEMM_DMMA, s, (upper_only ? 1.0 : 2.0) * M * N * K, 8.0 * (2.0 * M * N + M * K + K * N));
+    k_gemm_dmma<<<grid, NTHREADS, SMEM_BYTES, s>>>(tmA, tmB, C, ldc, (int)M, (int)N, (int)K, cur_abort(),
+                                                   upper_only ? 1 : 0);
     OXI_LAUNCH_CHECK();
 }
 

@@ -319,9 +319,10 @@ void launch_gemm_simt(T *C, i64 ldc, const T *A, i64 lda, const T *B, i64 ldb, i
 template <typename T>
 void launch_gemm_ref(T *C, i64 ldc, const T *A, i64 lda, const T *B, i64 ldb, i64 M, i64 N,
                      i64 K, cudaStream_t s);
-// FP64 tensor-core (DMMA, TMA-fed) version.
+// FP64 tensor-core (DMMA, TMA-fed) version.  upper_only: only the tiles that
+// reach the upper triangle of C (M == N, a symmetric update) are computed.
 void launch_gemm_dmma(double *C, i64 ldc, const double *A, i64 lda, const double *B, i64 ldb,
-                      i64 M, i64 N, i64 K, cudaStream_t s);
+                      i64 M, i64 N, i64 K, cudaStream_t s, bool upper_only = false);
 
 // tcgen05 GEMM: C (FP32 row-major) -= scale * A16 * B16^T, 16-bit K-major operands.
 void launch_gemm_tc(int fmt, float *C, i64 ldc, const void *A16, i64 lda16, const void *B16,

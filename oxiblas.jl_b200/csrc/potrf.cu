@@ -1,0 +1,262 @@
+// Dense Cholesky factorization A = L L^T (FP64) and its solve.
+//
+// Replaces cholesky_factor / _cholesky_factor! (src/lapack/factorizations.jl:
+// 205-291, LAPACK potrf2 recursion with 64-column leaves) and the solve of a
+// CholeskyFactor (:293-305) behind OxiBLAS.cholesky / cholesky! and
+// ldiv!(F::Cholesky, B) (src/api/linalg_api.jl:221-290).
+//
+// Layout: the lower triangle of the caller's column-major A, read with the
+// same leading dimension as a ROW-major matrix, is the upper triangle of that
+// matrix, and L (column-major, lower) is U = L^T (row-major, upper) in the same
+// memory.  So the factorization runs in place, row-oriented, with no copy:
+// blocks of NB rows of U, each
+//   1. U_kk = chol(A_kk) and W = U_kk^-1, one CTA, the block in shared memory;
+//   2. U_k,right = W^T A_k,right on the FP64 tensor cores (the block-row solve
+//      as a product with the inverted diagonal block, into a scratch block row
+//      X, then copied into place);
+//   3. A_right,right -= X^T X on the FP64 tensor cores, upper triangle only
+//      (tiles wholly below the diagonal skipped, crossing tiles write only on
+//      and above it), its left operand a transposed copy of X so that both
+//      operands are K-contiguous.
+// The reference solves the block row by substitution (trsm!); the product with
+// the inverted 128 x 128 block is the same solve with another association of
+// the sums (the diagonal blocks of a positive definite matrix's factor are
+// well conditioned: cond(U_kk)^2 <= cond(A)).
+// A pivot that is not finite and positive stops the factorization there: info
+// is its 1-based column (PosDefException(info)); the inverse of that block and
+// of every later one is written as zero, so the later products change nothing,
+// and the block rows are not copied back.
+#include <algorithm>
+#include <cmath>
+#include "oxi_internal.h"
+#include "tma_util.cuh"
+
+namespace oxi {
+
+namespace {
+constexpr int PO_NB = 128;          // block rows per step
+constexpr int PO_NT = 512;          // threads of the diagonal-block kernel (4 per column of the inverse)
+}  // namespace
+
+// Cholesky of the t x t diagonal block (row-major upper, ld) in shared memory:
+// for each row c, d = sqrt(a_cc), the row scaled by d, then the rank-1 update
+// of the upper triangle below it, a_ij = fma(-u_ci, u_cj, a_ij) for c < i <= j
+// (the reference leaf's column updates, src/lapack/factorizations.jl:266-282,
+// read through the transposition).  Then W = U^-1 by columns, four threads per
+// column (w_jj = 1/u_jj; w_ij = -(sum_{p=i+1..j} u_ip w_pj) / u_ii for i = j-1
+// down to 0), W^T kept in the block's unused strict lower triangle, and
+// Wneg = -W^T (t x t, row-major, lower) written for the block-row product.
+__global__ void __launch_bounds__(PO_NT) k_potrf_diag(double *__restrict__ U, i64 ld, int t, i64 g0,
+                                                      int64_t *__restrict__ info, double *__restrict__ Wneg) {
+    extern __shared__ __align__(16) double po_smem[];
+    const int lp = t + 1;
+    double *S = po_smem;
+    double *s_inv = po_smem + (size_t)t * lp;  // 1 / u_ii
+    __shared__ int s_fail;
+    const int tid = threadIdx.x;
+    if (tid == 0) s_fail = (*(volatile int64_t *)info != 0) ? 1 : 0;
+    __syncthreads();
+    if (s_fail) {  // an earlier block failed: later products change nothing
+        for (int e = tid; e < t * t; e += PO_NT) Wneg[e] = 0.0;
+        return;
+    }
+    for (int e = tid; e < t * t; e += PO_NT) {
+        const int i = e / t, j = e - i * t;
+        S[i * lp + j] = (j >= i) ? U[(i64)i * ld + j] : 0.0;
+    }
+    __syncthreads();
+    for (int c = 0; c < t; ++c) {
+        double d = S[c * lp + c];
+        if (!(d > 0.0) || !isfinite(d)) {  // not positive definite at global column g0 + c + 1
+            if (tid == 0) {
+                s_fail = 1;
+                if (*info == 0) *info = g0 + c + 1;
+            }
+            break;
+        }
+        d = sqrt(d);
+        // the row right of the pivot (the pivot itself is written after the
+        // barrier: every thread has read it by then)
+        for (int j = c + 1 + tid; j < t; j += PO_NT) S[c * lp + j] = S[c * lp + j] / d;
+        __syncthreads();
+        if (tid == 0) S[c * lp + c] = d;
+        // rows i below c, columns j >= i: 16 row groups x 32 columns of threads
+        const int tx = tid & 31, ty = tid >> 5;
+        for (int i = c + 1 + ty; i < t; i += PO_NT / 32) {
+            const double ui = S[c * lp + i];
+            for (int j = i + tx; j < t; j += 32) S[i * lp + j] = fma(-ui, S[c * lp + j], S[i * lp + j]);
+        }
+        __syncthreads();
+    }
+    __syncthreads();
+    for (int e = tid; e < t * t; e += PO_NT) {
+        const int i = e / t, j = e - i * t;
+        if (j >= i) U[(i64)i * ld + j] = S[i * lp + j];
+    }
+    if (s_fail) {
+        for (int e = tid; e < t * t; e += PO_NT) Wneg[e] = 0.0;
+        return;
+    }
+    // W = U^-1, column j by the four threads 4j .. 4j+3 (one warp holds 8 columns)
+    for (int i = tid; i < t; i += PO_NT) s_inv[i] = 1.0 / S[i * lp + i];
+    __syncthreads();
+    {
+        const int j = tid >> 2, sub = tid & 3;
+        const unsigned quad = 0xFu << ((threadIdx.x & 31) & ~3);
+        if (j < t) {
+            double *wrow = S + j * lp;  // W^T row j = W column j, entries 0..j-1 (strict lower of S)
+            const double wjj = s_inv[j];
+            for (int i = j - 1; i >= 0; --i) {
+                const double *urow = S + i * lp;
+                double part = 0.0;
+                for (int p = i + 1 + sub; p <= j; p += 4) part = fma(urow[p], (p == j) ? wjj : wrow[p], part);
+                part += __shfl_xor_sync(quad, part, 1);
+                part += __shfl_xor_sync(quad, part, 2);
+                if (sub == 0) wrow[i] = -part * s_inv[i];
+                __syncwarp(quad);
+            }
+        }
+    }
+    __syncthreads();
+    // Wneg = -W^T: row i holds -w_pi for p <= i
+    for (int e = tid; e < t * t; e += PO_NT) {
+        const int i = e / t, p = e - i * t;
+        Wneg[e] = (p < i) ? -S[i * lp + p] : (p == i ? -s_inv[i] : 0.0);
+    }
+}
+
+// The solved block row back into place (row-major t x N), unless the
+// factorization failed.
+__global__ void k_copy_block_row(const double *__restrict__ X, i64 ldx, double *__restrict__ B, i64 ldb, int t,
+                                 i64 N, const int64_t *__restrict__ info) {
+    if (*(volatile const int64_t *)info != 0) return;
+    const i64 idx = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (i64)t * N) return;
+    const i64 i = idx / N, c = idx - i * N;
+    B[i * ldb + c] = X[i * ldx + c];
+}
+
+// The strict lower triangle of the row-major view (the strict upper triangle
+// of the caller's column-major matrix) set to zero, as the reference does.
+__global__ void k_zero_strict_lower(double *__restrict__ U, i64 ld, int n, const int64_t *__restrict__ info) {
+    if (*info != 0) return;  // as the reference: a failed factorization keeps its other triangle
+    const i64 idx = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (i64)n * n) return;
+    const int i = (int)(idx / n), j = (int)(idx - (i64)i * n);
+    if (j < i) U[(i64)i * ld + j] = 0.0;
+}
+
+// Workspace of one factorization: T (n x NB), Bc and X (NB x ldx each), Wneg (NB x NB).
+static size_t potrf_work_doubles(i64 n) {
+    const i64 ldx = (n + 1) / 2 * 2;
+    return (size_t)n * PO_NB + 2 * (size_t)PO_NB * ldx + (size_t)PO_NB * PO_NB + 64;
+}
+
+// One factorization: U in place (row-major view), *d_info set on failure.
+static void potrf_rowmajor(oxi_handle_s *h, double *U, i64 ld, i64 n, int64_t *d_info, double *work) {
+    cudaStream_t s = h->stream;
+    const i64 ldx = (n + 1) / 2 * 2;
+    double *T = work;
+    double *Bc = T + (size_t)n * PO_NB;
+    double *X = Bc + (size_t)PO_NB * ldx;
+    double *Wneg = X + (size_t)PO_NB * ldx;
+    for (i64 k0 = 0; k0 < n; k0 += PO_NB) {
+        const int t = (int)std::min<i64>(PO_NB, n - k0);
+        double *Ukk = U + k0 * ld + k0;
+        {
+            const size_t smem = sizeof(double) * ((size_t)t * (t + 1) + t);
+            set_max_dyn_smem((const void *)k_potrf_diag, (int)(sizeof(double) * (PO_NB * (PO_NB + 1) + PO_NB)));
+            ProfScope ps(KC_LEAF, s, (double)t * t * t * (2.0 / 3.0), 16.0 * t * t);
+            k_potrf_diag<<<1, PO_NT, smem, s>>>(Ukk, ld, t, k0, d_info, Wneg);
+            OXI_LAUNCH_CHECK();
+        }
+        const i64 right = n - k0 - t;
+        if (right <= 0) break;
+        double *Bk = Ukk + t;  // rows k0..k0+t, columns k0+t..n
+        // the tensor-core GEMM reads its operands through TMA (16-byte aligned
+        // rows); a block row at an odd offset or pitch is copied first
+        const double *Bop = Bk;
+        i64 ldb_op = ld;
+        if ((uintptr_t)Bk % 16 != 0 || ld % 2 != 0) {
+            OXI_CUDA(cudaMemcpy2DAsync(Bc, sizeof(double) * ldx, Bk, sizeof(double) * ld, sizeof(double) * right,
+                                       (size_t)t, cudaMemcpyDeviceToDevice, s));
+            Bop = Bc;
+            ldb_op = ldx;
+        }
+        // X = 0 - (-W^T) A_k,right = U_kk^-T A_k,right
+        OXI_CUDA(cudaMemsetAsync(X, 0, sizeof(double) * (size_t)t * ldx, s));
+        launch_gemm_dmma(X, ldx, Wneg, t, Bop, ldb_op, t, right, t, s);
+        k_copy_block_row<<<(unsigned)(((i64)t * right + 255) / 256), 256, 0, s>>>(X, ldx, Bk, ld, t, right, d_info);
+        OXI_LAUNCH_CHECK();
+        // T = X^T (right x t, row-major): X read as a column-major right x t matrix
+        launch_cm_to_rm<double, double>(X, ldx, T, t, right, t, s);
+        double *A22 = U + (k0 + t) * ld + (k0 + t);
+        launch_gemm_dmma(A22, ld, T, t, X, ldx, right, right, t, s, /*upper_only=*/true);
+    }
+    const i64 tot = n * n;
+    k_zero_strict_lower<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(U, ld, (int)n, d_info);
+    OXI_LAUNCH_CHECK();
+}
+
+// ---------------------------------------------------------------------------
+// Solves with the factor: L y = b, then L^T x = y (the reference's two
+// triangular solves, src/lapack/factorizations.jl:293-305).  L is the caller's
+// column-major lower factor: the non-unit lower block-operator solve and its
+// transpose (solve.cu).
+// ---------------------------------------------------------------------------
+template <typename T>
+void potrs_colmajor(oxi_handle_s *h, i64 n, i64 nrhs, const T *L, i64 ldl, T *B, i64 ldb, int *d_err);
+
+}  // namespace oxi
+
+extern "C" int oxi_dpotrf(oxi_handle_t h, int64_t n, double *dA, int64_t lda, int64_t *h_info) {
+    using namespace oxi;
+    if (!h || !h_info || n < 0 || lda < std::max<int64_t>(1, n)) return OXI_EINVAL;
+    *h_info = 0;
+    if (n == 0) return OXI_OK;
+    if (!dA || n >= (1ll << 31)) return OXI_EINVAL;
+    try {
+        ProfGuard pg(&h->prof);
+        OXI_CUDA(cudaSetDevice(h->device));
+        AbortScope ab(h);
+        char *sc = (char *)h->scratch.get(kScratchBytes);
+        int64_t *d_info = (int64_t *)sc;
+        OXI_CUDA(cudaMemsetAsync(d_info, 0, sizeof(int64_t), h->stream));
+        // T (the transposed block row, n x NB) and room for an aligned copy of the block row
+        double *work = (double *)h->work.get(sizeof(double) * potrf_work_doubles(n));
+        potrf_rowmajor(h, dA, lda, n, d_info, work);
+        int64_t *hi = (int64_t *)h->host_ws.get(64);
+        OXI_CUDA(cudaMemcpyAsync(hi, d_info, sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
+        queue_abort_read(h, (int *)(hi + 2));
+        OXI_CUDA(cudaStreamSynchronize(h->stream));
+        *h_info = hi[0];
+        const int we = check_abort(h, (const int *)(hi + 2));
+        if (we != OXI_OK) return we;
+        return hi[0] > 0 ? OXI_ENOTPOSDEF : OXI_OK;
+    } catch (const CudaError &e) {
+        h->last_error = std::string(e.what) + ": " + cudaGetErrorString(e.code);
+        return OXI_ECUDA;
+    }
+}
+
+extern "C" int oxi_dpotrs(oxi_handle_t h, int64_t n, int64_t nrhs, const double *dL, int64_t ldl, double *dB,
+                          int64_t ldb) {
+    using namespace oxi;
+    if (!h || n < 0 || nrhs < 0 || ldl < std::max<int64_t>(1, n) || ldb < std::max<int64_t>(1, n))
+        return OXI_EINVAL;
+    if (n == 0 || nrhs == 0) return OXI_OK;
+    if (!dL || !dB || n >= (1ll << 31)) return OXI_EINVAL;
+    try {
+        ProfGuard pg(&h->prof);
+        OXI_CUDA(cudaSetDevice(h->device));
+        AbortScope ab(h);
+        potrs_colmajor<double>(h, n, nrhs, dL, ldl, dB, ldb, ab.word);
+        int *he = (int *)h->host_ws.get(64);
+        queue_abort_read(h, he);
+        OXI_CUDA(cudaStreamSynchronize(h->stream));
+        return check_abort(h, he);
+    } catch (const CudaError &e) {
+        h->last_error = std::string(e.what) + ": " + cudaGetErrorString(e.code);
+        return OXI_ECUDA;
+    }
+}

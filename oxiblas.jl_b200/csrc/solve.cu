@@ -805,6 +805,29 @@ void getrs_perm(oxi_handle_s *h, char trans, i64 n, i64 nrhs, const T *LU, i64 l
         OXI_LAUNCH_CHECK();
     }
 }
+// Cholesky solve with the column-major lower factor L: L Y = B (non-unit lower),
+// then L^T X = Y (its transpose, upper); B overwritten.
+template <typename T>
+void potrs_colmajor(oxi_handle_s *h, i64 n, i64 nrhs, const T *L, i64 ldl, T *B, i64 ldb, int *d_err) {
+    cudaStream_t s = h->stream;
+    const i64 nb = (n + SB - 1) / SB;
+    char *ws = (char *)h->solve_ws.get(sizeof(T) * (size_t)n * nrhs + sizeof(int) * (nb + 8) + 256);
+    T *X = (T *)ws;
+    int *ctl = (int *)(ws + ((sizeof(T) * (size_t)n * nrhs + 255) & ~size_t(255)));
+    T *P1 = (T *)h->trsv_ws.get(2 * sizeof(T) * (size_t)nb * TRSV_OPS);
+    T *P2 = P1 + (size_t)nb * TRSV_OPS;
+    unsigned long long *xtag = xtag_words(h, n);
+    OXI_CUDA(cudaMemcpy2DAsync(X, n * sizeof(T), B, ldb * sizeof(T), n * sizeof(T), nrhs,
+                               cudaMemcpyDeviceToDevice, s));
+    trsv_prep_launch<T, false, false, false>(L, ldl, (int)n, P1, s);
+    trsv_prep_launch<T, false, false, true>(L, ldl, (int)n, P2, s);
+    trsv3_launch<T, false, false>(L, ldl, X, n, (int)n, (int)nrhs, ctl, d_err, s, P1, xtag);
+    trsv3_launch<T, false, true>(L, ldl, X, n, (int)n, (int)nrhs, ctl, d_err, s, P2, xtag);
+    OXI_CUDA(cudaMemcpy2DAsync(B, ldb * sizeof(T), X, n * sizeof(T), n * sizeof(T), nrhs,
+                               cudaMemcpyDeviceToDevice, s));
+}
+template void potrs_colmajor<double>(oxi_handle_s *, i64, i64, const double *, i64, double *, i64, int *);
+
 template void getrs_perm<double>(oxi_handle_s *, char, i64, i64, const double *, i64, const int64_t *, double *, i64, int *);
 template void getrs_perm<float>(oxi_handle_s *, char, i64, i64, const float *, i64, const int64_t *, float *, i64, int *);
 

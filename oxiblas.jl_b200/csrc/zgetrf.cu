@@ -1,0 +1,469 @@
+// Complex (ComplexF64) partial-pivoted LU and its solves.
+//
+// Replaces _lu_factor! / _lu_panel! for Complex{Float64} (src/lapack/
+// factorizations.jl:30-152: blocked right-looking with nb = 128, recursive
+// panel with 16-column leaves for complex types (:113), the complex pivot rule
+// of _lu_pivot (:92-107): the largest abs2, strict '>' so the first row wins,
+// redone with abs when the largest square is not finite) and ldiv! with
+// trans 'N' / 'T' / 'C' (src/api/linalg_api.jl:168-184).
+//
+// Layout: the caller's interleaved column-major A is split into two row-major
+// FP64 planes (real, imaginary) in the handle's working matrix, so that a row
+// interchange moves contiguous segments and the trailing update is four real
+// products on the FP64 tensor cores (DMMA):
+//   Cr -= Ar Br;  Cr -= (-Ai) Bi;  Ci -= Ar Bi;  Ci -= Ai Br,
+// with -Ai a negated copy of the panel's imaginary plane.  The panel's leaves
+// run in one CTA each (16 columns, every row of the panel), their interchanges
+// are then applied to the other columns (laswp), and the U block row is solved
+// by a unit-lower substitution kernel.
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <vector>
+#include "oxi_internal.h"
+
+namespace oxi {
+
+namespace {
+constexpr int ZLEAF = 16;      // complex leaf (the reference's _lu_leaf for complex types)
+constexpr int ZLEAF_NT = 1024;
+inline i64 zrup(i64 x, i64 a) { return (x + a - 1) / a * a; }
+}  // namespace
+
+struct zd {
+    double r, i;
+};
+__device__ __forceinline__ zd zmul(zd a, zd b) { return {a.r * b.r - a.i * b.i, a.r * b.i + a.i * b.r}; }
+// c - a b: the product, then the difference (muladd(-a, b, c) of the reference)
+__device__ __forceinline__ zd zmsub(zd c, zd a, zd b) {
+    return {c.r - (a.r * b.r - a.i * b.i), c.i - (a.r * b.i + a.i * b.r)};
+}
+// a / b, scaled by the larger of |b.r|, |b.i| (no spurious overflow)
+__device__ __forceinline__ zd zdivd(zd a, zd b) {
+    double s = fmax(fabs(b.r), fabs(b.i));
+    if (s == 0.0) s = 1.0;  // a zero divisor: the quotients below become infinite or NaN
+    const double br = b.r / s, bi = b.i / s, ar = a.r / s, ai = a.i / s;
+    const double den = br * br + bi * bi;
+    return {(ar * br + ai * bi) / den, (ai * br - ar * bi) / den};
+}
+
+// (key, position) argmax over the CTA: the largest key, the smallest position
+// among equal keys; keys are non-negative doubles (NaN never enters).
+__device__ __forceinline__ void cta_argmax(double &key, int &pos, double *s_key, int *s_pos) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int off = 16; off > 0; off >>= 1) {
+        const double ok = __shfl_xor_sync(0xffffffffu, key, off);
+        const int op = __shfl_xor_sync(0xffffffffu, pos, off);
+        if (ok > key || (ok == key && op < pos)) { key = ok; pos = op; }
+    }
+    if (lane == 0) { s_key[warp] = key; s_pos[warp] = pos; }
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = blockDim.x >> 5;
+        key = lane < nw ? s_key[lane] : -1.0;
+        pos = lane < nw ? s_pos[lane] : INT_MAX;
+        for (int off = 16; off > 0; off >>= 1) {
+            const double ok = __shfl_xor_sync(0xffffffffu, key, off);
+            const int op = __shfl_xor_sync(0xffffffffu, pos, off);
+            if (ok > key || (ok == key && op < pos)) { key = ok; pos = op; }
+        }
+        if (lane == 0) { s_key[0] = key; s_pos[0] = pos; }
+    }
+    __syncthreads();
+    key = s_key[0];
+    pos = s_pos[0];
+    __syncthreads();
+}
+
+// Leaf: the m x w (w <= 16) block at (Wr, Wi) (row-major planes, ld), one CTA.
+// Column j: the pivot row (largest abs2 among rows >= j; with abs when that
+// square is not finite; the row itself when nothing beats it), the interchange
+// within the leaf's columns, the multipliers l = a / d and the rank-1 update of
+// the leaf's later columns.  ipiv gets gofs + p + 1, info the first zero pivot.
+__global__ void __launch_bounds__(ZLEAF_NT) k_zleaf(double *__restrict__ Wr, double *__restrict__ Wi, i64 ld, int m,
+                                                    int w, i64 gofs, int64_t *__restrict__ ipiv,
+                                                    int64_t *__restrict__ info) {
+    __shared__ double s_key[32];
+    __shared__ int s_pos[32];
+    __shared__ zd s_prow[ZLEAF];
+    const int tid = threadIdx.x;
+    const int q = m < w ? m : w;
+    for (int j = 0; j < q; ++j) {
+        // candidates by abs2
+        double key = -1.0;
+        int pos = INT_MAX;
+        bool nonfinite = false;
+        for (int i = j + tid; i < m; i += ZLEAF_NT) {
+            const double ar = Wr[(i64)i * ld + j], ai = Wi[(i64)i * ld + j];
+            const double v = ar * ar + ai * ai;
+            if (v == v && v > key) { key = v; pos = i; }
+        }
+        // the reference starts from row j: a NaN there keeps row j
+        {
+            const double ar = Wr[(i64)j * ld + j], ai = Wi[(i64)j * ld + j];
+            const double v0 = ar * ar + ai * ai;
+            if (v0 != v0) { key = (tid == 0) ? INFINITY : -1.0; pos = (tid == 0) ? j : INT_MAX; }
+        }
+        cta_argmax(key, pos, s_key, s_pos);
+        nonfinite = !(key < INFINITY);
+        if (nonfinite) {  // redo with abs (hypot) when the largest square overflowed
+            double k2 = -1.0;
+            int p2 = INT_MAX;
+            for (int i = j + tid; i < m; i += ZLEAF_NT) {
+                const double v = hypot(Wr[(i64)i * ld + j], Wi[(i64)i * ld + j]);
+                if (v == v && v > k2) { k2 = v; p2 = i; }
+            }
+            const double v0 = hypot(Wr[(i64)j * ld + j], Wi[(i64)j * ld + j]);
+            if (v0 != v0) { k2 = (tid == 0) ? INFINITY : -1.0; p2 = (tid == 0) ? j : INT_MAX; }
+            cta_argmax(k2, p2, s_key, s_pos);
+            pos = p2;
+        }
+        const int p = (pos == INT_MAX) ? j : pos;
+        if (tid == 0) ipiv[gofs + j] = gofs + p + 1;
+        if (p != j && tid < w) {  // the interchange within the leaf's columns
+            const double tr = Wr[(i64)j * ld + tid], ti = Wi[(i64)j * ld + tid];
+            Wr[(i64)j * ld + tid] = Wr[(i64)p * ld + tid];
+            Wi[(i64)j * ld + tid] = Wi[(i64)p * ld + tid];
+            Wr[(i64)p * ld + tid] = tr;
+            Wi[(i64)p * ld + tid] = ti;
+        }
+        __syncthreads();
+        if (tid < w) s_prow[tid] = {Wr[(i64)j * ld + tid], Wi[(i64)j * ld + tid]};
+        __syncthreads();
+        const zd d = s_prow[j];
+        if (d.r == 0.0 && d.i == 0.0) {
+            if (tid == 0 && *info == 0) *info = gofs + j + 1;
+            continue;
+        }
+        for (int i = j + 1 + tid; i < m; i += ZLEAF_NT) {
+            double *rr = Wr + (i64)i * ld, *ri = Wi + (i64)i * ld;
+            const zd l = zdivd({rr[j], ri[j]}, d);
+            rr[j] = l.r;
+            ri[j] = l.i;
+            for (int c = j + 1; c < w; ++c) {
+                const zd v = zmsub({rr[c], ri[c]}, l, s_prow[c]);
+                rr[c] = v.r;
+                ri[c] = v.i;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// laswp: the interchanges ipiv[k0 .. k0+cnt) (global 1-based rows) on columns
+// [c_lo, c_hi) of both planes, in order, one thread per column.
+__global__ void k_zlaswp(double *__restrict__ Wr, double *__restrict__ Wi, i64 ld, const int64_t *__restrict__ ipiv,
+                         i64 k0, int cnt, i64 c_lo, i64 c_hi, i64 skip_lo, i64 skip_hi) {
+    const i64 c = c_lo + (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= c_hi || (c >= skip_lo && c < skip_hi)) return;
+    for (int t = 0; t < cnt; ++t) {
+        const i64 j = k0 + t, p = ipiv[j] - 1;
+        if (p != j) {
+            const double r = Wr[j * ld + c], im = Wi[j * ld + c];
+            Wr[j * ld + c] = Wr[p * ld + c];
+            Wi[j * ld + c] = Wi[p * ld + c];
+            Wr[p * ld + c] = r;
+            Wi[p * ld + c] = im;
+        }
+    }
+}
+
+// B (t x N at (Br, Bi), ld) <- L^-1 B, L the unit lower t x t block at (Lr, Li):
+// one thread per column, s = b_i; s -= l_ip x_p for p < i in order.
+__global__ void k_ztrsm_lunit(const double *__restrict__ Lr, const double *__restrict__ Li, double *__restrict__ Br,
+                              double *__restrict__ Bi, i64 ld, int t, i64 N) {
+    const i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= N) return;
+    for (int i = 1; i < t; ++i) {
+        zd s = {Br[(i64)i * ld + c], Bi[(i64)i * ld + c]};
+        for (int p = 0; p < i; ++p)
+            s = zmsub(s, {__ldg(Lr + (i64)i * ld + p), __ldg(Li + (i64)i * ld + p)}, {Br[(i64)p * ld + c], Bi[(i64)p * ld + c]});
+        Br[(i64)i * ld + c] = s.r;
+        Bi[(i64)i * ld + c] = s.i;
+    }
+}
+
+// dst = -src (rows x cols, row-major, lds / ldd)
+__global__ void k_negate(const double *__restrict__ src, i64 lds, double *__restrict__ dst, i64 ldd, i64 rows,
+                         i64 cols) {
+    const i64 idx = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= rows * cols) return;
+    const i64 r = idx / cols, c = idx - r * cols;
+    dst[r * ldd + c] = -src[r * lds + c];
+}
+
+// interleaved column-major (m x n, lda) <-> two row-major planes (ld)
+__global__ void k_z_split(const double2 *__restrict__ A, i64 lda, double *__restrict__ Wr, double *__restrict__ Wi,
+                          i64 ld, i64 m, i64 n) {
+    __shared__ double2 tile[32][33];
+    const i64 i0 = (i64)blockIdx.x * 32, j0 = (i64)blockIdx.y * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    for (int r = ty; r < 32; r += 8) {
+        const i64 i = i0 + tx, j = j0 + r;
+        if (i < m && j < n) tile[r][tx] = A[i + j * lda];
+    }
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {
+        const i64 i = i0 + r, j = j0 + tx;
+        if (i < m && j < n) {
+            const double2 v = tile[tx][r];
+            Wr[i * ld + j] = v.x;
+            Wi[i * ld + j] = v.y;
+        }
+    }
+}
+__global__ void k_z_merge(const double *__restrict__ Wr, const double *__restrict__ Wi, i64 ld, double2 *__restrict__ A,
+                          i64 lda, i64 m, i64 n) {
+    __shared__ double2 tile[32][33];
+    const i64 i0 = (i64)blockIdx.x * 32, j0 = (i64)blockIdx.y * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    for (int r = ty; r < 32; r += 8) {
+        const i64 i = i0 + r, j = j0 + tx;
+        if (i < m && j < n) tile[r][tx] = make_double2(Wr[i * ld + j], Wi[i * ld + j]);
+    }
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {
+        const i64 i = i0 + tx, j = j0 + r;
+        if (i < m && j < n) A[i + j * lda] = tile[tx][r];
+    }
+}
+
+struct ZRun {
+    oxi_handle_s *h;
+    double *Wr, *Wi;
+    i64 ld, m, n;
+    int64_t *ipiv, *info;
+    double *neg;  // -Ai scratch (m x (nb + 2))
+    i64 nb;       // panel width (lu_factor's blocksize, 128 by default)
+};
+
+// C -= A B on complex planes (row-major, common ld): four FP64 tensor-core
+// products, the imaginary part of A negated once into scratch.
+static void zgemm_minus(ZRun &R, i64 cr, i64 cc, i64 ar, i64 ac, i64 br, i64 bc, i64 M, i64 N, i64 K) {
+    if (M <= 0 || N <= 0 || K <= 0) return;
+    cudaStream_t s = R.h->stream;
+    const i64 ld = R.ld;
+    double *Cr = R.Wr + cr * ld + cc, *Ci = R.Wi + cr * ld + cc;
+    const double *Ar = R.Wr + ar * ld + ac, *Ai = R.Wi + ar * ld + ac;
+    const double *Bre = R.Wr + br * ld + bc, *Bim = R.Wi + br * ld + bc;
+    const i64 ldn = zrup(K, 2);
+    k_negate<<<(unsigned)((M * K + 255) / 256), 256, 0, s>>>(Ai, ld, R.neg, ldn, M, K);
+    OXI_LAUNCH_CHECK();
+    launch_gemm_dmma(Cr, ld, Ar, ld, Bre, ld, M, N, K, s);
+    launch_gemm_dmma(Cr, ld, R.neg, ldn, Bim, ld, M, N, K, s);
+    launch_gemm_dmma(Ci, ld, Ar, ld, Bim, ld, M, N, K, s);
+    launch_gemm_dmma(Ci, ld, Ai, ld, Bre, ld, M, N, K, s);
+}
+
+static void ztrsm(ZRun &R, i64 r0, i64 c0, int t, i64 bc, i64 N) {
+    if (t <= 1 || N <= 0) return;
+    const i64 ld = R.ld;
+    k_ztrsm_lunit<<<(unsigned)((N + 127) / 128), 128, 0, R.h->stream>>>(
+        R.Wr + r0 * ld + c0, R.Wi + r0 * ld + c0, R.Wr + r0 * ld + bc, R.Wi + r0 * ld + bc, ld, t, N);
+    OXI_LAUNCH_CHECK();
+}
+
+static void zlaswp(ZRun &R, i64 k0, int cnt, i64 c_lo, i64 c_hi, i64 skip_lo, i64 skip_hi) {
+    if (c_hi <= c_lo || cnt <= 0) return;
+    const i64 cols = c_hi - c_lo;
+    k_zlaswp<<<(unsigned)((cols + 127) / 128), 128, 0, R.h->stream>>>(R.Wr, R.Wi, R.ld, R.ipiv, k0, cnt, c_lo, c_hi,
+                                                                        skip_lo, skip_hi);
+    OXI_LAUNCH_CHECK();
+}
+
+// _lu_panel! on columns [c0, c0+nc), rows [c0, m): the leaf's interchanges go
+// to every other column of the matrix right after it (the reference applies
+// them to the panel's columns in the recursion and to the rest per panel; each
+// column receives the same sequence)
+static void zpanel(ZRun &R, i64 c0, i64 nc) {
+    const i64 mrows = R.m - c0;
+    if (mrows <= 0 || nc <= 0) return;
+    if (nc <= ZLEAF) {
+        k_zleaf<<<1, ZLEAF_NT, 0, R.h->stream>>>(R.Wr + c0 * R.ld + c0, R.Wi + c0 * R.ld + c0, R.ld, (int)mrows,
+                                                 (int)nc, c0, R.ipiv, R.info);
+        OXI_LAUNCH_CHECK();
+        const int cnt = (int)std::min<i64>(nc, mrows);
+        zlaswp(R, c0, cnt, 0, R.n, c0, c0 + nc);
+        return;
+    }
+    const i64 h = nc / 2;
+    zpanel(R, c0, h);
+    ztrsm(R, c0, c0, (int)h, c0 + h, nc - h);
+    if (mrows > h) {
+        zgemm_minus(R, c0 + h, c0 + h, c0 + h, c0, c0, c0 + h, mrows - h, nc - h, h);
+        zpanel(R, c0 + h, nc - h);
+    }
+}
+
+static void zgetrf_planes(ZRun &R) {
+    const i64 q = std::min(R.m, R.n);
+    for (i64 f = 0; f < q; f += R.nb) {
+        const i64 l = std::min(q, f + R.nb);
+        zpanel(R, f, l - f);
+        if (l >= R.n) continue;
+        ztrsm(R, f, f, (int)(l - f), l, R.n - l);
+        if (l >= R.m) continue;
+        zgemm_minus(R, l, l, l, f, f, l, R.m - l, R.n - l, l - f);
+    }
+}
+
+// ---- solves: one CTA per right-hand side, the substitutions row by row with
+// a CTA-wide dot product per row (factor rows are contiguous in column-major
+// only along columns, so each dot product reads one row of the triangle) ----
+__device__ __forceinline__ zd cta_sum(zd v, zd *s_buf) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int off = 16; off > 0; off >>= 1) {
+        v.r += __shfl_xor_sync(0xffffffffu, v.r, off);
+        v.i += __shfl_xor_sync(0xffffffffu, v.i, off);
+    }
+    if (lane == 0) s_buf[warp] = v;
+    __syncthreads();
+    zd t = {0.0, 0.0};
+    if (threadIdx.x == 0)
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { t.r += s_buf[w].r; t.i += s_buf[w].i; }
+    __syncthreads();
+    return t;  // valid in thread 0
+}
+
+// x <- op(T)^-1 x for the n x n factor LU (interleaved column-major):
+// lower (unit L) or upper (U), op = none / transpose / conjugate transpose.
+__global__ void __launch_bounds__(256) k_ztrsv(const double2 *__restrict__ LU, i64 lda, double2 *__restrict__ X,
+                                               i64 ldx, int n, int lower_solve, int unit, int transposed,
+                                               int conjugate) {
+    __shared__ zd s_buf[8];
+    double2 *x = X + (i64)blockIdx.x * ldx;
+    for (int step = 0; step < n; ++step) {
+        const int i = lower_solve ? step : n - 1 - step;
+        zd acc = {0.0, 0.0};
+        const int p0 = lower_solve ? 0 : i + 1, p1 = lower_solve ? i : n;
+        for (int p = p0 + threadIdx.x; p < p1; p += 256) {
+            const double2 a2 = transposed ? LU[p + (i64)i * lda] : LU[i + (i64)p * lda];
+            const zd a = {a2.x, conjugate ? -a2.y : a2.y};
+            const double2 xp = x[p];
+            const zd pr = zmul(a, {xp.x, xp.y});
+            acc.r += pr.r;
+            acc.i += pr.i;
+        }
+        acc = cta_sum(acc, s_buf);
+        if (threadIdx.x == 0) {
+            const double2 b = x[i];
+            zd v = {b.x - acc.r, b.y - acc.i};
+            if (!unit) {
+                const double2 d2 = LU[i + (i64)i * lda];
+                v = zdivd(v, {d2.x, conjugate ? -d2.y : d2.y});
+            }
+            x[i] = make_double2(v.r, v.i);
+        }
+        __syncthreads();
+    }
+}
+
+// the interchanges on the columns of X: forward (before the 'N' solves) or in
+// reverse (after the 'T' / 'C' solves), one thread per right-hand side
+__global__ void k_zperm(double2 *__restrict__ X, i64 ldx, int n, int nrhs, const int64_t *__restrict__ ipiv,
+                        int reverse) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nrhs) return;
+    double2 *x = X + (i64)c * ldx;
+    for (int s = 0; s < n; ++s) {
+        const int j = reverse ? n - 1 - s : s;
+        const int p = (int)ipiv[j] - 1;
+        if (p != j) {
+            const double2 t = x[j];
+            x[j] = x[p];
+            x[p] = t;
+        }
+    }
+}
+
+}  // namespace oxi
+
+extern "C" int oxi_zgetrf(oxi_handle_t h, int64_t m, int64_t n, void *dA, int64_t lda, int64_t *d_ipiv,
+                          int64_t *h_info) {
+    using namespace oxi;
+    if (!h || !h_info || m < 0 || n < 0 || lda < std::max<int64_t>(1, m)) return OXI_EINVAL;
+    *h_info = 0;
+    if (m == 0 || n == 0) return OXI_OK;
+    if (!dA || !d_ipiv || m >= (1ll << 31) || n >= (1ll << 31)) return OXI_EINVAL;
+    if ((uintptr_t)dA % 16) return OXI_EINVAL;  // ComplexF64 elements are 16-byte aligned
+    try {
+        ProfGuard pg(&h->prof);
+        OXI_CUDA(cudaSetDevice(h->device));
+        AbortScope ab(h);
+        const i64 ld = zrup(n, 32), nb = std::max<i64>(1, h->opt.blocksize);
+        double *W = (double *)h->work.get(sizeof(double) * (2 * (size_t)m * ld + (size_t)m * (nb + 2) + 64));
+        ZRun R{h, W, W + (size_t)m * ld, ld, m, n, d_ipiv, nullptr, W + 2 * (size_t)m * ld, nb};
+        char *sc = (char *)h->scratch.get(kScratchBytes);
+        R.info = (int64_t *)sc;
+        cudaStream_t s = h->stream;
+        OXI_CUDA(cudaMemsetAsync(R.info, 0, sizeof(int64_t), s));
+        dim3 g((unsigned)((m + 31) / 32), (unsigned)((n + 31) / 32));
+        k_z_split<<<g, dim3(32, 8), 0, s>>>((const double2 *)dA, lda, R.Wr, R.Wi, ld, m, n);
+        OXI_LAUNCH_CHECK();
+        zgetrf_planes(R);
+        k_z_merge<<<g, dim3(32, 8), 0, s>>>(R.Wr, R.Wi, ld, (double2 *)dA, lda, m, n);
+        OXI_LAUNCH_CHECK();
+        int64_t *hi = (int64_t *)h->host_ws.get(64);
+        OXI_CUDA(cudaMemcpyAsync(hi, R.info, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        queue_abort_read(h, (int *)(hi + 2));
+        OXI_CUDA(cudaStreamSynchronize(s));
+        *h_info = hi[0];
+        const int we = check_abort(h, (const int *)(hi + 2));
+        if (we != OXI_OK) return we;
+        return hi[0] > 0 ? OXI_ESINGULAR : OXI_OK;
+    } catch (const CudaError &e) {
+        h->last_error = std::string(e.what) + ": " + cudaGetErrorString(e.code);
+        return OXI_ECUDA;
+    }
+}
+
+extern "C" int oxi_zgetrs(oxi_handle_t h, char trans, int64_t n, int64_t nrhs, const void *dLU, int64_t lda,
+                          const int64_t *d_ipiv, void *dB, int64_t ldb) {
+    using namespace oxi;
+    if (!h) return OXI_EINVAL;
+    if (trans != 'N' && trans != 'T' && trans != 'C') return OXI_EINVAL;
+    if (n < 0 || nrhs < 0 || lda < std::max<int64_t>(1, n) || ldb < std::max<int64_t>(1, n)) return OXI_EINVAL;
+    if (n == 0 || nrhs == 0) return OXI_OK;
+    if (!dLU || !d_ipiv || !dB || n >= (1ll << 31) || nrhs >= (1ll << 31)) return OXI_EINVAL;
+    if ((uintptr_t)dLU % 16 || (uintptr_t)dB % 16) return OXI_EINVAL;
+    try {
+        ProfGuard pg(&h->prof);
+        OXI_CUDA(cudaSetDevice(h->device));
+        AbortScope ab(h);
+        // the pivots are validated on the host (one copy of n entries)
+        std::vector<int64_t> ip(n);
+        OXI_CUDA(cudaMemcpyAsync(ip.data(), d_ipiv, sizeof(int64_t) * n, cudaMemcpyDeviceToHost, h->stream));
+        OXI_CUDA(cudaStreamSynchronize(h->stream));
+        for (i64 j = 0; j < n; ++j)
+            if (ip[j] < 1 || ip[j] > n) return OXI_EINVAL;
+        cudaStream_t s = h->stream;
+        const double2 *LU = (const double2 *)dLU;
+        double2 *X = (double2 *)dB;
+        const unsigned gp = (unsigned)((nrhs + 127) / 128);
+        if (trans == 'N') {
+            k_zperm<<<gp, 128, 0, s>>>(X, ldb, (int)n, (int)nrhs, d_ipiv, 0);
+            OXI_LAUNCH_CHECK();
+            k_ztrsv<<<(unsigned)nrhs, 256, 0, s>>>(LU, lda, X, ldb, (int)n, 1, 1, 0, 0);
+            OXI_LAUNCH_CHECK();
+            k_ztrsv<<<(unsigned)nrhs, 256, 0, s>>>(LU, lda, X, ldb, (int)n, 0, 0, 0, 0);
+            OXI_LAUNCH_CHECK();
+        } else {
+            const int cj = trans == 'C';
+            // U^T (U^H) is lower, non-unit; L^T (L^H) upper, unit
+            k_ztrsv<<<(unsigned)nrhs, 256, 0, s>>>(LU, lda, X, ldb, (int)n, 1, 0, 1, cj);
+            OXI_LAUNCH_CHECK();
+            k_ztrsv<<<(unsigned)nrhs, 256, 0, s>>>(LU, lda, X, ldb, (int)n, 0, 1, 1, cj);
+            OXI_LAUNCH_CHECK();
+            k_zperm<<<gp, 128, 0, s>>>(X, ldb, (int)n, (int)nrhs, d_ipiv, 1);
+            OXI_LAUNCH_CHECK();
+        }
+        int *he = (int *)h->host_ws.get(64);
+        queue_abort_read(h, he);
+        OXI_CUDA(cudaStreamSynchronize(s));
+        return check_abort(h, he);
+    } catch (const CudaError &e) {
+        h->last_error = std::string(e.what) + ": " + cudaGetErrorString(e.code);
+        return OXI_ECUDA;
+    }
+}

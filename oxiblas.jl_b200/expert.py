@@ -10,8 +10,9 @@
         src/api/linalg_api.jl:1143-1144 (native_inverse for a matrix,
         LinearAlgebra's inv over ldiv! for a factorization)
     factorize(A)
-        src/api/linalg_api.jl:1101-1112: a dense square matrix goes to lu; the
-        other branches (QR for rectangular input, Cholesky / Bunch-Kaufman for
+        src/api/linalg_api.jl:1101-1112: a dense square matrix goes to lu, a
+        Hermitian one with a positive diagonal to cholesky when that succeeds;
+        the other branches (QR for rectangular input, Bunch-Kaufman for other
         Hermitian input) are not part of this engine and raise ArgumentError.
 
 Each returns what the reference returns (the NamedTuples as dicts).  All of the
@@ -156,6 +157,11 @@ def inv(A) -> torch.Tensor:
     """OxiBLAS.inv: the inverse of a square matrix (factored first) or of a
     factorization F, as an n x n CUDA tensor."""
     F = A if isinstance(A, LU) else lu(_square_fp64(A))
+    if isinstance(F, LU) and F.dtype == torch.complex128:
+        # ComplexF64: the solve with the identity on the complex engine
+        F._ready()
+        n = F.shape[0]
+        return F.ldiv_(torch.eye(n, dtype=torch.complex128, device=F._buf.device))
     F = _factors_of(F)
     n = F.shape[0]
     Xcm = torch.empty((n, n), dtype=torch.float64, device=F._buf.device)
@@ -182,6 +188,13 @@ def factorize(A):
     if m != n:
         raise ArgumentError("factorize: rectangular input dispatches to QR, which this engine does not provide")
     if _is_hermitian(At):
-        raise ArgumentError("factorize: Hermitian input dispatches to Cholesky / Bunch-Kaufman, which this "
-                            "engine does not provide")
+        # linalg_api.jl:1105-1109: a positive real diagonal tries Cholesky first
+        d = torch.diagonal(At)
+        if bool(torch.all(torch.isfinite(d)).item()) and bool(torch.all(d > 0).item()) and not At.is_complex():
+            from .cholesky import cholesky
+            C = cholesky(At, check=False)
+            if C.issuccess():
+                return C
+        raise ArgumentError("factorize: a Hermitian matrix that is not positive definite dispatches to "
+                            "Bunch-Kaufman, which this engine does not provide")
     return lu(At)

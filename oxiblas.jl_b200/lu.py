@@ -26,7 +26,7 @@ import torch
 from ._lib import (ArgumentError, DimensionMismatch, Handle, SingularException, OPT_BLOCKSIZE,
                    OPT_GEMM, OPT_LOOKAHEAD, OPT_TOURNAMENT, OPT_TRSM_LEAF, OXI_ESINGULAR)
 
-_KIND = {torch.float64: "d", torch.float32: "s"}
+_KIND = {torch.float64: "d", torch.float32: "s", torch.complex128: "z"}
 
 
 def _device():
@@ -88,13 +88,14 @@ def options(blocksize=None, gemm=None, trsm_leaf=None, lookahead=None, tournamen
 
 
 class _AdjointLU:
-    """transpose(F) / F': solves with A^T (real factors: the same solve)."""
+    """transpose(F) / F': solves with A^T / A^H (real factors: the same solve)."""
 
-    def __init__(self, F):
+    def __init__(self, F, trans: bytes = b"T"):
         self.parent = F
+        self.trans = trans if F.dtype.is_complex else b"T"
 
     def ldiv_(self, B):
-        return self.parent._ldiv_inplace(B, b"T")
+        return self.parent._ldiv_inplace(B, self.trans)
 
     def solve(self, B):
         return ldiv(self, B)
@@ -183,11 +184,11 @@ class LU:
 
     @property
     def T(self):
-        return _AdjointLU(self)
+        return _AdjointLU(self, b"T")
 
     @property
     def H(self):
-        return _AdjointLU(self)
+        return _AdjointLU(self, b"C")
 
     def _ready(self):
         if self._m != self._n:
@@ -212,6 +213,8 @@ class LU:
             self._ldiv_inplace(im, trans)
             B.copy_(torch.complex(re, im))
             return B
+        if B.dtype != self.dtype and self.dtype.is_complex and not B.is_complex():
+            raise ArgumentError("a real right-hand side cannot hold a complex solution in place")
         if B.dtype != self.dtype or B.device != self._buf.device:
             X = B.to(device=self._buf.device, dtype=self.dtype)
             X = self._ldiv_inplace(X.clone(), trans)
@@ -224,7 +227,7 @@ class LU:
         cm = torch.empty((nrhs, n), dtype=self.dtype, device=self._buf.device)
         cm.copy_(X2.t())
         h = Handle.get()
-        fn = h.lib.oxi_dgetrs if self.dtype == torch.float64 else h.lib.oxi_sgetrs
+        fn = {"d": h.lib.oxi_dgetrs, "s": h.lib.oxi_sgetrs, "z": h.lib.oxi_zgetrs}[_KIND[self.dtype]]
         st = fn(h.ptr, trans, n, nrhs, ctypes.c_void_p(self._buf.data_ptr()), self._lda,
                 ctypes.c_void_p(self._ipiv.data_ptr()), ctypes.c_void_p(cm.data_ptr()), max(1, n))
         h.check(st)
@@ -243,11 +246,13 @@ class LU:
         return int(np.count_nonzero(piv != np.arange(1, len(piv) + 1)))
 
     def logabsdet(self):
+        """(sum log|u_ii|, prod sign(u_ii) negated for an odd permutation);
+        sign(u) = u / |u| for complex factors."""
         if self._m != self._n:
             raise DimensionMismatch("matrix is not square")
         d = torch.diagonal(self.factors)
         la = float(torch.log(torch.abs(d)).sum())
-        s = float(torch.prod(torch.sign(d)))
+        s = torch.prod(torch.sgn(d)).item()
         if self._nswaps() % 2 == 1:
             s = -s
         return la, s
@@ -256,7 +261,7 @@ class LU:
         if self._m != self._n:
             raise DimensionMismatch("matrix is not square")
         d = torch.diagonal(self.factors)
-        v = float(torch.prod(d))
+        v = torch.prod(d).item()
         return -v if self._nswaps() % 2 == 1 else v
 
 
@@ -271,7 +276,7 @@ def _getrf(buf: torch.Tensor, m: int, n: int, check: bool, lda=None, factors=Non
     q = min(m, n)
     ipiv = torch.zeros(max(q, 1), dtype=torch.int64, device=buf.device)[:q]
     info = ctypes.c_int64(0)
-    fn = h.lib.oxi_dgetrf if kind == "d" else h.lib.oxi_sgetrf
+    fn = {"d": h.lib.oxi_dgetrf, "s": h.lib.oxi_sgetrf, "z": h.lib.oxi_zgetrf}[kind]
     st = fn(h.ptr, m, n, ctypes.c_void_p(buf.data_ptr()), lda,
             ctypes.c_void_p(ipiv.data_ptr()), ctypes.byref(info))
     if st == OXI_ESINGULAR:
@@ -288,7 +293,7 @@ def lu(A, pivot=None, *, check: bool = True, blocksize=None) -> LU:
         raise ArgumentError("only partial (row-maximum) pivoting is on this path")
     buf = colmajor_copy(A)
     if buf.dtype not in _KIND:
-        buf = buf.to(torch.float64)
+        buf = buf.to(torch.complex128 if buf.is_complex() else torch.float64)
     m, n = buf.shape[1], buf.shape[0]
     if blocksize is not None:
         with options(blocksize=blocksize):
@@ -303,7 +308,7 @@ def lu_(A: torch.Tensor, *, check: bool = True, blocksize=None) -> LU:
     F.factors is A; a row-major A is factored through a column-major copy and the
     factors are written back into A."""
     if not isinstance(A, torch.Tensor) or not A.is_cuda or A.dtype not in _KIND:
-        raise TypeError("lu_ needs a CUDA float32/float64 tensor (no implicit conversion)")
+        raise TypeError("lu_ needs a CUDA float32/float64/complex128 tensor (no implicit conversion)")
     m, n = A.shape
     ctx = options(blocksize=blocksize) if blocksize is not None else contextlib.nullcontext()
     with ctx:

@@ -99,6 +99,8 @@ def test_inv_and_factorize(pkg, oracle):
         pkg.factorize(rng.standard_normal((5, 4)))
     S = rng.standard_normal((6, 6))
     with pytest.raises(pkg.ArgumentError):
-        pkg.factorize(S + S.T)
+        pkg.factorize(S + S.T - 20 * np.eye(6))  # Hermitian, negative diagonal: Bunch-Kaufman
+    C = pkg.factorize(S @ S.T + 6 * np.eye(6))  # Hermitian positive definite: Cholesky
+    assert isinstance(C, pkg.Cholesky) and C.issuccess()
     with pytest.raises(pkg.SingularException):
         pkg.inv(np.zeros((4, 4)))

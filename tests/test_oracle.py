@@ -134,3 +134,73 @@ def test_oracle_expert_solves(oracle):
     assert np.isclose(rs["rcond_estimate"], 1 / (np.linalg.norm(A, 1) * est), rtol=1e-12)
     X = oracle.inverse(F, ip)
     assert np.allclose(X @ A, np.eye(n), atol=1e-8)
+
+
+def _py_zgetf2(A):
+    """Unblocked complex LU by the pivot rule of _lu_pivot (abs2 with strict
+    '>', abs when the largest square is not finite; factorizations.jl:92-107)
+    in plain Python loops, an independent restatement for small cases."""
+    with np.errstate(over="ignore", invalid="ignore"):
+        return _py_zgetf2_body(np.array(A, dtype=np.complex128))
+
+
+def _py_zgetf2_body(A):
+    m, n = A.shape
+    piv = []
+    for j in range(min(m, n)):
+        p, best = j, A[j, j].real ** 2 + A[j, j].imag ** 2
+        for i in range(j + 1, m):
+            v = A[i, j].real ** 2 + A[i, j].imag ** 2
+            if v > best:
+                best, p = v, i
+        if not np.isfinite(best):
+            p, best = j, abs(A[j, j])
+            for i in range(j + 1, m):
+                v = abs(A[i, j])
+                if v > best:
+                    best, p = v, i
+        piv.append(p + 1)
+        A[[j, p], :] = A[[p, j], :]
+        d = A[j, j]
+        if d == 0:
+            continue
+        A[j + 1:, j] /= d
+        A[j + 1:, j + 1:] -= np.outer(A[j + 1:, j], A[j, j + 1:])
+    return A, np.array(piv, dtype=np.int64)
+
+
+@pytest.mark.parametrize("m,n", [(12, 12), (40, 25), (25, 40), (70, 70)])
+def test_oracle_complex_lu(oracle, m, n):
+    rng = np.random.default_rng(m * n)
+    A = rng.standard_normal((m, n)) + 1j * rng.standard_normal((m, n))
+    LU, ipiv, info = oracle.zgetrf(A, blocksize=16)
+    F2, piv2 = _py_zgetf2(A)
+    assert info == 0
+    assert np.array_equal(ipiv, piv2)
+    assert np.linalg.norm(LU - F2) <= 1e-13 * np.linalg.norm(F2)
+    q = min(m, n)
+    L = np.tril(LU[:, :q], -1) + np.eye(m, q)
+    U = np.triu(LU[:q, :])
+    p = oracle.perm_from_ipiv(ipiv, m)
+    assert bwd(L @ U - A[p, :], A) <= 30
+    assert np.all(np.abs(L) <= 1 + 1e-12)  # the largest-modulus pivot
+    if m == n:
+        b = rng.standard_normal((n, 2)) + 1j * rng.standard_normal((n, 2))
+        for t, M in (("N", A), ("T", A.T), ("C", A.conj().T)):
+            x = oracle.zgetrs(LU, ipiv, b, t)
+            assert np.linalg.norm(M @ x - b) <= 1e-10 * np.linalg.norm(M) * np.linalg.norm(x)
+
+
+def test_oracle_complex_pivot_overflow_and_zero(oracle):
+    rng = np.random.default_rng(11)
+    A = rng.standard_normal((20, 20)) + 1j * rng.standard_normal((20, 20))
+    A[3, 0] = 3e200 + 1e200j
+    A[9, 0] = 1e200 - 3.1e200j  # larger modulus; both squares overflow
+    _, ipiv, _ = oracle.zgetrf(A)
+    _, piv2 = _py_zgetf2(A)
+    assert ipiv[0] == 10 and np.array_equal(ipiv, piv2)
+    S = A.copy()
+    S[:, 4] = 0
+    S[3, 0], S[9, 0] = 1.0, 2.0
+    _, _, info = oracle.zgetrf(S, check=False)
+    assert info == 5
