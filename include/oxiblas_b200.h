@@ -251,6 +251,17 @@ int oxi_dgesv_mixed(oxi_handle_t h, int prec, int refine, int64_t n, int64_t nrh
                     const double *dA, int64_t lda, const double *dB, int64_t ldb, double *dX,
                     int64_t ldx, int maxiter, double rtol, oxi_refine_report *out);
 
+/* mixed_solve(A, b; factorization=:cholesky) (src/lapack/extended_lapack.jl:
+ * 175-226, Cholesky family): one global scale max|a_ij| keeps the matrix
+ * symmetric, the low-precision Cholesky of the lower triangle of A / scale
+ * (FP32 panels, the symmetric update in prec on the tensor cores), FP64
+ * refinement as oxi_dgesv_mixed.  A low factor that is not positive definite
+ * falls back to the FP64 Cholesky (report fallback = 1); if that fails too:
+ * OXI_ENOTPOSDEF with report->info the failing column. */
+int oxi_dposv_mixed(oxi_handle_t h, int prec, int refine, int64_t n, int64_t nrhs,
+                    const double *dA, int64_t lda, const double *dB, int64_t ldb, double *dX,
+                    int64_t ldx, int maxiter, double rtol, oxi_refine_report *out);
+
 /* ---------------------------------------------------------------------------
  * Expert solves and the condition estimate (FP64).
  * ------------------------------------------------------------------------- */

@@ -79,6 +79,9 @@ def lib():
         L.orc_zgetrf.restype = ctypes.c_int
         L.orc_zgetrs.argtypes = [ctypes.c_char, _i64, _i64, _zp, _i64, _ip, _zp, _i64]
         L.orc_zgetrs.restype = ctypes.c_int
+        L.orc_mixed_solve_chol.argtypes = [_i64, _i64, _dp, _i64, _dp, _i64, _dp, _i64, _i64, ctypes.c_double,
+                                           ctypes.c_int, _ip, _dp, _dp, ctypes.POINTER(ctypes.c_int), _ip]
+        L.orc_mixed_solve_chol.restype = ctypes.c_int
         L.orc_lu_adjoint.argtypes = [_i64, _dp, _i64, _ip, _dp, _dp, _dp, _dp, _i64]
         L.orc_lu_adjoint.restype = ctypes.c_int
         for P, fp in (("d", _dp), ("s", _fp)):
@@ -380,3 +383,31 @@ def zgetrs(LU, ipiv, B, trans: str = "N"):
     lib().orc_zgetrs(trans.encode(), n, nrhs, ctypes.c_void_p(LU.ctypes.data), max(n, 1),
                      _ptr(ipiv, ctypes.c_int64), ctypes.c_void_p(X.ctypes.data), max(n, 1))
     return X[:, 0].copy() if vec else X
+
+
+def mixed_solve_chol(A, b, maxiter: int = 10, rtol: float = 1e-13, normwise: bool = False):
+    """mixed_solve(A, b; factorization=:cholesky) (Float32 Cholesky of A / max|A|,
+    Float64 refinement).  Returns dict(x, converged, iterations,
+    backward_error, backward_error_normwise, fallback, info)."""
+    A = np.asfortranarray(A, dtype=np.float64)
+    n = A.shape[0]
+    vec = np.ndim(b) == 1
+    B = np.asfortranarray(np.reshape(b, (n, -1)), dtype=np.float64)
+    nrhs = B.shape[1]
+    X = np.zeros((n, nrhs), order="F")
+    it = np.zeros(1, dtype=np.int64)
+    info = np.zeros(1, dtype=np.int64)
+    cw = np.zeros(1)
+    nw = np.zeros(1)
+    fb = ctypes.c_int(0)
+    rc = lib().orc_mixed_solve_chol(n, nrhs, _ptr(A), max(n, 1), _ptr(B), max(n, 1), _ptr(X), max(n, 1),
+                                    maxiter, rtol, 1 if normwise else 0, _ptr(it, ctypes.c_int64), _ptr(cw),
+                                    _ptr(nw), ctypes.byref(fb), _ptr(info, ctypes.c_int64))
+    if rc == 1:
+        raise ValueError(f"PosDefException({int(info[0])})")
+    if rc != 0:
+        raise OverflowError("mixed solve conversion overflow")
+    e = float(nw[0] if normwise else cw[0])
+    return dict(x=X[:, 0] if vec else X, converged=e <= rtol, iterations=int(it[0]),
+                backward_error=float(cw[0]), backward_error_normwise=float(nw[0]), fallback=bool(fb.value),
+                info=int(info[0]))

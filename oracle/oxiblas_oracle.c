@@ -943,6 +943,163 @@ void orc_dpotrs(i64 n, i64 nrhs, const double *L, i64 ldl, double *B, i64 ldb) {
     }
 }
 
+/* The same recursion in Float32 (cholesky_factor of the low-precision matrix
+ * inside mixed_solve, src/lapack/extended_lapack.jl:157-158). */
+static i64 chol_rec_f(float *L, i64 ld, i64 n, i64 offset, i64 leaf) {
+    if (n <= leaf) {
+        for (i64 c = 0; c < n; ++c) {
+            float d = L[c + c * ld];
+            if (!(isfinite(d) && d > 0)) return offset + c + 1;
+            d = sqrtf(d);
+            L[c + c * ld] = d;
+            for (i64 i = c + 1; i < n; ++i) L[i + c * ld] /= d;
+            for (i64 j = c + 1; j < n; ++j) {
+                const float cj = L[j + c * ld];
+                for (i64 i = j; i < n; ++i) L[i + j * ld] = fmaf(-L[i + c * ld], cj, L[i + j * ld]);
+            }
+        }
+        return 0;
+    }
+    const i64 h = n / 2;
+    i64 info = chol_rec_f(L, ld, h, offset, leaf);
+    if (info) return info;
+    float *L21 = L + h;
+#pragma omp parallel for schedule(static) if ((n - h) * h > 65536)
+    for (i64 r = 0; r < n - h; ++r) {
+        for (i64 j = 0; j < h; ++j) {
+            float s = L21[r + j * ld];
+            for (i64 p = 0; p < j; ++p) s = fmaf(-L21[r + p * ld], L[j + p * ld], s);
+            L21[r + j * ld] = s / L[j + j * ld];
+        }
+    }
+    float *A22 = L + h + h * ld;
+    const i64 m = n - h;
+#pragma omp parallel for schedule(dynamic, 8) if (m * m * h > 2000000)
+    for (i64 j = 0; j < m; ++j)
+        for (i64 i = j; i < m; ++i) {
+            float s = 0.0f;
+            for (i64 p = 0; p < h; ++p) s = fmaf(L21[i + p * ld], L21[j + p * ld], s);
+            A22[i + j * ld] -= s;
+        }
+    return chol_rec_f(A22, ld, m, offset + h, leaf);
+}
+
+static void spotrs_lower(i64 n, i64 nrhs, const float *L, i64 ldl, float *B, i64 ldb) {
+    for (i64 c = 0; c < nrhs; ++c) {
+        float *b = B + c * ldb;
+        for (i64 i = 0; i < n; ++i) {
+            float s = b[i];
+            for (i64 p = 0; p < i; ++p) s = fmaf(-L[i + p * ldl], b[p], s);
+            b[i] = s / L[i + i * ldl];
+        }
+        for (i64 i = n - 1; i >= 0; --i) {
+            float s = b[i];
+            for (i64 p = i + 1; p < n; ++p) s = fmaf(-L[p + i * ldl], b[p], s);
+            b[i] = s / L[i + i * ldl];
+        }
+    }
+}
+
+/* mixed_solve(A, b; factorization=:cholesky): _mixed_precision_impl,
+ * src/lapack/extended_lapack.jl:175-226, Cholesky family, Low = Float32.
+ * One global positive scale (max |a_ij|, one if zero) keeps the matrix
+ * symmetric: E = A / scale, rows = scale, columns = 1 (:187-193); the Float32
+ * Cholesky of E, or on PosDefException / an overflowing conversion the Float64
+ * one (:196-202); the corrections of _mixed_extended_correction (:114-131);
+ * the componentwise (or normwise) stop.  Returns 0, 1 (not positive definite
+ * in working precision too; *fallback = 1), 4 overflow. */
+int orc_mixed_solve_chol(i64 n, i64 nrhs, const double *A, i64 lda, const double *B, i64 ldb,
+                         double *X, i64 ldx, i64 maxiter, double rtol, int stop_normwise,
+                         i64 *iterations, double *berr, double *berr_nw, int *fallback, i64 *info_out) {
+    double scale = 0.0;
+    for (i64 j = 0; j < n; ++j)
+        for (i64 i = 0; i < n; ++i) scale = fmax(scale, fabs(A[i + j * lda]));
+    if (scale == 0.0) scale = 1.0;
+    double *E = (double *)malloc(sizeof(double) * (size_t)(n > 0 ? n * n : 1));
+    float *F = (float *)malloc(sizeof(float) * (size_t)(n > 0 ? n * n : 1));
+    double *R = (double *)malloc(sizeof(double) * (size_t)(n * nrhs > 0 ? n * nrhs : 1));
+    double *Cc = (double *)malloc(sizeof(double) * (size_t)(n * nrhs > 0 ? n * nrhs : 1));
+    float *work = (float *)malloc(sizeof(float) * (size_t)(n * nrhs > 0 ? n * nrhs : 1));
+    int rc = 0, lowok = 1;
+    *fallback = 0;
+    *info_out = 0;
+    for (i64 j = 0; j < n; ++j)
+        for (i64 i = 0; i < n; ++i) {
+            E[i + j * n] = A[i + j * lda] / scale;
+            F[i + j * n] = (float)E[i + j * n];
+            if (!isfinite(F[i + j * n])) lowok = 0;
+        }
+    i64 info = lowok ? chol_rec_f(F, n, n, 0, 64) : -1;
+    *info_out = info > 0 ? info : 0;
+    if (info != 0) {
+        *fallback = 1;
+        info = chol_rec(E, n, n, 0, 64);
+        if (info != 0) { *info_out = info; rc = 1; goto done; }
+    }
+#define CCORRECT(RES, LDRES, OUT, LDOUT)                                                   \
+    do {                                                                                 \
+        double mag = 0.0;                                                                \
+        for (i64 j = 0; j < nrhs; ++j)                                                   \
+            for (i64 i = 0; i < n; ++i) {                                                \
+                double v = fabs(RES[i + j * LDRES] / scale);                             \
+                if (v > mag || isnan(v)) mag = v;                                        \
+            }                                                                            \
+        if (mag == 0.0) {                                                                \
+            for (i64 j = 0; j < nrhs; ++j)                                               \
+                for (i64 i = 0; i < n; ++i) OUT[i + j * LDOUT] = 0.0;                    \
+            break;                                                                       \
+        }                                                                                \
+        if (!isfinite(mag)) { rc = 4; goto done; }                                       \
+        int ex; frexp(mag, &ex);                                                         \
+        const double p2 = ldexp(1.0, ex - 1);                                            \
+        if (!*fallback) {                                                                \
+            for (i64 j = 0; j < nrhs; ++j)                                               \
+                for (i64 i = 0; i < n; ++i) {                                            \
+                    float v = (float)((RES[i + j * LDRES] / scale) / p2);                \
+                    if (!isfinite(v)) { rc = 4; goto done; }                             \
+                    work[i + j * n] = v;                                                 \
+                }                                                                        \
+            spotrs_lower(n, nrhs, F, n, work, n);                                        \
+            for (i64 j = 0; j < nrhs; ++j)                                               \
+                for (i64 i = 0; i < n; ++i) OUT[i + j * LDOUT] = (double)work[i + j * n] * p2; \
+        } else {                                                                         \
+            for (i64 j = 0; j < nrhs; ++j)                                               \
+                for (i64 i = 0; i < n; ++i) OUT[i + j * LDOUT] = (RES[i + j * LDRES] / scale) / p2; \
+            orc_dpotrs(n, nrhs, E, n, OUT, LDOUT);                                       \
+            for (i64 j = 0; j < nrhs; ++j)                                               \
+                for (i64 i = 0; i < n; ++i) OUT[i + j * LDOUT] *= p2;                    \
+        }                                                                                \
+    } while (0)
+    CCORRECT(B, ldb, X, ldx);
+    double anorm = 0.0;
+    if (stop_normwise) {
+        for (i64 i = 0; i < n; ++i) {
+            double rsum = 0.0;
+            for (i64 k = 0; k < n; ++k) rsum += fabs(A[i + k * lda]);
+            anorm = fmax(anorm, rsum);
+        }
+    }
+    double err = INFINITY, cw = INFINITY, nw = INFINITY;
+    i64 it = 0;
+    for (i64 iter = 0; iter <= maxiter; ++iter) {
+        cw = orc_refinement_residual(n, nrhs, A, lda, X, ldx, B, ldb, R, n);
+        nw = stop_normwise ? normwise_from_residual(n, nrhs, anorm, R, n, X, ldx, B, ldb) : NAN;
+        err = stop_normwise ? nw : cw;
+        it = iter;
+        if (err <= rtol || iter == maxiter || !isfinite(err)) break;
+        CCORRECT(R, n, Cc, n);
+        for (i64 j = 0; j < nrhs; ++j)
+            for (i64 i = 0; i < n; ++i) X[i + j * ldx] += Cc[i + j * n];
+    }
+#undef CCORRECT
+    *iterations = it;
+    *berr = cw;
+    *berr_nw = nw;
+done:
+    free(E); free(F); free(R); free(Cc); free(work);
+    return rc;
+}
+
 /* ------------------------------------------------------------------------ */
 /* Complex LU (ComplexF64)                                                   */
 /* ------------------------------------------------------------------------ */

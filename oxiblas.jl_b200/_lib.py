@@ -96,6 +96,8 @@ _SIGS = {
     "oxi_dequilibrate": ([_vp, _i64, _i64, _vp, _i64, _vp, _vp, _vp, _i64], ctypes.c_int),
     "oxi_dgesv_mixed": ([_vp, ctypes.c_int, ctypes.c_int, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64,
                          ctypes.c_int, ctypes.c_double, _vp], ctypes.c_int),
+    "oxi_dposv_mixed": ([_vp, ctypes.c_int, ctypes.c_int, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64,
+                         ctypes.c_int, ctypes.c_double, _vp], ctypes.c_int),
 }
 
 

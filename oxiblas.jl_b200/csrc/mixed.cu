@@ -138,6 +138,42 @@ __global__ void k_identity(double *__restrict__ X, i64 ldx, int n) {
     if (i < n) X[i + (i64)j * ldx] = (i == j) ? 1.0 : 0.0;
 }
 
+// Cholesky family of mixed_solve (src/lapack/extended_lapack.jl:187-193): one
+// global positive scale, max |a_ij| over the whole matrix (1 if zero), from the
+// row-statistics partials; rows = scale, columns = 1; perm = identity.
+__global__ void __launch_bounds__(1024) k_global_scale(const double *__restrict__ pmax, i64 count,
+                                                       double *__restrict__ out) {
+    double mx = 0.0;
+    for (i64 e = threadIdx.x; e < count; e += blockDim.x) mx = fmax(mx, pmax[e]);
+    for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+    __shared__ double red[32];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t = fmax(t, red[w]);
+        *out = (t == 0.0) ? 1.0 : t;
+    }
+}
+__global__ void k_chol_scales(const double *__restrict__ scale, double *__restrict__ rows,
+                              double *__restrict__ cols, int64_t *__restrict__ perm, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    rows[i] = *scale;
+    cols[i] = 1.0;
+    perm[i] = i;
+}
+// W (column-major, ldw) = T(A / scale): the matrix the low-precision Cholesky
+// factors (its lower triangle)
+template <typename T>
+__global__ void k_scaled_copy(const double *__restrict__ A, i64 lda, T *__restrict__ W, i64 ldw, int n,
+                              const double *__restrict__ scale) {
+    const i64 idx = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (i64)n * n) return;
+    const i64 j = idx / n, i = idx - j * n;
+    W[i + j * ldw] = (T)(A[i + j * lda] / *scale);
+}
+
 __global__ void k_fill(double *__restrict__ v, int n, double x) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) v[i] = x;
@@ -387,6 +423,7 @@ struct MixedRun {
     i64 ldw;
     void *dinvL, *dinvU;  // inverses of the 64 x 64 diagonal blocks of L and U
     bool fallback = false;
+    bool chol = false;  // Cholesky family: W holds the column-major lower factor L
     double *scal;  // device scalars (cw/rmax/xmax/bmax per rhs, r^2)
     int *err;      // device error word
     double anorm = 0.0;
@@ -459,14 +496,22 @@ static void precond(MixedRun &M, const double *Rin, i64 ldr, double *Z, i64 ldz,
     if (!M.fallback) {
         k_to_low<float><<<gb, 256, 0, s>>>(Rin, ldr, n, nr, M.rows, M.perm, M.mag, M.low32, M.err);
         OXI_LAUNCH_CHECK();
-        lu_solve_rowmajor<float>(M.h, (const float *)M.W, M.ldw, n, M.low32, n, nr, M.err,
-                                 (const float *)M.dinvL, (const float *)M.dinvU);
+        if (M.chol)
+            chol_solve_ops<float>(M.h, (const float *)M.W, M.ldw, n, M.low32, n, nr, M.err,
+                                  (const float *)M.dinvL, (const float *)M.dinvU);
+        else
+            lu_solve_rowmajor<float>(M.h, (const float *)M.W, M.ldw, n, M.low32, n, nr, M.err,
+                                     (const float *)M.dinvL, (const float *)M.dinvU);
         k_apply_corr<float><<<gb, 256, 0, s>>>(Z, ldz, n, nr, M.low32, M.mag, M.cols, 0);
     } else {
         k_to_low<double><<<gb, 256, 0, s>>>(Rin, ldr, n, nr, M.rows, M.perm, M.mag, M.low64, M.err);
         OXI_LAUNCH_CHECK();
-        lu_solve_rowmajor<double>(M.h, (const double *)M.W, M.ldw, n, M.low64, n, nr, M.err,
-                                  (const double *)M.dinvL, (const double *)M.dinvU);
+        if (M.chol)
+            chol_solve_ops<double>(M.h, (const double *)M.W, M.ldw, n, M.low64, n, nr, M.err,
+                                   (const double *)M.dinvL, (const double *)M.dinvU);
+        else
+            lu_solve_rowmajor<double>(M.h, (const double *)M.W, M.ldw, n, M.low64, n, nr, M.err,
+                                      (const double *)M.dinvL, (const double *)M.dinvU);
         k_apply_corr<double><<<gb, 256, 0, s>>>(Z, ldz, n, nr, M.low64, M.mag, M.cols, 0);
     }
     OXI_LAUNCH_CHECK();
@@ -588,7 +633,7 @@ struct ExpertOpts {
 
 static int dgesv_mixed(oxi_handle_s *h, int prec, int refine, i64 n, i64 nrhs, const double *dA,
                        i64 lda, const double *dB, i64 ldb, double *dX, i64 ldx, int maxiter, double rtol,
-                       oxi_refine_report *out, ExpertOpts *xo = nullptr) {
+                       oxi_refine_report *out, ExpertOpts *xo = nullptr, bool chol = false) {
     if (xo) {
         prec = OXI_PREC_FP64;
         refine = OXI_REFINE_IR;
@@ -597,6 +642,7 @@ static int dgesv_mixed(oxi_handle_s *h, int prec, int refine, i64 n, i64 nrhs, c
     MixedRun M;
     M.h = h; M.s = s; M.n = n; M.nrhs = nrhs; M.A = dA; M.lda = lda; M.B = dB; M.ldb = ldb;
     M.X = dX; M.ldx = ldx;
+    M.chol = chol;
     M.restart = std::max(2, std::min(h->opt.gmres_restart, GM_MAXV - 2));
     cudaEvent_t e0, e1, e2;
     OXI_CUDA(cudaEventCreate(&e0));
@@ -620,7 +666,8 @@ static int dgesv_mixed(oxi_handle_s *h, int prec, int refine, i64 n, i64 nrhs, c
                  o_perm = take(8 * n), o_ipiv = take(8 * n), o_V = take(8 * n * GM_MAXV),
                  o_gw = take(8 * n), o_gt = take(8 * n), o_gpart = take(8 * 120 * GM_MAXV),
                  o_gh = take(8 * GM_MAXV), o_gz = take(8 * n),
-                 o_dinv = take(2 * 8 * (size_t)lu_block_inverse_elems(n));
+                 o_dinv = take(2 * 8 * (size_t)lu_block_inverse_elems(n)),
+                 o_pwork = chol ? take(8 * potrf_work_elems(n)) : take(0);
     char *ws = (char *)h->mixed_ws.get(off);
     M.rows = (double *)(ws + o_rows); M.cols = (double *)(ws + o_cols);
     M.pmax = (double *)(ws + o_pmax); M.psum = (double *)(ws + o_psum);
@@ -662,7 +709,13 @@ static int dgesv_mixed(oxi_handle_s *h, int prec, int refine, i64 n, i64 nrhs, c
         k_row_stats_final<<<blocks_for(n), 256, 0, s>>>(M.pmax, M.psum, (int)n, RS, M.rows, M.scal, radix,
                                                          xo ? zrow : nullptr);
         OXI_LAUNCH_CHECK();
-        k_col_scale<<<(unsigned)n, 256, 0, s>>>(dA, lda, (int)n, M.rows, M.cols, radix);
+        if (chol) {
+            k_global_scale<<<1, 1024, 0, s>>>(M.pmax, (i64)n * RS, M.scal + 100);
+            OXI_LAUNCH_CHECK();
+            k_chol_scales<<<blocks_for(n), 256, 0, s>>>(M.scal + 100, M.rows, M.cols, M.perm, (int)n);
+        } else {
+            k_col_scale<<<(unsigned)n, 256, 0, s>>>(dA, lda, (int)n, M.rows, M.cols, radix);
+        }
         OXI_LAUNCH_CHECK();
         int *hflag = (int *)(M.hsc + 300);
         OXI_CUDA(cudaMemcpyAsync(hflag, nonfinite, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -688,7 +741,45 @@ static int dgesv_mixed(oxi_handle_s *h, int prec, int refine, i64 n, i64 nrhs, c
 
     // ---- 3. low-precision factorization ----
     int64_t info = 0;
+    auto factor_chol = [&](bool fp64) {
+        // the Cholesky family: T(A / scale), its lower triangle factored in place
+        OXI_CUDA(cudaMemsetAsync(d_info, 0, sizeof(int64_t), s));
+        const unsigned gb = blocks_for((i64)n * n);
+        M.dinvL = ws + o_dinv;
+        if (!fp64) {
+            float *W = (float *)h->work.get((size_t)n * ldw * sizeof(float));
+            M.W = W;
+            k_scaled_copy<float><<<gb, 256, 0, s>>>(dA, lda, W, ldw, (int)n, M.scal + 100);
+            OXI_LAUNCH_CHECK();
+            const int saved_tr = h->trailing;
+            h->trailing = prec;
+            try {
+                potrf_rowmajor<float>(h, W, ldw, n, d_info, (float *)(ws + o_pwork));
+            } catch (...) {
+                h->trailing = saved_tr;
+                throw;
+            }
+            h->trailing = saved_tr;
+            M.dinvU = (float *)M.dinvL + inv_elems;
+            chol_block_ops<float>(h, W, ldw, n, (float *)M.dinvL, (float *)M.dinvU);
+        } else {
+            double *W = (double *)h->work.get((size_t)n * ldw * sizeof(double));
+            M.W = W;
+            k_scaled_copy<double><<<gb, 256, 0, s>>>(dA, lda, W, ldw, (int)n, M.scal + 100);
+            OXI_LAUNCH_CHECK();
+            potrf_rowmajor<double>(h, W, ldw, n, d_info, (double *)(ws + o_pwork));
+            M.dinvU = (double *)M.dinvL + inv_elems;
+            chol_block_ops<double>(h, W, ldw, n, (double *)M.dinvL, (double *)M.dinvU);
+        }
+        OXI_CUDA(cudaMemcpyAsync(M.hpiv, d_info, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        OXI_CUDA(cudaStreamSynchronize(s));
+        info = M.hpiv[0];
+    };
     auto factor = [&](bool fp64) {
+        if (M.chol) {
+            factor_chol(fp64);
+            return;
+        }
         OXI_CUDA(cudaMemsetAsync(d_info, 0, sizeof(int64_t), s));
         dim3 g((unsigned)((n + 31) / 32), (unsigned)((n + 31) / 32));
         if (!fp64) {
@@ -749,8 +840,8 @@ static int dgesv_mixed(oxi_handle_s *h, int prec, int refine, i64 n, i64 nrhs, c
         used_fallback = true;
         factor(true);
     }
-    if (out) out->info = low_info;
-    if (info != 0) return OXI_ESINGULAR;
+    if (out) out->info = M.chol && info != 0 ? info : low_info;
+    if (info != 0) return M.chol ? OXI_ENOTPOSDEF : OXI_ESINGULAR;
     if (xo) {  // the scales and the factorization of the scaled matrix
         if (xo->rows_out)
             OXI_CUDA(cudaMemcpyAsync(xo->rows_out, M.rows, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
@@ -866,6 +957,37 @@ extern "C" int oxi_dgesv_mixed(oxi_handle_t h, int prec, int refine, int64_t n, 
         return we != OXI_OK ? we : st;
     } catch (const oxi::CudaError &e) {
         h->stall_at = 0;
+        h->last_error = std::string(e.what) + ": " + cudaGetErrorString(e.code);
+        return OXI_ECUDA;
+    }
+}
+
+// mixed_solve(A, b; factorization=:cholesky): the same driver with the
+// Cholesky family's scaling and factor (src/lapack/extended_lapack.jl:175-226).
+extern "C" int oxi_dposv_mixed(oxi_handle_t h, int prec, int refine, int64_t n, int64_t nrhs,
+                               const double *dA, int64_t lda, const double *dB, int64_t ldb,
+                               double *dX, int64_t ldx, int maxiter, double rtol,
+                               oxi_refine_report *out) {
+    if (!h) return OXI_EINVAL;
+    if (out) *out = oxi_refine_report{};
+    if (n < 0 || nrhs < 0 || maxiter < 0 || !(rtol >= 0) || !std::isfinite(rtol)) return OXI_EINVAL;
+    if (prec < OXI_PREC_FP32 || prec > OXI_PREC_FP16X3 || refine < 0 || refine > OXI_REFINE_AUTO)
+        return OXI_EINVAL;
+    if (n == 0 || nrhs == 0) return OXI_OK;
+    if (!dA || !dB || !dX || lda < n || ldb < n || ldx < n || nrhs > 16 || n >= (1ll << 31)) return OXI_EINVAL;
+    try {
+        oxi::ProfGuard pg(&h->prof);
+        OXI_CUDA(cudaSetDevice(h->device));
+        oxi::AbortScope ab(h);
+        const int st = oxi::dgesv_mixed(h, prec, refine, n, nrhs, dA, lda, dB, ldb, dX, ldx, maxiter, rtol, out,
+                                        nullptr, /*chol=*/true);
+        if (st == OXI_EOVERFLOW) return st;
+        int *he = (int *)h->host_ws.get(64);
+        oxi::queue_abort_read(h, he);
+        OXI_CUDA(cudaStreamSynchronize(h->stream));
+        const int we = oxi::check_abort(h, he);
+        return we != OXI_OK ? we : st;
+    } catch (const oxi::CudaError &e) {
         h->last_error = std::string(e.what) + ": " + cudaGetErrorString(e.code);
         return OXI_ECUDA;
     }

@@ -336,6 +336,21 @@ void launch_cvt_transpose16(int fmt, const float *src, i64 lds, void *dst, i64 l
 void gemm_trailing_f32(oxi_handle_s *h, float *C, i64 ldc, const float *A, i64 lda,
                        const float *B, i64 ldb, i64 M, i64 N, i64 K);
 
+// Cholesky of the lower triangle of a column-major matrix, in place as the upper
+// triangle of its row-major view (potrf.cu); work holds potrf_work_elems(n)
+// elements.  FP32 runs its symmetric update in h->trailing precision.
+size_t potrf_work_elems(i64 n);
+template <typename T>
+void potrf_rowmajor(oxi_handle_s *h, T *U, i64 ld, i64 n, int64_t *d_info, T *work);
+// Solves with a column-major lower Cholesky factor L: the block operators of L
+// and of L^T (lu_block_inverse_elems(n) elements each), then L L^T X = B in
+// place with them (solve.cu).
+template <typename T>
+void chol_block_ops(oxi_handle_s *h, const T *L, i64 ldl, i64 n, T *P1, T *P2);
+template <typename T>
+void chol_solve_ops(oxi_handle_s *h, const T *L, i64 ldl, i64 n, T *X, i64 ldx, i64 nrhs, int *d_err,
+                    const T *P1, const T *P2);
+
 // getrf_rowmajor through the handle's graph cache (same shape, buffers and
 // options: replay; second occurrence: capture; otherwise direct launches).
 template <typename T>

@@ -46,28 +46,29 @@ constexpr int PO_NT = 512;          // threads of the diagonal-block kernel (4 p
 // column (w_jj = 1/u_jj; w_ij = -(sum_{p=i+1..j} u_ip w_pj) / u_ii for i = j-1
 // down to 0), W^T kept in the block's unused strict lower triangle, and
 // Wneg = -W^T (t x t, row-major, lower) written for the block-row product.
-__global__ void __launch_bounds__(PO_NT) k_potrf_diag(double *__restrict__ U, i64 ld, int t, i64 g0,
-                                                      int64_t *__restrict__ info, double *__restrict__ Wneg) {
-    extern __shared__ __align__(16) double po_smem[];
+template <typename T>
+__global__ void __launch_bounds__(PO_NT) k_potrf_diag(T *__restrict__ U, i64 ld, int t, i64 g0,
+                                                      int64_t *__restrict__ info, T *__restrict__ Wneg) {
+    extern __shared__ __align__(16) unsigned char po_smem_raw[];
     const int lp = t + 1;
-    double *S = po_smem;
-    double *s_inv = po_smem + (size_t)t * lp;  // 1 / u_ii
+    T *S = (T *)po_smem_raw;
+    T *s_inv = S + (size_t)t * lp;  // 1 / u_ii
     __shared__ int s_fail;
     const int tid = threadIdx.x;
     if (tid == 0) s_fail = (*(volatile int64_t *)info != 0) ? 1 : 0;
     __syncthreads();
     if (s_fail) {  // an earlier block failed: later products change nothing
-        for (int e = tid; e < t * t; e += PO_NT) Wneg[e] = 0.0;
+        for (int e = tid; e < t * t; e += PO_NT) Wneg[e] = T(0);
         return;
     }
     for (int e = tid; e < t * t; e += PO_NT) {
         const int i = e / t, j = e - i * t;
-        S[i * lp + j] = (j >= i) ? U[(i64)i * ld + j] : 0.0;
+        S[i * lp + j] = (j >= i) ? U[(i64)i * ld + j] : T(0);
     }
     __syncthreads();
     for (int c = 0; c < t; ++c) {
-        double d = S[c * lp + c];
-        if (!(d > 0.0) || !isfinite(d)) {  // not positive definite at global column g0 + c + 1
+        T d = S[c * lp + c];
+        if (!(d > T(0)) || !isfinite(d)) {  // not positive definite at global column g0 + c + 1
             if (tid == 0) {
                 s_fail = 1;
                 if (*info == 0) *info = g0 + c + 1;
@@ -83,7 +84,7 @@ __global__ void __launch_bounds__(PO_NT) k_potrf_diag(double *__restrict__ U, i6
         // rows i below c, columns j >= i: 16 row groups x 32 columns of threads
         const int tx = tid & 31, ty = tid >> 5;
         for (int i = c + 1 + ty; i < t; i += PO_NT / 32) {
-            const double ui = S[c * lp + i];
+            const T ui = S[c * lp + i];
             for (int j = i + tx; j < t; j += 32) S[i * lp + j] = fma(-ui, S[c * lp + j], S[i * lp + j]);
         }
         __syncthreads();
@@ -94,21 +95,21 @@ __global__ void __launch_bounds__(PO_NT) k_potrf_diag(double *__restrict__ U, i6
         if (j >= i) U[(i64)i * ld + j] = S[i * lp + j];
     }
     if (s_fail) {
-        for (int e = tid; e < t * t; e += PO_NT) Wneg[e] = 0.0;
+        for (int e = tid; e < t * t; e += PO_NT) Wneg[e] = T(0);
         return;
     }
     // W = U^-1, column j by the four threads 4j .. 4j+3 (one warp holds 8 columns)
-    for (int i = tid; i < t; i += PO_NT) s_inv[i] = 1.0 / S[i * lp + i];
+    for (int i = tid; i < t; i += PO_NT) s_inv[i] = T(1) / S[i * lp + i];
     __syncthreads();
     {
         const int j = tid >> 2, sub = tid & 3;
         const unsigned quad = 0xFu << ((threadIdx.x & 31) & ~3);
         if (j < t) {
-            double *wrow = S + j * lp;  // W^T row j = W column j, entries 0..j-1 (strict lower of S)
-            const double wjj = s_inv[j];
+            T *wrow = S + j * lp;  // W^T row j = W column j, entries 0..j-1 (strict lower of S)
+            const T wjj = s_inv[j];
             for (int i = j - 1; i >= 0; --i) {
-                const double *urow = S + i * lp;
-                double part = 0.0;
+                const T *urow = S + i * lp;
+                T part = T(0);
                 for (int p = i + 1 + sub; p <= j; p += 4) part = fma(urow[p], (p == j) ? wjj : wrow[p], part);
                 part += __shfl_xor_sync(quad, part, 1);
                 part += __shfl_xor_sync(quad, part, 2);
@@ -121,13 +122,14 @@ __global__ void __launch_bounds__(PO_NT) k_potrf_diag(double *__restrict__ U, i6
     // Wneg = -W^T: row i holds -w_pi for p <= i
     for (int e = tid; e < t * t; e += PO_NT) {
         const int i = e / t, p = e - i * t;
-        Wneg[e] = (p < i) ? -S[i * lp + p] : (p == i ? -s_inv[i] : 0.0);
+        Wneg[e] = (p < i) ? -S[i * lp + p] : (p == i ? -s_inv[i] : T(0));
     }
 }
 
 // The solved block row back into place (row-major t x N), unless the
 // factorization failed.
-__global__ void k_copy_block_row(const double *__restrict__ X, i64 ldx, double *__restrict__ B, i64 ldb, int t,
+template <typename T>
+__global__ void k_copy_block_row(const T *__restrict__ X, i64 ldx, T *__restrict__ B, i64 ldb, int t,
                                  i64 N, const int64_t *__restrict__ info) {
     if (*(volatile const int64_t *)info != 0) return;
     const i64 idx = (i64)blockIdx.x * blockDim.x + threadIdx.x;
@@ -138,65 +140,93 @@ __global__ void k_copy_block_row(const double *__restrict__ X, i64 ldx, double *
 
 // The strict lower triangle of the row-major view (the strict upper triangle
 // of the caller's column-major matrix) set to zero, as the reference does.
-__global__ void k_zero_strict_lower(double *__restrict__ U, i64 ld, int n, const int64_t *__restrict__ info) {
+template <typename T>
+__global__ void k_zero_strict_lower(T *__restrict__ U, i64 ld, int n, const int64_t *__restrict__ info) {
     if (*info != 0) return;  // as the reference: a failed factorization keeps its other triangle
     const i64 idx = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (i64)n * n) return;
     const int i = (int)(idx / n), j = (int)(idx - (i64)i * n);
-    if (j < i) U[(i64)i * ld + j] = 0.0;
+    if (j < i) U[(i64)i * ld + j] = T(0);
 }
 
-// Workspace of one factorization: T (n x NB), Bc and X (NB x ldx each), Wneg (NB x NB).
-static size_t potrf_work_doubles(i64 n) {
-    const i64 ldx = (n + 1) / 2 * 2;
+// Workspace of one factorization, in elements: T (n x NB), Bc and X (NB x ldx
+// each), Wneg (NB x NB).
+size_t potrf_work_elems(i64 n) {
+    const i64 ldx = (n + 3) / 4 * 4;
     return (size_t)n * PO_NB + 2 * (size_t)PO_NB * ldx + (size_t)PO_NB * PO_NB + 64;
 }
 
+// X (t x N) = 0 - Wneg B and the symmetric update A22 -= T X (T = X^T), upper
+// triangle of the row-major view: FP64 on the DMMA tensor-core GEMM; FP32 (the
+// mixed solve's low-precision factor, a private copy) with the product on the
+// CUDA cores and the update in the handle's trailing precision (tcgen05 for the
+// 16-bit kinds; the whole square, the other triangle being scratch there).
+static void po_block_row(oxi_handle_s *h, double *X, i64 ldx, const double *Wneg, int t, const double *B, i64 ldb,
+                         i64 N, cudaStream_t s) {
+    launch_gemm_dmma(X, ldx, Wneg, t, B, ldb, t, N, t, s);
+}
+static void po_block_row(oxi_handle_s *, float *X, i64 ldx, const float *Wneg, int t, const float *B, i64 ldb,
+                         i64 N, cudaStream_t s) {
+    launch_gemm_simt<float>(X, ldx, Wneg, t, B, ldb, t, N, t, s);
+}
+static void po_sym_update(oxi_handle_s *, double *A22, i64 ld, const double *T, int t, const double *X, i64 ldx,
+                          i64 N, cudaStream_t s) {
+    launch_gemm_dmma(A22, ld, T, t, X, ldx, N, N, t, s, /*upper_only=*/true);
+}
+static void po_sym_update(oxi_handle_s *h, float *A22, i64 ld, const float *T, int t, const float *X, i64 ldx,
+                          i64 N, cudaStream_t s) {
+    if (h->trailing == TRAIL_NATIVE) launch_gemm_simt<float>(A22, ld, T, t, X, ldx, N, N, t, s);
+    else gemm_trailing_f32(h, A22, ld, T, t, X, ldx, N, N, t);
+}
+
 // One factorization: U in place (row-major view), *d_info set on failure.
-static void potrf_rowmajor(oxi_handle_s *h, double *U, i64 ld, i64 n, int64_t *d_info, double *work) {
+template <typename T>
+void potrf_rowmajor(oxi_handle_s *h, T *U, i64 ld, i64 n, int64_t *d_info, T *work) {
     cudaStream_t s = h->stream;
-    const i64 ldx = (n + 1) / 2 * 2;
-    double *T = work;
-    double *Bc = T + (size_t)n * PO_NB;
-    double *X = Bc + (size_t)PO_NB * ldx;
-    double *Wneg = X + (size_t)PO_NB * ldx;
+    const i64 ldx = (n + 3) / 4 * 4;  // 16-byte rows for the TMA-fed GEMMs
+    T *Tt = work;
+    T *Bc = Tt + (size_t)n * PO_NB;
+    T *X = Bc + (size_t)PO_NB * ldx;
+    T *Wneg = X + (size_t)PO_NB * ldx;
     for (i64 k0 = 0; k0 < n; k0 += PO_NB) {
         const int t = (int)std::min<i64>(PO_NB, n - k0);
-        double *Ukk = U + k0 * ld + k0;
+        T *Ukk = U + k0 * ld + k0;
         {
-            const size_t smem = sizeof(double) * ((size_t)t * (t + 1) + t);
-            set_max_dyn_smem((const void *)k_potrf_diag, (int)(sizeof(double) * (PO_NB * (PO_NB + 1) + PO_NB)));
-            ProfScope ps(KC_LEAF, s, (double)t * t * t * (2.0 / 3.0), 16.0 * t * t);
-            k_potrf_diag<<<1, PO_NT, smem, s>>>(Ukk, ld, t, k0, d_info, Wneg);
+            const size_t smem = sizeof(T) * ((size_t)t * (t + 1) + t);
+            set_max_dyn_smem((const void *)k_potrf_diag<T>, (int)(sizeof(T) * (PO_NB * (PO_NB + 1) + PO_NB)));
+            ProfScope ps(KC_LEAF, s, (double)t * t * t * (2.0 / 3.0), 2.0 * sizeof(T) * t * t);
+            k_potrf_diag<T><<<1, PO_NT, smem, s>>>(Ukk, ld, t, k0, d_info, Wneg);
             OXI_LAUNCH_CHECK();
         }
         const i64 right = n - k0 - t;
         if (right <= 0) break;
-        double *Bk = Ukk + t;  // rows k0..k0+t, columns k0+t..n
+        T *Bk = Ukk + t;  // rows k0..k0+t, columns k0+t..n
         // the tensor-core GEMM reads its operands through TMA (16-byte aligned
         // rows); a block row at an odd offset or pitch is copied first
-        const double *Bop = Bk;
+        const T *Bop = Bk;
         i64 ldb_op = ld;
-        if ((uintptr_t)Bk % 16 != 0 || ld % 2 != 0) {
-            OXI_CUDA(cudaMemcpy2DAsync(Bc, sizeof(double) * ldx, Bk, sizeof(double) * ld, sizeof(double) * right,
-                                       (size_t)t, cudaMemcpyDeviceToDevice, s));
+        if ((uintptr_t)Bk % 16 != 0 || (ld * (i64)sizeof(T)) % 16 != 0) {
+            OXI_CUDA(cudaMemcpy2DAsync(Bc, sizeof(T) * ldx, Bk, sizeof(T) * ld, sizeof(T) * right, (size_t)t,
+                                       cudaMemcpyDeviceToDevice, s));
             Bop = Bc;
             ldb_op = ldx;
         }
         // X = 0 - (-W^T) A_k,right = U_kk^-T A_k,right
-        OXI_CUDA(cudaMemsetAsync(X, 0, sizeof(double) * (size_t)t * ldx, s));
-        launch_gemm_dmma(X, ldx, Wneg, t, Bop, ldb_op, t, right, t, s);
-        k_copy_block_row<<<(unsigned)(((i64)t * right + 255) / 256), 256, 0, s>>>(X, ldx, Bk, ld, t, right, d_info);
+        OXI_CUDA(cudaMemsetAsync(X, 0, sizeof(T) * (size_t)t * ldx, s));
+        po_block_row(h, X, ldx, Wneg, t, Bop, ldb_op, right, s);
+        k_copy_block_row<T><<<(unsigned)(((i64)t * right + 255) / 256), 256, 0, s>>>(X, ldx, Bk, ld, t, right, d_info);
         OXI_LAUNCH_CHECK();
-        // T = X^T (right x t, row-major): X read as a column-major right x t matrix
-        launch_cm_to_rm<double, double>(X, ldx, T, t, right, t, s);
-        double *A22 = U + (k0 + t) * ld + (k0 + t);
-        launch_gemm_dmma(A22, ld, T, t, X, ldx, right, right, t, s, /*upper_only=*/true);
+        // Tt = X^T (right x t, row-major): X read as a column-major right x t matrix
+        launch_cm_to_rm<T, T>(X, ldx, Tt, t, right, t, s);
+        T *A22 = U + (k0 + t) * ld + (k0 + t);
+        po_sym_update(h, A22, ld, Tt, t, X, ldx, right, s);
     }
     const i64 tot = n * n;
-    k_zero_strict_lower<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(U, ld, (int)n, d_info);
+    k_zero_strict_lower<T><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(U, ld, (int)n, d_info);
     OXI_LAUNCH_CHECK();
 }
+template void potrf_rowmajor<double>(oxi_handle_s *, double *, i64, i64, int64_t *, double *);
+template void potrf_rowmajor<float>(oxi_handle_s *, float *, i64, i64, int64_t *, float *);
 
 // ---------------------------------------------------------------------------
 // Solves with the factor: L y = b, then L^T x = y (the reference's two
@@ -223,8 +253,8 @@ extern "C" int oxi_dpotrf(oxi_handle_t h, int64_t n, double *dA, int64_t lda, in
         int64_t *d_info = (int64_t *)sc;
         OXI_CUDA(cudaMemsetAsync(d_info, 0, sizeof(int64_t), h->stream));
         // T (the transposed block row, n x NB) and room for an aligned copy of the block row
-        double *work = (double *)h->work.get(sizeof(double) * potrf_work_doubles(n));
-        potrf_rowmajor(h, dA, lda, n, d_info, work);
+        double *work = (double *)h->work.get(sizeof(double) * potrf_work_elems(n));
+        potrf_rowmajor<double>(h, dA, lda, n, d_info, work);
         int64_t *hi = (int64_t *)h->host_ws.get(64);
         OXI_CUDA(cudaMemcpyAsync(hi, d_info, sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
         queue_abort_read(h, (int *)(hi + 2));

@@ -863,6 +863,29 @@ template void lu_block_inverses_rowmajor<float>(oxi_handle_s *, const float *, i
 template void lu_block_inverses_rowmajor<double>(oxi_handle_s *, const double *, i64, i64, double *, double *);
 i64 lu_block_inverse_elems(i64 n) { return ((n + SB - 1) / SB) * (i64)TRSV_OPS; }
 
+template <typename T>
+void chol_block_ops(oxi_handle_s *h, const T *L, i64 ldl, i64 n, T *P1, T *P2) {
+    trsv_prep_launch<T, false, false, false>(L, ldl, (int)n, P1, h->stream);
+    trsv_prep_launch<T, false, false, true>(L, ldl, (int)n, P2, h->stream);
+}
+template void chol_block_ops<float>(oxi_handle_s *, const float *, i64, i64, float *, float *);
+template void chol_block_ops<double>(oxi_handle_s *, const double *, i64, i64, double *, double *);
+
+template <typename T>
+void chol_solve_ops(oxi_handle_s *h, const T *L, i64 ldl, i64 n, T *X, i64 ldx, i64 nrhs, int *d_err,
+                    const T *P1, const T *P2) {
+    const i64 nb = (n + SB - 1) / SB;
+    if (nb + 1 > kTrsvCtlInts) throw CudaError{cudaErrorInvalidValue, "system too large for the solve control block"};
+    int *ctl = (int *)((char *)h->scratch.get(kScratchBytes) + kScratchTrsvOff);
+    unsigned long long *xtag = xtag_words(h, n);
+    trsv3_launch<T, false, false>(L, ldl, X, ldx, (int)n, (int)nrhs, ctl, d_err, h->stream, P1, xtag);
+    trsv3_launch<T, false, true>(L, ldl, X, ldx, (int)n, (int)nrhs, ctl, d_err, h->stream, P2, xtag);
+}
+template void chol_solve_ops<float>(oxi_handle_s *, const float *, i64, i64, float *, i64, i64, int *, const float *,
+                                    const float *);
+template void chol_solve_ops<double>(oxi_handle_s *, const double *, i64, i64, double *, i64, i64, int *,
+                                     const double *, const double *);
+
 // LUFactor.p from the interchange sequence (src/lapack/factorizations.jl:72-75).
 void perm_from_ipiv(const int64_t *ipiv, i64 q, i64 m, int64_t *perm) {
     for (i64 i = 0; i < m; ++i) perm[i] = i;

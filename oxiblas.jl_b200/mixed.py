@@ -12,6 +12,10 @@ refine    : "ir" (classical, the reference's loop), "gmres" (GMRES-IR),
             "auto" (IR, switching to GMRES-IR when it stagnates).
 normwise  : stop on the normwise backward error instead of the componentwise
             one (the reference's metric).
+factorization : "lu" (default) or "cholesky" (the Cholesky family: one global
+            scale max|a_ij|, the low-precision Cholesky of the lower triangle;
+            a factor that is not positive definite falls back to FP64, and
+            PosDefException if that fails too).
 Returns a dict with the reference's NamedTuple fields (x, converged,
 iterations, residual, backward_error, metric, low_type, fallback, finite,
 reason) plus backward_error_normwise, gmres_iterations, factor_ms, refine_ms.
@@ -25,6 +29,8 @@ import torch
 
 from ._lib import (ArgumentError, DimensionMismatch, Handle, SingularException, OPT_STOP_NORMWISE,
                    OXI_ENONFINITE, OXI_ENOTCONVERGED, OXI_ESINGULAR, OXI_OK)
+
+OXI_ENOTPOSDEF = 10
 from .lu import colmajor_copy, _as_tensor
 
 PREC = {"fp32": 0, "bf16": 1, "fp16": 2, "fp64": 3, "bf16x3": 4, "fp16x3": 5}
@@ -43,7 +49,8 @@ class RefineReport(ctypes.Structure):
 
 
 def mixed_solve_device(Acm: torch.Tensor, Bcm: torch.Tensor, Xcm: torch.Tensor, n: int, nrhs: int,
-                       maxiter=10, rtol=1e-13, precision="fp32", refine="ir", normwise=False):
+                       maxiter=10, rtol=1e-13, precision="fp32", refine="ir", normwise=False,
+                       factorization="lu"):
     """Device-resident call: Acm (n, n) contiguous is the column-major A, Bcm and
     Xcm (nrhs, n) contiguous are column-major B and X.  Returns (status, report)."""
     h = Handle.get()
@@ -51,7 +58,8 @@ def mixed_solve_device(Acm: torch.Tensor, Bcm: torch.Tensor, Xcm: torch.Tensor, 
     old = h.get_option(OPT_STOP_NORMWISE)
     h.set_option(OPT_STOP_NORMWISE, 1 if normwise else 0)
     try:
-        st = h.lib.oxi_dgesv_mixed(h.ptr, PREC[precision], REFINE[refine], n, nrhs,
+        fn = h.lib.oxi_dposv_mixed if factorization == "cholesky" else h.lib.oxi_dgesv_mixed
+        st = fn(h.ptr, PREC[precision], REFINE[refine], n, nrhs,
                                    ctypes.c_void_p(Acm.data_ptr()), max(1, n),
                                    ctypes.c_void_p(Bcm.data_ptr()), max(1, n),
                                    ctypes.c_void_p(Xcm.data_ptr()), max(1, n), int(maxiter),
@@ -62,7 +70,10 @@ def mixed_solve_device(Acm: torch.Tensor, Bcm: torch.Tensor, Xcm: torch.Tensor, 
 
 
 def mixed_solve(A, b, *, maxiter: int = 10, rtol: float = 1e-13, precision: str = "fp32",
-                refine: str = "ir", normwise: bool = False, fallback: bool = True):
+                refine: str = "ir", normwise: bool = False, fallback: bool = True,
+                factorization: str = "lu"):
+    if factorization not in ("lu", "cholesky"):
+        raise ArgumentError("unknown mixed factorization")
     if precision not in PREC:
         raise ArgumentError("low precision type must be one of " + ", ".join(PREC))
     if refine not in REFINE:
@@ -92,15 +103,21 @@ def mixed_solve(A, b, *, maxiter: int = 10, rtol: float = 1e-13, precision: str 
     for k0 in range(0, nrhs, 16):
         k1 = min(nrhs, k0 + 16)
         st, rep = mixed_solve_device(Acm, Bcm[k0:k1], Xcm[k0:k1], n, k1 - k0, maxiter, rtol,
-                                     precision, refine, normwise)
+                                     precision, refine, normwise, factorization)
         h = Handle.get()
         if st == OXI_ENONFINITE:
             raise ArgumentError("finite mixed input required")
         if st == OXI_ESINGULAR:
             raise SingularException(rep.info)
+        if st == OXI_ENOTPOSDEF:
+            from .cholesky import PosDefException
+            raise PosDefException(rep.info)
         if st not in (OXI_OK, OXI_ENOTCONVERGED):
             h.check(st)
         if rep.fallback and not fallback:
+            if factorization == "cholesky":
+                from .cholesky import PosDefException
+                raise PosDefException(rep.info)
             raise SingularException(rep.info)
         reps.append(rep)
     X = Xcm.t()
@@ -114,7 +131,7 @@ def mixed_solve(A, b, *, maxiter: int = 10, rtol: float = 1e-13, precision: str 
                 backward_error=err,
                 backward_error_normwise=max(r.backward_error_normwise for r in reps),
                 metric="componentwise_backward_error", low_type=precision,
-                fallback=any(r.fallback for r in reps), finite=finite,
+                fallback=any(r.fallback for r in reps), finite=finite, factorization=factorization,
                 reason=REASONS[worst.reason] if finite else "nonfinite_iteration",
                 gmres_iterations=sum(r.gmres_iterations for r in reps),
                 refine_used=("ir", "gmres", "auto")[worst.refine_used],

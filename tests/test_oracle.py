@@ -204,3 +204,19 @@ def test_oracle_complex_pivot_overflow_and_zero(oracle):
     S[3, 0], S[9, 0] = 1.0, 2.0
     _, _, info = oracle.zgetrf(S, check=False)
     assert info == 5
+
+
+def test_oracle_mixed_cholesky(oracle):
+    rng = np.random.default_rng(21)
+    n = 200
+    G = rng.standard_normal((n, n))
+    A = G @ G.T + n * np.eye(n)
+    b = rng.standard_normal(n)
+    r = oracle.mixed_solve_chol(A, b, maxiter=20, rtol=1e-13)
+    assert r["converged"] and not r["fallback"]
+    x = np.linalg.solve(A, b)
+    assert np.linalg.norm(r["x"] - x) <= 1e-11 * np.linalg.norm(x)
+    N = A.copy()
+    N[50, 50] = -1.0
+    with pytest.raises(ValueError):
+        oracle.mixed_solve_chol(N, b)
