@@ -191,18 +191,15 @@ __device__ void lu_blocked(T *W, int ldw, int n, int nb, bool in_smem, T *sP, T 
         } else {
             P = sP;
             ldp = m;
-            for (int e = threadIdx.x; e < m * jb; e += NT) {
-                const int r = e % m, c = e / m;
-                sP[r + c * ldp] = W[(k + r) + (i64)(k + c) * ldw];
-            }
+            // a warp per column, its lanes down the rows (coalesced, no index division)
+            for (int c = (int)(threadIdx.x >> 5); c < jb; c += NW)
+                for (int r = (int)(threadIdx.x & 31); r < m; r += 32) sP[r + c * ldp] = W[(k + r) + (i64)(k + c) * ldw];
             __syncthreads();
         }
         panel_lu(P, ldp, m, jb, k, S);
         if (!in_smem) {
-            for (int e = threadIdx.x; e < m * jb; e += NT) {
-                const int r = e % m, c = e / m;
-                W[(k + r) + (i64)(k + c) * ldw] = sP[r + c * ldp];
-            }
+            for (int c = (int)(threadIdx.x >> 5); c < jb; c += NW)
+                for (int r = (int)(threadIdx.x & 31); r < m; r += 32) W[(k + r) + (i64)(k + c) * ldw] = sP[r + c * ldp];
         }
         // interchanges on the other columns, then U12 = L11^-1 A12
         const int c2 = k + jb;
@@ -229,16 +226,23 @@ __device__ void lu_blocked(T *W, int ldw, int n, int nb, bool in_smem, T *sP, T 
                 const int ccap = (nb * NMAX) / nmv;  // columns per pass (>= 128)
                 for (int cb = 0; cb < n; cb += ccap) {
                     const int cn = min(ccap, n - cb);
-                    for (int e = threadIdx.x; e < nmv * cn; e += NT) {
-                        const int mv = e / cn, c = cb + e % cn;
-                        if (c >= k && c < c2) continue;
-                        sU[mv * ccap + (c - cb)] = W[S.rowat[S.mvpos[mv]] + (i64)c * ldw];
+                    // a warp per moved row, its lanes across the columns
+                    for (int mv = (int)(threadIdx.x >> 5); mv < nmv; mv += NW) {
+                        const int src = S.rowat[S.mvpos[mv]];
+                        for (int cc = (int)(threadIdx.x & 31); cc < cn; cc += 32) {
+                            const int c = cb + cc;
+                            if (c >= k && c < c2) continue;
+                            sU[mv * ccap + cc] = W[src + (i64)c * ldw];
+                        }
                     }
                     __syncthreads();
-                    for (int e = threadIdx.x; e < nmv * cn; e += NT) {
-                        const int mv = e / cn, c = cb + e % cn;
-                        if (c >= k && c < c2) continue;
-                        W[S.mvpos[mv] + (i64)c * ldw] = sU[mv * ccap + (c - cb)];
+                    for (int mv = (int)(threadIdx.x >> 5); mv < nmv; mv += NW) {
+                        const int dst = S.mvpos[mv];
+                        for (int cc = (int)(threadIdx.x & 31); cc < cn; cc += 32) {
+                            const int c = cb + cc;
+                            if (c >= k && c < c2) continue;
+                            W[dst + (i64)c * ldw] = sU[mv * ccap + cc];
+                        }
                     }
                     __syncthreads();
                 }
@@ -374,10 +378,8 @@ __device__ void block_lu_solve(const T *W, int ldw, int n, T *stage, int cw, boo
     for (int j0 = 0; j0 < n; j0 += cw) {  // forward, unit lower
         const int jn = min(cw, n - j0);
         __syncthreads();
-        for (int e = threadIdx.x; e < jn * n; e += NT) {
-            const int j = e / n, r = e - j * n;
-            stage[r + j * NMAX] = W[r + (i64)(j0 + j) * ldw];
-        }
+        for (int j = (int)(threadIdx.x >> 5); j < jn; j += NW)
+            for (int r = lane; r < n; r += 32) stage[r + j * NMAX] = W[r + (i64)(j0 + j) * ldw];
         __syncthreads();
         if (active) {
             for (int jj = 0; jj < jn; ++jj) {
@@ -399,10 +401,8 @@ __device__ void block_lu_solve(const T *W, int ldw, int n, T *stage, int cw, boo
     for (int j1 = n; j1 > 0; j1 -= cw) {  // backward, upper
         const int j0 = max(0, j1 - cw), jn = j1 - j0;
         __syncthreads();
-        for (int e = threadIdx.x; e < jn * n; e += NT) {
-            const int j = e / n, r = e - j * n;
-            stage[r + j * NMAX] = W[r + (i64)(j0 + j) * ldw];
-        }
+        for (int j = (int)(threadIdx.x >> 5); j < jn; j += NW)
+            for (int r = lane; r < n; r += 32) stage[r + j * NMAX] = W[r + (i64)(j0 + j) * ldw];
         __syncthreads();
         if (active) {
             for (int j = j1 - 1; j >= j0; --j) {
@@ -523,10 +523,8 @@ __global__ void __launch_bounds__(bt::NT, 2) k_lu_batched(const __grid_constant_
             if (in_smem) {
                 W = sW;
                 ldw = n;
-                for (int e = tid; e < n * n; e += NT) {
-                    const int r = e % n, c = e / n;
-                    W[r + c * ldw] = (T)A[r + (i64)c * lda];
-                }
+                for (int c = warp; c < n; c += NW)
+                    for (int r = lane; r < n; r += 32) W[r + c * ldw] = (T)A[r + (i64)c * lda];
             } else {
                 W = (T *)A;
                 ldw = (int)lda;
@@ -566,10 +564,8 @@ __global__ void __launch_bounds__(bt::NT, 2) k_lu_batched(const __grid_constant_
                 __syncthreads();
                 continue;
             }
-            for (int e = tid; e < n * n; e += NT) {
-                const int r = e % n, c = e / n;
-                W[r + c * ldw] = (T)(A[r + (i64)c * lda] / S.rows[r] / S.cols[c]);
-            }
+            for (int c = warp; c < n; c += NW)
+                for (int r = lane; r < n; r += 32) W[r + c * ldw] = (T)(A[r + (i64)c * lda] / S.rows[r] / S.cols[c]);
             __syncthreads();
         }
 
@@ -585,10 +581,8 @@ __global__ void __launch_bounds__(bt::NT, 2) k_lu_batched(const __grid_constant_
             for (int j = tid; j < n; j += NT) ip[j] = S.piv[j] + 1;
         if constexpr (sizeof(T) == 8) {
             if (in_smem)
-                for (int e = tid; e < n * n; e += NT) {
-                    const int r = e % n, c = e / n;
-                    A[r + (i64)c * lda] = W[r + c * ldw];
-                }
+                for (int c = warp; c < n; c += NW)
+                    for (int r = lane; r < n; r += 32) A[r + (i64)c * lda] = W[r + c * ldw];
         }
         if (d.mode == MODE_GETRF || info != 0 || nr == 0) {
             if (d.mode == MODE_MIXED && tid == 0) {
@@ -677,10 +671,8 @@ __global__ void __launch_bounds__(bt::NT, 2) k_lu_batched(const __grid_constant_
                 }
                 __syncthreads();
             };
-            for (int e = tid; e < n * nr; e += NT) {
-                const int i = e % n, r = e / n;
-                sR[r * NMAX + i] = B[i + (i64)r * ldb];
-            }
+            for (int r = warp; r < nr; r += NW)
+                for (int i = lane; i < n; i += 32) sR[r * NMAX + i] = B[i + (i64)r * ldb];
             __syncthreads();
             correct(false);
             double err = INFINITY;
@@ -737,10 +729,8 @@ __global__ void __launch_bounds__(bt::NT, 2) k_lu_batched(const __grid_constant_
                 if (err <= d.rtol || iter >= d.maxiter || !isfinite(err)) break;
                 correct(true);
             }
-            for (int e = tid; e < n * nr; e += NT) {
-                const int i = e % n, r = e / n;
-                Xo[i + (i64)r * ldxo] = sX[r * NMAX + i];
-            }
+            for (int r = warp; r < nr; r += NW)
+                for (int i = lane; i < n; i += 32) Xo[i + (i64)r * ldxo] = sX[r * NMAX + i];
             if (tid == 0) {
                 if (d.iters) d.iters[mi] = iter;
                 if (d.berr) d.berr[mi] = err;

@@ -48,6 +48,15 @@ __device__ __forceinline__ zd zdivd(zd a, zd b) {
     return {(ar * br + ai * bi) / den, (ai * br - ar * bi) / den};
 }
 
+// 1 / b, scaled by the larger of |b.r|, |b.i| (no spurious overflow)
+__device__ __forceinline__ zd zrecip(zd b) {
+    double s = fmax(fabs(b.r), fabs(b.i));
+    if (s == 0.0) s = 1.0;
+    const double br = b.r / s, bi = b.i / s;
+    const double den = (br * br + bi * bi) * s;
+    return {br / den, -bi / den};
+}
+
 // (key, position) argmax over the CTA: the largest key, the smallest position
 // among equal keys; keys are non-negative doubles (NaN never enters).
 __device__ __forceinline__ void cta_argmax(double &key, int &pos, double *s_key, int *s_pos) {
@@ -136,9 +145,13 @@ __global__ void __launch_bounds__(ZLEAF_NT) k_zleaf(double *__restrict__ Wr, dou
             if (tid == 0 && *info == 0) *info = gofs + j + 1;
             continue;
         }
+        // the multipliers a / d as a times the reciprocal of d, formed once per
+        // column (the reference divides each element; the results agree to
+        // rounding)
+        const zd dinv = zrecip(d);
         for (int i = j + 1 + tid; i < m; i += ZLEAF_NT) {
             double *rr = Wr + (i64)i * ld, *ri = Wi + (i64)i * ld;
-            const zd l = zdivd({rr[j], ri[j]}, d);
+            const zd l = zmul({rr[j], ri[j]}, dinv);
             rr[j] = l.r;
             ri[j] = l.i;
             for (int c = j + 1; c < w; ++c) {
@@ -359,6 +372,51 @@ __global__ void __launch_bounds__(256) k_ztrsv(const double2 *__restrict__ LU, i
     }
 }
 
+// x <- T^-1 x for the untransposed factors, column by column with x in shared
+// memory: the forward unit-lower solve (x_i -= l_ij x_j for i > j once x_j is
+// final) or the backward upper one (x_j /= u_jj, then x_i -= u_ij x_j for
+// i < j).  Each step reads one column of the factor, contiguous in memory.
+// One CTA per right-hand side; n <= ZCOLS_MAXN.
+constexpr int ZCOLS_NT = 512;
+constexpr int ZCOLS_MAXN = 12288;
+__global__ void __launch_bounds__(ZCOLS_NT) k_ztrsv_cols(const double2 *__restrict__ LU, i64 lda,
+                                                         double2 *__restrict__ X, i64 ldx, int n, int lower) {
+    extern __shared__ double2 zx[];
+    double2 *x = X + (i64)blockIdx.x * ldx;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < n; i += ZCOLS_NT) zx[i] = x[i];
+    __syncthreads();
+    if (lower) {
+        for (int j = 0; j < n - 1; ++j) {
+            const double2 xv = zx[j];
+            const zd xj = {xv.x, xv.y};
+            const double2 *col = LU + (i64)j * lda;
+            for (int i = j + 1 + tid; i < n; i += ZCOLS_NT) {
+                const double2 l = col[i], b = zx[i];
+                const zd v = zmsub({b.x, b.y}, {l.x, l.y}, xj);
+                zx[i] = make_double2(v.r, v.i);
+            }
+            __syncthreads();
+        }
+        for (int i = tid; i < n; i += ZCOLS_NT) x[i] = zx[i];
+    } else {
+        // zx[j] is not written in step j (every thread divides it for itself),
+        // and not read after it: the solution goes straight to x[j]
+        for (int j = n - 1; j >= 0; --j) {
+            const double2 xv = zx[j], d = LU[j + (i64)j * lda];
+            const zd xj = zdivd({xv.x, xv.y}, {d.x, d.y});
+            const double2 *col = LU + (i64)j * lda;
+            for (int i = tid; i < j; i += ZCOLS_NT) {
+                const double2 u = col[i], b = zx[i];
+                const zd v = zmsub({b.x, b.y}, {u.x, u.y}, xj);
+                zx[i] = make_double2(v.r, v.i);
+            }
+            if (tid == 0) x[j] = make_double2(xj.r, xj.i);
+            __syncthreads();
+        }
+    }
+}
+
 // the interchanges on the columns of X: forward (before the 'N' solves) or in
 // reverse (after the 'T' / 'C' solves), one thread per right-hand side
 __global__ void k_zperm(double2 *__restrict__ X, i64 ldx, int n, int nrhs, const int64_t *__restrict__ ipiv,
@@ -444,10 +502,19 @@ extern "C" int oxi_zgetrs(oxi_handle_t h, char trans, int64_t n, int64_t nrhs, c
         if (trans == 'N') {
             k_zperm<<<gp, 128, 0, s>>>(X, ldb, (int)n, (int)nrhs, d_ipiv, 0);
             OXI_LAUNCH_CHECK();
-            k_ztrsv<<<(unsigned)nrhs, 256, 0, s>>>(LU, lda, X, ldb, (int)n, 1, 1, 0, 0);
-            OXI_LAUNCH_CHECK();
-            k_ztrsv<<<(unsigned)nrhs, 256, 0, s>>>(LU, lda, X, ldb, (int)n, 0, 0, 0, 0);
-            OXI_LAUNCH_CHECK();
+            if (n <= ZCOLS_MAXN) {
+                const int smem = (int)(sizeof(double2) * n);
+                set_max_dyn_smem((const void *)k_ztrsv_cols, (int)(sizeof(double2) * ZCOLS_MAXN));
+                k_ztrsv_cols<<<(unsigned)nrhs, ZCOLS_NT, smem, s>>>(LU, lda, X, ldb, (int)n, 1);
+                OXI_LAUNCH_CHECK();
+                k_ztrsv_cols<<<(unsigned)nrhs, ZCOLS_NT, smem, s>>>(LU, lda, X, ldb, (int)n, 0);
+                OXI_LAUNCH_CHECK();
+            } else {
+                k_ztrsv<<<(unsigned)nrhs, 256, 0, s>>>(LU, lda, X, ldb, (int)n, 1, 1, 0, 0);
+                OXI_LAUNCH_CHECK();
+                k_ztrsv<<<(unsigned)nrhs, 256, 0, s>>>(LU, lda, X, ldb, (int)n, 0, 0, 0, 0);
+                OXI_LAUNCH_CHECK();
+            }
         } else {
             const int cj = trans == 'C';
             // U^T (U^H) is lower, non-unit; L^T (L^H) upper, unit
