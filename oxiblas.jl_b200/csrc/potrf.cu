@@ -42,9 +42,9 @@ constexpr int PO_NT = 512;          // threads of the diagonal-block kernel (4 p
 // for each row c, d = sqrt(a_cc), the row scaled by d, then the rank-1 update
 // of the upper triangle below it, a_ij = fma(-u_ci, u_cj, a_ij) for c < i <= j
 // (the reference leaf's column updates, src/lapack/factorizations.jl:266-282,
-// read through the transposition).  Then W = U^-1 by columns, four threads per
-// column (w_jj = 1/u_jj; w_ij = -(sum_{p=i+1..j} u_ip w_pj) / u_ii for i = j-1
-// down to 0), W^T kept in the block's unused strict lower triangle, and
+// read through the transposition).  Then W = U^-1 by rows from the bottom
+// (w_jj = 1/u_jj; w_ij = -(sum_{p=i+1..j} u_ip w_pj) / u_ii, the columns of a
+// row in parallel), W^T kept in the block's unused strict lower triangle, and
 // Wneg = -W^T (t x t, row-major, lower) written for the block-row product.
 template <typename T>
 __global__ void __launch_bounds__(PO_NT) k_potrf_diag(T *__restrict__ U, i64 ld, int t, i64 g0,
@@ -98,27 +98,28 @@ __global__ void __launch_bounds__(PO_NT) k_potrf_diag(T *__restrict__ U, i64 ld,
         for (int e = tid; e < t * t; e += PO_NT) Wneg[e] = T(0);
         return;
     }
-    // W = U^-1, column j by the four threads 4j .. 4j+3 (one warp holds 8 columns)
+    // W = U^-1 row by row from the bottom: for row i every later column j is
+    // independent, four threads per column (j = i + 1 + tid / 4) splitting the
+    // sum w_ij = -(sum_{p=i+1..j} u_ip w_pj) / u_ii; one barrier per row.
     for (int i = tid; i < t; i += PO_NT) s_inv[i] = T(1) / S[i * lp + i];
     __syncthreads();
     {
-        const int j = tid >> 2, sub = tid & 3;
+        const int sub = tid & 3;
         const unsigned quad = 0xFu << ((threadIdx.x & 31) & ~3);
-        if (j < t) {
-            T *wrow = S + j * lp;  // W^T row j = W column j, entries 0..j-1 (strict lower of S)
-            const T wjj = s_inv[j];
-            for (int i = j - 1; i >= 0; --i) {
+        for (int i = t - 2; i >= 0; --i) {
+            const int j = i + 1 + (tid >> 2);
+            if (j < t) {
                 const T *urow = S + i * lp;
+                const T *wcol = S + j * lp;  // W column j (rows p < j), kept in the strict lower part of S
                 T part = T(0);
-                for (int p = i + 1 + sub; p <= j; p += 4) part = fma(urow[p], (p == j) ? wjj : wrow[p], part);
+                for (int p = i + 1 + sub; p <= j; p += 4) part = fma(urow[p], (p == j) ? s_inv[j] : wcol[p], part);
                 part += __shfl_xor_sync(quad, part, 1);
                 part += __shfl_xor_sync(quad, part, 2);
-                if (sub == 0) wrow[i] = -part * s_inv[i];
-                __syncwarp(quad);
+                if (sub == 0) S[j * lp + i] = -part * s_inv[i];
             }
+            __syncthreads();
         }
     }
-    __syncthreads();
     // Wneg = -W^T: row i holds -w_pi for p <= i
     for (int e = tid; e < t * t; e += PO_NT) {
         const int i = e / t, p = e - i * t;

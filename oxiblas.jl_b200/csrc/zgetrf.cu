@@ -182,19 +182,40 @@ __global__ void k_zlaswp(double *__restrict__ Wr, double *__restrict__ Wi, i64 l
     }
 }
 
-// B (t x N at (Br, Bi), ld) <- L^-1 B, L the unit lower t x t block at (Lr, Li):
-// one thread per column, s = b_i; s -= l_ip x_p for p < i in order.
-__global__ void k_ztrsm_lunit(const double *__restrict__ Lr, const double *__restrict__ Li, double *__restrict__ Br,
-                              double *__restrict__ Bi, i64 ld, int t, i64 N) {
-    const i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= N) return;
-    for (int i = 1; i < t; ++i) {
-        zd s = {Br[(i64)i * ld + c], Bi[(i64)i * ld + c]};
-        for (int p = 0; p < i; ++p)
-            s = zmsub(s, {__ldg(Lr + (i64)i * ld + p), __ldg(Li + (i64)i * ld + p)}, {Br[(i64)p * ld + c], Bi[(i64)p * ld + c]});
-        Br[(i64)i * ld + c] = s.r;
-        Bi[(i64)i * ld + c] = s.i;
+// B (t x N at (Br, Bi), ld) <- L^-1 B, L the unit lower t x t block at (Lr, Li),
+// t <= ZT_MAXT: a CTA per 32 columns, the t x 32 tile in shared memory; once
+// row i is final every later row r is updated, x_r -= l_ri x_i (8 row groups of
+// a warp each, its lanes across the columns: l_ri is one broadcast load).
+constexpr int ZT_NT = 256, ZT_CW = 32, ZT_MAXT = 128;
+__global__ void __launch_bounds__(ZT_NT) k_ztrsm_lunit(const double *__restrict__ Lr, const double *__restrict__ Li,
+                                                       double *__restrict__ Br, double *__restrict__ Bi, i64 ld,
+                                                       int t, i64 N) {
+    extern __shared__ double2 zt[];  // [t][ZT_CW]
+    const int tid = threadIdx.x, cl = tid & (ZT_CW - 1), rg = tid / ZT_CW;
+    constexpr int RG = ZT_NT / ZT_CW;
+    const i64 c0 = (i64)blockIdx.x * ZT_CW;
+    const bool live = c0 + cl < N;
+    for (int r = rg; r < t; r += RG)
+        zt[r * ZT_CW + cl] = live ? make_double2(Br[(i64)r * ld + c0 + cl], Bi[(i64)r * ld + c0 + cl])
+                                  : make_double2(0.0, 0.0);
+    __syncthreads();
+    for (int i = 0; i < t - 1; ++i) {
+        const double2 xv = zt[i * ZT_CW + cl];
+        const zd xi = {xv.x, xv.y};
+        for (int r = i + 1 + rg; r < t; r += RG) {
+            const zd l = {__ldg(Lr + (i64)r * ld + i), __ldg(Li + (i64)r * ld + i)};
+            const double2 bv = zt[r * ZT_CW + cl];
+            const zd v = zmsub({bv.x, bv.y}, l, xi);
+            zt[r * ZT_CW + cl] = make_double2(v.r, v.i);
+        }
+        __syncthreads();
     }
+    if (live)
+        for (int r = rg + (rg == 0 ? RG : 0); r < t; r += RG) {  // row 0 is unchanged
+            const double2 v = zt[r * ZT_CW + cl];
+            Br[(i64)r * ld + c0 + cl] = v.x;
+            Bi[(i64)r * ld + c0 + cl] = v.y;
+        }
 }
 
 // dst = -src (rows x cols, row-major, lds / ldd)
@@ -272,7 +293,16 @@ static void zgemm_minus(ZRun &R, i64 cr, i64 cc, i64 ar, i64 ac, i64 br, i64 bc,
 static void ztrsm(ZRun &R, i64 r0, i64 c0, int t, i64 bc, i64 N) {
     if (t <= 1 || N <= 0) return;
     const i64 ld = R.ld;
-    k_ztrsm_lunit<<<(unsigned)((N + 127) / 128), 128, 0, R.h->stream>>>(
+    if (t > ZT_MAXT) {  // a wider block (blocksize > 128): the top rows, their update of the rest, the rest
+        const int h = ZT_MAXT;
+        ztrsm(R, r0, c0, h, bc, N);
+        zgemm_minus(R, r0 + h, bc, r0 + h, c0, r0, bc, t - h, N, h);
+        ztrsm(R, r0 + h, c0 + h, t - h, bc, N);
+        return;
+    }
+    const int smem = (int)(sizeof(double2) * t * ZT_CW);
+    set_max_dyn_smem((const void *)k_ztrsm_lunit, (int)(sizeof(double2) * ZT_MAXT * ZT_CW));
+    k_ztrsm_lunit<<<(unsigned)((N + ZT_CW - 1) / ZT_CW), ZT_NT, smem, R.h->stream>>>(
         R.Wr + r0 * ld + c0, R.Wi + r0 * ld + c0, R.Wr + r0 * ld + bc, R.Wi + r0 * ld + bc, ld, t, N);
     OXI_LAUNCH_CHECK();
 }
