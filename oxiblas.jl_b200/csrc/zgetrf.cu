@@ -164,22 +164,60 @@ __global__ void __launch_bounds__(ZLEAF_NT) k_zleaf(double *__restrict__ Wr, dou
     }
 }
 
-// laswp: the interchanges ipiv[k0 .. k0+cnt) (global 1-based rows) on columns
-// [c_lo, c_hi) of both planes, in order, one thread per column.
+// laswp: the interchanges ipiv[k0 .. k0+cnt) (global 1-based rows, cnt <= 16)
+// on columns [c_lo, c_hi) of both planes.  Their net effect is at most 2 cnt
+// row moves (dst <- src); thread 0 of each CTA folds the sequence into that
+// list, then every thread moves its column: all sources read, then all
+// destinations written (one round trip instead of cnt dependent swaps).
+constexpr int ZSWP_MAX = 2 * ZLEAF;
 __global__ void k_zlaswp(double *__restrict__ Wr, double *__restrict__ Wi, i64 ld, const int64_t *__restrict__ ipiv,
                          i64 k0, int cnt, i64 c_lo, i64 c_hi, i64 skip_lo, i64 skip_hi) {
-    const i64 c = c_lo + (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= c_hi || (c >= skip_lo && c < skip_hi)) return;
-    for (int t = 0; t < cnt; ++t) {
-        const i64 j = k0 + t, p = ipiv[j] - 1;
-        if (p != j) {
-            const double r = Wr[j * ld + c], im = Wi[j * ld + c];
-            Wr[j * ld + c] = Wr[p * ld + c];
-            Wi[j * ld + c] = Wi[p * ld + c];
-            Wr[p * ld + c] = r;
-            Wi[p * ld + c] = im;
+    __shared__ i64 s_dst[ZSWP_MAX], s_src[ZSWP_MAX];
+    __shared__ int s_n;
+    if (threadIdx.x == 0) {
+        i64 key[ZSWP_MAX], val[ZSWP_MAX];  // position -> row now there (absent: itself)
+        int nk = 0;
+        auto find = [&](i64 x) {
+            for (int q = 0; q < nk; ++q)
+                if (key[q] == x) return q;
+            key[nk] = x;
+            val[nk] = x;
+            return nk++;
+        };
+        for (int t = 0; t < cnt; ++t) {
+            const i64 j = k0 + t, p = ipiv[j] - 1;
+            if (p == j) continue;
+            const int a = find(j), b = find(p);
+            const i64 tmp = val[a];
+            val[a] = val[b];
+            val[b] = tmp;
         }
+        int nm = 0;
+        for (int q = 0; q < nk; ++q)
+            if (val[q] != key[q]) {
+                s_dst[nm] = key[q];
+                s_src[nm] = val[q];
+                ++nm;
+            }
+        s_n = nm;
     }
+    __syncthreads();
+    const int nm = s_n;
+    const i64 c = c_lo + (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (nm == 0 || c >= c_hi || (c >= skip_lo && c < skip_hi)) return;
+    double vr[ZSWP_MAX], vi[ZSWP_MAX];
+#pragma unroll
+    for (int q = 0; q < ZSWP_MAX; ++q)
+        if (q < nm) {
+            vr[q] = Wr[s_src[q] * ld + c];
+            vi[q] = Wi[s_src[q] * ld + c];
+        }
+#pragma unroll
+    for (int q = 0; q < ZSWP_MAX; ++q)
+        if (q < nm) {
+            Wr[s_dst[q] * ld + c] = vr[q];
+            Wi[s_dst[q] * ld + c] = vi[q];
+        }
 }
 
 // B (t x N at (Br, Bi), ld) <- L^-1 B, L the unit lower t x t block at (Lr, Li),
@@ -309,6 +347,7 @@ static void ztrsm(ZRun &R, i64 r0, i64 c0, int t, i64 bc, i64 N) {
 
 static void zlaswp(ZRun &R, i64 k0, int cnt, i64 c_lo, i64 c_hi, i64 skip_lo, i64 skip_hi) {
     if (c_hi <= c_lo || cnt <= 0) return;
+    if (cnt > ZLEAF) throw CudaError{cudaErrorInvalidValue, "more interchanges than a complex leaf makes"};
     const i64 cols = c_hi - c_lo;
     k_zlaswp<<<(unsigned)((cols + 127) / 128), 128, 0, R.h->stream>>>(R.Wr, R.Wi, R.ld, R.ipiv, k0, cnt, c_lo, c_hi,
                                                                         skip_lo, skip_hi);
