@@ -279,7 +279,10 @@ k_leaf_lu(T *__restrict__ P, i64 ld, int m, int wact, i64 gofs, int64_t *__restr
 #pragma unroll
         for (int k = 0; k < R; ++k) {
             const int i = k * G + g;
-            const uint64_t key = pivot_key(r[k][0]);
+            // _lu_pivot starts from row j with strict '>': a NaN at row j keeps
+            // row j (the largest key), a NaN below never wins (key 0)
+            const T v = r[k][0];
+            const uint64_t key = (i == j && v != v) ? ~0ull : pivot_key(v);
             if (i >= j && i < m && (bp == INT_MAX || key > bk)) { bk = key; bp = i; }  // slots ascend in i
         }
         // (b) warp winner

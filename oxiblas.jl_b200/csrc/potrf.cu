@@ -42,9 +42,9 @@ constexpr int PO_NT = 512;          // threads of the diagonal-block kernel (4 p
 // for each row c, d = sqrt(a_cc), the row scaled by d, then the rank-1 update
 // of the upper triangle below it, a_ij = fma(-u_ci, u_cj, a_ij) for c < i <= j
 // (the reference leaf's column updates, src/lapack/factorizations.jl:266-282,
-// read through the transposition).  Then W = U^-1 by rows from the bottom
-// (w_jj = 1/u_jj; w_ij = -(sum_{p=i+1..j} u_ip w_pj) / u_ii, the columns of a
-// row in parallel), W^T kept in the block's unused strict lower triangle, and
+// read through the transposition).  Then W = U^-1 by 32 x 32 diagonal blocks
+// and the off-diagonal blocks of the 64 and 128 levels, W^T kept in the
+// block's unused strict lower triangle, and
 // Wneg = -W^T (t x t, row-major, lower) written for the block-row product.
 template <typename T>
 __global__ void __launch_bounds__(PO_NT) k_potrf_diag(T *__restrict__ U, i64 ld, int t, i64 g0,
@@ -98,27 +98,49 @@ __global__ void __launch_bounds__(PO_NT) k_potrf_diag(T *__restrict__ U, i64 ld,
         for (int e = tid; e < t * t; e += PO_NT) Wneg[e] = T(0);
         return;
     }
-    // W = U^-1 row by row from the bottom: for row i every later column j is
-    // independent, four threads per column (j = i + 1 + tid / 4) splitting the
-    // sum w_ij = -(sum_{p=i+1..j} u_ip w_pj) / u_ii; one barrier per row.
+    // W = U^-1 by blocks (only the full 128-row blocks have a block row to the
+    // right; a shorter last block needs no inverse): the four 32 x 32 diagonal
+    // blocks column by column (a thread per column, the columns independent),
+    // then the off-diagonal block of each 64 x 64 and of the 128 x 128 level,
+    //   W[A, C] = -W[A, A] (U[A, C] W[C, C]),
+    // as two products in shared memory.  W (upper) is kept transposed in the
+    // strict lower part of S (w_rc at S[c * lp + r], r < c), its diagonal in s_inv.
+    if (t != PO_NB) {
+        for (int e = tid; e < t * t; e += PO_NT) Wneg[e] = T(0);
+        return;
+    }
     for (int i = tid; i < t; i += PO_NT) s_inv[i] = T(1) / S[i * lp + i];
     __syncthreads();
-    {
-        const int sub = tid & 3;
-        const unsigned quad = 0xFu << ((threadIdx.x & 31) & ~3);
-        for (int i = t - 2; i >= 0; --i) {
-            const int j = i + 1 + (tid >> 2);
-            if (j < t) {
-                const T *urow = S + i * lp;
-                const T *wcol = S + j * lp;  // W column j (rows p < j), kept in the strict lower part of S
-                T part = T(0);
-                for (int p = i + 1 + sub; p <= j; p += 4) part = fma(urow[p], (p == j) ? s_inv[j] : wcol[p], part);
-                part += __shfl_xor_sync(quad, part, 1);
-                part += __shfl_xor_sync(quad, part, 2);
-                if (sub == 0) S[j * lp + i] = -part * s_inv[i];
-            }
-            __syncthreads();
+    if (tid < t) {
+        const int c = tid, b0 = c & ~31;
+        for (int i = c - 1; i >= b0; --i) {
+            T part = T(0);
+            for (int p = i + 1; p <= c; ++p) part = fma(S[i * lp + p], (p == c) ? s_inv[c] : S[c * lp + p], part);
+            S[c * lp + i] = -part * s_inv[i];
         }
+    }
+    __syncthreads();
+    T *Tm = s_inv + t;  // (t / 2h) blocks of h x h: U[A, C] W[C, C]
+    for (int hh = 32; hh < t; hh *= 2) {
+        const int nel = (t / (2 * hh)) * hh * hh;
+        for (int e = tid; e < nel; e += PO_NT) {
+            const int blk = e / (hh * hh), rc = e - blk * hh * hh, r = rc / hh, c = rc - r * hh;
+            const int a0 = blk * 2 * hh, c0 = a0 + hh;
+            T acc = T(0);
+            for (int p = 0; p <= c; ++p)
+                acc = fma(S[(a0 + r) * lp + c0 + p], (p == c) ? s_inv[c0 + c] : S[(c0 + c) * lp + c0 + p], acc);
+            Tm[e] = acc;
+        }
+        __syncthreads();
+        for (int e = tid; e < nel; e += PO_NT) {
+            const int blk = e / (hh * hh), rc = e - blk * hh * hh, r = rc / hh, c = rc - r * hh;
+            const int a0 = blk * 2 * hh, c0 = a0 + hh;
+            const T *tcol = Tm + blk * hh * hh + c;
+            T acc = T(0);
+            for (int q = r; q < hh; ++q) acc = fma((q == r) ? s_inv[a0 + r] : S[(a0 + q) * lp + a0 + r], tcol[q * hh], acc);
+            S[(c0 + c) * lp + a0 + r] = -acc;
+        }
+        __syncthreads();
     }
     // Wneg = -W^T: row i holds -w_pi for p <= i
     for (int e = tid; e < t * t; e += PO_NT) {
@@ -193,8 +215,10 @@ void potrf_rowmajor(oxi_handle_s *h, T *U, i64 ld, i64 n, int64_t *d_info, T *wo
         const int t = (int)std::min<i64>(PO_NB, n - k0);
         T *Ukk = U + k0 * ld + k0;
         {
-            const size_t smem = sizeof(T) * ((size_t)t * (t + 1) + t);
-            set_max_dyn_smem((const void *)k_potrf_diag<T>, (int)(sizeof(T) * (PO_NB * (PO_NB + 1) + PO_NB)));
+            // the block, 1 / u_ii, and the inverse's product scratch (h x h at the top level)
+            const size_t smem = sizeof(T) * ((size_t)t * (t + 1) + t + (size_t)(PO_NB / 2) * (PO_NB / 2));
+            set_max_dyn_smem((const void *)k_potrf_diag<T>,
+                             (int)(sizeof(T) * (PO_NB * (PO_NB + 1) + PO_NB + (PO_NB / 2) * (PO_NB / 2))));
             ProfScope ps(KC_LEAF, s, (double)t * t * t * (2.0 / 3.0), 2.0 * sizeof(T) * t * t);
             k_potrf_diag<T><<<1, PO_NT, smem, s>>>(Ukk, ld, t, k0, d_info, Wneg);
             OXI_LAUNCH_CHECK();

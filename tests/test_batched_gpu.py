@@ -147,3 +147,26 @@ def test_autotune_keeps_a_valid_tuning(pkg, oracle):
     _check_factors(P, mats, oracle, "tuned")
     ns32, nb32, ms32 = pkg.batched_autotune(orders, "fp32", nrhs=2)
     assert ms32 > 0 and all(v in (8, 16, 32) for v in nb32)
+
+
+@pytest.mark.parametrize("n_smem", [64, 0])
+def test_getrf_batched_nan_pivot_rule(pkg, oracle, n_smem):
+    """_lu_pivot starts from row j with strict '>' (src/lapack/factorizations.jl:
+    92-107): a NaN at row j keeps row j although finite rows lie below, and a
+    NaN below never wins.  Pivots must equal the oracle's (which restates it)."""
+    rng = np.random.default_rng(33)
+    A = rng.standard_normal((40, 40))
+    A[3, 3] = np.nan          # column 3: row 3 kept
+    B = rng.standard_normal((24, 24))
+    B[10, 0] = np.nan         # column 0: a NaN below the diagonal never wins
+    pkg.batched_set_tuning("fp64", n_smem, [16] * 8)
+    try:
+        P = pkg.BatchedLU([40, 24])
+        P.load([A, B])
+        P.getrf()
+        for i, M in enumerate((A, B)):
+            Fo, ipo, _ = oracle.getrf(M, check=False)
+            assert np.array_equal(_np(P.ipiv(i)), ipo), i
+        assert _np(P.ipiv(0))[3] == 4
+    finally:
+        pkg.batched_set_tuning("fp64", 64, [8, 8, 16, 16, 16, 16, 16, 16])

@@ -246,3 +246,21 @@ def test_many_rhs_solves_every_chunk_width(pkg, dtype):
             assert np.abs(X[:, j] - xj).max() <= same * np.abs(xj).max(), (dtype, j)
         bw = np.linalg.norm(M @ X - B64) / (np.linalg.norm(M) * np.linalg.norm(X))
         assert bw <= 30 * n * eps, (dtype, bw)
+
+
+@pytest.mark.parametrize("m,n", [(300, 300), (9000, 64)])
+def test_nan_pivot_rule_matches_oracle(pkg, oracle, m, n):
+    """_lu_pivot (src/lapack/factorizations.jl:92-107) starts from row j with a
+    strict '>': a NaN at row j keeps row j although larger finite rows lie
+    below; a NaN below the diagonal never wins.  The GPU leaf follows it, so
+    the pivots (and the bits) equal the oracle's."""
+    rng = np.random.default_rng(m + n)
+    A = rng.standard_normal((m, n))
+    A[5, 5] = np.nan          # column 5: row 5 kept
+    A[40, 2] = np.nan         # column 2: never the pivot
+    F = pkg.lu(A, check=False)
+    Fo, ipo, _ = oracle.getrf(A, check=False)
+    ipiv = _np(F.ipiv)
+    assert ipiv[5] == 6
+    assert np.array_equal(ipiv, ipo)
+    assert np.array_equal(_np(F.factors), Fo, equal_nan=True)
