@@ -101,6 +101,8 @@ __device__ __forceinline__ void argmax_combine(double &v, int &i, double v2, int
 }
 
 struct Misc {
+    double red_v[2][bt::NW];
+    int red_i[2][bt::NW];
     double red_m[bt::NW][bt::MAXRHS];
     int piv[bt::NMAX];   // pivot row (0-based, within the matrix) of each column
     int rowat[bt::NMAX]; // a panel's net permutation: position p holds row rowat[p]
@@ -111,61 +113,76 @@ struct Misc {
     int item, info, bad;
 };
 
-// Unblocked LU of the panel P (m x jb, column-major, ldp) holding columns
-// k..k+jb of rows k..n; records S.piv[k + j] and the first zero pivot.  Warp 0
-// alone works through the columns, the other warps wait at the closing
-// barrier: each column costs warp shuffles and __syncwarp, not CTA barriers.
-// Pivot rule of _lu_pivot (src/lapack/factorizations.jl:92-107) exactly: start
-// from row j, strict '>' over the rows below (the first maximum wins; a NaN at
-// row j keeps row j; a NaN below never wins).  Same arithmetic per element as
-// panel_lu: l = a_ij / d, then a_ic = fma(-l, a_jc, a_ic).
+// Row of the largest |col[i]|, i in [j0, m), first index on ties (all threads);
+// INT_MAX when no row compares (none, or all NaN).
 template <typename T>
-__device__ void panel_lu_warp(T *P, int ldp, int m, int jb, int k, Misc &S) {
-    if (threadIdx.x < 32) {
-        const int lane = threadIdx.x;
-        for (int j = 0; j < jb; ++j) {
-            T *colj = P + (i64)j * ldp;
-            double bv = -1.0;
-            int bi = INT_MAX;
-            for (int i = j + 1 + lane; i < m; i += 32) {
-                const double v = fabs((double)colj[i]);
-                if (v > bv) {  // rows ascend per lane: its first maximum
-                    bv = v;
-                    bi = i;
-                }
-            }
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) {
-                const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
-                const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
-                argmax_combine(bv, bi, ov, oi);
-            }
-            const double v0 = fabs((double)colj[j]);
-            const int p = (bi != INT_MAX && bv > v0) ? bi : j;
-            const T d = colj[p];
-            if (lane == 0) S.piv[k + j] = k + p;
-            if (d == T(0)) {  // zero column: info, no interchange, no elimination
-                if (lane == 0 && S.info == 0) S.info = k + j + 1;
-                __syncwarp();
-                continue;
-            }
-            if (p != j) {
-                for (int c = lane; c < jb; c += 32) {
-                    const T t = P[j + (i64)c * ldp];
-                    P[j + (i64)c * ldp] = P[p + (i64)c * ldp];
-                    P[p + (i64)c * ldp] = t;
-                }
-            }
-            __syncwarp();
-            for (int i = j + 1 + lane; i < m; i += 32) {
-                const T l = P[i + (i64)j * ldp] / d;
-                P[i + (i64)j * ldp] = l;
-                for (int c = j + 1; c < jb; ++c) P[i + (i64)c * ldp] = fma(-l, P[j + (i64)c * ldp], P[i + (i64)c * ldp]);
-            }
-            __syncwarp();
+__device__ int block_argmax(const T *col, int j0, int m, Misc &S, int par, double &best) {
+    using namespace bt;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double bv = -1.0;
+    int bi = INT_MAX;
+    for (int i = j0 + threadIdx.x; i < m; i += NT) {
+        const double v = fabs((double)col[i]);
+        if (v > bv) {
+            bv = v;
+            bi = i;
         }
     }
-    __syncthreads();  // S.piv / S.info and the panel are visible to all
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+        argmax_combine(bv, bi, ov, oi);
+    }
+    if (lane == 0) {
+        S.red_v[par][warp] = bv;
+        S.red_i[par][warp] = bi;
+    }
+    __syncthreads();
+    bv = S.red_v[par][0];
+    bi = S.red_i[par][0];
+#pragma unroll
+    for (int w = 1; w < NW; ++w) argmax_combine(bv, bi, S.red_v[par][w], S.red_i[par][w]);
+    best = bv;
+    return bi;
+}
+
+// Unblocked LU of the panel P (m x jb, column-major, ldp) holding columns
+// k..k+jb of rows k..n; records S.piv[k + j] and the first zero pivot.
+template <typename T>
+__device__ void panel_lu(T *P, int ldp, int m, int jb, int k, Misc &S) {
+    using namespace bt;
+    for (int j = 0; j < jb; ++j) {
+        T *colj = P + (i64)j * ldp;
+        // _lu_pivot (src/lapack/factorizations.jl:92-107): start from row j with
+        // strict '>' -- the first maximum; a NaN at row j keeps row j, a NaN
+        // below never wins
+        double bv;
+        const int pb = block_argmax(colj, j + 1, m, S, j & 1, bv);
+        const double v0 = fabs((double)colj[j]);
+        const int p = (pb != INT_MAX && bv > v0) ? pb : j;
+        const T d = colj[p];
+        if (threadIdx.x == 0) S.piv[k + j] = k + p;
+        if (d == T(0)) {  // zero column: info, no interchange, no elimination
+            if (threadIdx.x == 0 && S.info == 0) S.info = k + j + 1;
+            continue;
+        }
+        if (p != j) {
+            for (int c = threadIdx.x; c < jb; c += NT) {
+                const T t = P[j + (i64)c * ldp];
+                P[j + (i64)c * ldp] = P[p + (i64)c * ldp];
+                P[p + (i64)c * ldp] = t;
+            }
+        }
+        __syncthreads();
+        for (int i = j + 1 + threadIdx.x; i < m; i += NT) {
+            const T l = P[i + (i64)j * ldp] / d;
+            P[i + (i64)j * ldp] = l;
+            for (int c = j + 1; c < jb; ++c) P[i + (i64)c * ldp] = fma(-l, P[j + (i64)c * ldp], P[i + (i64)c * ldp]);
+        }
+        __syncthreads();
+    }
+    __syncthreads();  // S.piv / S.info of a final zero column are visible to all
 }
 
 // Right-looking blocked LU of W (n x n, column-major, ldw; shared or global).
@@ -187,7 +204,7 @@ __device__ void lu_blocked(T *W, int ldw, int n, int nb, bool in_smem, T *sP, T 
                 for (int r = (int)(threadIdx.x & 31); r < m; r += 32) sP[r + c * ldp] = W[(k + r) + (i64)(k + c) * ldw];
             __syncthreads();
         }
-        panel_lu_warp(P, ldp, m, jb, k, S);
+        panel_lu(P, ldp, m, jb, k, S);
         if (!in_smem) {
             for (int c = (int)(threadIdx.x >> 5); c < jb; c += NW)
                 for (int r = (int)(threadIdx.x & 31); r < m; r += 32) W[(k + r) + (i64)(k + c) * ldw] = sP[r + c * ldp];

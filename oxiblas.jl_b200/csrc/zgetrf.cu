@@ -16,6 +16,7 @@
 // run in one CTA each (16 columns, every row of the panel), their interchanges
 // are then applied to the other columns (laswp), and the U block row is solved
 // by a unit-lower substitution kernel.
+#include <cooperative_groups.h>
 #include <algorithm>
 #include <climits>
 #include <cmath>
@@ -161,6 +162,141 @@ __global__ void __launch_bounds__(ZLEAF_NT) k_zleaf(double *__restrict__ Wr, dou
             }
         }
         __syncthreads();
+    }
+}
+
+// The same leaf on a cluster of CS CTAs (1..16) that hold the panel's rows in
+// shared memory (CTA r: rows [r RP, (r + 1) RP), both planes, 16 columns), so a
+// column step reads no global memory: each CTA's candidate (the largest abs2
+// and, for the overflow rule, the largest abs, of its rows below j, first index
+// on ties), one cluster barrier, every CTA picks the same pivot from the CS
+// candidates and |a_jj| (row j lives in CTA 0: j < 16 <= RP), reads the pivot
+// row and row j through distributed shared memory, a second barrier, the two
+// owners write the interchanged rows, then each CTA eliminates its own rows.
+// Cluster barriers are hardware barriers every CTA meets the same number of
+// times; there is no spin wait.
+namespace cgz = cooperative_groups;
+constexpr int ZCL_NT = 512;
+constexpr int ZCL_MAXRP = 768;  // rows per CTA (192 KB of shared memory)
+struct ZCand {
+    double k2, kh;  // largest abs2 / abs among the CTA's rows below j (-1: none)
+    int p2, ph;     // their rows (INT_MAX: none)
+};
+__device__ __forceinline__ void zcand_combine(double &k, int &p, double k2, int p2) {
+    if (k2 > k || (k2 == k && p2 < p)) { k = k2; p = p2; }
+}
+__global__ void __launch_bounds__(ZCL_NT, 1) k_zleaf_cl(double *__restrict__ Wr, double *__restrict__ Wi, i64 ld, int m,
+                                                         int w, int RP, i64 gofs, int64_t *__restrict__ ipiv,
+                                                         int64_t *__restrict__ info) {
+    cgz::cluster_group cl = cgz::this_cluster();
+    const int CS = (int)cl.num_blocks(), cr = (int)cl.block_rank();
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    extern __shared__ double2 zcl[];  // [RP][ZLEAF] complex
+    __shared__ ZCand s_cand[2];
+    __shared__ double s_rk[ZCL_NT / 32][2];
+    __shared__ int s_rp[ZCL_NT / 32][2];
+    __shared__ zd s_prow[ZLEAF], s_jrow[ZLEAF];
+    __shared__ int s_piv[ZLEAF], s_info;
+    const int r0 = cr * RP;
+    const int nr = max(0, min(m - r0, RP));
+    if (tid == 0) s_info = 0;
+    for (int e = tid; e < nr * ZLEAF; e += ZCL_NT) {
+        const int li = e / ZLEAF, c = e - li * ZLEAF;
+        const i64 g = (i64)(r0 + li) * ld + c;
+        zcl[e] = (c < w) ? make_double2(Wr[g], Wi[g]) : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    const int q = m < w ? m : w;
+    for (int j = 0; j < q; ++j) {
+        const int par = j & 1;
+        // (1) this CTA's candidates among its rows below j
+        double k2 = -1.0, kh = -1.0;
+        int p2 = INT_MAX, ph = INT_MAX;
+        for (int li = max(0, j + 1 - r0) + tid; li < nr; li += ZCL_NT) {
+            const double2 a = zcl[li * ZLEAF + j];
+            const double v2 = a.x * a.x + a.y * a.y, vh = hypot(a.x, a.y);
+            if (v2 == v2 && v2 > k2) { k2 = v2; p2 = r0 + li; }  // rows ascend per thread: first maximum
+            if (vh == vh && vh > kh) { kh = vh; ph = r0 + li; }
+        }
+        for (int off = 16; off > 0; off >>= 1) {
+            zcand_combine(k2, p2, __shfl_xor_sync(0xffffffffu, k2, off), __shfl_xor_sync(0xffffffffu, p2, off));
+            zcand_combine(kh, ph, __shfl_xor_sync(0xffffffffu, kh, off), __shfl_xor_sync(0xffffffffu, ph, off));
+        }
+        if (lane == 0) { s_rk[warp][0] = k2; s_rp[warp][0] = p2; s_rk[warp][1] = kh; s_rp[warp][1] = ph; }
+        __syncthreads();
+        if (tid == 0) {
+            for (int wv = 1; wv < ZCL_NT / 32; ++wv) {
+                zcand_combine(k2, p2, s_rk[wv][0], s_rp[wv][0]);
+                zcand_combine(kh, ph, s_rk[wv][1], s_rp[wv][1]);
+            }
+            s_cand[par] = ZCand{k2, kh, p2, ph};
+        }
+        cl.sync();  // (2) every CTA's candidate is published
+        // (3) the pivot, identical in every CTA: _lu_pivot's abs2 scan from row j
+        // with strict '>', redone with abs when that square is not finite
+        double b2 = -1.0, bh = -1.0;
+        int q2 = INT_MAX, qh = INT_MAX;
+        for (int rr = 0; rr < CS; ++rr) {
+            const ZCand cd = *cl.map_shared_rank(&s_cand[par], rr);
+            zcand_combine(b2, q2, cd.k2, cd.p2);
+            zcand_combine(bh, qh, cd.kh, cd.ph);
+        }
+        const double2 ajj = *cl.map_shared_rank(&zcl[j * ZLEAF + j], 0);
+        const double v2 = ajj.x * ajj.x + ajj.y * ajj.y;
+        int p = j;
+        double best = v2;
+        if (q2 != INT_MAX && b2 > v2) { best = b2; p = q2; }
+        if (!(best < INFINITY)) {  // NaN start or an overflowing square: the abs scan
+            const double vh = hypot(ajj.x, ajj.y);
+            p = (qh != INT_MAX && bh > vh) ? qh : j;
+        }
+        // (4) the pivot row and row j through distributed shared memory
+        const int cp = p / RP;
+        if (tid < ZLEAF) {
+            const double2 pv = *cl.map_shared_rank(&zcl[(p - cp * RP) * ZLEAF + tid], cp);
+            s_prow[tid] = {pv.x, pv.y};
+            const double2 jv = *cl.map_shared_rank(&zcl[j * ZLEAF + tid], 0);
+            s_jrow[tid] = {jv.x, jv.y};
+        }
+        if (cr == 0 && tid == 0) s_piv[j] = p;
+        cl.sync();  // (5) every CTA has read both rows before they are rewritten
+        if (p != j && tid < ZLEAF) {
+            if (cr == 0) zcl[j * ZLEAF + tid] = make_double2(s_prow[tid].r, s_prow[tid].i);
+            if (cr == cp) zcl[(p - r0) * ZLEAF + tid] = make_double2(s_jrow[tid].r, s_jrow[tid].i);
+        }
+        __syncthreads();
+        // (6) elimination of this CTA's rows below j
+        const zd d = s_prow[j];
+        if (d.r == 0.0 && d.i == 0.0) {
+            if (cr == 0 && tid == 0 && s_info == 0) s_info = j + 1;
+            continue;
+        }
+        const zd dinv = zrecip(d);
+        for (int li = max(0, j + 1 - r0) + tid; li < nr; li += ZCL_NT) {
+            double2 *row = zcl + li * ZLEAF;
+            const double2 a = row[j];
+            const zd l = zmul({a.x, a.y}, dinv);
+            row[j] = make_double2(l.r, l.i);
+            for (int c = j + 1; c < w; ++c) {
+                const double2 b = row[c];
+                const zd v = zmsub({b.x, b.y}, l, s_prow[c]);
+                row[c] = make_double2(v.r, v.i);
+            }
+        }
+        __syncthreads();
+    }
+    cl.sync();  // no CTA leaves while another may still read its rows
+    for (int e = tid; e < nr * ZLEAF; e += ZCL_NT) {
+        const int li = e / ZLEAF, c = e - li * ZLEAF;
+        if (c < w) {
+            const i64 g = (i64)(r0 + li) * ld + c;
+            Wr[g] = zcl[e].x;
+            Wi[g] = zcl[e].y;
+        }
+    }
+    if (cr == 0) {
+        if (tid < q) ipiv[gofs + tid] = gofs + s_piv[tid] + 1;
+        if (tid == 0 && s_info != 0 && *info == 0) *info = gofs + s_info;
     }
 }
 
@@ -362,8 +498,32 @@ static void zpanel(ZRun &R, i64 c0, i64 nc) {
     const i64 mrows = R.m - c0;
     if (mrows <= 0 || nc <= 0) return;
     if (nc <= ZLEAF) {
-        k_zleaf<<<1, ZLEAF_NT, 0, R.h->stream>>>(R.Wr + c0 * R.ld + c0, R.Wi + c0 * R.ld + c0, R.ld, (int)mrows,
-                                                 (int)nc, c0, R.ipiv, R.info);
+        if (mrows <= (i64)ZCL_MAXRP * 16) {
+            // rows over a cluster of up to 16 CTAs, in shared memory
+            int cs = (int)std::min<i64>(16, std::max<i64>(1, (mrows + 511) / 512));
+            int rp = (int)((mrows + cs - 1) / cs);
+            while (rp > ZCL_MAXRP) rp = (int)((mrows + (++cs) - 1) / cs);
+            const size_t smem = sizeof(double2) * (size_t)rp * ZLEAF;
+            set_max_dyn_smem((const void *)k_zleaf_cl, (int)(sizeof(double2) * ZCL_MAXRP * ZLEAF));
+            if (cs > 8) OXI_CUDA(cudaFuncSetAttribute(k_zleaf_cl, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(cs);
+            cfg.blockDim = dim3(ZCL_NT);
+            cfg.dynamicSmemBytes = smem;
+            cfg.stream = R.h->stream;
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = cs;
+            at[0].val.clusterDim.y = 1;
+            at[0].val.clusterDim.z = 1;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            OXI_CUDA(cudaLaunchKernelEx(&cfg, k_zleaf_cl, R.Wr + c0 * R.ld + c0, R.Wi + c0 * R.ld + c0, R.ld,
+                                        (int)mrows, (int)nc, rp, c0, R.ipiv, R.info));
+        } else {
+            k_zleaf<<<1, ZLEAF_NT, 0, R.h->stream>>>(R.Wr + c0 * R.ld + c0, R.Wi + c0 * R.ld + c0, R.ld, (int)mrows,
+                                                     (int)nc, c0, R.ipiv, R.info);
+        }
         OXI_LAUNCH_CHECK();
         const int cnt = (int)std::min<i64>(nc, mrows);
         zlaswp(R, c0, cnt, 0, R.n, c0, c0 + nc);

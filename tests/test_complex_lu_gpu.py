@@ -113,7 +113,7 @@ def test_lu_inplace_on_views_complex(pkg, n):
 
 @pytest.mark.parametrize("m,n,bs", [(64, 64, 128), (300, 300, 128), (1000, 1000, 128), (2048, 2048, 128),
                                     (500, 300, 128), (300, 500, 128), (777, 777, 100), (1500, 1500, 64),
-                                    (900, 900, 256)])
+                                    (900, 900, 256), (9000, 64, 128), (13000, 48, 128)])
 def test_complex_pivots_and_factors_vs_oracle(pkg, oracle, m, n, bs):
     rng = np.random.default_rng(m * 7 + n + bs)
     A = _crandn(rng, m, n)
