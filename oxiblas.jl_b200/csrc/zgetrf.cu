@@ -610,20 +610,33 @@ constexpr int ZCOLS_NT = 512;
 constexpr int ZCOLS_MAXN = 12288;
 __global__ void __launch_bounds__(ZCOLS_NT) k_ztrsv_cols(const double2 *__restrict__ LU, i64 lda,
                                                          double2 *__restrict__ X, i64 ldx, int n, int lower) {
+    // a step's column entries for this thread are loaded together into
+    // registers before any is used: one global latency per step, not one per row
+    constexpr int PER = ZCOLS_MAXN / ZCOLS_NT;
     extern __shared__ double2 zx[];
     double2 *x = X + (i64)blockIdx.x * ldx;
     const int tid = threadIdx.x;
     for (int i = tid; i < n; i += ZCOLS_NT) zx[i] = x[i];
     __syncthreads();
+    double2 cv[PER];
     if (lower) {
         for (int j = 0; j < n - 1; ++j) {
+            const double2 *col = LU + (i64)j * lda;
+#pragma unroll
+            for (int q = 0; q < PER; ++q) {
+                const int i = j + 1 + tid + q * ZCOLS_NT;
+                if (i < n) cv[q] = col[i];
+            }
             const double2 xv = zx[j];
             const zd xj = {xv.x, xv.y};
-            const double2 *col = LU + (i64)j * lda;
-            for (int i = j + 1 + tid; i < n; i += ZCOLS_NT) {
-                const double2 l = col[i], b = zx[i];
-                const zd v = zmsub({b.x, b.y}, {l.x, l.y}, xj);
-                zx[i] = make_double2(v.r, v.i);
+#pragma unroll
+            for (int q = 0; q < PER; ++q) {
+                const int i = j + 1 + tid + q * ZCOLS_NT;
+                if (i < n) {
+                    const double2 b = zx[i];
+                    const zd v = zmsub({b.x, b.y}, {cv[q].x, cv[q].y}, xj);
+                    zx[i] = make_double2(v.r, v.i);
+                }
             }
             __syncthreads();
         }
@@ -632,13 +645,22 @@ __global__ void __launch_bounds__(ZCOLS_NT) k_ztrsv_cols(const double2 *__restri
         // zx[j] is not written in step j (every thread divides it for itself),
         // and not read after it: the solution goes straight to x[j]
         for (int j = n - 1; j >= 0; --j) {
-            const double2 xv = zx[j], d = LU[j + (i64)j * lda];
-            const zd xj = zdivd({xv.x, xv.y}, {d.x, d.y});
             const double2 *col = LU + (i64)j * lda;
-            for (int i = tid; i < j; i += ZCOLS_NT) {
-                const double2 u = col[i], b = zx[i];
-                const zd v = zmsub({b.x, b.y}, {u.x, u.y}, xj);
-                zx[i] = make_double2(v.r, v.i);
+#pragma unroll
+            for (int q = 0; q < PER; ++q) {
+                const int i = tid + q * ZCOLS_NT;
+                if (i < j) cv[q] = col[i];
+            }
+            const double2 xv = zx[j], d = col[j];
+            const zd xj = zdivd({xv.x, xv.y}, {d.x, d.y});
+#pragma unroll
+            for (int q = 0; q < PER; ++q) {
+                const int i = tid + q * ZCOLS_NT;
+                if (i < j) {
+                    const double2 b = zx[i];
+                    const zd v = zmsub({b.x, b.y}, {cv[q].x, cv[q].y}, xj);
+                    zx[i] = make_double2(v.r, v.i);
+                }
             }
             if (tid == 0) x[j] = make_double2(xj.r, xj.i);
             __syncthreads();
