@@ -309,31 +309,6 @@ __device__ void lu_blocked(T *W, int ldw, int n, int nb, bool in_smem, T *sP, T 
                 for (int u = 0; u < 4; ++u)
 #pragma unroll
                     for (int v = 0; v < 4; ++v) acc[u][v] = T(0);
-                if (r0 + 3 < m2 && cc0 + 3 < m2) {
-                    // a whole tile: no predicates, the operands by pointer steps
-                    // (the same fma order: kk ascending from zero, then C - acc)
-                    const T *ap = Ap + r0;
-                    const T *bp = Bp + (i64)cc0 * bsc;
-                    const int b1 = bsc, b2 = 2 * bsc, b3 = 3 * bsc;
-#pragma unroll 4
-                    for (int kk = 0; kk < jb; ++kk) {
-                        const T a0 = ap[0], a1 = ap[1], a2 = ap[2], a3 = ap[3];
-                        const T bv0 = bp[0], bv1 = bp[b1], bv2 = bp[b2], bv3 = bp[b3];
-                        ap += ldp;
-                        bp += bsk;
-                        const T a[4] = {a0, a1, a2, a3}, b[4] = {bv0, bv1, bv2, bv3};
-#pragma unroll
-                        for (int u = 0; u < 4; ++u)
-#pragma unroll
-                            for (int v = 0; v < 4; ++v) acc[u][v] = fma(a[u], b[v], acc[u][v]);
-                    }
-                    T *cp = Cp + r0 + (i64)cc0 * ldw;
-#pragma unroll
-                    for (int v = 0; v < 4; ++v)
-#pragma unroll
-                        for (int u = 0; u < 4; ++u) cp[u + (i64)v * ldw] -= acc[u][v];
-                    continue;
-                }
                 for (int kk = 0; kk < jb; ++kk) {
                     T a[4], b[4];
 #pragma unroll

@@ -36,8 +36,14 @@ void gemm_minus(oxi_handle_s *h, T *C, i64 ldc, const T *A, i64 lda, const T *B,
                 i64 N, i64 K) {
     if (M <= 0 || N <= 0 || K <= 0) return;
     if (h->opt.gemm == 0) {
-        if constexpr (sizeof(T) == 8) launch_gemm_dmma(C, ldc, A, lda, B, ldb, M, N, K, h->stream);
-        else launch_gemm_simt<T>(C, ldc, A, lda, B, ldb, M, N, K, h->stream);
+        if constexpr (sizeof(T) == 8) {
+            // the lookahead's trailing update on whole GPCs, beside the next panel
+            if (h->gemm_ctas < 0 && launch_gemm_dmma_gpc(C, ldc, A, lda, B, ldb, M, N, K, h->stream, -h->gemm_ctas))
+                return;
+            launch_gemm_dmma(C, ldc, A, lda, B, ldb, M, N, K, h->stream);
+        } else {
+            launch_gemm_simt<T>(C, ldc, A, lda, B, ldb, M, N, K, h->stream);
+        }
         return;
     }
     launch_gemm_ref<T>(C, ldc, A, lda, B, ldb, M, N, K, h->stream);
@@ -270,13 +276,14 @@ void getrf_rowmajor(oxi_handle_s *h, T *W, i64 ld, i64 m, i64 n, int64_t *d_ipiv
     // trailing update runs on a second stream, concurrently with the next panel's
     // factorization, which touches only its own columns.  Its row moves and U12
     // solve, which do touch the other columns, wait for that update.
-    // Applied where the trailing update is the persistent tensor-core GEMM, whose
-    // CTA count can leave SMs to the panel; the FP64 DMMA update fills every SM
-    // and delays the panel's cluster instead (measured: no gain), so FP64 runs
-    // the plain schedule.
-    bool la = h->opt.lookahead && compose;
-    if constexpr (sizeof(T) == 8) la = false;
-    else if (h->trailing == TRAIL_NATIVE) la = false;
+    // Applied where the trailing update is a persistent tensor-core GEMM whose
+    // clusters fill whole GPCs and leave one to the panel: tcgen05 for the mixed
+    // solve's 16-bit factor, the GPC-shaped DMMA kernel for FP64 (the reference
+    // summation-order mode and the FP32 CUDA-core update run the plain schedule).
+    bool la = h->opt.lookahead && compose && h->opt.gemm == 0;
+    if constexpr (sizeof(T) == 4) {
+        if (h->trailing == TRAIL_NATIVE) la = false;
+    }
     // With lookahead the panels run on a stream of the highest priority and the
     // trailing update on one of the lowest: when SMs free up, the block scheduler
     // serves the panel's kernels (the leaf's 16-CTA cluster needs 16 SMs of one
@@ -359,11 +366,17 @@ void getrf_rowmajor(oxi_handle_s *h, T *W, i64 ld, i64 m, i64 n, int64_t *d_ipiv
             // 0.6 ms measured at n = 16384; ~17 ns per tile per K column on one
             // SM), the rest left to the next panel: early updates take all but
             // one GPC, late ones one or two.
-            {
+            if constexpr (sizeof(T) == 4) {
                 const double tiles = (double)((m - l + 127) / 128) * (double)((n - l2 + 255) / 256);
                 const double kq = (h->trailing == TRAIL_FP16X3 || h->trailing == TRAIL_BF16X3) ? 3.0 : 1.0;
                 const double us = tiles * kq * (double)(l - f) * 0.017 / GEMM_GPC_CLUSTER;
                 h->gemm_ctas = -std::max(2, (int)std::ceil(us / 600.0));
+            } else {
+                // DMMA: about 0.16 us per 256 x 64 tile per K column on one SM (30 TF/s
+                // over 148 SMs); enough GPCs to finish in about one FP64 panel (0.5 ms)
+                const double tiles = (double)((m - l + 255) / 256) * (double)((n - l2 + 63) / 64);
+                const double us = tiles * (double)(l - f) * 0.164 / GEMM_GPC_CLUSTER;
+                h->gemm_ctas = -std::max(2, (int)std::ceil(us / 500.0));
             }
             launch_rowmoves_big<T>(W, ld, f, list, listcnt, maxcnt, 0, f, h->stream);
             launch_rowmoves_big<T>(W, ld, f, list, listcnt, maxcnt, l2, R.ncols_moved, h->stream);

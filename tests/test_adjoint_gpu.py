@@ -163,7 +163,9 @@ def test_batched_adjoint_1024_problems(pkg, oracle):
         bb, Ab = _np(P.Bbar(i))[:, 0], _np(P.Abar(i))
         worst = max(worst, np.linalg.norm(bb - bo) / np.linalg.norm(bo),
                     np.linalg.norm(Ab - Ao) / np.linalg.norm(Ao))
-    assert worst <= 1e-12, worst
+    # the two pullbacks associate the transposed solve's sums differently: they
+    # agree to about kappa * n * eps (1e3 * 128 * 1.1e-16 = 1.4e-11)
+    assert worst <= 1e-11, worst
     h = 1e-6
     for i in rng.choice(len(orders), 8, replace=False):
         A, b = mats[i], rhs[i]
