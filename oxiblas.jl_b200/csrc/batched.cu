@@ -93,15 +93,9 @@ static int batch_smem_layout(int esize, int mode, int n_smem, int nbmax, BatchDe
 
 namespace {
 
-__device__ __forceinline__ void argmax_combine(double &v, int &i, double v2, int i2) {
-    if (v2 > v || (v2 == v && i2 < i)) {
-        v = v2;
-        i = i2;
-    }
-}
 
 struct Misc {
-    double red_v[2][bt::NW];
+    double red_v[2][bt::NW], red_x[2][bt::NW];
     int red_i[2][bt::NW];
     double red_m[bt::NW][bt::MAXRHS];
     int piv[bt::NMAX];   // pivot row (0-based, within the matrix) of each column
@@ -113,37 +107,58 @@ struct Misc {
     int item, info, bad;
 };
 
-// Row of the largest |col[i]|, i in [j0, m), first index on ties (all threads);
-// INT_MAX when no row compares (none, or all NaN).
+// The pivot candidates of column j (all threads): the row of the largest
+// |col[i]|, i in (j, m), first index on ties (INT_MAX when none compares), its
+// value, and col[j] -- every value read before the barrier, so no thread can
+// see a row the interchange that follows has already moved.
 template <typename T>
-__device__ int block_argmax(const T *col, int j0, int m, Misc &S, int par, double &best) {
+__device__ int block_argmax(const T *col, int j, int m, Misc &S, int par, double &best, double &val,
+                            double &vj) {
     using namespace bt;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double bv = -1.0;
+    vj = (double)col[j];
+    double bv = -1.0, bx = 0.0;
     int bi = INT_MAX;
-    for (int i = j0 + threadIdx.x; i < m; i += NT) {
-        const double v = fabs((double)col[i]);
+    for (int i = j + 1 + threadIdx.x; i < m; i += NT) {
+        const double x = (double)col[i], v = fabs(x);
         if (v > bv) {
             bv = v;
             bi = i;
+            bx = x;
         }
     }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
         const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
+        const double ox = __shfl_xor_sync(0xffffffffu, bx, off);
         const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
-        argmax_combine(bv, bi, ov, oi);
+        if (ov > bv || (ov == bv && oi < bi)) {
+            bv = ov;
+            bi = oi;
+            bx = ox;
+        }
     }
     if (lane == 0) {
         S.red_v[par][warp] = bv;
         S.red_i[par][warp] = bi;
+        S.red_x[par][warp] = bx;
     }
     __syncthreads();
     bv = S.red_v[par][0];
     bi = S.red_i[par][0];
+    bx = S.red_x[par][0];
 #pragma unroll
-    for (int w = 1; w < NW; ++w) argmax_combine(bv, bi, S.red_v[par][w], S.red_i[par][w]);
+    for (int w = 1; w < NW; ++w) {
+        const double ov = S.red_v[par][w];
+        const int oi = S.red_i[par][w];
+        if (ov > bv || (ov == bv && oi < bi)) {
+            bv = ov;
+            bi = oi;
+            bx = S.red_x[par][w];
+        }
+    }
     best = bv;
+    val = bx;
     return bi;
 }
 
@@ -157,11 +172,11 @@ __device__ void panel_lu(T *P, int ldp, int m, int jb, int k, Misc &S) {
         // _lu_pivot (src/lapack/factorizations.jl:92-107): start from row j with
         // strict '>' -- the first maximum; a NaN at row j keeps row j, a NaN
         // below never wins
-        double bv;
-        const int pb = block_argmax(colj, j + 1, m, S, j & 1, bv);
-        const double v0 = fabs((double)colj[j]);
-        const int p = (pb != INT_MAX && bv > v0) ? pb : j;
-        const T d = colj[p];
+        double bv, bx, vj;
+        const int pb = block_argmax(colj, j, m, S, j & 1, bv, bx, vj);
+        const bool below = pb != INT_MAX && bv > fabs(vj);
+        const int p = below ? pb : j;
+        const T d = (T)(below ? bx : vj);
         if (threadIdx.x == 0) S.piv[k + j] = k + p;
         if (d == T(0)) {  // zero column: info, no interchange, no elimination
             if (threadIdx.x == 0 && S.info == 0) S.info = k + j + 1;
