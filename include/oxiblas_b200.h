@@ -55,10 +55,12 @@ const char *oxi_last_error(oxi_handle_t h);
  *  OXI_OPT_TRSM_LEAF   recursive TRSM leaf size (reference default 8, level3.jl:524)
  *  OXI_OPT_LOOKAHEAD   1 (default) = overlap panel k+1 with the trailing update of
  *                      panel k on a second stream (the reference's threaded
- *                      lookahead, factorizations.jl:41-70).  Applied where the
- *                      trailing update is the persistent tensor-core GEMM (the
- *                      mixed solve's 16-bit factor); the FP64 update fills every
- *                      SM and keeps the plain schedule.  Results are identical. */
+ *                      lookahead, factorizations.jl:41-70): the mixed solve's
+ *                      16-bit update as the persistent tcgen05 GEMM on whole GPCs
+ *                      with one GPC left to the panel, the FP64 update as the
+ *                      DMMA GEMM on a low-priority stream.  The reference-order
+ *                      GEMM mode keeps the plain schedule.  Results are identical
+ *                      bit for bit. */
 enum oxi_option {
     OXI_OPT_BLOCKSIZE = 1,
     OXI_OPT_GEMM = 2,

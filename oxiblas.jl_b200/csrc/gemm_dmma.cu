@@ -187,198 +187,6 @@ k_gemm_dmma(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUt
         }
 }
 
-// ---------------------------------------------------------------------------
-// The same product as a persistent kernel on whole GPCs, for the lookahead of
-// the FP64 factorization: the trailing update runs beside the next panel, which
-// needs one GPC to itself (the leaf's cluster of up to 16 CTAs).  Clusters of
-// 16 CTAs, one CTA per SM (256 x 64 tiles, 16 consumer warps: the per-SM warp
-// count of the two-CTA kernel), at most one cluster fewer than fit; each CTA
-// walks tiles t = blockIdx.x, + gridDim.x, ... with its stage pipeline running
-// on across tiles, so the next tile's loads overlap this tile's epilogue.  Every
-// output element is the same FMA chain as in k_gemm_dmma: the results agree
-// bit for bit.
-namespace {
-constexpr int GBM = 256, GNCW = 16;  // rows per tile, consumer warps (8 x 2)
-constexpr int GA_STAGE = GBM * BK * 8;  // 32 KB
-constexpr int GSTAGE = GA_STAGE + B_STAGE_BYTES;
-constexpr int GNTHREADS = (GNCW + 1) * 32;
-constexpr int GSMEM = STAGES * GSTAGE + 1024 + 256;
-}  // namespace
-
-__global__ void __maxnreg__(112)
-k_gemm_dmma_gpc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                double *__restrict__ C, i64 ldc, int M, int N, int K, int *__restrict__ ab) {
-    extern __shared__ uint8_t smem_raw[];
-    uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~uintptr_t(1023));
-    uint64_t *full = (uint64_t *)(smem + STAGES * GSTAGE);
-    uint64_t *empty = full + STAGES;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int KT = (K + BK - 1) / BK;
-    const int tiles_n = (N + BN - 1) / BN, tiles = ((M + GBM - 1) / GBM) * tiles_n;
-    __shared__ int s_skip;
-    if (threadIdx.x == 0) {
-        for (int st = 0; st < STAGES; ++st) {
-            mbar_init(&full[st], 1);
-            mbar_init(&empty[st], GNCW);
-        }
-        s_skip = aborted(ab) ? 1 : 0;
-        fence_barrier_init();
-    }
-    __syncthreads();
-    if (s_skip) return;
-
-    if (warp == GNCW) {
-        // ---------------- producer: stages of every tile of this CTA in turn ----------------
-        if (lane == 0) {
-            prefetch_tmap(&tmA);
-            prefetch_tmap(&tmB);
-            int g = 0;  // stage uses so far, across tiles
-            for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
-                const int m0 = (t / tiles_n) * GBM, n0 = (t % tiles_n) * BN;
-                for (int kt = 0; kt < KT; ++kt, ++g) {
-                    const int st = g % STAGES;
-                    if (g >= STAGES && !mbar_wait<false>(&empty[st], ((g / STAGES) + 1) & 1, ab, 2)) return;
-                    uint8_t *sa = smem + st * GSTAGE;
-                    uint8_t *sb = sa + GA_STAGE;
-                    mbar_arrive_expect_tx(&full[st], GSTAGE);
-                    tma_load_2d(sa, &tmA, &full[st], kt * BK, m0);
-#pragma unroll
-                    for (int q = 0; q < BN / 8; ++q)
-                        tma_load_2d(sb + q * (BK * 8 * 8), &tmB, &full[st], n0 + 8 * q, kt * BK);
-                }
-            }
-        }
-        return;
-    }
-
-    // ---------------- consumers ----------------
-    const int wm = warp & 7, wn = warp >> 3;  // 8 x 2 warps of 32 x 32
-    const int gid = lane >> 2, tig = lane & 3;
-    const bool vec2 = ((ldc & 1) == 0) && ((((uintptr_t)C) & 15) == 0);
-    int g = 0;
-    for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
-        const int m0 = (t / tiles_n) * GBM, n0 = (t % tiles_n) * BN;
-        double acc[2][4][4];
-#pragma unroll
-        for (int a = 0; a < 2; ++a)
-#pragma unroll
-            for (int b = 0; b < 4; ++b)
-#pragma unroll
-                for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.0;
-        for (int kt = 0; kt < KT; ++kt, ++g) {
-            const int st = g % STAGES;
-            if (!mbar_wait<false>(&full[st], (g / STAGES) & 1, ab, 2)) return;
-            const uint8_t *sa = smem + st * GSTAGE;
-            const uint8_t *sb = sa + GA_STAGE;
-#pragma unroll
-            for (int k4 = 0; k4 < BK / 4; ++k4) {
-                double af[2][2], bf[4];
-                const int kc = k4 * 4 + tig;
-#pragma unroll
-                for (int mt = 0; mt < 2; ++mt) {
-#pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        const int r = wm * 32 + mt * 16 + gid + 8 * h;
-                        const int off = r * 128 + ((((kc * 8) >> 4) ^ (r & 7)) << 4) + ((kc * 8) & 15);
-                        af[mt][h] = *(const double *)(sa + off);
-                    }
-                }
-#pragma unroll
-                for (int nt = 0; nt < 4; ++nt) {
-                    const int q = (wn * 32 + nt * 8) >> 3;
-                    bf[nt] = *(const double *)(sb + q * (BK * 64) + kc * 64 + gid * 8);
-                }
-#pragma unroll
-                for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-                    for (int nt = 0; nt < 4; ++nt)
-                        asm volatile(
-                            "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, "
-                            "{%6}, {%0,%1,%2,%3};"
-                            : "+d"(acc[mt][nt][0]), "+d"(acc[mt][nt][1]), "+d"(acc[mt][nt][2]),
-                              "+d"(acc[mt][nt][3])
-                            : "d"(af[mt][0]), "d"(af[mt][1]), "d"(bf[nt]));
-            }
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&empty[st]);
-        }
-        // epilogue: C -= acc (the producer is already loading the next tile)
-#pragma unroll
-        for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int r = m0 + wm * 32 + mt * 16 + gid + 8 * h;
-                if (r >= M) continue;
-                double *crow = C + (i64)r * ldc;
-                double2 cv[4];
-#pragma unroll
-                for (int nt = 0; nt < 4; ++nt) {
-                    const int c = n0 + wn * 32 + nt * 8 + 2 * tig;
-                    if (c + 1 < N && vec2) cv[nt] = __ldcs((const double2 *)(crow + c));
-                    else {
-                        cv[nt].x = (c < N) ? crow[c] : 0.0;
-                        cv[nt].y = (c + 1 < N) ? crow[c + 1] : 0.0;
-                    }
-                }
-#pragma unroll
-                for (int nt = 0; nt < 4; ++nt) {
-                    const int c = n0 + wn * 32 + nt * 8 + 2 * tig;
-                    double2 v;
-                    v.x = cv[nt].x - acc[mt][nt][2 * h];
-                    v.y = cv[nt].y - acc[mt][nt][2 * h + 1];
-                    if (c + 1 < N && vec2) __stcs((double2 *)(crow + c), v);
-                    else {
-                        if (c < N) crow[c] = v.x;
-                        if (c + 1 < N) crow[c + 1] = v.y;
-                    }
-                }
-            }
-    }
-}
-
-bool launch_gemm_dmma_gpc(double *C, i64 ldc, const double *A, i64 lda, const double *B, i64 ldb, i64 M, i64 N,
-                          i64 K, cudaStream_t s, int max_clusters) {
-    if (M <= 0 || N <= 0 || K <= 0) return true;
-    const bool aligned = ((uintptr_t)A % 16 == 0) && ((uintptr_t)B % 16 == 0) && (lda % 2 == 0) &&
-                         (ldb % 2 == 0) && M < (1 << 30) && N < (1 << 30) && K < (1 << 30);
-    if (!aligned) return false;
-    static int ncl = -1;  // clusters of 16 that fit at once (whole GPCs)
-    cudaLaunchConfig_t cfg = {};
-    cfg.blockDim = dim3(GNTHREADS);
-    cfg.dynamicSmemBytes = GSMEM;
-    cfg.stream = s;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeClusterDimension;
-    at[0].val.clusterDim.x = GEMM_GPC_CLUSTER;
-    at[0].val.clusterDim.y = 1;
-    at[0].val.clusterDim.z = 1;
-    cfg.attrs = at;
-    cfg.numAttrs = 1;
-    set_max_dyn_smem((const void *)k_gemm_dmma_gpc, GSMEM);
-    if (ncl < 0) {
-        OXI_CUDA(cudaFuncSetAttribute(k_gemm_dmma_gpc, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-        cfg.gridDim = dim3(GEMM_GPC_CLUSTER);
-        int v = 0;
-        if (cudaOccupancyMaxActiveClusters(&v, k_gemm_dmma_gpc, &cfg) != cudaSuccess) {
-            cudaGetLastError();
-            v = 0;
-        }
-        ncl = v;
-    }
-    if (ncl < 2) return false;  // no whole GPC to spare: the caller runs the plain kernel
-    const i64 tiles = ((M + GBM - 1) / GBM) * ((N + BN - 1) / BN);
-    const i64 want = (tiles + GEMM_GPC_CLUSTER - 1) / GEMM_GPC_CLUSTER;
-    const int use = (int)std::min<i64>(want, std::max(1, std::min(ncl - 1, max_clusters)));
-    cfg.gridDim = dim3((unsigned)(use * GEMM_GPC_CLUSTER));
-    CUtensorMap tmA, tmB;
-    make_tmap_2d(&tmA, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, A, K, M, lda, BK, GBM, CU_TENSOR_MAP_SWIZZLE_128B);
-    make_tmap_2d(&tmB, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, B, N, K, ldb, 8, BK, CU_TENSOR_MAP_SWIZZLE_NONE);
-    ProfScope ps(KC_GEMM_DMMA, s, 2.0 * M * N * K, 8.0 * (2.0 * M * N + M * K + K * N));
-    OXI_CUDA(cudaLaunchKernelEx(&cfg, k_gemm_dmma_gpc, tmA, tmB, C, ldc, (int)M, (int)N, (int)K, cur_abort()));
-    count_launch();
-    return true;
-}
-
 void launch_gemm_dmma(double *C, i64 ldc, const double *A, i64 lda, const double *B, i64 ldb, i64 M,
                       i64 N, i64 K, cudaStream_t s, bool upper_only) {
     if (M <= 0 || N <= 0 || K <= 0) return;

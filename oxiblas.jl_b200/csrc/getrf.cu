@@ -36,14 +36,8 @@ void gemm_minus(oxi_handle_s *h, T *C, i64 ldc, const T *A, i64 lda, const T *B,
                 i64 N, i64 K) {
     if (M <= 0 || N <= 0 || K <= 0) return;
     if (h->opt.gemm == 0) {
-        if constexpr (sizeof(T) == 8) {
-            // the lookahead's trailing update on whole GPCs, beside the next panel
-            if (h->gemm_ctas < 0 && launch_gemm_dmma_gpc(C, ldc, A, lda, B, ldb, M, N, K, h->stream, -h->gemm_ctas))
-                return;
-            launch_gemm_dmma(C, ldc, A, lda, B, ldb, M, N, K, h->stream);
-        } else {
-            launch_gemm_simt<T>(C, ldc, A, lda, B, ldb, M, N, K, h->stream);
-        }
+        if constexpr (sizeof(T) == 8) launch_gemm_dmma(C, ldc, A, lda, B, ldb, M, N, K, h->stream);
+        else launch_gemm_simt<T>(C, ldc, A, lda, B, ldb, M, N, K, h->stream);
         return;
     }
     launch_gemm_ref<T>(C, ldc, A, lda, B, ldb, M, N, K, h->stream);
@@ -276,10 +270,13 @@ void getrf_rowmajor(oxi_handle_s *h, T *W, i64 ld, i64 m, i64 n, int64_t *d_ipiv
     // trailing update runs on a second stream, concurrently with the next panel's
     // factorization, which touches only its own columns.  Its row moves and U12
     // solve, which do touch the other columns, wait for that update.
-    // Applied where the trailing update is a persistent tensor-core GEMM whose
-    // clusters fill whole GPCs and leave one to the panel: tcgen05 for the mixed
-    // solve's 16-bit factor, the GPC-shaped DMMA kernel for FP64 (the reference
-    // summation-order mode and the FP32 CUDA-core update run the plain schedule).
+    // The mixed solve's 16-bit update is the persistent tcgen05 GEMM, launched in
+    // clusters that fill whole GPCs and leave one to the panel.  The FP64 update
+    // is the DMMA kernel on the low-priority stream: its CTAs are short (one
+    // 128 x 64 tile each), so the panel's kernels, on the high-priority stream,
+    // take SMs as those CTAs finish (measured: n=16384 plain FP64 157 -> 130 ms).
+    // The reference summation-order mode and the FP32 CUDA-core update run the
+    // plain schedule.
     bool la = h->opt.lookahead && compose && h->opt.gemm == 0;
     if constexpr (sizeof(T) == 4) {
         if (h->trailing == TRAIL_NATIVE) la = false;
@@ -371,12 +368,6 @@ void getrf_rowmajor(oxi_handle_s *h, T *W, i64 ld, i64 m, i64 n, int64_t *d_ipiv
                 const double kq = (h->trailing == TRAIL_FP16X3 || h->trailing == TRAIL_BF16X3) ? 3.0 : 1.0;
                 const double us = tiles * kq * (double)(l - f) * 0.017 / GEMM_GPC_CLUSTER;
                 h->gemm_ctas = -std::max(2, (int)std::ceil(us / 600.0));
-            } else {
-                // DMMA: about 0.16 us per 256 x 64 tile per K column on one SM (30 TF/s
-                // over 148 SMs); enough GPCs to finish in about one FP64 panel (0.5 ms)
-                const double tiles = (double)((m - l + 255) / 256) * (double)((n - l2 + 63) / 64);
-                const double us = tiles * (double)(l - f) * 0.164 / GEMM_GPC_CLUSTER;
-                h->gemm_ctas = -std::max(2, (int)std::ceil(us / 500.0));
             }
             launch_rowmoves_big<T>(W, ld, f, list, listcnt, maxcnt, 0, f, h->stream);
             launch_rowmoves_big<T>(W, ld, f, list, listcnt, maxcnt, l2, R.ncols_moved, h->stream);

@@ -323,12 +323,6 @@ void launch_gemm_ref(T *C, i64 ldc, const T *A, i64 lda, const T *B, i64 ldb, i6
 // reach the upper triangle of C (M == N, a symmetric update) are computed.
 void launch_gemm_dmma(double *C, i64 ldc, const double *A, i64 lda, const double *B, i64 ldb,
                       i64 M, i64 N, i64 K, cudaStream_t s, bool upper_only = false);
-// The same product as a persistent kernel in clusters of 16 CTAs (whole GPCs),
-// at most max_clusters of them and one GPC fewer than fit: the FP64 lookahead's
-// trailing update.  Returns false (nothing launched) when the operands are not
-// TMA-aligned or no GPC can be spared.
-bool launch_gemm_dmma_gpc(double *C, i64 ldc, const double *A, i64 lda, const double *B, i64 ldb, i64 M, i64 N,
-                          i64 K, cudaStream_t s, int max_clusters);
 
 // tcgen05 GEMM: C (FP32 row-major) -= scale * A16 * B16^T, 16-bit K-major operands.
 void launch_gemm_tc(int fmt, float *C, i64 ldc, const void *A16, i64 lda16, const void *B16,
