@@ -31,6 +31,18 @@ static inline i64 split_point(const oxi_handle_s *h, i64 n) {
     return a >= 8 ? a : half;
 }
 
+void ensure_lookahead_streams(oxi_handle_s *h) {
+    if (h->la_stream) return;
+    int lo = 0, hi = 0;
+    OXI_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    OXI_CUDA(cudaStreamCreateWithPriority(&h->la_stream, cudaStreamNonBlocking, lo));
+    OXI_CUDA(cudaStreamCreateWithPriority(&h->la_main, cudaStreamNonBlocking, hi));
+    OXI_CUDA(cudaEventCreateWithFlags(&h->la_fork, cudaEventDisableTiming));
+    OXI_CUDA(cudaEventCreateWithFlags(&h->la_join, cudaEventDisableTiming));
+    OXI_CUDA(cudaEventCreateWithFlags(&h->la_in, cudaEventDisableTiming));
+    OXI_CUDA(cudaEventCreateWithFlags(&h->la_out, cudaEventDisableTiming));
+}
+
 template <typename T>
 void gemm_minus(oxi_handle_s *h, T *C, i64 ldc, const T *A, i64 lda, const T *B, i64 ldb, i64 M,
                 i64 N, i64 K) {
@@ -286,16 +298,7 @@ void getrf_rowmajor(oxi_handle_s *h, T *W, i64 ld, i64 m, i64 n, int64_t *d_ipiv
     // serves the panel's kernels (the leaf's 16-CTA cluster needs 16 SMs of one
     // GPC) before the update's.
     const cudaStream_t caller = h->stream;
-    if (la && !h->la_stream) {
-        int lo = 0, hi = 0;
-        OXI_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
-        OXI_CUDA(cudaStreamCreateWithPriority(&h->la_stream, cudaStreamNonBlocking, lo));
-        OXI_CUDA(cudaStreamCreateWithPriority(&h->la_main, cudaStreamNonBlocking, hi));
-        OXI_CUDA(cudaEventCreateWithFlags(&h->la_fork, cudaEventDisableTiming));
-        OXI_CUDA(cudaEventCreateWithFlags(&h->la_join, cudaEventDisableTiming));
-        OXI_CUDA(cudaEventCreateWithFlags(&h->la_in, cudaEventDisableTiming));
-        OXI_CUDA(cudaEventCreateWithFlags(&h->la_out, cudaEventDisableTiming));
-    }
+    if (la) ensure_lookahead_streams(h);
     if (la) {
         OXI_CUDA(cudaEventRecord(h->la_in, caller));
         OXI_CUDA(cudaStreamWaitEvent(h->la_main, h->la_in, 0));

@@ -340,6 +340,9 @@ void gemm_trailing_f32(oxi_handle_s *h, float *C, i64 ldc, const float *A, i64 l
 // triangle of its row-major view (potrf.cu); work holds potrf_work_elems(n)
 // elements.  FP32 runs its symmetric update in h->trailing precision.
 size_t potrf_work_elems(i64 n);
+// The lookahead's two streams (panels at the highest priority, the trailing
+// update at the lowest) and its events, created once per handle.
+void ensure_lookahead_streams(oxi_handle_s *h);
 template <typename T>
 void potrf_rowmajor(oxi_handle_s *h, T *U, i64 ld, i64 n, int64_t *d_info, T *work);
 // Solves with a column-major lower Cholesky factor L: the block operators of L

@@ -172,11 +172,12 @@ __global__ void k_zero_strict_lower(T *__restrict__ U, i64 ld, int n, const int6
     if (j < i) U[(i64)i * ld + j] = T(0);
 }
 
-// Workspace of one factorization, in elements: T (n x NB), Bc and X (NB x ldx
-// each), Wneg (NB x NB).
+// Workspace of one factorization, in elements: T (n x NB) and X (NB x ldx),
+// two of each (the lookahead's update of block k reads them while block k + 1
+// writes the other pair), Bc (NB x ldx), Wneg (NB x NB).
 size_t potrf_work_elems(i64 n) {
     const i64 ldx = (n + 3) / 4 * 4;
-    return (size_t)n * PO_NB + 2 * (size_t)PO_NB * ldx + (size_t)PO_NB * PO_NB + 64;
+    return 2 * (size_t)n * PO_NB + 3 * (size_t)PO_NB * ldx + (size_t)PO_NB * PO_NB + 64;
 }
 
 // X (t x N) = 0 - Wneg B and the symmetric update A22 -= T X (T = X^T), upper
@@ -192,63 +193,121 @@ static void po_block_row(oxi_handle_s *, float *X, i64 ldx, const float *Wneg, i
                          i64 N, cudaStream_t s) {
     launch_gemm_simt<float>(X, ldx, Wneg, t, B, ldb, t, N, t, s);
 }
+// rows x N block of the symmetric update whose (0, 0) is on the diagonal
+// (M <= N): FP64 only on and above the diagonal
 static void po_sym_update(oxi_handle_s *, double *A22, i64 ld, const double *T, int t, const double *X, i64 ldx,
-                          i64 N, cudaStream_t s) {
-    launch_gemm_dmma(A22, ld, T, t, X, ldx, N, N, t, s, /*upper_only=*/true);
+                          i64 M, i64 N, cudaStream_t s) {
+    launch_gemm_dmma(A22, ld, T, t, X, ldx, M, N, t, s, /*upper_only=*/true);
 }
 static void po_sym_update(oxi_handle_s *h, float *A22, i64 ld, const float *T, int t, const float *X, i64 ldx,
-                          i64 N, cudaStream_t s) {
-    if (h->trailing == TRAIL_NATIVE) launch_gemm_simt<float>(A22, ld, T, t, X, ldx, N, N, t, s);
-    else gemm_trailing_f32(h, A22, ld, T, t, X, ldx, N, N, t);
+                          i64 M, i64 N, cudaStream_t s) {
+    if (h->trailing == TRAIL_NATIVE) launch_gemm_simt<float>(A22, ld, T, t, X, ldx, M, N, t, s);
+    else gemm_trailing_f32(h, A22, ld, T, t, X, ldx, M, N, t);
 }
 
 // One factorization: U in place (row-major view), *d_info set on failure.
+// With the lookahead (OXI_OPT_LOOKAHEAD, the reference GEMM mode excluded)
+// block k's symmetric update is split: the next block's rows first, on the
+// panel stream (they are what block k + 1 needs), the rest on the low-priority
+// stream beside block k + 1's diagonal factor and block-row product; the
+// next block's rows wait for that rest of block k - 1's update.  Every element
+// is updated by the same products in the same order: the factor is the same.
 template <typename T>
 void potrf_rowmajor(oxi_handle_s *h, T *U, i64 ld, i64 n, int64_t *d_info, T *work) {
-    cudaStream_t s = h->stream;
+    const cudaStream_t caller = h->stream;
+    const bool la = h->opt.lookahead && h->opt.gemm == 0 && n > 2 * PO_NB;
     const i64 ldx = (n + 3) / 4 * 4;  // 16-byte rows for the TMA-fed GEMMs
-    T *Tt = work;
-    T *Bc = Tt + (size_t)n * PO_NB;
-    T *X = Bc + (size_t)PO_NB * ldx;
-    T *Wneg = X + (size_t)PO_NB * ldx;
-    for (i64 k0 = 0; k0 < n; k0 += PO_NB) {
-        const int t = (int)std::min<i64>(PO_NB, n - k0);
-        T *Ukk = U + k0 * ld + k0;
-        {
-            // the block, 1 / u_ii, and the inverse's product scratch (h x h at the top level)
-            const size_t smem = sizeof(T) * ((size_t)t * (t + 1) + t + (size_t)(PO_NB / 2) * (PO_NB / 2));
-            set_max_dyn_smem((const void *)k_potrf_diag<T>,
-                             (int)(sizeof(T) * (PO_NB * (PO_NB + 1) + PO_NB + (PO_NB / 2) * (PO_NB / 2))));
-            ProfScope ps(KC_LEAF, s, (double)t * t * t * (2.0 / 3.0), 2.0 * sizeof(T) * t * t);
-            k_potrf_diag<T><<<1, PO_NT, smem, s>>>(Ukk, ld, t, k0, d_info, Wneg);
-            OXI_LAUNCH_CHECK();
-        }
-        const i64 right = n - k0 - t;
-        if (right <= 0) break;
-        T *Bk = Ukk + t;  // rows k0..k0+t, columns k0+t..n
-        // the tensor-core GEMM reads its operands through TMA (16-byte aligned
-        // rows); a block row at an odd offset or pitch is copied first
-        const T *Bop = Bk;
-        i64 ldb_op = ld;
-        if ((uintptr_t)Bk % 16 != 0 || (ld * (i64)sizeof(T)) % 16 != 0) {
-            OXI_CUDA(cudaMemcpy2DAsync(Bc, sizeof(T) * ldx, Bk, sizeof(T) * ld, sizeof(T) * right, (size_t)t,
-                                       cudaMemcpyDeviceToDevice, s));
-            Bop = Bc;
-            ldb_op = ldx;
-        }
-        // X = 0 - (-W^T) A_k,right = U_kk^-T A_k,right
-        OXI_CUDA(cudaMemsetAsync(X, 0, sizeof(T) * (size_t)t * ldx, s));
-        po_block_row(h, X, ldx, Wneg, t, Bop, ldb_op, right, s);
-        k_copy_block_row<T><<<(unsigned)(((i64)t * right + 255) / 256), 256, 0, s>>>(X, ldx, Bk, ld, t, right, d_info);
-        OXI_LAUNCH_CHECK();
-        // Tt = X^T (right x t, row-major): X read as a column-major right x t matrix
-        launch_cm_to_rm<T, T>(X, ldx, Tt, t, right, t, s);
-        T *A22 = U + (k0 + t) * ld + (k0 + t);
-        po_sym_update(h, A22, ld, Tt, t, X, ldx, right, s);
+    T *Tt2[2] = {work, work + (size_t)n * PO_NB};
+    T *X2[2] = {work + 2 * (size_t)n * PO_NB, work + 2 * (size_t)n * PO_NB + (size_t)PO_NB * ldx};
+    T *Bc = X2[1] + (size_t)PO_NB * ldx;
+    T *Wneg = Bc + (size_t)PO_NB * ldx;
+    if (la) {
+        ensure_lookahead_streams(h);
+        OXI_CUDA(cudaEventRecord(h->la_in, caller));
+        OXI_CUDA(cudaStreamWaitEvent(h->la_main, h->la_in, 0));
+        h->stream = h->la_main;
     }
-    const i64 tot = n * n;
-    k_zero_strict_lower<T><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(U, ld, (int)n, d_info);
-    OXI_LAUNCH_CHECK();
+    const cudaStream_t s = h->stream;
+    bool b_pending = false;
+    try {
+        for (i64 k0 = 0, kb = 0; k0 < n; k0 += PO_NB, ++kb) {
+            const int t = (int)std::min<i64>(PO_NB, n - k0);
+            T *Ukk = U + k0 * ld + k0;
+            T *Tt = Tt2[kb & 1], *X = X2[kb & 1];
+            {
+                // the block, 1 / u_ii, and the inverse's product scratch (h x h at the top level)
+                const size_t smem = sizeof(T) * ((size_t)t * (t + 1) + t + (size_t)(PO_NB / 2) * (PO_NB / 2));
+                set_max_dyn_smem((const void *)k_potrf_diag<T>,
+                                 (int)(sizeof(T) * (PO_NB * (PO_NB + 1) + PO_NB + (PO_NB / 2) * (PO_NB / 2))));
+                ProfScope ps(KC_LEAF, s, (double)t * t * t * (2.0 / 3.0), 2.0 * sizeof(T) * t * t);
+                k_potrf_diag<T><<<1, PO_NT, smem, s>>>(Ukk, ld, t, k0, d_info, Wneg);
+                OXI_LAUNCH_CHECK();
+            }
+            const i64 right = n - k0 - t;
+            if (right <= 0) break;
+            T *Bk = Ukk + t;  // rows k0..k0+t, columns k0+t..n
+            // the tensor-core GEMM reads its operands through TMA (16-byte aligned
+            // rows); a block row at an odd offset or pitch is copied first
+            const T *Bop = Bk;
+            i64 ldb_op = ld;
+            if ((uintptr_t)Bk % 16 != 0 || (ld * (i64)sizeof(T)) % 16 != 0) {
+                OXI_CUDA(cudaMemcpy2DAsync(Bc, sizeof(T) * ldx, Bk, sizeof(T) * ld, sizeof(T) * right, (size_t)t,
+                                           cudaMemcpyDeviceToDevice, s));
+                Bop = Bc;
+                ldb_op = ldx;
+            }
+            // X = 0 - (-W^T) A_k,right = U_kk^-T A_k,right
+            OXI_CUDA(cudaMemsetAsync(X, 0, sizeof(T) * (size_t)t * ldx, s));
+            po_block_row(h, X, ldx, Wneg, t, Bop, ldb_op, right, s);
+            k_copy_block_row<T><<<(unsigned)(((i64)t * right + 255) / 256), 256, 0, s>>>(X, ldx, Bk, ld, t, right,
+                                                                                        d_info);
+            OXI_LAUNCH_CHECK();
+            // Tt = X^T (right x t, row-major): X read as a column-major right x t matrix
+            launch_cm_to_rm<T, T>(X, ldx, Tt, t, right, t, s);
+            T *A22 = U + (k0 + t) * ld + (k0 + t);
+            if (!la) {
+                po_sym_update(h, A22, ld, Tt, t, X, ldx, right, right, s);
+                continue;
+            }
+            // the next block's rows, after the rest of the previous update
+            if (b_pending) {
+                OXI_CUDA(cudaStreamWaitEvent(s, h->la_join, 0));
+                b_pending = false;
+            }
+            const i64 t2 = std::min<i64>(PO_NB, right);
+            po_sym_update(h, A22, ld, Tt, t, X, ldx, t2, right, s);
+            if (right > t2) {  // the rest on the low-priority stream
+                OXI_CUDA(cudaEventRecord(h->la_fork, s));
+                OXI_CUDA(cudaStreamWaitEvent(h->la_stream, h->la_fork, 0));
+                h->stream = h->la_stream;
+                h->tc_slot = 1;
+                // tcgen05: persistent clusters on every GPC but one, which stays free for
+                // the next block's diagonal factor and block-row product
+                if constexpr (sizeof(T) == 4) h->gemm_ctas = -64;
+                po_sym_update(h, A22 + t2 * ld + t2, ld, Tt + t2 * t, t, X + t2, ldx, right - t2, right - t2,
+                              h->la_stream);
+                h->stream = s;
+                h->tc_slot = 0;
+                h->gemm_ctas = 0;
+                OXI_CUDA(cudaEventRecord(h->la_join, h->la_stream));
+                b_pending = true;
+            }
+        }
+        if (b_pending) OXI_CUDA(cudaStreamWaitEvent(s, h->la_join, 0));
+        const i64 tot = n * n;
+        k_zero_strict_lower<T><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(U, ld, (int)n, d_info);
+        OXI_LAUNCH_CHECK();
+        if (la) {
+            OXI_CUDA(cudaEventRecord(h->la_out, s));
+            OXI_CUDA(cudaStreamWaitEvent(caller, h->la_out, 0));
+        }
+        h->stream = caller;
+    } catch (...) {
+        h->stream = caller;
+        h->tc_slot = 0;
+        h->gemm_ctas = 0;
+        throw;
+    }
 }
 template void potrf_rowmajor<double>(oxi_handle_s *, double *, i64, i64, int64_t *, double *);
 template void potrf_rowmajor<float>(oxi_handle_s *, float *, i64, i64, int64_t *, float *);

@@ -119,3 +119,16 @@ def test_cholesky_inplace_failure_keeps_upper_triangle(pkg, oracle, ld_extra):
     Lo, _ = oracle.potrf(B)
     assert np.linalg.norm(_np(G.L) - Lo) / np.linalg.norm(Lo) <= 1e-13
     assert np.all(np.triu(_np(Acm), 1) == 0)
+
+
+@pytest.mark.parametrize("n", [700, 2049])
+def test_cholesky_lookahead_gives_identical_factor(pkg, n):
+    """The lookahead (next block's rows first, the rest of the symmetric update
+    on a second stream) changes only the schedule: the same factor, bit for bit."""
+    rng = np.random.default_rng(n + 5)
+    A = _spd(rng, n, cond=1e5)
+    with pkg.options(lookahead=0):
+        L0 = _np(pkg.cholesky(A).L)
+    with pkg.options(lookahead=1):
+        L1 = _np(pkg.cholesky(A).L)
+    assert np.array_equal(L0, L1)
