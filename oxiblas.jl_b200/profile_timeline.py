@@ -1,6 +1,8 @@
 """Launch timeline of one mixed-precision solve and one plain FP64 LU + solve.
 
 Usage: python oxiblas.jl_b200/profile_timeline.py [--n 16384] [--nrhs 1] [--prec fp16x3] [--json out.json]
+       python oxiblas.jl_b200/profile_timeline.py --kind cholesky [--n 8192]   (FP64 Cholesky, SPD G G^T + n I)
+       python oxiblas.jl_b200/profile_timeline.py --kind complex [--n 4096]    (ComplexF64 LU of randn + i randn)
 
 Runs the solves on the same seeded synthetic system as bench.py (Haar U, V,
 sigma log-uniform on [1e-4, 1]) with the library's profiler on: every kernel
@@ -49,6 +51,39 @@ def summarize(records, title):
         print(f"  stream {s}: {len(rs)} launches, busy {busy:.2f} ms, from {rs[0][2]:.2f} to {rs[-1][3]:.2f} ms")
 
 
+def other_factorization(pkg, args):
+    """Two warm-up factorizations, then one profiled: FP64 Cholesky of G G^T + n I
+    or the ComplexF64 LU of a random complex matrix (seeded)."""
+    import torch
+    n = args.n
+    dev = torch.device("cuda", 0)
+    g = torch.Generator(device=dev).manual_seed(20261106)
+    if args.kind == "cholesky":
+        G = torch.randn(n, n, dtype=torch.float64, device=dev, generator=g)
+        Acm = (G @ G.t() + n * torch.eye(n, dtype=torch.float64, device=dev)).t().contiguous()
+        del G
+        factor = pkg.cholesky_
+    else:
+        Acm = torch.complex(torch.randn(n, n, dtype=torch.float64, device=dev, generator=g),
+                            torch.randn(n, n, dtype=torch.float64, device=dev, generator=g)).t().contiguous()
+        factor = pkg.lu_
+    work = torch.empty_like(Acm)
+    h = pkg.Handle.get()
+    for _ in range(2):
+        work.copy_(Acm)
+        factor(work.t())
+    torch.cuda.synchronize()
+    work.copy_(Acm)
+    h.profile(True)
+    factor(work.t())
+    tl = h.profile_timeline()
+    h.profile(False)
+    summarize(tl, f"{args.kind} factorization, n={n}")
+    if args.json:
+        with open(args.json, "w") as f:
+            json.dump({args.kind: tl}, f)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--n", type=int, default=16384)
@@ -56,9 +91,13 @@ def main():
     ap.add_argument("--kappa", type=float, default=1e4)
     ap.add_argument("--prec", default="fp16x3")
     ap.add_argument("--json", default=None)
+    ap.add_argument("--kind", default="lu", choices=["lu", "cholesky", "complex"])
     args = ap.parse_args()
     import torch
     pkg = _load()
+    if args.kind != "lu":
+        other_factorization(pkg, args)
+        return
     n, nr = args.n, args.nrhs
     dev = torch.device("cuda", 0)
     A = pkg.synthetic.kappa_matrix(n, args.kappa, seed=20261104, device=dev)
