@@ -339,6 +339,15 @@ int oxi_zgetrf(oxi_handle_t h, int64_t m, int64_t n, void *dA, int64_t lda, int6
 int oxi_zgetrs(oxi_handle_t h, char trans, int64_t n, int64_t nrhs, const void *dLU, int64_t lda,
                const int64_t *d_ipiv, void *dB, int64_t ldb);
 
+/* Layout: dB (n x m, column-major, ldb) = dA^T for the m x n column-major dA
+ * (lda), elements of elem_bytes = 4, 8 or 16 bytes (float, double, ComplexF64).
+ * A row-major host array (Python, C) is the column-major transpose of the
+ * matrix it holds: this makes the column-major copy the other entry points
+ * take, on the device.  No reference counterpart (Julia arrays are already
+ * column-major).  Stream-ordered; no synchronisation. */
+int oxi_transpose(oxi_handle_t h, int elem_bytes, int64_t m, int64_t n, const void *dA, int64_t lda, void *dB,
+                  int64_t ldb);
+
 /* Radix equilibration, the first step of the mixed solve, as its own call:
  * equilibrate(A; radix=true) (src/lapack/dense_utilities.jl:191-213).  For the
  * m x n column-major A: d_rows[i] = 2^round(log2 max_j |A[i,j]|) (1 for a zero

@@ -91,6 +91,7 @@ _SIGS = {
     "oxi_dgetri": ([_vp, _i64, _vp, _i64, _vp, _vp, _i64], ctypes.c_int),
     "oxi_dpotrf": ([_vp, _i64, _vp, _i64, ctypes.POINTER(_i64)], ctypes.c_int),
     "oxi_dpotrs": ([_vp, _i64, _i64, _vp, _i64, _vp, _i64], ctypes.c_int),
+    "oxi_transpose": ([_vp, ctypes.c_int, _i64, _i64, _vp, _i64, _vp, _i64], ctypes.c_int),
     "oxi_zgetrf": ([_vp, _i64, _i64, _vp, _i64, _vp, ctypes.POINTER(_i64)], ctypes.c_int),
     "oxi_zgetrs": ([_vp, ctypes.c_char, _i64, _i64, _vp, _i64, _vp, _vp, _i64], ctypes.c_int),
     "oxi_dequilibrate": ([_vp, _i64, _i64, _vp, _i64, _vp, _vp, _vp, _i64], ctypes.c_int),

@@ -351,3 +351,29 @@ int oxi_launch_count_reset(oxi_handle_t h) {
 }
 
 }  // extern "C"
+
+// B (n x m, column-major, ldb) = A^T for the m x n column-major A (lda), with
+// 4-, 8- or 16-byte elements: the column-major copy of a row-major host array
+// (a row-major m x n array is the column-major n x m matrix A^T) that the other
+// entry points take.  A tiled transpose at HBM speed, stream-ordered.
+extern "C" int oxi_transpose(oxi_handle_t h, int elem_bytes, int64_t m, int64_t n, const void *dA, int64_t lda,
+                             void *dB, int64_t ldb) {
+    using namespace oxi;
+    if (!h || m < 0 || n < 0 || lda < std::max<int64_t>(1, m) || ldb < std::max<int64_t>(1, n)) return OXI_EINVAL;
+    if (elem_bytes != 4 && elem_bytes != 8 && elem_bytes != 16) return OXI_EINVAL;
+    if (m == 0 || n == 0) return OXI_OK;
+    if (!dA || !dB) return OXI_EINVAL;
+    try {
+        OXI_CUDA(cudaSetDevice(h->device));
+        if (elem_bytes == 4)
+            launch_cm_to_rm<float, float>((const float *)dA, lda, (float *)dB, ldb, m, n, h->stream);
+        else if (elem_bytes == 8)
+            launch_cm_to_rm<double, double>((const double *)dA, lda, (double *)dB, ldb, m, n, h->stream);
+        else
+            launch_cm_to_rm<double2, double2>((const double2 *)dA, lda, (double2 *)dB, ldb, m, n, h->stream);
+        return OXI_OK;
+    } catch (const CudaError &e) {
+        h->last_error = std::string(e.what) + ": " + cudaGetErrorString(e.code);
+        return OXI_ECUDA;
+    }
+}

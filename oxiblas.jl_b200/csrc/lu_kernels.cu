@@ -71,6 +71,7 @@ void launch_rm_to_cm(const TS *W, i64 ldw, TD *A, i64 lda, i64 m, i64 n, cudaStr
 template void launch_cm_to_rm<double, double>(const double *, i64, double *, i64, i64, i64, cudaStream_t);
 template void launch_cm_to_rm<float, float>(const float *, i64, float *, i64, i64, i64, cudaStream_t);
 template void launch_cm_to_rm<double, float>(const double *, i64, float *, i64, i64, i64, cudaStream_t);
+template void launch_cm_to_rm<double2, double2>(const double2 *, i64, double2 *, i64, i64, i64, cudaStream_t);
 template void launch_rm_to_cm<double, double>(const double *, i64, double *, i64, i64, i64, cudaStream_t);
 template void launch_rm_to_cm<float, float>(const float *, i64, float *, i64, i64, i64, cudaStream_t);
 template void launch_rm_to_cm<float, double>(const float *, i64, double *, i64, i64, i64, cudaStream_t);

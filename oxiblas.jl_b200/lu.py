@@ -55,7 +55,16 @@ def colmajor_copy(A, dtype=None) -> torch.Tensor:
     if dtype is not None:
         t = t.to(dtype)
     out = torch.empty((t.shape[1], t.shape[0]), dtype=t.dtype, device=dev)
-    out.copy_(t.t())
+    esize = {torch.float32: 4, torch.float64: 8, torch.complex128: 16}.get(t.dtype)
+    if esize is not None and t.is_contiguous() and t.numel() > 0:
+        # the row-major (m, n) tensor is the column-major n x m matrix t^T: the
+        # engine's transpose makes the column-major m x n copy
+        m, n = t.shape
+        h = Handle.get()
+        h.check(h.lib.oxi_transpose(h.ptr, esize, n, m, ctypes.c_void_p(t.data_ptr()), max(1, n),
+                                    ctypes.c_void_p(out.data_ptr()), max(1, m)))
+    else:
+        out.copy_(t.t())
     return out
 
 

@@ -264,3 +264,19 @@ def test_nan_pivot_rule_matches_oracle(pkg, oracle, m, n):
     assert ipiv[5] == 6
     assert np.array_equal(ipiv, ipo)
     assert np.array_equal(_np(F.factors), Fo, equal_nan=True)
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64, torch.complex128])
+def test_layout_copy_on_the_engine(pkg, dtype):
+    """colmajor_copy runs oxi_transpose (the engine's tiled transpose) for
+    contiguous row-major inputs: the column-major copy equals torch's."""
+    g = torch.Generator(device="cuda").manual_seed(3)
+    for m, n in ((1, 1), (33, 65), (1000, 7), (640, 1031)):
+        if dtype.is_complex:
+            t = torch.complex(torch.randn(m, n, generator=g, device="cuda", dtype=torch.float64),
+                              torch.randn(m, n, generator=g, device="cuda", dtype=torch.float64))
+        else:
+            t = torch.randn(m, n, generator=g, device="cuda", dtype=dtype)
+        out = pkg.colmajor_copy(t)
+        assert out.shape == (n, m)
+        assert torch.equal(out, t.t().contiguous())
