@@ -103,9 +103,28 @@ struct Misc {
     int mvpos[2 * bt::NBMAX];
     int nmv;
     int perm[bt::NMAX];  // net permutation: row i of L U is row perm[i] of A
-    double rows[bt::NMAX], cols[bt::NMAX];
+    // reciprocals of the radix row and column scales: powers of two in
+    // [2^-1023, 2^1022], so x * rrow[i] is exactly x / (row scale i)
+    double rrow[bt::NMAX], rcol[bt::NMAX];
     int item, info, bad;
 };
+
+// Rows [0, m) of a column from global memory into dst (m <= NMAX, one warp):
+// every lane issues its loads before its stores, so the round trips overlap.
+template <typename T, typename U>
+__device__ __forceinline__ void load_col(T *dst, const U *src, int m, int lane) {
+    T v[bt::NQ];
+#pragma unroll
+    for (int q = 0; q < bt::NQ; ++q) {
+        const int r = lane + 32 * q;
+        v[q] = r < m ? (T)src[r] : T(0);
+    }
+#pragma unroll
+    for (int q = 0; q < bt::NQ; ++q) {
+        const int r = lane + 32 * q;
+        if (r < m) dst[r] = v[q];
+    }
+}
 
 // The pivot candidates of column j (all threads): the row of the largest
 // |col[i]|, i in (j, m), first index on ties (INT_MAX when none compares), its
@@ -200,6 +219,78 @@ __device__ void panel_lu(T *P, int ldp, int m, int jb, int k, Misc &S) {
     __syncthreads();  // S.piv / S.info of a final zero column are visible to all
 }
 
+// One column of U12 = L11^-1 A12 (unit lower L11 in P, ldp): rows k..k+jb of
+// column wc, forward substitution in registers; the result back to wc and,
+// when su is given, to su[i NMAX] (the staged U12 the update reads).  JB is
+// the panel width at compile time (JB = jb), or NBMAX with jb <= JB checked
+// per step for a narrower last panel.
+template <typename T, int JB>
+__device__ __forceinline__ void u12_column(T *wc, int k, int jb, const T *P, int ldp, T *su) {
+    T x[JB];
+#pragma unroll
+    for (int i = 0; i < JB; ++i) x[i] = (i < jb) ? wc[k + i] : T(0);
+#pragma unroll
+    for (int i = 1; i < JB; ++i) {
+        if (i < jb) {
+            T s = x[i];
+#pragma unroll
+            for (int q = 0; q < i; ++q) s = fma(-P[i + (i64)q * ldp], x[q], s);
+            x[i] = s;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < JB; ++i) {
+        if (i < jb) {
+            wc[k + i] = x[i];
+            if (su) su[i * bt::NMAX] = x[i];
+        }
+    }
+}
+
+// C (m2 x m2, column-major, ldc) -= A B, A m2 x jb (column-major, lda), B jb x m2
+// with element (kk, c) at B[kk bsk + c bsc]: each product accumulated from zero
+// in kk order, then subtracted (gemm!(C, A, B, -1, 1)).  One warp, columns
+// c0..c0+3 of rows r0..r0+32 NU: lane l holds rows r0 + l + 32 u, so every A
+// load and C access covers 32 consecutive rows (no shared-memory bank
+// conflicts, whole sectors in global memory), and two columns' C elements
+// are loaded before any of them is stored.
+template <typename T, int NU>
+__device__ __forceinline__ void update_tile(const T *Ap, int lda, const T *Bp, int bsk, int bsc, T *Cp,
+                                            int ldc, int m2, int jb, int r0, int c0, int lane) {
+    T acc[NU][4];
+#pragma unroll
+    for (int u = 0; u < NU; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc[u][v] = T(0);
+    const int r = r0 + lane;
+    for (int kk = 0; kk < jb; ++kk) {
+        T a[NU], b[4];
+#pragma unroll
+        for (int u = 0; u < NU; ++u) a[u] = (r + 32 * u < m2) ? Ap[(r + 32 * u) + (i64)kk * lda] : T(0);
+#pragma unroll
+        for (int v = 0; v < 4; ++v) b[v] = (c0 + v < m2) ? Bp[(i64)kk * bsk + (i64)(c0 + v) * bsc] : T(0);
+#pragma unroll
+        for (int u = 0; u < NU; ++u)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) acc[u][v] = fma(a[u], b[v], acc[u][v]);
+    }
+#pragma unroll
+    for (int h = 0; h < 4; h += 2) {  // two columns' C elements loaded before any is stored
+        T cv[NU][2];
+#pragma unroll
+        for (int v = 0; v < 2; ++v)
+#pragma unroll
+            for (int u = 0; u < NU; ++u)
+                cv[u][v] = (r + 32 * u < m2 && c0 + h + v < m2) ? Cp[(r + 32 * u) + (i64)(c0 + h + v) * ldc] : T(0);
+#pragma unroll
+        for (int v = 0; v < 2; ++v)
+#pragma unroll
+            for (int u = 0; u < NU; ++u)
+                if (r + 32 * u < m2 && c0 + h + v < m2)
+                    Cp[(r + 32 * u) + (i64)(c0 + h + v) * ldc] = cv[u][v] - acc[u][h + v];
+    }
+}
+
 // Right-looking blocked LU of W (n x n, column-major, ldw; shared or global).
 template <typename T>
 __device__ void lu_blocked(T *W, int ldw, int n, int nb, bool in_smem, T *sP, T *sU, Misc &S) {
@@ -216,7 +307,7 @@ __device__ void lu_blocked(T *W, int ldw, int n, int nb, bool in_smem, T *sP, T 
             ldp = m;
             // a warp per column, its lanes down the rows (coalesced, no index division)
             for (int c = (int)(threadIdx.x >> 5); c < jb; c += NW)
-                for (int r = (int)(threadIdx.x & 31); r < m; r += 32) sP[r + c * ldp] = W[(k + r) + (i64)(k + c) * ldw];
+                load_col(sP + c * ldp, W + k + (i64)(k + c) * ldw, m, (int)(threadIdx.x & 31));
             __syncthreads();
         }
         panel_lu(P, ldp, m, jb, k, S);
@@ -250,12 +341,19 @@ __device__ void lu_blocked(T *W, int ldw, int n, int nb, bool in_smem, T *sP, T 
                 for (int cb = 0; cb < n; cb += ccap) {
                     const int cn = min(ccap, n - cb);
                     // a warp per moved row, its lanes across the columns
+                    // cn <= n <= 32 NQ: a lane's columns of a moved row in one batch of loads
                     for (int mv = (int)(threadIdx.x >> 5); mv < nmv; mv += NW) {
                         const int src = S.rowat[S.mvpos[mv]];
-                        for (int cc = (int)(threadIdx.x & 31); cc < cn; cc += 32) {
-                            const int c = cb + cc;
-                            if (c >= k && c < c2) continue;
-                            sU[mv * ccap + cc] = W[src + (i64)c * ldw];
+                        T v[NQ];
+#pragma unroll
+                        for (int q = 0; q < NQ; ++q) {
+                            const int cc = (int)(threadIdx.x & 31) + 32 * q, c = cb + cc;
+                            v[q] = (cc < cn && !(c >= k && c < c2)) ? W[src + (i64)c * ldw] : T(0);
+                        }
+#pragma unroll
+                        for (int q = 0; q < NQ; ++q) {
+                            const int cc = (int)(threadIdx.x & 31) + 32 * q, c = cb + cc;
+                            if (cc < cn && !(c >= k && c < c2)) sU[mv * ccap + cc] = v[q];
                         }
                     }
                     __syncthreads();
@@ -284,30 +382,16 @@ __device__ void lu_blocked(T *W, int ldw, int n, int nb, bool in_smem, T *sP, T 
                     }
                 }
             }
-            if (c >= c2) {
-                T x[NBMAX];
-#pragma unroll
-                for (int i = 0; i < NBMAX; ++i) x[i] = (i < jb) ? wc[k + i] : T(0);
-#pragma unroll
-                for (int i = 1; i < NBMAX; ++i) {
-                    if (i < jb) {
-                        T s = x[i];
-#pragma unroll
-                        for (int q = 0; q < i; ++q) s = fma(-P[i + (i64)q * ldp], x[q], s);
-                        x[i] = s;
-                    }
-                }
-#pragma unroll
-                for (int i = 0; i < NBMAX; ++i) {
-                    if (i < jb) {
-                        wc[k + i] = x[i];
-                        if (!in_smem) sU[i * NMAX + (c - c2)] = x[i];
-                    }
-                }
+            if (c >= c2) {  // full panels at a compile-time width: no predicated steps
+                T *su = in_smem ? nullptr : sU + (c - c2);
+                if (jb == 16) u12_column<T, 16>(wc, k, 16, P, ldp, su);
+                else if (jb == 8) u12_column<T, 8>(wc, k, 8, P, ldp, su);
+                else if (jb == 32) u12_column<T, 32>(wc, k, 32, P, ldp, su);
+                else u12_column<T, NBMAX>(wc, k, jb, P, ldp, su);
             }
         }
         __syncthreads();
-        // A22 -= L21 U12, 4 x 4 register tiles
+        // A22 -= L21 U12: a warp takes up to 128 rows x 4 columns (update_tile)
         const int m2 = n - c2;
         if (m2 > 0) {
             const T *Ap = P + jb;
@@ -315,33 +399,15 @@ __device__ void lu_blocked(T *W, int ldw, int n, int nb, bool in_smem, T *sP, T 
             const T *Bp = in_smem ? W + k + (i64)c2 * ldw : sU;
             const int bsk = in_smem ? 1 : NMAX;
             const int bsc = in_smem ? ldw : 1;
-            const int RT = (m2 + 3) >> 2;
-            const int tiles = RT * RT;
-            for (int t = threadIdx.x; t < tiles; t += NT) {
-                const int r0 = (t % RT) * 4, cc0 = (t / RT) * 4;
-                T acc[4][4];
-#pragma unroll
-                for (int u = 0; u < 4; ++u)
-#pragma unroll
-                    for (int v = 0; v < 4; ++v) acc[u][v] = T(0);
-                for (int kk = 0; kk < jb; ++kk) {
-                    T a[4], b[4];
-#pragma unroll
-                    for (int u = 0; u < 4; ++u) a[u] = (r0 + u < m2) ? Ap[(r0 + u) + (i64)kk * ldp] : T(0);
-#pragma unroll
-                    for (int v = 0; v < 4; ++v) b[v] = (cc0 + v < m2) ? Bp[(i64)kk * bsk + (i64)(cc0 + v) * bsc] : T(0);
-#pragma unroll
-                    for (int u = 0; u < 4; ++u)
-#pragma unroll
-                        for (int v = 0; v < 4; ++v) acc[u][v] = fma(a[u], b[v], acc[u][v]);
-                }
-#pragma unroll
-                for (int v = 0; v < 4; ++v) {
-                    if (cc0 + v >= m2) continue;
-#pragma unroll
-                    for (int u = 0; u < 4; ++u)
-                        if (r0 + u < m2) Cp[(r0 + u) + (i64)(cc0 + v) * ldw] -= acc[u][v];
-                }
+            const int RB = (m2 + 127) >> 7, tasks = RB * ((m2 + 3) >> 2);
+            const int lane = (int)(threadIdx.x & 31);
+            for (int t = (int)(threadIdx.x >> 5); t < tasks; t += NW) {
+                const int r0 = (t % RB) * 128, c0 = (t / RB) * 4;
+                const int nu = min(4, (m2 - r0 + 31) >> 5);  // warp-uniform
+                if (nu == 4) update_tile<T, 4>(Ap, ldp, Bp, bsk, bsc, Cp, ldw, m2, jb, r0, c0, lane);
+                else if (nu == 3) update_tile<T, 3>(Ap, ldp, Bp, bsk, bsc, Cp, ldw, m2, jb, r0, c0, lane);
+                else if (nu == 2) update_tile<T, 2>(Ap, ldp, Bp, bsk, bsc, Cp, ldw, m2, jb, r0, c0, lane);
+                else update_tile<T, 1>(Ap, ldp, Bp, bsk, bsc, Cp, ldw, m2, jb, r0, c0, lane);
             }
         }
         __syncthreads();
@@ -392,27 +458,60 @@ __device__ void warp_lu_solve(const T *W, int ldw, int n, T (&y)[bt::NQ]) {
 
 // The whole CTA solves L U y = z for the right-hand sides held by its active
 // warps (y distributed as in warp_lu_solve), the factor read from global
-// memory in chunks of cw columns staged in shared memory (cw * NMAX elements),
-// so each dependent step reads shared memory, not L2.  Every thread calls it.
+// memory in chunks of cs columns staged in shared memory (two buffers of cs
+// columns in stage, which holds cap columns of NMAX): while the active warps
+// run the dependent steps of one chunk, every warp's loads of the next chunk
+// are in flight (two columns a warp), so each step reads shared memory and the
+// L2 round trips overlap the steps.  Every thread calls it.
 template <typename T>
-__device__ void block_lu_solve(const T *W, int ldw, int n, T *stage, int cw, bool active, T (&y)[bt::NQ]) {
+__device__ void block_lu_solve(const T *W, int ldw, int n, T *stage, int cap, bool active, T (&y)[bt::NQ]) {
     using namespace bt;
-    const int lane = threadIdx.x & 31;
-    for (int j0 = 0; j0 < n; j0 += cw) {  // forward, unit lower
-        const int jn = min(cw, n - j0);
-        __syncthreads();
-        for (int j = (int)(threadIdx.x >> 5); j < jn; j += NW)
-            for (int r = lane; r < n; r += 32) stage[r + j * NMAX] = W[r + (i64)(j0 + j) * ldw];
-        __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int cs = min(2 * NW, cap / 2);
+    T pv[2][NQ];
+    auto fetch = [&](int a, int b) {  // columns a + warp, a + warp + NW of [a, b)
+#pragma unroll
+        for (int t = 0; t < 2; ++t) {
+            const int jj = warp + NW * t, j = a + jj;
+            const bool mine = jj < cs && j < b;
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) {
+                const int r = lane + 32 * q;
+                pv[t][q] = (mine && r < n) ? W[r + (i64)j * ldw] : T(0);
+            }
+        }
+    };
+    auto put = [&](T *buf, int a, int b) {
+#pragma unroll
+        for (int t = 0; t < 2; ++t) {
+            const int jj = warp + NW * t;
+            if (jj < cs && a + jj < b) {
+#pragma unroll
+                for (int q = 0; q < NQ; ++q) {
+                    const int r = lane + 32 * q;
+                    if (r < n) buf[r + jj * NMAX] = pv[t][q];
+                }
+            }
+        }
+    };
+    T *cur = stage, *nxt = stage + cs * NMAX;
+    __syncthreads();  // the stage's previous use is over
+    fetch(0, min(cs, n));
+    put(cur, 0, min(cs, n));
+    __syncthreads();
+    for (int j0 = 0; j0 < n; j0 += cs) {  // forward, unit lower
+        const int j1 = min(j0 + cs, n);
+        const bool more = j1 < n;
+        if (more) fetch(j1, min(j1 + cs, n));
         if (active) {
-            for (int jj = 0; jj < jn; ++jj) {
-                const int j = j0 + jj, qj = j >> 5, lj = j & 31;
+            for (int j = j0; j < j1; ++j) {
+                const int qj = j >> 5, lj = j & 31;
                 T src = y[0];
 #pragma unroll
                 for (int q = 1; q < NQ; ++q)
                     if (q == qj) src = y[q];
                 const T yj = __shfl_sync(0xffffffffu, src, lj);
-                const T *col = stage + jj * NMAX;
+                const T *col = cur + (j - j0) * NMAX;
 #pragma unroll
                 for (int q = 0; q < NQ; ++q) {
                     const int i = lane + 32 * q;
@@ -420,21 +519,30 @@ __device__ void block_lu_solve(const T *W, int ldw, int n, T *stage, int cw, boo
                 }
             }
         }
+        if (more) put(nxt, j1, min(j1 + cs, n));
+        __syncthreads();
+        T *t = cur;
+        cur = nxt;
+        nxt = t;
     }
-    for (int j1 = n; j1 > 0; j1 -= cw) {  // backward, upper
-        const int j0 = max(0, j1 - cw), jn = j1 - j0;
+    {
+        const int a0 = max(0, n - cs);
+        fetch(a0, n);
+        put(cur, a0, n);
         __syncthreads();
-        for (int j = (int)(threadIdx.x >> 5); j < jn; j += NW)
-            for (int r = lane; r < n; r += 32) stage[r + j * NMAX] = W[r + (i64)(j0 + j) * ldw];
-        __syncthreads();
+    }
+    for (int b = n; b > 0; b -= cs) {  // backward, upper
+        const int a = max(0, b - cs), na = max(0, a - cs);
+        const bool more = a > 0;
+        if (more) fetch(na, a);
         if (active) {
-            for (int j = j1 - 1; j >= j0; --j) {
+            for (int j = b - 1; j >= a; --j) {
                 const int qj = j >> 5, lj = j & 31;
                 T src = y[0];
 #pragma unroll
                 for (int q = 1; q < NQ; ++q)
                     if (q == qj) src = y[q];
-                const T *col = stage + (j - j0) * NMAX;
+                const T *col = cur + (j - a) * NMAX;
                 const T xj = __shfl_sync(0xffffffffu, src, lj) / col[j];
                 if (lane == lj) {
 #pragma unroll
@@ -448,8 +556,12 @@ __device__ void block_lu_solve(const T *W, int ldw, int n, T *stage, int cw, boo
                 }
             }
         }
+        if (more) put(nxt, na, a);
+        __syncthreads();
+        T *t = cur;
+        cur = nxt;
+        nxt = t;
     }
-    __syncthreads();
 }
 
 __device__ __forceinline__ int bucket_of(int n) { return (n - 1) >> 5; }
@@ -546,8 +658,7 @@ __global__ void __launch_bounds__(bt::NT, 2) k_lu_batched(const __grid_constant_
             if (in_smem) {
                 W = sW;
                 ldw = n;
-                for (int c = warp; c < n; c += NW)
-                    for (int r = lane; r < n; r += 32) W[r + c * ldw] = (T)A[r + (i64)c * lda];
+                for (int c = warp; c < n; c += NW) load_col(W + c * ldw, A + (i64)c * lda, n, lane);
             } else {
                 W = (T *)A;
                 ldw = (int)lda;
@@ -560,21 +671,18 @@ __global__ void __launch_bounds__(bt::NT, 2) k_lu_batched(const __grid_constant_
             for (int i = tid; i < n; i += NT) {
                 double mx = 0.0;
                 bool nf = false;
-                for (int j = 0; j < n; ++j) {
-                    const double v = fabs(A[i + (i64)j * lda]);
-                    nf |= !isfinite(v);
-                    mx = fmax(mx, v);
-                }
-                S.rows[i] = mx > 0.0 ? radix_scale(mx) : 1.0;
-                if (nf) S.bad = 1;
-            }
-            __syncthreads();
-            for (int j = warp; j < n; j += NW) {
-                double mx = 0.0;
-                for (int i = lane; i < n; i += 32) mx = fmax(mx, fabs(A[i + (i64)j * lda]) / S.rows[i]);
+                for (int j0 = 0; j0 < n; j0 += 8) {  // eight loads in flight
+                    double v[8];
 #pragma unroll
-                for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
-                if (lane == 0) S.cols[j] = mx > 0.0 ? radix_scale(mx) : 1.0;
+                    for (int u = 0; u < 8; ++u) v[u] = (j0 + u < n) ? fabs(A[i + (i64)(j0 + u) * lda]) : 0.0;
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) {
+                        nf |= !isfinite(v[u]);
+                        mx = fmax(mx, v[u]);
+                    }
+                }
+                S.rrow[i] = mx > 0.0 ? 1.0 / radix_scale(mx) : 1.0;
+                if (nf) S.bad = 1;
             }
             __syncthreads();
             if (S.bad) {
@@ -587,8 +695,28 @@ __global__ void __launch_bounds__(bt::NT, 2) k_lu_batched(const __grid_constant_
                 __syncthreads();
                 continue;
             }
-            for (int c = warp; c < n; c += NW)
-                for (int r = lane; r < n; r += 32) W[r + c * ldw] = (T)(A[r + (i64)c * lda] / S.rows[r] / S.cols[c]);
+            // column scales and the scaled FP32 copy in one pass: a warp per column,
+            // the column's values (times the row scales) kept in registers
+            for (int j = warp; j < n; j += NW) {
+                double v[NQ];
+#pragma unroll
+                for (int q = 0; q < NQ; ++q) {
+                    const int i = lane + 32 * q;
+                    v[q] = i < n ? A[i + (i64)j * lda] * S.rrow[i] : 0.0;
+                }
+                double mx = fabs(v[0]);
+#pragma unroll
+                for (int q = 1; q < NQ; ++q) mx = fmax(mx, fabs(v[q]));
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+                const double rc = mx > 0.0 ? 1.0 / radix_scale(mx) : 1.0;
+                if (lane == 0) S.rcol[j] = rc;
+#pragma unroll
+                for (int q = 0; q < NQ; ++q) {
+                    const int i = lane + 32 * q;
+                    if (i < n) W[i + j * ldw] = (T)(v[q] * rc);
+                }
+            }
             __syncthreads();
         }
 
@@ -641,7 +769,7 @@ __global__ void __launch_bounds__(bt::NT, 2) k_lu_batched(const __grid_constant_
                 if (in_smem) {
                     if (active) warp_lu_solve<T>(W, ldw, n, y);
                 } else {
-                    block_lu_solve<T>(W, ldw, n, sP, nb, active, y);
+                    block_lu_solve<T>(W, ldw, n, sP, 2 * d.nbmax, active, y);
                 }
                 if (active) {
 #pragma unroll
@@ -663,7 +791,7 @@ __global__ void __launch_bounds__(bt::NT, 2) k_lu_batched(const __grid_constant_
                 if (active) {
                     const double *rr = sR + warp * NMAX;
                     double mx = 0.0;
-                    for (int i = lane; i < n; i += 32) mx = fmax(mx, fabs(rr[i] / S.rows[i]));
+                    for (int i = lane; i < n; i += 32) mx = fmax(mx, fabs(rr[i] * S.rrow[i]));
 #pragma unroll
                     for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
                     sc = isfinite(mx) ? binary_scale(mx) : 0.0;
@@ -672,14 +800,14 @@ __global__ void __launch_bounds__(bt::NT, 2) k_lu_batched(const __grid_constant_
                         const int i = lane + 32 * q;
                         if (i < n && sc != 0.0) {
                             const int p = S.perm[i];
-                            y[q] = (T)((rr[p] / S.rows[p]) / sc);
+                            y[q] = (T)((rr[p] * S.rrow[p]) / sc);
                         }
                     }
                 }
                 if (in_smem) {
                     if (active) warp_lu_solve<T>(W, ldw, n, y);
                 } else {
-                    block_lu_solve<T>(W, ldw, n, sP, nb, active, y);
+                    block_lu_solve<T>(W, ldw, n, sP, 2 * d.nbmax, active, y);
                 }
                 if (active) {
                     double *xx = sX + warp * NMAX;
@@ -687,7 +815,7 @@ __global__ void __launch_bounds__(bt::NT, 2) k_lu_batched(const __grid_constant_
                     for (int q = 0; q < NQ; ++q) {
                         const int i = lane + 32 * q;
                         if (i < n) {
-                            const double c = ((double)y[q] * sc) / S.cols[i];
+                            const double c = ((double)y[q] * sc) * S.rcol[i];
                             xx[i] = add ? xx[i] + c : c;
                         }
                     }
@@ -712,14 +840,21 @@ __global__ void __launch_bounds__(bt::NT, 2) k_lu_batched(const __grid_constant_
                         ax[r] = 0.0;
                         den[r] = 0.0;
                     }
-                    for (int j = 0; j < n; ++j) {
-                        const double a = A[i + (i64)j * lda];
+                    for (int j0 = 0; j0 < n; j0 += 8) {  // eight loads in flight, then the
+                        double av[8];                    // sums in column order
 #pragma unroll
-                        for (int r = 0; r < MAXRHS; ++r) {
-                            if (r < nr) {
-                                const double x = sX[r * NMAX + j];
-                                ax[r] = fma(a, x, ax[r]);
-                                den[r] = fma(fabs(a), fabs(x), den[r]);
+                        for (int u = 0; u < 8; ++u) av[u] = (j0 + u < n) ? A[i + (i64)(j0 + u) * lda] : 0.0;
+#pragma unroll
+                        for (int u = 0; u < 8; ++u) {
+                            if (j0 + u >= n) break;
+                            const double a = av[u];
+#pragma unroll
+                            for (int r = 0; r < MAXRHS; ++r) {
+                                if (r < nr) {
+                                    const double x = sX[r * NMAX + j0 + u];
+                                    ax[r] = fma(a, x, ax[r]);
+                                    den[r] = fma(fabs(a), fabs(x), den[r]);
+                                }
                             }
                         }
                     }
