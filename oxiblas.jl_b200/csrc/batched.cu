@@ -106,6 +106,8 @@ struct Misc {
     // reciprocals of the radix row and column scales: powers of two in
     // [2^-1023, 2^1022], so x * rrow[i] is exactly x / (row scale i)
     double rrow[bt::NMAX], rcol[bt::NMAX];
+    double prow[2][bt::NBMAX];  // register panel: the pivot row and the old row j
+    double vjv[2];
     int item, info, bad;
 };
 
@@ -291,6 +293,99 @@ __device__ __forceinline__ void update_tile(const T *Ap, int lda, const T *Bp, i
     }
 }
 
+// Unblocked LU of a full panel of JB columns (m <= NT rows, P column-major,
+// ldp) with thread i holding row i in registers: per column one reduction for
+// the pivot (the reference's rule, as panel_lu), the pivot row and the old
+// row j exchanged through shared memory, the rank-1 update on registers -- two
+// barriers a column instead of three and no shared-memory round trip per
+// updated element.  Same operations in the same order as panel_lu.
+template <typename T, int JB>
+__device__ void panel_lu_reg(T *P, int ldp, int m, int k, Misc &S) {
+    using namespace bt;
+    const int i = threadIdx.x, lane = i & 31, warp = i >> 5;
+    const bool own = i < m;
+    T row[JB];
+#pragma unroll
+    for (int c = 0; c < JB; ++c) row[c] = own ? P[i + (i64)c * ldp] : T(0);
+#pragma unroll
+    for (int j = 0; j < JB; ++j) {
+        const int par = j & 1;
+        // candidates: rows below j (a NaN never becomes one: NaN > -1 is false)
+        const double ax = fabs((double)row[j]);
+        const bool cand = own && i > j && ax > -1.0;
+        double bv = cand ? ax : -1.0, bx = cand ? (double)row[j] : 0.0;
+        int bi = cand ? i : INT_MAX;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
+            const double ox = __shfl_xor_sync(0xffffffffu, bx, off);
+            const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+            if (ov > bv || (ov == bv && oi < bi)) {
+                bv = ov;
+                bi = oi;
+                bx = ox;
+            }
+        }
+        if (lane == 0) {
+            S.red_v[par][warp] = bv;
+            S.red_i[par][warp] = bi;
+            S.red_x[par][warp] = bx;
+        }
+        if (i == j) S.vjv[par] = (double)row[j];
+        __syncthreads();
+        bv = S.red_v[par][0];
+        bi = S.red_i[par][0];
+        bx = S.red_x[par][0];
+#pragma unroll
+        for (int w = 1; w < NW; ++w) {
+            const double ov = S.red_v[par][w];
+            const int oi = S.red_i[par][w];
+            if (ov > bv || (ov == bv && oi < bi)) {
+                bv = ov;
+                bi = oi;
+                bx = S.red_x[par][w];
+            }
+        }
+        const double vj = S.vjv[par];
+        const bool below = bi != INT_MAX && bv > fabs(vj);
+        const int p = below ? bi : j;
+        const T d = (T)(below ? bx : vj);
+        if (i == 0) S.piv[k + j] = k + p;
+        if (d == T(0)) {  // zero column: info, no interchange, no elimination
+            if (i == 0 && S.info == 0) S.info = k + j + 1;
+            continue;
+        }
+        double *pa = S.prow[0], *pj = S.prow[1];
+        if (i == p) {
+#pragma unroll
+            for (int c = 0; c < JB; ++c) pa[c] = (double)row[c];
+        }
+        if (p != j && i == j) {
+#pragma unroll
+            for (int c = 0; c < JB; ++c) pj[c] = (double)row[c];
+        }
+        __syncthreads();
+        if (i == j) {
+#pragma unroll
+            for (int c = 0; c < JB; ++c) row[c] = (T)pa[c];
+        } else if (p != j && i == p) {
+#pragma unroll
+            for (int c = 0; c < JB; ++c) row[c] = (T)pj[c];
+        }
+        if (own && i > j) {
+            const T l = row[j] / d;
+            row[j] = l;
+#pragma unroll
+            for (int c = j + 1; c < JB; ++c) row[c] = fma(-l, (T)pa[c], row[c]);
+        }
+    }
+    if (own) {
+#pragma unroll
+        for (int c = 0; c < JB; ++c) P[i + (i64)c * ldp] = row[c];
+    }
+    __syncthreads();  // the panel, S.piv and S.info visible to all
+}
+
 // Right-looking blocked LU of W (n x n, column-major, ldw; shared or global).
 template <typename T>
 __device__ void lu_blocked(T *W, int ldw, int n, int nb, bool in_smem, T *sP, T *sU, Misc &S) {
@@ -310,7 +405,9 @@ __device__ void lu_blocked(T *W, int ldw, int n, int nb, bool in_smem, T *sP, T 
                 load_col(sP + c * ldp, W + k + (i64)(k + c) * ldw, m, (int)(threadIdx.x & 31));
             __syncthreads();
         }
-        panel_lu(P, ldp, m, jb, k, S);
+        if (jb == 16) panel_lu_reg<T, 16>(P, ldp, m, k, S);
+        else if (jb == 8) panel_lu_reg<T, 8>(P, ldp, m, k, S);
+        else panel_lu(P, ldp, m, jb, k, S);
         if (!in_smem) {
             for (int c = (int)(threadIdx.x >> 5); c < jb; c += NW)
                 for (int r = (int)(threadIdx.x & 31); r < m; r += 32) W[(k + r) + (i64)(k + c) * ldw] = sP[r + c * ldp];
