@@ -407,6 +407,7 @@ __device__ void lu_blocked(T *W, int ldw, int n, int nb, bool in_smem, T *sP, T 
         }
         if (jb == 16) panel_lu_reg<T, 16>(P, ldp, m, k, S);
         else if (jb == 8) panel_lu_reg<T, 8>(P, ldp, m, k, S);
+        else if (jb == 32) panel_lu_reg<T, 32>(P, ldp, m, k, S);
         else panel_lu(P, ldp, m, jb, k, S);
         if (!in_smem) {
             for (int c = (int)(threadIdx.x >> 5); c < jb; c += NW)
