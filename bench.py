@@ -610,7 +610,8 @@ def batched_workload(args, ws, rank, local):
 
 
 def adjoint_workload(args, ws, rank, local):
-    """rrule of x = A \\ b, n = 2048, kappa 1e3: pullback time with the stored factors."""
+    """rrule of x = A \\ b, n = 2048, kappa 1e3: pullback time with the stored factors; the
+    batched rrule (1024 problems, n ~ U{32..128}) beside it."""
     import torch
     import __graft_entry__ as E
     pkg = E.load_package()
@@ -634,6 +635,35 @@ def adjoint_workload(args, ws, rank, local):
     for _ in range(args.warmup):
         fwd_bwd()
     t2 = _timed_each(stream, fwd_bwd, args.steps)
+
+    # the batched rrule: 1024 problems, n ~ U{32..128}, N(0,1) + n I, one
+    # right-hand side each, loss 0.5||x||^2 (xbar = x): the batched FP64 solve,
+    # then the pullback of every problem from the stored factors
+    import numpy as np
+    rng = np.random.default_rng(20261105)
+    orders = rng.integers(32, 129, size=1024)
+    P = pkg.BatchedLU(orders, np.ones_like(orders), device=dev)
+    gb = torch.Generator(device=dev).manual_seed(4244 + rank)
+    P.poolA.normal_(generator=gb)
+    P.poolB.normal_(generator=gb)
+    diag = np.concatenate([P._offA[i] + np.arange(m) * (m + 1) for i, m in enumerate(orders)])
+    P.poolA[torch.from_numpy(diag).to(dev)] += torch.from_numpy(
+        np.concatenate([np.full(m, float(m)) for m in orders])).to(dev)
+    A0, B0 = P.poolA.clone(), P.poolB.clone()
+
+    def restore():
+        P.poolA.copy_(A0)
+        P.poolB.copy_(B0)
+
+    for _ in range(args.warmup):
+        restore()
+        P.gesv("fp64")
+    tb_fwd = _timed_each(stream, lambda: P.gesv("fp64"), args.steps, pre=restore)
+    P._adjoint_pools()
+    P.poolXbar.copy_(P.poolB)
+    for _ in range(args.warmup):
+        P.adjoint()
+    tb_bwd = _timed_each(stream, lambda: P.adjoint(), args.steps)
     ms = max_over_ranks(ws, statistics.median(t))
     line = {"metric": "adjoint of x = A\\b (n=2048, kappa 1e3): pullback time with stored LU factors",
             "value": round(ms, 4), "unit": "ms", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
@@ -642,7 +672,10 @@ def adjoint_workload(args, ws, rank, local):
             "config": {"workload": "rrule x = A\\b, n=2048, sigma log-uniform [1e-3, 1], loss 0.5||x||^2",
                        "parallelism": f"replicas{ws}"},
             "forward_plus_backward_ms": round(max_over_ranks(ws, statistics.median(t2)), 4),
-            "abar_write_gbs": round(8.0 * n * n / (ms / 1e3) / 1e9, 1)}
+            "abar_write_gbs": round(8.0 * n * n / (ms / 1e3) / 1e9, 1),
+            "batched_1024": {"workload": "1024 problems, n~U{32..128}, N(0,1)+nI, 1 RHS, loss 0.5||x||^2",
+                             "forward_solve_ms": round(max_over_ranks(ws, statistics.median(tb_fwd)), 4),
+                             "pullback_ms": round(max_over_ranks(ws, statistics.median(tb_bwd)), 4)}}
     if rank == 0:
         print(json.dumps(line), flush=True)
 
