@@ -164,7 +164,8 @@ int oxi_dlu_adjoint(oxi_handle_t h, int64_t n, int64_t nrhs, const double *dLU, 
  * oxi_dgetrf_batched_uneven / oxi_dgesv_batched_uneven with prec FP64), one
  * launch: per problem i, Bbar_i = A_i^-T Xbar_i and Abar_i = -Bbar_i X_i^T.  All
  * arrays are DEVICE arrays of `count` entries (d_nrhs nullable: one right-hand
- * side each); Bbar_i may be Xbar_i itself.  d_info[i]: 0, -1 for bad arguments
+ * side each); Bbar_i may be Xbar_i itself, Abar_i overlaps nothing else.
+ * d_info[i]: 0, -1 for bad arguments
  * of that problem, or the first zero diagonal of its U.  Returns OXI_EINVAL /
  * OXI_ESINGULAR when any problem had that outcome.  The reference has no
  * batched factorization; its batching precedent is gemm_batched!

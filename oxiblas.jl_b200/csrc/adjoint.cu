@@ -194,9 +194,9 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
-__global__ void __launch_bounds__(BADJ_NT) k_lu_adjoint_batched(const __grid_constant__ BatchAdjDesc d) {
+__global__ void __launch_bounds__(BADJ_NT, 8) k_lu_adjoint_batched(const __grid_constant__ BatchAdjDesc d) {
     __shared__ double s_w[BADJ_KMAX][BADJ_NMAX];  // Xbar -> W -> V -> Bbar, per right-hand side
-    __shared__ double s_x[BADJ_KMAX][BADJ_NMAX];  // X
+    __shared__ int s_ip[BADJ_NMAX];               // the interchanges, 0-based
     __shared__ int s_bad;
     const int pi = blockIdx.x;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -222,19 +222,24 @@ __global__ void __launch_bounds__(BADJ_NT) k_lu_adjoint_batched(const __grid_con
     for (int e = tid; e < n * k; e += BADJ_NT) {
         const int i = e % n, r = e / n;
         s_w[r][i] = Xb[i + (i64)r * ldxb];
-        s_x[r][i] = X[i + (i64)r * ldx];
     }
+    for (int j = tid; j < n; j += BADJ_NT) s_ip[j] = (int)d.ipiv[pi][j] - 1;
     __syncthreads();
     if (warp < k) {
         double *w = s_w[warp];
         // U^T W = Xbar: w_i = (xbar_i - sum_{p<i} U[p,i] w_p) / U[i,i]
         for (int i = 0; i < n; ++i) {
             const double *col = LU + (i64)i * ld;
+            const double u = lane == 0 ? col[i] : 0.0;  // requested with the column
+            double cv[BADJ_NMAX / 32];  // the lane's rows, all requested together
+#pragma unroll
+            for (int q = 0; q < BADJ_NMAX / 32; ++q) cv[q] = (lane + 32 * q < i) ? col[lane + 32 * q] : 0.0;
             double acc = 0.0;
-            for (int p = lane; p < i; p += 32) acc = fma(col[p], w[p], acc);
+#pragma unroll
+            for (int q = 0; q < BADJ_NMAX / 32; ++q)
+                if (lane + 32 * q < i) acc = fma(cv[q], w[lane + 32 * q], acc);
             acc = warp_sum(acc);
             if (lane == 0) {
-                const double u = col[i];
                 if (u == 0.0) s_bad = i + 1;
                 w[i] = (w[i] - acc) / u;
             }
@@ -243,17 +248,26 @@ __global__ void __launch_bounds__(BADJ_NT) k_lu_adjoint_batched(const __grid_con
         // L^T V = W (unit): v_i = w_i - sum_{p>i} L[p,i] v_p
         for (int i = n - 1; i >= 0; --i) {
             const double *col = LU + (i64)i * ld;
+            double cv[BADJ_NMAX / 32];
+#pragma unroll
+            for (int q = 0; q < BADJ_NMAX / 32; ++q) {
+                const int p = i + 1 + lane + 32 * q;
+                cv[q] = p < n ? col[p] : 0.0;
+            }
             double acc = 0.0;
-            for (int p = i + 1 + lane; p < n; p += 32) acc = fma(col[p], w[p], acc);
+#pragma unroll
+            for (int q = 0; q < BADJ_NMAX / 32; ++q) {
+                const int p = i + 1 + lane + 32 * q;
+                if (p < n) acc = fma(cv[q], w[p], acc);
+            }
             acc = warp_sum(acc);
             if (lane == 0) w[i] -= acc;
             __syncwarp();
         }
         // the interchanges undone in reverse order
         if (lane == 0) {
-            const int64_t *ip = d.ipiv[pi];
             for (int j = n - 1; j >= 0; --j) {
-                const int q = (int)ip[j] - 1;
+                const int q = s_ip[j];
                 if (q != j && q >= 0 && q < n) {
                     const double t = w[j];
                     w[j] = w[q];
@@ -272,7 +286,7 @@ __global__ void __launch_bounds__(BADJ_NT) k_lu_adjoint_batched(const __grid_con
     for (int e = tid; e < n * n; e += BADJ_NT) {
         const int i = e % n, j = e / n;
         double v = 0.0;
-        for (int r = 0; r < k; ++r) v = fma(s_w[r][i], s_x[r][j], v);
+        for (int r = 0; r < k; ++r) v = fma(s_w[r][i], X[j + (i64)r * ldx], v);  // X[j, r]: one address a warp
         Ab[i + (i64)j * ldab] = -v;
     }
     if (tid == 0) {
