@@ -162,9 +162,10 @@ extern "C" int oxi_dlu_adjoint(oxi_handle_t h, int64_t n, int64_t nrhs, const do
 //                        order (as ldiv!(transpose(F), B), src/api/linalg_api.jl:
 //                        176-184);
 //   Abar = -Bbar X^T  -- n x n, written once, coalesced down the columns.
-// Each right-hand side's two substitutions run on one warp: step i reads the
-// contiguous column i of the factors (coalesced), reduces it against the
-// solved entries across the warp, and the lane that owns row i finishes it.
+// Each right-hand side's two substitutions run on one warp: step i requests
+// all of the lane's rows of the contiguous column i of the factors at once
+// (coalesced, with U[i,i]), reduces them against the solved entries across
+// the warp, and lane 0 finishes the step.
 // ---------------------------------------------------------------------------
 namespace oxi {
 namespace {
