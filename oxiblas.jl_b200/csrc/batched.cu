@@ -10,13 +10,14 @@
 // the algorithm is the same right-looking partial-pivoted LU:
 //   panel (jb columns) factored unblocked with the reference's pivot rule
 //   (largest |a|, first index on ties; a zero pivot records info and skips the
-//   interchange and the elimination), its interchanges applied to the other
+//   interchange and the elimination; full panels with each thread's row in
+//   registers), its interchanges applied to the other
 //   columns, U12 = L11^-1 A12, A22 -= L21 U12 (product accumulated from zero,
 //   then subtracted, as gemm!(C, A, B, -1, 1)).
 // Where the working matrix lives is a tuning choice: orders up to n_smem keep
 // it in shared memory; larger ones work in place in global memory (the plain
 // FP64 mode: the caller's matrix; the mixed mode: a per-CTA FP32 workspace),
-// which stays L2-resident, with the panel and U12 staged in shared memory so
+// which mostly stays in L2, with the panel and U12 staged in shared memory so
 // the trailing update reads them on chip.  The panel width per size bucket and
 // n_smem are picked by oxi_batched_autotune.
 //
